@@ -1,0 +1,162 @@
+/*
+ * em2g.h -- C ABI of libem2g.so, a B200 (sm_100a) implementation of the
+ * time step of em2, the 2D3V relativistic electromagnetic PIC code of
+ * fanyumeng666/maccpic (pic/).
+ *
+ * em2's step is four parameterless Fortran subroutines that act on the
+ * module `global` (pic/global.f90:31-45), called from the main loop
+ * (pic/main.f90:286-303):
+ *     call move; call curnt; [output]; it = it + 1; call fields
+ * plus `smooth2(sm)` (pic/smooth.f90:95) which fields calls.  This library
+ * keeps the state that `global` holds -- E, B, rho, the six current arrays
+ * and the particles -- resident on one GPU and exposes one entry point per
+ * subroutine, plus host/device copies of that state, so that a thin
+ * iso_c_binding shim can stand in for move.o, curnt.o, fields.o and
+ * smooth.o (pic/Makefile:4) without touching main.f90 or output.f90.
+ *
+ * Conventions
+ *  - Every function returns an int status: EM2G_OK (0) or an EM2G_ERR_*
+ *    code; em2g_last_error() then gives a message (per host thread).
+ *  - Field arrays are the reference's (0:nx+2, 0:ny+2) REAL(8) arrays,
+ *    x fastest: element (ix,iy) at iy*(nx+3)+ix, (nx+3)*(ny+3) doubles.
+ *  - Particle arrays of species isp (0-based) are the reference's
+ *    x(:,isp), y, vx, vy, vz, gamma: x, y in cells in [0,nx) x [0,ny)
+ *    (values up to n+0.5, which em2's own loader produces and its guard
+ *    cells absorb, are accepted), v in units of c, gamma stored.
+ *  - One context per GPU stream; calls on one context must come from one
+ *    host thread at a time.  Different contexts are independent.
+ *  - The library owns its device memory; host pointers are only read or
+ *    written during the call.  Device-pointer variants take pointers in the
+ *    context's device memory space and enqueue on the context's stream.
+ */
+#ifndef EM2G_H
+#define EM2G_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EM2G_ABI_VERSION 1
+#define EM2G_MAX_SPECIES 4
+
+enum em2g_status {
+  EM2G_OK = 0,
+  EM2G_ERR_INVALID = 1,     /* bad argument or parameter */
+  EM2G_ERR_CUDA = 2,        /* a CUDA runtime call failed */
+  EM2G_ERR_NOMEM = 3,       /* device allocation failed */
+  EM2G_ERR_RANGE = 4,       /* particle outside the grid, count > capacity */
+  EM2G_ERR_TIMEOUT = 5,     /* a bounded device-side wait gave up */
+  EM2G_ERR_NONFINITE = 6    /* NaN/Inf found in host-provided input */
+};
+
+enum em2g_precision {
+  EM2G_FP64 = 0,  /* the drop-in path: em2's arithmetic in FP64 */
+  EM2G_FP32 = 1   /* mixed: FP32 push/deposit/Yee, FP64 reductions */
+};
+
+/* field ids, in the order of the reference's arrays (pic/global.f90:127-129) */
+enum em2g_field {
+  EM2G_EX = 0, EM2G_EY, EM2G_EZ, EM2G_BX, EM2G_BY, EM2G_BZ, EM2G_RHO,
+  EM2G_JXM, EM2G_JXP, EM2G_JYM, EM2G_JYP, EM2G_JZM, EM2G_JZP, EM2G_NFIELD
+};
+
+/* Run constants.  They replace the compile-time parameters of
+ * pic/input.f90:9-43 and the derived constants of pic/global.f90:101-114;
+ * per-species values are those of com_den (pic/input.f90:61-69) and init
+ * (pic/init.f90:295-297).  Fill with em2g_params_init() first. */
+typedef struct em2g_params {
+  uint32_t struct_size;  /* = sizeof(em2g_params) */
+  int32_t nx, ny;        /* cells (>= 4 each) */
+  int32_t nsp;           /* species, 1..EM2G_MAX_SPECIES */
+  int32_t isav;          /* E/B filtering and energy interval (fields) */
+  int32_t precision;     /* enum em2g_precision */
+  double dx, dy, dt, c;
+  double qm[EM2G_MAX_SPECIES];  /* charge/mass */
+  double q[EM2G_MAX_SPECIES];   /* macro-particle charge */
+  double dn[EM2G_MAX_SPECIES];  /* relative density */
+  double am[EM2G_MAX_SPECIES];  /* macro-particle mass (kinetic energy) */
+  double tx[EM2G_MAX_SPECIES];  /* background rotation terms of move (0 in em2) */
+  double ty[EM2G_MAX_SPECIES];
+  int64_t np_max[EM2G_MAX_SPECIES]; /* particle capacity per species */
+  int32_t cg_maxits;     /* 10000 in cgm (pic/fields.f90:518) */
+  int32_t energy_mode;   /* 0: whole grid; 1: rows 88..168 x ny/80 as em2 */
+  double cg_eps;         /* 1e-9 in cgm (pic/fields.f90:519) */
+  double qme, wpe;       /* -1, 1 (pic/input.f90:43) */
+  int32_t device;        /* CUDA device ordinal */
+  int32_t sort_interval; /* steps between particle sorts on the fast path; 0 = never */
+  int32_t reserved[16];
+} em2g_params;
+
+typedef struct em2g_ctx em2g_ctx;
+
+/* version of this header the library was built from */
+int em2g_abi_version(void);
+/* message for the last failing call on this host thread ("" if none) */
+const char *em2g_last_error(void);
+/* defaults: em2's constants (c=1, qme=-1, wpe=1, cg 10000 / 1e-9, isav 20) */
+int em2g_params_init(em2g_params *p);
+
+int em2g_create(const em2g_params *p, em2g_ctx **out);
+int em2g_destroy(em2g_ctx *ctx);
+/* enqueue all further work of ctx on this cudaStream_t (NULL = ctx's own) */
+int em2g_set_stream(em2g_ctx *ctx, void *cuda_stream);
+int em2g_synchronize(em2g_ctx *ctx);
+
+/* ---- state copies (host memory) ------------------------------------ */
+/* one field array, (nx+3)*(ny+3) doubles, Fortran layout */
+int em2g_set_field(em2g_ctx *ctx, int field_id, const double *host);
+int em2g_get_field(em2g_ctx *ctx, int field_id, double *host);
+/* all 13 arrays back to back in enum em2g_field order */
+int em2g_set_fields(em2g_ctx *ctx, const double *host13);
+int em2g_get_fields(em2g_ctx *ctx, double *host13);
+/* n particles of species isp (0-based), in slot order j = 0..n-1 */
+int em2g_set_particles(em2g_ctx *ctx, int isp, int64_t n, const double *x,
+                       const double *y, const double *vx, const double *vy,
+                       const double *vz, const double *gamma);
+/* returns them in the slot order they were given in, whatever the library
+ * did to its internal order; *n receives the count.  With all six array
+ * pointers NULL it only reports the count. */
+int em2g_get_particles(em2g_ctx *ctx, int isp, int64_t *n, double *x, double *y,
+                       double *vx, double *vy, double *vz, double *gamma);
+/* the step counter `it` of pic/global.f90:117 (fields reads it) */
+int em2g_set_step(em2g_ctx *ctx, int it);
+int em2g_get_step(em2g_ctx *ctx, int *it);
+
+/* ---- state copies (device memory, on the context's stream) --------- */
+int em2g_set_fields_device(em2g_ctx *ctx, const double *dev13);
+int em2g_get_fields_device(em2g_ctx *ctx, double *dev13);
+/* device pointer of one field array owned by the library (FP64 path) */
+int em2g_field_device_ptr(em2g_ctx *ctx, int field_id, void **dptr);
+
+/* ---- the subroutines ------------------------------------------------ */
+/* move (pic/move.f90:2-217): gather + relativistic Boris for every species.
+ * ake_out (nsp doubles, may be NULL) receives ake(isp) = am*dn*sum(gamma-1)
+ * as after the MPI_ALLREDUCE of pic/move.f90:214 (one rank: identity). */
+int em2g_move(em2g_ctx *ctx, double *ake_out);
+/* curnt (pic/curnt.f90:2-379): deposit jm, move and wrap x, y, deposit rho
+ * and jp, accumulating into the resident rho/J arrays (not folded). */
+int em2g_curnt(em2g_ctx *ctx);
+/* fields (pic/fields.f90:2-367) for step `it`: fold, Yee B/2-E-B/2,
+ * smooth2(rho), smooth2(E,B) if it%isav==0, Poisson/cgm, energies if
+ * it%isav==0 (into energies_out[6] = exe,eye,eze,bxe,bye,bze; may be NULL),
+ * zero rho/J.  cg_iters_out (may be NULL) receives cgm's exit count n
+ * (cg_maxits+1 when MAXITS was exceeded; em2 carries on then, so does this). */
+int em2g_fields(em2g_ctx *ctx, int it, double *energies_out, int *cg_iters_out);
+/* smooth2 (pic/smooth.f90:95-179) in place on one resident field array */
+int em2g_smooth2(em2g_ctx *ctx, int field_id);
+
+/* ---- fused fast path -------------------------------------------------
+ * nsteps iterations of { move; curnt; it = it + 1; fields(it) } with the
+ * particle work of move and curnt in one fused kernel per species.  The
+ * outputs refer to the last iteration (energies_out written only when the
+ * last `it` is a multiple of isav). */
+int em2g_step(em2g_ctx *ctx, int nsteps, double *ake_out, double *energies_out,
+              int *cg_iters_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EM2G_H */

@@ -1,0 +1,418 @@
+// em2g_api.cu -- the C ABI of libem2g.so (declared in include/em2g.h):
+// context life cycle, state copies, and the move / curnt / fields /
+// smooth2 entry points that stand in for em2's subroutines.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "em2g_internal.cuh"
+
+namespace em2g {
+
+static thread_local std::string g_last_error;
+
+int fail(int status, const std::string &msg) {
+  g_last_error = msg;
+  return status;
+}
+
+int cuda_fail(cudaError_t e, const char *what) {
+  g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
+  return e == cudaErrorMemoryAllocation ? EM2G_ERR_NOMEM : EM2G_ERR_CUDA;
+}
+
+namespace {
+
+// slot-order restore: dst[slot[j]] = src[j] for the 6 arrays
+__global__ void k_unsort(const double *__restrict__ src, const int32_t *__restrict__ slot,
+                         double *__restrict__ dst, int64_t n, int64_t cap) {
+  const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const int64_t s = slot[j];
+  for (int k = 0; k < 6; ++k) dst[k * cap + s] = src[k * cap + j];
+}
+
+__global__ void k_iota(int32_t *slot, int64_t n) {
+  const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < n) slot[j] = (int32_t)j;
+}
+
+int check_ctx(em2g_ctx *c) {
+  if (!c) return fail(EM2G_ERR_INVALID, "null context");
+  EM2G_CUDA(cudaSetDevice(c->device));
+  return EM2G_OK;
+}
+
+int validate(const em2g_params *p) {
+  if (!p) return fail(EM2G_ERR_INVALID, "null params");
+  if (p->struct_size != sizeof(em2g_params))
+    return fail(EM2G_ERR_INVALID, "em2g_params.struct_size mismatch (header/library version)");
+  if (p->nx < 4 || p->ny < 4) return fail(EM2G_ERR_INVALID, "nx and ny must be >= 4");
+  if ((int64_t)(p->nx + 3) * (p->ny + 3) > (int64_t)1 << 31)
+    return fail(EM2G_ERR_INVALID, "grid too large");
+  if (p->nsp < 1 || p->nsp > EM2G_MAX_SPECIES)
+    return fail(EM2G_ERR_INVALID, "nsp must be 1..4");
+  if (p->isav < 1) return fail(EM2G_ERR_INVALID, "isav must be >= 1");
+  if (p->precision != EM2G_FP64 && p->precision != EM2G_FP32)
+    return fail(EM2G_ERR_INVALID, "unknown precision");
+  if (!(p->dx > 0) || !(p->dy > 0) || !(p->dt > 0) || !(p->c > 0))
+    return fail(EM2G_ERR_INVALID, "dx, dy, dt, c must be > 0");
+  if (p->c * p->dt >= p->dx || p->c * p->dt >= p->dy)
+    return fail(EM2G_ERR_INVALID, "c*dt must be < dx and dy (one wrap per step)");
+  if (p->energy_mode == 1 && p->ny < 170)
+    return fail(EM2G_ERR_INVALID, "energy_mode 1 reads rows 88..168 and needs ny >= 170");
+  if (p->cg_maxits < 1) return fail(EM2G_ERR_INVALID, "cg_maxits must be >= 1");
+  for (int s = 0; s < p->nsp; ++s) {
+    if (p->np_max[s] < 0 || p->np_max[s] > ((int64_t)1 << 31) - 1)
+      return fail(EM2G_ERR_INVALID, "np_max out of range");
+    if (!std::isfinite(p->qm[s]) || !std::isfinite(p->q[s]) || !std::isfinite(p->dn[s]) ||
+        !std::isfinite(p->am[s]))
+      return fail(EM2G_ERR_NONFINITE, "non-finite species constant");
+  }
+  return EM2G_OK;
+}
+
+int finish_outputs(em2g_ctx *c, double *ake_out, double *energies_out, int *cg_iters_out,
+                   bool energies_valid) {
+  EM2G_CUDA(cudaMemcpyAsync(c->host_out, c->dev_out, sizeof(double) * 16,
+                            cudaMemcpyDeviceToHost, c->stream));
+  int st[2] = {0, 0};
+  EM2G_CUDA(cudaMemcpyAsync(st, c->cg.status, sizeof(st), cudaMemcpyDeviceToHost, c->stream));
+  EM2G_CUDA(cudaStreamSynchronize(c->stream));
+  EM2G_CUDA(cudaGetLastError());
+  if (st[0] != 0) return fail(EM2G_ERR_TIMEOUT, "cg: a grid barrier wait timed out");
+  if (ake_out)
+    for (int s = 0; s < c->P.nsp; ++s) ake_out[s] = c->host_out[s];
+  if (energies_out && energies_valid)
+    for (int k = 0; k < 6; ++k) energies_out[k] = c->host_out[4 + k];
+  if (cg_iters_out) *cg_iters_out = st[1];
+  return EM2G_OK;
+}
+
+}  // namespace
+}  // namespace em2g
+
+using namespace em2g;
+
+extern "C" {
+
+int em2g_abi_version(void) { return EM2G_ABI_VERSION; }
+
+const char *em2g_last_error(void) { return g_last_error.c_str(); }
+
+int em2g_params_init(em2g_params *p) {
+  if (!p) return fail(EM2G_ERR_INVALID, "null params");
+  std::memset(p, 0, sizeof(*p));
+  p->struct_size = sizeof(em2g_params);
+  p->nsp = 2;
+  p->isav = 20;
+  p->precision = EM2G_FP64;
+  p->c = 1.0;
+  p->cg_maxits = 10000;
+  p->cg_eps = 1e-9;
+  p->qme = -1.0;
+  p->wpe = 1.0;
+  return EM2G_OK;
+}
+
+int em2g_create(const em2g_params *p, em2g_ctx **out) {
+  if (!out) return fail(EM2G_ERR_INVALID, "null output pointer");
+  *out = nullptr;
+  int rc = validate(p);
+  if (rc) return rc;
+  if (p->precision != EM2G_FP64)
+    return fail(EM2G_ERR_INVALID, "this entry point creates FP64 contexts");
+  em2g_ctx *c = new (std::nothrow) em2g_ctx();
+  if (!c) return fail(EM2G_ERR_NOMEM, "host allocation failed");
+  c->P = *p;
+  c->device = p->device;
+  c->g.nx = p->nx;
+  c->g.ny = p->ny;
+  c->g.nxg = p->nx + 3;
+  c->g.w = (int64_t)(p->nx + 3) * (p->ny + 3);
+  auto bail = [&](int code) {
+    em2g_destroy(c);
+    return code;
+  };
+  cudaError_t e = cudaSetDevice(c->device);
+  if (e != cudaSuccess) return bail(cuda_fail(e, "cudaSetDevice"));
+  e = cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device);
+  if (e != cudaSuccess) return bail(cuda_fail(e, "cudaDeviceGetAttribute"));
+  e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return bail(cuda_fail(e, "cudaStreamCreate"));
+  c->stream = c->own_stream;
+  const int64_t w = c->g.w;
+#define ALLOC(ptr, bytes)                                            \
+  do {                                                               \
+    e = cudaMalloc((void **)&(ptr), (bytes));                        \
+    if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc " #ptr)); \
+  } while (0)
+  ALLOC(c->fld, sizeof(double) * EM2G_NFIELD * w);
+  ALLOC(c->scaled, sizeof(double) * 6 * w * p->nsp);
+  ALLOC(c->smooth_tmp, sizeof(double) * w);
+  int64_t maxn = 0;
+  for (int s = 0; s < p->nsp; ++s) {
+    Species &S = c->sp[s];
+    S.cap = p->np_max[s] > 0 ? p->np_max[s] : 1;
+    if (S.cap > maxn) maxn = S.cap;
+    ALLOC(S.part, sizeof(double) * 6 * S.cap);
+    ALLOC(S.part_alt, sizeof(double) * 6 * S.cap);
+    ALLOC(S.slot, sizeof(int32_t) * S.cap);
+    ALLOC(S.slot_alt, sizeof(int32_t) * S.cap);
+  }
+  c->red_blocks = (int)((maxn + 255) / 256);
+  if (c->red_blocks < 6 * kEnergyBlocks) c->red_blocks = 6 * kEnergyBlocks;
+  ALLOC(c->red, sizeof(double) * c->red_blocks);
+  ALLOC(c->dev_out, sizeof(double) * 16);
+#undef ALLOC
+  e = cudaMallocHost((void **)&c->host_out, sizeof(double) * 16);
+  if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMallocHost"));
+  e = cudaMemset(c->fld, 0, sizeof(double) * EM2G_NFIELD * w);
+  if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMemset"));
+  e = cudaMemset(c->dev_out, 0, sizeof(double) * 16);
+  if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMemset"));
+  rc = cg_init(c);
+  if (rc) return bail(rc);
+  e = cudaMemset(c->cg.status, 0, sizeof(int) * 2);
+  if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMemset"));
+  e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return bail(cuda_fail(e, "cudaDeviceSynchronize"));
+  *out = c;
+  return EM2G_OK;
+}
+
+int em2g_destroy(em2g_ctx *c) {
+  if (!c) return EM2G_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  cudaFree(c->fld);
+  cudaFree(c->scaled);
+  cudaFree(c->smooth_tmp);
+  for (auto &S : c->sp) {
+    cudaFree(S.part);
+    cudaFree(S.part_alt);
+    cudaFree(S.slot);
+    cudaFree(S.slot_alt);
+  }
+  cudaFree(c->red);
+  cudaFree(c->dev_out);
+  if (c->host_out) cudaFreeHost(c->host_out);
+  cg_free(c);
+  if (c->own_stream) cudaStreamDestroy(c->own_stream);
+  delete c;
+  return EM2G_OK;
+}
+
+int em2g_set_stream(em2g_ctx *c, void *stream) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+  return EM2G_OK;
+}
+
+int em2g_synchronize(em2g_ctx *c) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  EM2G_CUDA(cudaStreamSynchronize(c->stream));
+  return EM2G_OK;
+}
+
+int em2g_set_field(em2g_ctx *c, int id, const double *host) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (id < 0 || id >= EM2G_NFIELD || !host) return fail(EM2G_ERR_INVALID, "bad field id or pointer");
+  for (int64_t k = 0; k < c->g.w; ++k)
+    if (!std::isfinite(host[k])) return fail(EM2G_ERR_NONFINITE, "non-finite field value");
+  EM2G_CUDA(cudaMemcpyAsync(c->fld + id * c->g.w, host, sizeof(double) * c->g.w,
+                            cudaMemcpyHostToDevice, c->stream));
+  EM2G_CUDA(cudaStreamSynchronize(c->stream));
+  return EM2G_OK;
+}
+
+int em2g_get_field(em2g_ctx *c, int id, double *host) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (id < 0 || id >= EM2G_NFIELD || !host) return fail(EM2G_ERR_INVALID, "bad field id or pointer");
+  EM2G_CUDA(cudaMemcpyAsync(host, c->fld + id * c->g.w, sizeof(double) * c->g.w,
+                            cudaMemcpyDeviceToHost, c->stream));
+  EM2G_CUDA(cudaStreamSynchronize(c->stream));
+  return EM2G_OK;
+}
+
+int em2g_set_fields(em2g_ctx *c, const double *host13) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!host13) return fail(EM2G_ERR_INVALID, "null pointer");
+  const int64_t n = EM2G_NFIELD * c->g.w;
+  for (int64_t k = 0; k < n; ++k)
+    if (!std::isfinite(host13[k])) return fail(EM2G_ERR_NONFINITE, "non-finite field value");
+  EM2G_CUDA(cudaMemcpyAsync(c->fld, host13, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+  EM2G_CUDA(cudaStreamSynchronize(c->stream));
+  return EM2G_OK;
+}
+
+int em2g_get_fields(em2g_ctx *c, double *host13) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!host13) return fail(EM2G_ERR_INVALID, "null pointer");
+  EM2G_CUDA(cudaMemcpyAsync(host13, c->fld, sizeof(double) * EM2G_NFIELD * c->g.w,
+                            cudaMemcpyDeviceToHost, c->stream));
+  EM2G_CUDA(cudaStreamSynchronize(c->stream));
+  return EM2G_OK;
+}
+
+int em2g_set_fields_device(em2g_ctx *c, const double *dev13) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!dev13) return fail(EM2G_ERR_INVALID, "null pointer");
+  EM2G_CUDA(cudaMemcpyAsync(c->fld, dev13, sizeof(double) * EM2G_NFIELD * c->g.w,
+                            cudaMemcpyDeviceToDevice, c->stream));
+  return EM2G_OK;
+}
+
+int em2g_get_fields_device(em2g_ctx *c, double *dev13) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!dev13) return fail(EM2G_ERR_INVALID, "null pointer");
+  EM2G_CUDA(cudaMemcpyAsync(dev13, c->fld, sizeof(double) * EM2G_NFIELD * c->g.w,
+                            cudaMemcpyDeviceToDevice, c->stream));
+  return EM2G_OK;
+}
+
+int em2g_field_device_ptr(em2g_ctx *c, int id, void **dptr) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (id < 0 || id >= EM2G_NFIELD || !dptr) return fail(EM2G_ERR_INVALID, "bad field id or pointer");
+  *dptr = c->fld + id * c->g.w;
+  return EM2G_OK;
+}
+
+int em2g_set_particles(em2g_ctx *c, int isp, int64_t n, const double *x, const double *y,
+                       const double *vx, const double *vy, const double *vz,
+                       const double *gamma) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (isp < 0 || isp >= c->P.nsp) return fail(EM2G_ERR_INVALID, "bad species index");
+  Species &S = c->sp[isp];
+  if (n < 0 || n > S.cap) return fail(EM2G_ERR_RANGE, "particle count exceeds np_max");
+  if (n > 0 && (!x || !y || !vx || !vy || !vz || !gamma))
+    return fail(EM2G_ERR_INVALID, "null particle array");
+  // Positions must keep every stencil inside the (0:n+2) arrays: 0 <= x < n+0.5
+  const double xlim = c->P.nx + 0.5, ylim = c->P.ny + 0.5;
+  for (int64_t j = 0; j < n; ++j) {
+    if (!std::isfinite(x[j]) || !std::isfinite(y[j]) || !std::isfinite(vx[j]) ||
+        !std::isfinite(vy[j]) || !std::isfinite(vz[j]) || !std::isfinite(gamma[j]))
+      return fail(EM2G_ERR_NONFINITE, "non-finite particle value at slot " + std::to_string(j));
+    if (!(x[j] >= 0.0 && x[j] < xlim && y[j] >= 0.0 && y[j] < ylim))
+      return fail(EM2G_ERR_RANGE, "particle outside the grid at slot " + std::to_string(j));
+  }
+  const double *src[6] = {x, y, vx, vy, vz, gamma};
+  for (int k = 0; k < 6; ++k)
+    if (n > 0)
+      EM2G_CUDA(cudaMemcpyAsync(S.part + k * S.cap, src[k], sizeof(double) * n,
+                                cudaMemcpyHostToDevice, c->stream));
+  if (n > 0) {
+    k_iota<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(S.slot, n);
+    EM2G_CUDA(cudaGetLastError());
+  }
+  S.n = n;
+  EM2G_CUDA(cudaStreamSynchronize(c->stream));
+  return EM2G_OK;
+}
+
+int em2g_get_particles(em2g_ctx *c, int isp, int64_t *n, double *x, double *y, double *vx,
+                       double *vy, double *vz, double *gamma) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (isp < 0 || isp >= c->P.nsp) return fail(EM2G_ERR_INVALID, "bad species index");
+  Species &S = c->sp[isp];
+  if (n) *n = S.n;
+  if (S.n == 0) return EM2G_OK;
+  if (!x && !y && !vx && !vy && !vz && !gamma) return EM2G_OK;  // count query
+  if (!x || !y || !vx || !vy || !vz || !gamma) return fail(EM2G_ERR_INVALID, "null particle array");
+  k_unsort<<<(unsigned)((S.n + 255) / 256), 256, 0, c->stream>>>(S.part, S.slot, S.part_alt,
+                                                                  S.n, S.cap);
+  EM2G_CUDA(cudaGetLastError());
+  double *dst[6] = {x, y, vx, vy, vz, gamma};
+  for (int k = 0; k < 6; ++k)
+    EM2G_CUDA(cudaMemcpyAsync(dst[k], S.part_alt + k * S.cap, sizeof(double) * S.n,
+                              cudaMemcpyDeviceToHost, c->stream));
+  EM2G_CUDA(cudaStreamSynchronize(c->stream));
+  return EM2G_OK;
+}
+
+int em2g_set_step(em2g_ctx *c, int it) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  c->it = it;
+  return EM2G_OK;
+}
+
+int em2g_get_step(em2g_ctx *c, int *it) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!it) return fail(EM2G_ERR_INVALID, "null pointer");
+  *it = c->it;
+  return EM2G_OK;
+}
+
+int em2g_move(em2g_ctx *c, double *ake_out) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  for (int s = 0; s < c->P.nsp; ++s) {
+    if ((rc = launch_prescale(c, s))) return rc;
+    if ((rc = launch_push_f64(c, s, 1))) return rc;
+  }
+  return finish_outputs(c, ake_out, nullptr, nullptr, false);
+}
+
+int em2g_curnt(em2g_ctx *c) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  for (int s = 0; s < c->P.nsp; ++s)
+    if ((rc = launch_push_f64(c, s, 2))) return rc;
+  EM2G_CUDA(cudaStreamSynchronize(c->stream));
+  EM2G_CUDA(cudaGetLastError());
+  return EM2G_OK;
+}
+
+int em2g_fields(em2g_ctx *c, int it, double *energies_out, int *cg_iters_out) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  EM2G_CUDA(cudaMemsetAsync(c->cg.status, 0, sizeof(int) * 2, c->stream));
+  c->it = it;
+  if ((rc = fields_f64(c, it, true, nullptr))) return rc;
+  return finish_outputs(c, nullptr, energies_out, cg_iters_out, it % c->P.isav == 0);
+}
+
+int em2g_smooth2(em2g_ctx *c, int id) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (id < 0 || id >= EM2G_NFIELD) return fail(EM2G_ERR_INVALID, "bad field id");
+  if ((rc = smooth2_f64(c, c->fld + id * c->g.w))) return rc;
+  EM2G_CUDA(cudaStreamSynchronize(c->stream));
+  return EM2G_OK;
+}
+
+int em2g_step(em2g_ctx *c, int nsteps, double *ake_out, double *energies_out,
+              int *cg_iters_out) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (nsteps < 0) return fail(EM2G_ERR_INVALID, "nsteps < 0");
+  EM2G_CUDA(cudaMemsetAsync(c->cg.status, 0, sizeof(int) * 2, c->stream));
+  for (int k = 0; k < nsteps; ++k) {
+    for (int s = 0; s < c->P.nsp; ++s) {
+      if ((rc = launch_prescale(c, s))) return rc;
+      if ((rc = launch_push_f64(c, s, 3))) return rc;
+    }
+    c->it += 1;
+    if ((rc = fields_f64(c, c->it, true, nullptr))) return rc;
+  }
+  return finish_outputs(c, ake_out, energies_out, cg_iters_out,
+                        nsteps > 0 && c->it % c->P.isav == 0);
+}
+
+}  // extern "C"

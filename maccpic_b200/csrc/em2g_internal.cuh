@@ -1,0 +1,88 @@
+// em2g_internal.cuh -- context layout and kernel entry points shared by the
+// translation units of libem2g.so.  Not part of the public ABI.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+
+#include "../../include/em2g.h"
+
+namespace em2g {
+
+constexpr int kEnergyBlocks = 296;  // partial sums per field in the energy reduction
+
+// Sets the per-thread error message and returns the status (api.cu).
+int fail(int status, const std::string &msg);
+int cuda_fail(cudaError_t e, const char *what);
+
+#define EM2G_CUDA(call)                                  \
+  do {                                                   \
+    cudaError_t _e = (call);                             \
+    if (_e != cudaSuccess) return cuda_fail(_e, #call);  \
+  } while (0)
+
+// Grid geometry of the (0:nx+2, 0:ny+2) arrays.
+struct Grid {
+  int nx, ny;
+  int nxg;      // nx + 3
+  int64_t w;    // (nx+3)*(ny+3)
+};
+
+// One species' particles on the device, FP64 layout of the reference:
+// six arrays of `cap` doubles (x, y, vx, vy, vz, gamma) back to back,
+// plus the original slot of each entry (for returning particles in slot
+// order after sorting).
+struct Species {
+  int64_t n = 0, cap = 0;
+  double *part = nullptr;      // 6*cap
+  int32_t *slot = nullptr;     // cap
+  double *part_alt = nullptr;  // 6*cap, sort target
+  int32_t *slot_alt = nullptr;
+};
+
+// Device workspace of the Poisson/cgm solve (pic/fields.f90:370-651).
+struct CgWork {
+  double *u = nullptr, *r = nullptr, *p = nullptr, *ap = nullptr;  // nx*ny each
+  double *partial = nullptr;   // 2 * max_blocks
+  unsigned *bar = nullptr;     // barrier counter + generation
+  int *status = nullptr;       // [0] timeout flag, [1] iterations
+  int blocks = 0, threads = 256;
+};
+
+}  // namespace em2g
+
+struct em2g_ctx {
+  em2g_params P;
+  em2g::Grid g;
+  int device = 0;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  int it = 0;
+  // 13 field arrays of w doubles back to back (enum em2g_field order)
+  double *fld = nullptr;
+  // per-species copies of E and B scaled by (q/m)dt/2 (pic/move.f90:52-64)
+  double *scaled = nullptr;  // nsp * 6 * w
+  double *smooth_tmp = nullptr;  // w, the `dummy` array of smooth2
+  em2g::Species sp[EM2G_MAX_SPECIES];
+  em2g::CgWork cg;
+  // reductions: ake partials per species, energy partials
+  double *red = nullptr;       // reduction scratch
+  int red_blocks = 0;
+  double *dev_out = nullptr;   // small device results (ake[4], e[6])
+  double *host_out = nullptr;  // pinned mirror of dev_out
+  int num_sms = 0;
+};
+
+namespace em2g {
+
+// ---- kernels launched from api.cu (defined in push_f64.cu / fields_f64.cu)
+int launch_prescale(em2g_ctx *c, int isp);
+// mode bit 1: move (gather + Boris); bit 2: curnt (deposit, move, deposit)
+int launch_push_f64(em2g_ctx *c, int isp, int mode);
+int launch_ake_finish(em2g_ctx *c, int isp, int nblocks_used);
+int fields_f64(em2g_ctx *c, int it, bool want_energies, int *cg_iters);
+int smooth2_f64(em2g_ctx *c, double *a);
+int cg_init(em2g_ctx *c);
+void cg_free(em2g_ctx *c);
+
+}  // namespace em2g

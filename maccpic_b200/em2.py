@@ -1,0 +1,195 @@
+"""Host-side mirror of em2's step interface on the GPU.
+
+em2 (fanyumeng666/maccpic, pic/) advances its state with parameterless
+subroutines acting on the module ``global`` (pic/global.f90:117-131):
+
+    call move     ! pic/move.f90:2     -> Em2Gpu.move()   (returns ake)
+    call curnt    ! pic/curnt.f90:2    -> Em2Gpu.curnt()
+    it = it + 1
+    call fields   ! pic/fields.f90:2   -> Em2Gpu.fields(it)
+    call smooth2(sm)  ! pic/smooth.f90:95 -> Em2Gpu.smooth2(name)
+
+:class:`Em2Gpu` owns one libem2g context; the state that ``global`` holds
+lives on the GPU and is copied in and out with :meth:`set_fields`,
+:meth:`get_fields`, :meth:`set_particles`, :meth:`get_particles`, in the
+reference's layouts ((ny+3, nx+3) REAL(8) field arrays; x, y, vx, vy, vz,
+gamma per species).  Errors raise :class:`~maccpic_b200._lib.Em2gError`,
+where em2 itself would print and continue or stop.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from ._lib import FIELD_ID, FIELD_NAMES, NFIELD, check
+
+
+@dataclass
+class RunParams:
+    """Run constants: pic/input.f90:9-43 and derived pic/global.f90:101-114.
+
+    Per-species values follow com_den (pic/input.f90:61-69) and init
+    (pic/init.f90:295-297): ``qm`` charge/mass, ``q`` macro charge, ``dn``
+    relative density, ``am`` macro mass."""
+    nx: int
+    ny: int
+    dx: float
+    dy: float
+    dt: float
+    qm: list
+    q: list
+    dn: list
+    am: list
+    np_max: list
+    nsp: int = 2
+    isav: int = 20
+    c: float = 1.0
+    tx: list = field(default_factory=lambda: [0.0] * 4)
+    ty: list = field(default_factory=lambda: [0.0] * 4)
+    cg_maxits: int = 10000
+    cg_eps: float = 1e-9
+    energy_mode: int = 0
+    qme: float = -1.0
+    wpe: float = 1.0
+    precision: int = _lib.FP64
+    device: int = 0
+    sort_interval: int = 0
+
+    @property
+    def shape(self):
+        return (self.ny + 3, self.nx + 3)
+
+    def ctype(self) -> _lib.Em2gParams:
+        P = _lib.Em2gParams()
+        check(_lib.lib().em2g_params_init(C.byref(P)))
+        for name in ("nx", "ny", "nsp", "isav", "precision", "dx", "dy", "dt", "c",
+                     "cg_maxits", "energy_mode", "cg_eps", "qme", "wpe", "device",
+                     "sort_interval"):
+            setattr(P, name, getattr(self, name))
+        for name in ("qm", "q", "dn", "am", "tx", "ty"):
+            arr = getattr(P, name)
+            vals = list(getattr(self, name)) + [0.0] * 4
+            for i in range(4):
+                arr[i] = float(vals[i])
+        vals = list(self.np_max) + [0] * 4
+        for i in range(4):
+            P.np_max[i] = int(vals[i])
+        return P
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class Em2Gpu:
+    """One em2 run resident on one GPU."""
+
+    def __init__(self, params: RunParams):
+        self.p = params
+        self._L = _lib.lib()
+        self._P = params.ctype()
+        h = C.c_void_p()
+        check(self._L.em2g_create(C.byref(self._P), C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            check(self._L.em2g_destroy(self._h))
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---- state copies ---------------------------------------------------
+    def set_fields(self, fld: np.ndarray) -> None:
+        """All 13 arrays, shape (13, ny+3, nx+3), enum em2g_field order."""
+        a = np.ascontiguousarray(fld, dtype=np.float64)
+        if a.shape != (NFIELD,) + self.p.shape:
+            raise ValueError(f"fields must have shape {(NFIELD,) + self.p.shape}")
+        check(self._L.em2g_set_fields(self._h, _dp(a)))
+
+    def get_fields(self) -> np.ndarray:
+        out = np.empty((NFIELD,) + self.p.shape)
+        check(self._L.em2g_get_fields(self._h, _dp(out)))
+        return out
+
+    def set_field(self, name: str, a: np.ndarray) -> None:
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        if a.shape != self.p.shape:
+            raise ValueError(f"field must have shape {self.p.shape}")
+        check(self._L.em2g_set_field(self._h, FIELD_ID[name], _dp(a)))
+
+    def get_field(self, name: str) -> np.ndarray:
+        out = np.empty(self.p.shape)
+        check(self._L.em2g_get_field(self._h, FIELD_ID[name], _dp(out)))
+        return out
+
+    def set_particles(self, isp: int, part: np.ndarray) -> None:
+        """part: (6, n) = x, y, vx, vy, vz, gamma in slot order."""
+        a = np.ascontiguousarray(part, dtype=np.float64)
+        if a.ndim != 2 or a.shape[0] != 6:
+            raise ValueError("particles must have shape (6, n)")
+        n = a.shape[1]
+        check(self._L.em2g_set_particles(self._h, isp, n, *[_dp(a[k]) for k in range(6)]))
+
+    def get_particles(self, isp: int) -> np.ndarray:
+        n = C.c_int64()
+        check(self._L.em2g_get_particles(self._h, isp, C.byref(n), *([None] * 6)))
+        out = np.empty((6, n.value))
+        if n.value:
+            check(self._L.em2g_get_particles(self._h, isp, C.byref(n),
+                                             *[_dp(out[k]) for k in range(6)]))
+        return out
+
+    @property
+    def it(self) -> int:
+        v = C.c_int()
+        check(self._L.em2g_get_step(self._h, C.byref(v)))
+        return v.value
+
+    @it.setter
+    def it(self, value: int) -> None:
+        check(self._L.em2g_set_step(self._h, int(value)))
+
+    # ---- the subroutines --------------------------------------------------
+    def move(self) -> np.ndarray:
+        """pic/move.f90: gather + Boris; returns ake(1:nsp)."""
+        ake = np.zeros(4)
+        check(self._L.em2g_move(self._h, _dp(ake)))
+        return ake[: self.p.nsp]
+
+    def curnt(self) -> None:
+        """pic/curnt.f90: deposit jm, move + wrap, deposit rho and jp."""
+        check(self._L.em2g_curnt(self._h))
+
+    def fields(self, it: int):
+        """pic/fields.f90 for step ``it``; returns (cg iterations, energies or None)."""
+        e6 = np.full(6, np.nan)
+        n = C.c_int()
+        check(self._L.em2g_fields(self._h, int(it), _dp(e6), C.byref(n)))
+        return n.value, (e6 if it % self.p.isav == 0 else None)
+
+    def smooth2(self, name: str) -> None:
+        """pic/smooth.f90:95 on one resident field array."""
+        check(self._L.em2g_smooth2(self._h, FIELD_ID[name]))
+
+    def step(self, nsteps: int = 1) -> dict:
+        """nsteps of {move; curnt; it+=1; fields(it)} on the fused fast path."""
+        ake = np.zeros(4)
+        e6 = np.full(6, np.nan)
+        n = C.c_int()
+        check(self._L.em2g_step(self._h, int(nsteps), _dp(ake), _dp(e6), C.byref(n)))
+        return {"ake": ake[: self.p.nsp].copy(), "cg_iters": n.value,
+                "energies": e6 if self.it % self.p.isav == 0 else None}
