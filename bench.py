@@ -1,0 +1,388 @@
+#!/usr/bin/env python
+"""Throughput of em2's time step on B200: particle-steps/s.
+
+One step is em2's main-loop pass move -> curnt -> it+1 -> fields
+(pic/main.f90:286-303) over the whole synthetic double-Harris workload
+(default 2048x1024 cells, 64 particles per cell per species, 268M
+particles), run through libem2g.  Prints one JSON line (rank 0).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--config NAME] [--precision fp64|fp32]
+
+value : device-resident state, K steps of em2g_step timed with CUDA events on
+        the library's stream (inputs of 13-26 GB are far larger than L2).
+e2e   : the same K steps through the drop-in entry points (em2g_move_curnt,
+        em2g_fields) starting from the state in pinned host memory: the
+        timed region includes the host->device upload of every field and
+        particle array, a device->host read of ake / CG count / energies each
+        step, and the download of the whole final state.
+--impl reference : the CPU restatement of em2 (oracle/, pthreads on all host
+        cores, one thread per em2 rank as em2's particle decomposition runs)
+        on the same workload; bounded to at most 1 warm-up and 2 timed steps.
+N > 1 : one process per GPU, each an independent replica of the workload
+        (weak scaling); the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", default="harris_2048x1024_ppc64")
+    ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_init():
+    import torch
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(ws, v):
+    if ws == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in getattr(self, "lines", []):
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(kernel_key):
+    """DRAM bytes per launch of the push kernel from the committed ncu summary
+    (profiles/<kernel_key>.json), or None."""
+    p = os.path.join(ROOT, "profiles", kernel_key + ".json")
+    if not os.path.exists(p):
+        return None
+    try:
+        return float(json.load(open(p))["dram_bytes_per_launch"])
+    except (KeyError, ValueError):
+        return None
+
+
+def cpu_baseline(cfg, fields, parts_host, budget_s=15.0):
+    """The oracle (pthreads, all cores) on a bounded sample of the workload:
+    the full grid and a slice of the particles sized for ~budget_s of work."""
+    import numpy as np
+    import oracle
+    cores = os.cpu_count() or 1
+    rp = cfg.run_params()
+    op = oracle.Params(nx=rp.nx, ny=rp.ny, dx=rp.dx, dy=rp.dy, dt=rp.dt, qm=rp.qm,
+                       q=rp.q, dn=rp.dn, am=rp.am, isav=rp.isav)
+    n = parts_host[0].shape[1]
+    # calibrate on a small slice
+    m0 = min(n, 1 << 20)
+    st = oracle.State(op, fields, [p[:, :m0] for p in parts_host])
+    t = time.perf_counter()
+    st.step(nthreads=cores)
+    dt0 = time.perf_counter() - t
+    per = dt0 / (2 * m0)
+    m = int(min(n, max(m0, budget_s / 2 / max(per, 1e-12) / 2)))
+    st = oracle.State(op, fields, [np.ascontiguousarray(p[:, :m]) for p in parts_host])
+    st.step(nthreads=cores)  # warm-up
+    t = time.perf_counter()
+    st.step(nthreads=cores)
+    el = time.perf_counter() - t
+    return {"value": 2 * m / el, "unit": METRIC, "cores": cores, "kind": "port",
+            "sample": f"1 step of the {cfg.nx}x{cfg.ny} grid with {m} of {n} particles per "
+                      f"species (C restatement of em2, {cores} threads, field solve serial "
+                      f"as in every em2 rank)"}
+
+
+def run_reference(args):
+    import numpy as np
+    import torch
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import oracle
+    from maccpic_b200 import loader
+    cfg = loader.PRESETS[args.config]
+    fields = loader.initial_fields(cfg)
+    # the state is drawn on the GPU when there is one (set-up, not timed)
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    parts = [p.cpu().numpy() for p in loader.sample_particles_torch(cfg, device=dev)]
+    rp = cfg.run_params()
+    op = oracle.Params(nx=rp.nx, ny=rp.ny, dx=rp.dx, dy=rp.dy, dt=rp.dt, qm=rp.qm,
+                       q=rp.q, dn=rp.dn, am=rp.am, isav=rp.isav)
+    st = oracle.State(op, fields, parts)
+    del parts
+    cores = os.cpu_count() or 1
+    warm, steps = min(args.warmup, 1), max(1, min(args.steps, 2))
+    for _ in range(warm):
+        st.step(nthreads=cores)
+    t = time.perf_counter()
+    for _ in range(steps):
+        st.step(nthreads=cores)
+    el = time.perf_counter() - t
+    n_total = sum(p.shape[1] for p in st.parts)
+    value = n_total * steps / el
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC,
+        "n_gpus": ws, "steps": steps, "warmup": warm, "ms_per_step": 1e3 * el / steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded double-Harris sampling)",
+        "config": {"workload": args.config, "grid": [cfg.nx, cfg.ny], "ppc": cfg.ppc,
+                   "particles": n_total, "mass_ratio": cfg.mass_ratio},
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": "port",
+                         "sample": f"{steps} full steps after {warm} warm-up (C restatement "
+                                   f"of em2; em2 itself needs gfortran+MPI, absent)"},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    from maccpic_b200 import build, loader
+    from maccpic_b200.em2 import Em2Gpu
+
+    ws, rank, local = dist_init()
+    build.build()
+    cfg = loader.PRESETS[args.config]
+    rp = cfg.run_params(device=local)
+    stream = torch.cuda.current_stream()
+    fields = loader.initial_fields(cfg)
+    n = cfg.nx * cfg.ny * cfg.ppc
+    n_total = 2 * n
+    W = (cfg.nx + 3) * (cfg.ny + 3)
+
+    g = Em2Gpu(rp)
+    g.set_stream(stream)
+    g.set_fields(fields)
+    parts = loader.sample_particles_torch(cfg, device=f"cuda:{local}")
+    for s in range(2):
+        g.set_particles_device(s, parts[s])
+    torch.cuda.synchronize()
+    parts_host = None
+    if rank == 0 and not args.no_e2e:
+        parts_host = [p.cpu().pin_memory() for p in parts]
+    del parts
+    torch.cuda.empty_cache()
+
+    for _ in range(args.warmup):
+        g.step(1)
+    g.reset_counters()
+    g.set_timing(True)
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(ws)
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        start.record(stream)
+        cg = []
+        for _ in range(args.steps):
+            r = g.step(1)
+            cg.append(r["cg_iters"])
+        stop.record(stream)
+        torch.cuda.synchronize()
+    barrier(ws)
+    ms = start.elapsed_time(stop)
+    ms = max_over_ranks(ws, ms)
+    cnt = g.counters()
+    g.set_timing(False)
+    value = n_total * ws * args.steps / (ms / 1e3)
+
+    # roofline of the dominant kernel (fused push): algorithmic bytes per
+    # launch = n * 96 B (x, y, vx, vy, vz, gamma read and written) + the grid
+    # arrays it touches: 6 scaled field arrays read and 7 deposit arrays
+    # read-modify-written, W * 8 * (6 + 14) B
+    bytes_launch = n * 96 + W * 8 * 20
+    avg_ms = cnt["push_ms"] / max(cnt["push_launches_timed"], 1)
+    achieved = bytes_launch / (avg_ms / 1e3) / 1e9
+    peak, peak_kind = peaks()
+    traffic = profile_traffic(f"push_f64_{args.config}")
+
+    e2e = None
+    if rank == 0 and not args.no_e2e:
+        e2e = run_e2e(args, cfg, rp, fields, parts_host)
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(cfg, fields, [p.numpy() for p in parts_host]
+                           if parts_host is not None else
+                           [p.cpu().numpy() for p in loader.sample_particles_torch(cfg)])
+    g.close()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded double-Harris sampling, GPU Philox)",
+            "config": {"workload": args.config, "grid": [cfg.nx, cfg.ny], "ppc": cfg.ppc,
+                       "particles_per_gpu": n_total, "mass_ratio": cfg.mass_ratio,
+                       "precision": args.precision, "path": "em2g_step (fused push)",
+                       "l2": "inputs larger than L2 (particle state 25.8 GB)",
+                       "parallelism": f"replicas x{ws}", "cg_iters_mean":
+                           sum(cg) / len(cg)},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "kernel": "k_push_f64<3>", "peak_kind": peak_kind,
+                         "bytes_per_launch": bytes_launch, "avg_launch_ms": avg_ms},
+            "gpu_launches": cnt["kernel_launches"],
+            "clocks": clk.summary(),
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def run_e2e(args, cfg, rp, fields, parts_host):
+    """Drop-in path from host memory: upload, K steps of move_curnt + fields
+    reading ake / CG count / energies back every step, download everything."""
+    import numpy as np
+    import torch
+    from maccpic_b200.em2 import Em2Gpu
+
+    fields_pin = torch.from_numpy(fields).pin_memory()
+    fnp = fields_pin.numpy()
+    pnp = [p.numpy() for p in parts_host]
+    g = Em2Gpu(rp)
+    out_f = torch.empty_like(fields_pin).pin_memory().numpy()
+    out_p = [torch.empty_like(p).pin_memory().numpy() for p in parts_host]
+    # warm-up (not timed): one full pass
+    g.set_fields(fnp)
+    for s in range(2):
+        g.set_particles(s, pnp[s])
+    g.move_curnt()
+    g.fields(1)
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    g.set_fields(fnp)
+    for s in range(2):
+        g.set_particles(s, pnp[s])
+    g.it = 0
+    for it in range(1, args.steps + 1):
+        g.move_curnt()
+        g.fields(it)
+    out_f[...] = g.get_fields()
+    for s in range(2):
+        n = C_get_particles_into(g, s, out_p[s])
+    el = time.perf_counter() - t
+    g.close()
+    n_total = sum(p.shape[1] for p in pnp)
+    state = fnp.nbytes + sum(p.nbytes for p in pnp)
+    small = 8 * (2 + 6) + 4
+    return {"value": n_total * args.steps / el, "unit": METRIC,
+            "h2d_bytes_per_step": state / args.steps,
+            "d2h_bytes_per_step": (state + small * args.steps) / args.steps,
+            "path": "em2g_set_fields/em2g_set_particles (pinned host), K x "
+                    "(em2g_move_curnt, em2g_fields), em2g_get_fields/em2g_get_particles"}
+
+
+def C_get_particles_into(g, s, out):
+    import ctypes as C
+    from maccpic_b200._lib import check
+    n = C.c_int64()
+    ptrs = [out[k].ctypes.data_as(C.POINTER(C.c_double)) for k in range(6)]
+    check(g._L.em2g_get_particles(g._h, s, C.byref(n), *ptrs))
+    return n.value
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

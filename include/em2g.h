@@ -116,6 +116,10 @@ int em2g_get_fields(em2g_ctx *ctx, double *host13);
 int em2g_set_particles(em2g_ctx *ctx, int isp, int64_t n, const double *x,
                        const double *y, const double *vx, const double *vy,
                        const double *vz, const double *gamma);
+/* the same from arrays in device memory (validated on the device) */
+int em2g_set_particles_device(em2g_ctx *ctx, int isp, int64_t n, const double *x,
+                              const double *y, const double *vx, const double *vy,
+                              const double *vz, const double *gamma);
 /* returns them in the slot order they were given in, whatever the library
  * did to its internal order; *n receives the count.  With all six array
  * pointers NULL it only reports the count. */
@@ -147,6 +151,11 @@ int em2g_curnt(em2g_ctx *ctx);
 int em2g_fields(em2g_ctx *ctx, int it, double *energies_out, int *cg_iters_out);
 /* smooth2 (pic/smooth.f90:95-179) in place on one resident field array */
 int em2g_smooth2(em2g_ctx *ctx, int field_id);
+/* move followed by curnt in one fused particle kernel per species: the same
+ * result as em2g_move then em2g_curnt.  A shim can map em2's `call move`
+ * to nothing and `call curnt` to this (nothing reads v between the two,
+ * pic/main.f90:287-288). */
+int em2g_move_curnt(em2g_ctx *ctx, double *ake_out);
 
 /* ---- fused fast path -------------------------------------------------
  * nsteps iterations of { move; curnt; it = it + 1; fields(it) } with the
@@ -155,6 +164,14 @@ int em2g_smooth2(em2g_ctx *ctx, int field_id);
  * last `it` is a multiple of isav). */
 int em2g_step(em2g_ctx *ctx, int nsteps, double *ake_out, double *energies_out,
               int *cg_iters_out);
+
+/* ---- instrumentation ------------------------------------------------- */
+/* kernel launches since the last reset; with timing on, the number of
+ * particle-push launches timed with CUDA events and their summed time */
+int em2g_set_timing(em2g_ctx *ctx, int on);
+int em2g_get_counters(em2g_ctx *ctx, int64_t *kernel_launches,
+                      int64_t *push_launches_timed, double *push_ms);
+int em2g_reset_counters(em2g_ctx *ctx);
 
 #ifdef __cplusplus
 }

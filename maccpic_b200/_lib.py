@@ -28,7 +28,8 @@ EXPORTS = [
     "em2g_get_field", "em2g_set_fields", "em2g_get_fields", "em2g_set_particles",
     "em2g_get_particles", "em2g_set_step", "em2g_get_step", "em2g_set_fields_device",
     "em2g_get_fields_device", "em2g_field_device_ptr", "em2g_move", "em2g_curnt",
-    "em2g_fields", "em2g_smooth2", "em2g_step",
+    "em2g_fields", "em2g_smooth2", "em2g_step", "em2g_set_particles_device",
+    "em2g_move_curnt", "em2g_set_timing", "em2g_get_counters", "em2g_reset_counters",
 ]
 
 
@@ -95,6 +96,11 @@ def lib() -> C.CDLL:
         "em2g_fields": (C.c_int, [ctx, C.c_int, dp, ip]),
         "em2g_smooth2": (C.c_int, [ctx, C.c_int]),
         "em2g_step": (C.c_int, [ctx, C.c_int, dp, dp, ip]),
+        "em2g_set_particles_device": (C.c_int, [ctx, C.c_int, C.c_int64] + [vp] * 6),
+        "em2g_move_curnt": (C.c_int, [ctx, dp]),
+        "em2g_set_timing": (C.c_int, [ctx, C.c_int]),
+        "em2g_get_counters": (C.c_int, [ctx, i64p, i64p, dp]),
+        "em2g_reset_counters": (C.c_int, [ctx]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -24,7 +24,55 @@ int cuda_fail(cudaError_t e, const char *what) {
   return e == cudaErrorMemoryAllocation ? EM2G_ERR_NOMEM : EM2G_ERR_CUDA;
 }
 
+int timing_begin(em2g_ctx *c) {
+  if (!c->timing) return EM2G_OK;
+  if (c->ev_used + 2 > c->ev.size()) {
+    for (int k = 0; k < 2; ++k) {
+      cudaEvent_t e;
+      EM2G_CUDA(cudaEventCreate(&e));
+      c->ev.push_back(e);
+    }
+  }
+  EM2G_CUDA(cudaEventRecord(c->ev[c->ev_used], c->stream));
+  return EM2G_OK;
+}
+
+int timing_end(em2g_ctx *c) {
+  if (!c->timing) return EM2G_OK;
+  EM2G_CUDA(cudaEventRecord(c->ev[c->ev_used + 1], c->stream));
+  c->ev_used += 2;
+  return EM2G_OK;
+}
+
+// after a stream synchronisation: fold the recorded pairs into push_ms
+static int timing_collect(em2g_ctx *c) {
+  for (size_t k = 0; k + 1 < c->ev_used; k += 2) {
+    float ms = 0.f;
+    EM2G_CUDA(cudaEventElapsedTime(&ms, c->ev[k], c->ev[k + 1]));
+    c->push_ms += ms;
+    c->push_timed += 1;
+  }
+  c->ev_used = 0;
+  return EM2G_OK;
+}
+
 namespace {
+
+// device-side check of uploaded particles: bad[0] counts positions outside
+// [0, n+0.5), bad[1] counts non-finite values
+__global__ void k_check_particles(const double *__restrict__ part, int64_t n, int64_t cap,
+                                  double xlim, double ylim, unsigned long long *bad) {
+  const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  bool finite = true;
+  for (int k = 0; k < 6; ++k) finite = finite && isfinite(part[k * cap + j]);
+  if (!finite) {
+    atomicAdd(bad + 1, 1ull);
+    return;
+  }
+  const double x = part[j], y = part[cap + j];
+  if (!(x >= 0.0 && x < xlim && y >= 0.0 && y < ylim)) atomicAdd(bad, 1ull);
+}
 
 // slot-order restore: dst[slot[j]] = src[j] for the 6 arrays
 __global__ void k_unsort(const double *__restrict__ src, const int32_t *__restrict__ slot,
@@ -83,6 +131,8 @@ int finish_outputs(em2g_ctx *c, double *ake_out, double *energies_out, int *cg_i
   EM2G_CUDA(cudaMemcpyAsync(st, c->cg.status, sizeof(st), cudaMemcpyDeviceToHost, c->stream));
   EM2G_CUDA(cudaStreamSynchronize(c->stream));
   EM2G_CUDA(cudaGetLastError());
+  int rc = timing_collect(c);
+  if (rc) return rc;
   if (st[0] != 0) return fail(EM2G_ERR_TIMEOUT, "cg: a grid barrier wait timed out");
   if (ake_out)
     for (int s = 0; s < c->P.nsp; ++s) ake_out[s] = c->host_out[s];
@@ -201,6 +251,7 @@ int em2g_destroy(em2g_ctx *c) {
   cudaFree(c->dev_out);
   if (c->host_out) cudaFreeHost(c->host_out);
   cg_free(c);
+  for (cudaEvent_t e : c->ev) cudaEventDestroy(e);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
   return EM2G_OK;
@@ -323,6 +374,45 @@ int em2g_set_particles(em2g_ctx *c, int isp, int64_t n, const double *x, const d
   return EM2G_OK;
 }
 
+int em2g_set_particles_device(em2g_ctx *c, int isp, int64_t n, const double *x,
+                              const double *y, const double *vx, const double *vy,
+                              const double *vz, const double *gamma) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (isp < 0 || isp >= c->P.nsp) return fail(EM2G_ERR_INVALID, "bad species index");
+  Species &S = c->sp[isp];
+  if (n < 0 || n > S.cap) return fail(EM2G_ERR_RANGE, "particle count exceeds np_max");
+  if (n == 0) {
+    S.n = 0;
+    return EM2G_OK;
+  }
+  if (!x || !y || !vx || !vy || !vz || !gamma) return fail(EM2G_ERR_INVALID, "null particle array");
+  const double *src[6] = {x, y, vx, vy, vz, gamma};
+  for (int k = 0; k < 6; ++k)
+    EM2G_CUDA(cudaMemcpyAsync(S.part + k * S.cap, src[k], sizeof(double) * n,
+                              cudaMemcpyDeviceToDevice, c->stream));
+  unsigned long long *bad = (unsigned long long *)c->red;  // 2 counters
+  EM2G_CUDA(cudaMemsetAsync(bad, 0, 2 * sizeof(unsigned long long), c->stream));
+  const unsigned nb = (unsigned)((n + 255) / 256);
+  k_check_particles<<<nb, 256, 0, c->stream>>>(S.part, n, S.cap, c->P.nx + 0.5, c->P.ny + 0.5,
+                                                bad);
+  k_iota<<<nb, 256, 0, c->stream>>>(S.slot, n);
+  EM2G_CUDA(cudaGetLastError());
+  unsigned long long hb[2] = {0, 0};
+  EM2G_CUDA(cudaMemcpyAsync(hb, bad, sizeof(hb), cudaMemcpyDeviceToHost, c->stream));
+  EM2G_CUDA(cudaStreamSynchronize(c->stream));
+  if (hb[1]) {
+    S.n = 0;
+    return fail(EM2G_ERR_NONFINITE, std::to_string(hb[1]) + " particles with non-finite values");
+  }
+  if (hb[0]) {
+    S.n = 0;
+    return fail(EM2G_ERR_RANGE, std::to_string(hb[0]) + " particles outside the grid");
+  }
+  S.n = n;
+  return EM2G_OK;
+}
+
 int em2g_get_particles(em2g_ctx *c, int isp, int64_t *n, double *x, double *y, double *vx,
                        double *vy, double *vz, double *gamma) {
   int rc = check_ctx(c);
@@ -367,6 +457,42 @@ int em2g_move(em2g_ctx *c, double *ake_out) {
     if ((rc = launch_push_f64(c, s, 1))) return rc;
   }
   return finish_outputs(c, ake_out, nullptr, nullptr, false);
+}
+
+int em2g_move_curnt(em2g_ctx *c, double *ake_out) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  for (int s = 0; s < c->P.nsp; ++s) {
+    if ((rc = launch_prescale(c, s))) return rc;
+    if ((rc = launch_push_f64(c, s, 3))) return rc;
+  }
+  return finish_outputs(c, ake_out, nullptr, nullptr, false);
+}
+
+int em2g_set_timing(em2g_ctx *c, int on) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  c->timing = on ? 1 : 0;
+  return EM2G_OK;
+}
+
+int em2g_get_counters(em2g_ctx *c, int64_t *kernel_launches, int64_t *push_launches_timed,
+                      double *push_ms) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (kernel_launches) *kernel_launches = c->launches;
+  if (push_launches_timed) *push_launches_timed = c->push_timed;
+  if (push_ms) *push_ms = c->push_ms;
+  return EM2G_OK;
+}
+
+int em2g_reset_counters(em2g_ctx *c) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  c->launches = 0;
+  c->push_timed = 0;
+  c->push_ms = 0.0;
+  return EM2G_OK;
 }
 
 int em2g_curnt(em2g_ctx *c) {

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <string>
+#include <vector>
 
 #include "../../include/em2g.h"
 
@@ -71,6 +72,14 @@ struct em2g_ctx {
   double *dev_out = nullptr;   // small device results (ake[4], e[6])
   double *host_out = nullptr;  // pinned mirror of dev_out
   int num_sms = 0;
+  // counters (em2g_get_counters): kernel launches, and when timing is on,
+  // CUDA-event time of the particle-push launches
+  int64_t launches = 0;
+  int timing = 0;
+  std::vector<cudaEvent_t> ev;  // start/stop pairs of the pending push launches
+  size_t ev_used = 0;
+  double push_ms = 0.0;
+  int64_t push_timed = 0;
 };
 
 namespace em2g {
@@ -83,6 +92,9 @@ int launch_ake_finish(em2g_ctx *c, int isp, int nblocks_used);
 int fields_f64(em2g_ctx *c, int it, bool want_energies, int *cg_iters);
 int smooth2_f64(em2g_ctx *c, double *a);
 int cg_init(em2g_ctx *c);
+// bracket one push launch with events when timing is on (api.cu)
+int timing_begin(em2g_ctx *c);
+int timing_end(em2g_ctx *c);
 void cg_free(em2g_ctx *c);
 
 }  // namespace em2g

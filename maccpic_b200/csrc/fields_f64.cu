@@ -356,6 +356,7 @@ int smooth2_f64(em2g_ctx *c, double *a) {
   const dim3 grd = grid_for(g.nx + 1, g.ny + 1), blk(TX, TY);
   k_smooth_binomial<<<grd, blk, 0, c->stream>>>(g, a, c->smooth_tmp);
   k_smooth_compensate<<<grd, blk, 0, c->stream>>>(g, c->smooth_tmp, a);
+  c->launches += 2;
   EM2G_CUDA(cudaGetLastError());
   return EM2G_OK;
 }
@@ -413,6 +414,7 @@ static int poisson_f64(em2g_ctx *c, int *iters) {
   EM2G_CUDA(cudaLaunchCooperativeKernel((const void *)k_cg, dim3(W.blocks), dim3(W.threads),
                                         args, 0, c->stream));
   k_poisson_correct<<<grid_for(g.nx, g.ny), blk, 0, c->stream>>>(g, c->fld, W.u, dx, dy);
+  c->launches += 3;
   EM2G_CUDA(cudaGetLastError());
   // status[0] (sticky timeout flag) and status[1] (iterations) are read by
   // the caller after its last launch; no host synchronisation here.
@@ -435,6 +437,7 @@ static int energies_f64(em2g_ctx *c) {
   k_energy_partial<<<dim3(nb, 6), 256, 0, c->stream>>>(g, c->fld, lo, hi, c->red);
   k_energy_finish<<<6, 256, 0, c->stream>>>(c->red, nb, anorml1, c->P.energy_mode == 1, g.ny,
                                             c->dev_out + 4);
+  c->launches += 2;
   EM2G_CUDA(cudaGetLastError());
   return EM2G_OK;
 }
@@ -452,6 +455,7 @@ int fields_f64(em2g_ctx *c, int it, bool want_energies, int *cg_iters) {
   k_b_half<<<grd, blk, 0, c->stream>>>(g, c->fld, ctxh, ctyh);
   k_e_full<<<grd, blk, 0, c->stream>>>(g, c->fld, ctx, cty, tem);
   k_b_half<<<grd, blk, 0, c->stream>>>(g, c->fld, ctxh, ctyh);
+  c->launches += 5;
   EM2G_CUDA(cudaGetLastError());
   // filters (pic/fields.f90:252-260)
   int rc = smooth2_f64(c, c->fld + EM2G_RHO * g.w);

@@ -260,6 +260,7 @@ int launch_prescale(em2g_ctx *c, int isp) {
   const int blocks = (int)((w + 255) / 256);
   k_prescale<<<blocks, 256, 0, c->stream>>>(c->fld, c->scaled + (int64_t)isp * 6 * w, w, ae,
                                             c->P.tx[isp], c->P.ty[isp]);
+  c->launches += 1;
   EM2G_CUDA(cudaGetLastError());
   return EM2G_OK;
 }
@@ -285,16 +286,21 @@ int launch_push_f64(em2g_ctx *c, int isp, int mode) {
   const int64_t nb64 = (S.n + kThreads - 1) / kThreads;
   if (nb64 > c->red_blocks) return fail(EM2G_ERR_RANGE, "particle count exceeds reduction scratch");
   const int nb = (int)(nb64 > 0 ? nb64 : 1);
+  if (mode < 1 || mode > 3) return fail(EM2G_ERR_INVALID, "bad push mode");
+  int rc = timing_begin(c);
+  if (rc) return rc;
   switch (mode) {
     case 1: k_push_f64<1><<<nb, kThreads, 0, c->stream>>>(a); break;
     case 2: k_push_f64<2><<<nb, kThreads, 0, c->stream>>>(a); break;
-    case 3: k_push_f64<3><<<nb, kThreads, 0, c->stream>>>(a); break;
-    default: return fail(EM2G_ERR_INVALID, "bad push mode");
+    default: k_push_f64<3><<<nb, kThreads, 0, c->stream>>>(a); break;
   }
+  c->launches += 1;
   EM2G_CUDA(cudaGetLastError());
+  if ((rc = timing_end(c))) return rc;
   if (mode & 1) {
     k_ake_finish<<<1, 256, 0, c->stream>>>(c->red, nb, c->P.am[isp], c->P.dn[isp],
                                            c->dev_out + isp);
+    c->launches += 1;
     EM2G_CUDA(cudaGetLastError());
   }
   return EM2G_OK;

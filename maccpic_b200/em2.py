@@ -144,6 +144,36 @@ class Em2Gpu:
         n = a.shape[1]
         check(self._L.em2g_set_particles(self._h, isp, n, *[_dp(a[k]) for k in range(6)]))
 
+    def set_particles_device(self, isp: int, part) -> None:
+        """part: a CUDA tensor (6, n) float64 on this context's device; the
+        library copies it on its stream (call set_stream first to order it
+        after the producer)."""
+        import torch
+        if part.dtype != torch.float64 or part.dim() != 2 or part.shape[0] != 6:
+            raise ValueError("particles must be a float64 tensor of shape (6, n)")
+        part = part.contiguous()
+        n = part.shape[1]
+        ptrs = [C.c_void_p(part[k].data_ptr()) for k in range(6)]
+        check(self._L.em2g_set_particles_device(self._h, isp, n, *ptrs))
+
+    def set_stream(self, stream) -> None:
+        """Enqueue further work on this cudaStream_t (int handle, or a torch
+        stream); None returns to the context's own stream."""
+        handle = getattr(stream, "cuda_stream", stream)
+        check(self._L.em2g_set_stream(self._h, C.c_void_p(handle or 0)))
+
+    def set_timing(self, on: bool) -> None:
+        check(self._L.em2g_set_timing(self._h, int(bool(on))))
+
+    def counters(self) -> dict:
+        a, b, ms = C.c_int64(), C.c_int64(), C.c_double()
+        check(self._L.em2g_get_counters(self._h, C.byref(a), C.byref(b), C.byref(ms)))
+        return {"kernel_launches": a.value, "push_launches_timed": b.value,
+                "push_ms": ms.value}
+
+    def reset_counters(self) -> None:
+        check(self._L.em2g_reset_counters(self._h))
+
     def get_particles(self, isp: int) -> np.ndarray:
         n = C.c_int64()
         check(self._L.em2g_get_particles(self._h, isp, C.byref(n), *([None] * 6)))
@@ -168,6 +198,12 @@ class Em2Gpu:
         """pic/move.f90: gather + Boris; returns ake(1:nsp)."""
         ake = np.zeros(4)
         check(self._L.em2g_move(self._h, _dp(ake)))
+        return ake[: self.p.nsp]
+
+    def move_curnt(self) -> np.ndarray:
+        """move then curnt in one fused particle kernel; returns ake."""
+        ake = np.zeros(4)
+        check(self._L.em2g_move_curnt(self._h, _dp(ake)))
         return ake[: self.p.nsp]
 
     def curnt(self) -> None:

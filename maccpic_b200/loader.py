@@ -183,3 +183,57 @@ def sample_particles(cfg: HarrisConfig, n: int | None = None):
 def initial_state(cfg: HarrisConfig, n: int | None = None):
     """(fields, [electrons, ions]) for the config."""
     return initial_fields(cfg), sample_particles(cfg, n)
+
+
+def sample_particles_torch(cfg: HarrisConfig, device="cuda", n: int | None = None,
+                           dtype=None):
+    """The same distribution as :func:`sample_particles`, drawn on the GPU
+    with torch's Philox generator (for workloads too large for host RAM).
+    Returns two (6, n) tensors (x, y, vx, vy, vz, gamma) on ``device``."""
+    import torch
+    dtype = dtype or torch.float64
+    nx, ny, dx = cfg.nx, cfg.ny, cfg.dx
+    n = n if n is not None else nx * ny * cfg.ppc
+    gen = torch.Generator(device=device)
+    gen.manual_seed(cfg.seed * 7919 + 0xE2)
+    lc = cfg.L / dx
+    sheet_w = cfg.csden * 2.0 * lc * 2.0
+    n_sheet = int(round(n * sheet_w / (ny + sheet_w)))
+    n_bg = n - n_sheet
+    f64 = torch.float64
+    y = torch.empty(n, dtype=f64, device=device)
+    y[:n_bg] = torch.rand(n_bg, generator=gen, dtype=f64, device=device) * ny
+    u = torch.rand(n_sheet, generator=gen, dtype=f64, device=device)
+    which = torch.rand(n_sheet, generator=gen, dtype=f64, device=device) < 0.5
+    centre = torch.where(which, torch.tensor(ny / 4.0, dtype=f64, device=device),
+                         torch.tensor(3.0 * ny / 4.0, dtype=f64, device=device))
+    ys = centre + lc * torch.atanh((2.0 * u - 1.0).clamp(-1 + 1e-15, 1 - 1e-15))
+    y[n_bg:] = torch.remainder(ys, ny)
+    x = torch.rand(n, generator=gen, dtype=f64, device=device) * nx
+    x[x >= nx] = 0.0
+    y[y >= ny] = 0.0
+    te, ti = cfg.temperatures()
+    vdiff = cfg.b0 / (cfg.L * cfg.csden)
+    ve = vdiff / (1.0 + cfg.ti_over_te)
+    vi = vdiff * cfg.ti_over_te / (1.0 + cfg.ti_over_te)
+    sign = torch.zeros(n, dtype=f64, device=device)
+    sign[n_bg:] = torch.where(which, -1.0, 1.0).to(f64)
+    out = []
+    for temp_over_m, vdrift in [(te, -ve), (ti / cfg.mass_ratio, vi)]:
+        uth = math.sqrt(temp_over_m)
+        ux, uy, uz = (torch.randn(n, generator=gen, dtype=f64, device=device) * uth
+                      for _ in range(3))
+        g1 = torch.sqrt(1.0 + ux * ux + uy * uy + uz * uz)
+        vx, vy, vz = ux / g1, uy / g1, uz / g1
+        del ux, uy, uz, g1
+        V = sign * vdrift
+        g0 = torch.sqrt(1.0 - V * V)
+        den = 1.0 + V * vz
+        vz2 = (V + vz) / den
+        vx2 = vx * g0 / den
+        vy2 = vy * g0 / den
+        del vx, vy, vz, V, g0, den
+        gam = 1.0 / torch.sqrt(1.0 - vx2 * vx2 - vy2 * vy2 - vz2 * vz2)
+        out.append(torch.stack([x, y, vx2, vy2, vz2, gam]).to(dtype))
+        del vx2, vy2, vz2, gam
+    return out

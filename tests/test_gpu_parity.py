@@ -21,6 +21,16 @@ def rel(a, b):
     return np.abs(a - b).max() / scale
 
 
+def periodize(a):
+    """Set the guard columns/rows of (ny+3, nx+3) arrays from the interior,
+    as em2 keeps them (periodic images 0 <- n, n+1 <- 1, n+2 <- 2)."""
+    a = a.copy()
+    nx, ny = a.shape[-1] - 3, a.shape[-2] - 3
+    a[..., :, 0], a[..., :, nx + 1], a[..., :, nx + 2] = a[..., :, nx], a[..., :, 1], a[..., :, 2]
+    a[..., 0, :], a[..., ny + 1, :], a[..., ny + 2, :] = a[..., ny, :], a[..., 1, :], a[..., 2, :]
+    return a
+
+
 def random_case(nx=40, ny=24, n=5000, seed=11, isav=2):
     import oracle
     from maccpic_b200.em2 import RunParams
@@ -30,7 +40,7 @@ def random_case(nx=40, ny=24, n=5000, seed=11, isav=2):
     op = oracle.Params(**kw)
     rp = RunParams(np_max=[n, n], **kw)
     fld = np.zeros((13, ny + 3, nx + 3))
-    fld[:6] = rng.normal(scale=0.05, size=(6, ny + 3, nx + 3))
+    fld[:6] = periodize(rng.normal(scale=0.05, size=(6, ny + 3, nx + 3)))
     parts = []
     for s in range(2):
         x = rng.random(n) * nx
@@ -106,7 +116,12 @@ def test_fields_stencils_bitwise_poisson_within_tolerance(gpu, oracle_lib, it):
     op, rp, fld, parts = random_case(isav=2)
     rng = np.random.default_rng(3)
     fld = fld.copy()
-    fld[6:] = rng.normal(scale=0.01, size=fld[6:].shape)
+    # unfolded deposits: interior values, zero guards; total charge zero so
+    # that the periodic Poisson problem is solvable
+    ny, nx = fld.shape[1] - 3, fld.shape[2] - 3
+    fld[6:] = 0.0
+    fld[6:, 1:ny + 1, 1:nx + 1] = rng.normal(scale=0.01, size=(7, ny, nx))
+    fld[6, 1:ny + 1, 1:nx + 1] -= fld[6, 1:ny + 1, 1:nx + 1].mean()
     st = oracle_lib.State(op, fld, parts)
     n_ref, e_ref = st.fields(it)
     with make_gpu(rp, fld, parts) as g:
