@@ -165,6 +165,20 @@ int em2g_move_curnt(em2g_ctx *ctx, double *ake_out);
 int em2g_step(em2g_ctx *ctx, int nsteps, double *ake_out, double *energies_out,
               int *cg_iters_out);
 
+/* ---- smooth2 without device allocation -------------------------------
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc
+ * (their device memory is managed by someone else, or they are inside a
+ * stream capture) and so cannot create a context: filters the caller's
+ * (nx+3)*(ny+3) device array in place, as smooth2 does, on cuda_stream.
+ * The scratch smooth2 needs is a static device array of
+ * EM2G_SMOOTH2_STATIC_MAX_POINTS doubles (4 MiB, held by every GPU that loads
+ * the library); larger grids are rejected with EM2G_ERR_RANGE.  The first
+ * call on a device looks up that array's device address (make it before any
+ * stream capture).  Calls share the scratch: calls that overlap on the GPU
+ * race, so order them.  No memory is allocated or freed. */
+#define EM2G_SMOOTH2_STATIC_MAX_POINTS (1 << 19)
+int em2g_smooth2_static(int nx, int ny, double *dev_array, void *cuda_stream);
+
 /* ---- instrumentation ------------------------------------------------- */
 /* kernel launches since the last reset; with timing on, the number of
  * particle-push launches timed with CUDA events and their summed time */

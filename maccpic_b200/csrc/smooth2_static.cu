@@ -1,0 +1,111 @@
+// smooth2_static.cu -- em2g_smooth2_static: smooth2 (pic/smooth.f90:95-179)
+// on a caller's device array, with no device allocation at all.
+//
+// Who needs it: callers that cannot call cudaMalloc and so cannot create an
+// em2g context -- host code that hands over device arrays it manages itself
+// under a fixed memory budget, code running while a stream is being
+// captured, or a process whose GPU memory is already reserved by another
+// allocator.  They pass the array in and get it back filtered in place.
+//
+// smooth2 needs one scratch array the size of its input (the reference's
+// local `dummy`).  Here that scratch is the file-scope device array below, of
+// EM2G_SMOOTH2_STATIC_MAX_POINTS doubles (4 MiB); every GPU that loads the
+// library holds it until the process exits.  All calls on a device share it:
+// two calls whose kernels overlap on the GPU race on it, so callers order
+// their calls (one stream, or events).  Each call overwrites every scratch
+// element it reads before reading it, so no clearing is needed and the
+// previous call's leftovers never leak into a result.
+//
+// In host code `g_smooth2_scratch` names a host-side stand-in, not a device
+// address: the device address is fetched once per device with
+// cudaGetSymbolAddress, on the first call made with that device current.
+// That first call must therefore come before any stream capture begins.
+#include <cuda_runtime.h>
+
+#include <mutex>
+#include <string>
+
+#include "em2g_internal.cuh"
+
+static __device__ __align__(256) double g_smooth2_scratch[EM2G_SMOOTH2_STATIC_MAX_POINTS];
+
+namespace {
+
+constexpr int kMaxDevices = 64;
+std::mutex g_setup_mutex;
+double *g_scratch_addr[kMaxDevices] = {nullptr};
+
+constexpr int TX = 32, TY = 8;
+
+// store v at (ix,iy) and at the guard cells that copy it
+// (columns 0/nx+2 from nx/2, rows 0/ny+2 from ny/2; pic/smooth.f90:148-155)
+__device__ __forceinline__ void put(double *a, int nx, int ny, int64_t nxg, int ix, int iy,
+                                    double v) {
+  a[(int64_t)iy * nxg + ix] = v;
+  const int mx = (ix == nx) ? 0 : ((ix == 2) ? nx + 2 : -1);
+  const int my = (iy == ny) ? 0 : ((iy == 2) ? ny + 2 : -1);
+  if (mx >= 0) a[(int64_t)iy * nxg + mx] = v;
+  if (my >= 0) a[(int64_t)my * nxg + ix] = v;
+  if (mx >= 0 && my >= 0) a[(int64_t)my * nxg + mx] = v;
+}
+
+// 9-point binomial pass, sm -> scratch (pic/smooth.f90:143-146)
+__global__ void k_binomial_static(int nx, int ny, const double *__restrict__ s, double *d) {
+  const int ix = 1 + blockIdx.x * TX + threadIdx.x;
+  const int iy = 1 + blockIdx.y * TY + threadIdx.y;
+  if (ix > nx + 1 || iy > ny + 1) return;
+  const int64_t n = nx + 3, c = (int64_t)iy * n + ix;
+  const double v = (4 * s[c] + 2 * (s[c - 1] + s[c + 1] + s[c - n] + s[c + n]) +
+                    s[c - 1 - n] + s[c - 1 + n] + s[c + 1 - n] + s[c + 1 + n]) /
+                   16.0;
+  put(d, nx, ny, n, ix, iy, v);
+}
+
+// compensation pass, scratch -> sm (pic/smooth.f90:163-166)
+__global__ void k_compensate_static(int nx, int ny, const double *__restrict__ d, double *s) {
+  const int ix = 1 + blockIdx.x * TX + threadIdx.x;
+  const int iy = 1 + blockIdx.y * TY + threadIdx.y;
+  if (ix > nx + 1 || iy > ny + 1) return;
+  const int64_t n = nx + 3, c = (int64_t)iy * n + ix;
+  const double v = (20 * d[c] - d[c - 1] - d[c + 1] - d[c - n] - d[c + n] - d[c - 1 - n] -
+                    d[c - 1 + n] - d[c + 1 - n] - d[c + 1 + n]) /
+                   12.0;
+  put(s, nx, ny, n, ix, iy, v);
+}
+
+}  // namespace
+
+extern "C" int em2g_smooth2_static(int nx, int ny, double *dev_array, void *cuda_stream) {
+  using em2g::fail;
+  if (nx < 4 || ny < 4) return fail(EM2G_ERR_INVALID, "smooth2_static: nx and ny must be >= 4");
+  if (!dev_array) return fail(EM2G_ERR_INVALID, "smooth2_static: null array");
+  const int64_t points = (int64_t)(nx + 3) * (ny + 3);
+  if (points > EM2G_SMOOTH2_STATIC_MAX_POINTS)
+    return fail(EM2G_ERR_RANGE,
+                "smooth2_static: (nx+3)*(ny+3) = " + std::to_string(points) +
+                    " exceeds the static scratch of " +
+                    std::to_string((long long)EM2G_SMOOTH2_STATIC_MAX_POINTS) +
+                    " points; use an em2g context and em2g_smooth2");
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return em2g::cuda_fail(e, "cudaGetDevice");
+  if (dev < 0 || dev >= kMaxDevices) return fail(EM2G_ERR_INVALID, "smooth2_static: device ordinal");
+  double *scratch = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_setup_mutex);
+    if (!g_scratch_addr[dev]) {
+      void *p = nullptr;
+      e = cudaGetSymbolAddress(&p, g_smooth2_scratch);
+      if (e != cudaSuccess) return em2g::cuda_fail(e, "cudaGetSymbolAddress(g_smooth2_scratch)");
+      g_scratch_addr[dev] = static_cast<double *>(p);
+    }
+    scratch = g_scratch_addr[dev];
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
+  const dim3 blk(TX, TY), grd((nx + 1 + TX - 1) / TX, (ny + 1 + TY - 1) / TY);
+  k_binomial_static<<<grd, blk, 0, st>>>(nx, ny, dev_array, scratch);
+  k_compensate_static<<<grd, blk, 0, st>>>(nx, ny, scratch, dev_array);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return em2g::cuda_fail(e, "smooth2_static launch");
+  return EM2G_OK;
+}
