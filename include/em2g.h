@@ -86,7 +86,7 @@ typedef struct em2g_params {
   double cg_eps;         /* 1e-9 in cgm (pic/fields.f90:519) */
   double qme, wpe;       /* -1, 1 (pic/input.f90:43) */
   int32_t device;        /* CUDA device ordinal */
-  int32_t sort_interval; /* steps between particle sorts on the fast path; 0 = never */
+  int32_t sort_interval; /* reserved, set 0 (the fast path re-sorts every step) */
   int32_t reserved[16];
 } em2g_params;
 
@@ -151,15 +151,18 @@ int em2g_curnt(em2g_ctx *ctx);
 int em2g_fields(em2g_ctx *ctx, int it, double *energies_out, int *cg_iters_out);
 /* smooth2 (pic/smooth.f90:95-179) in place on one resident field array */
 int em2g_smooth2(em2g_ctx *ctx, int field_id);
-/* move followed by curnt in one fused particle kernel per species: the same
- * result as em2g_move then em2g_curnt.  A shim can map em2's `call move`
- * to nothing and `call curnt` to this (nothing reads v between the two,
- * pic/main.f90:287-288). */
+/* move followed by curnt in one fused particle kernel per species, on the
+ * cell-sorted fast path: the particles, rho and jm+jp are those of
+ * em2g_move then em2g_curnt, but the current is kept as the sum jm+jp in
+ * the jxm/jym/jzm arrays with jxp/jyp/jzp zero (fields reads only the sum,
+ * pic/fields.f90:211-214).  A shim can map em2's `call move` to nothing and
+ * `call curnt` to this (nothing reads v between them, pic/main.f90:287-288). */
 int em2g_move_curnt(em2g_ctx *ctx, double *ake_out);
 
 /* ---- fused fast path -------------------------------------------------
  * nsteps iterations of { move; curnt; it = it + 1; fields(it) } with the
- * particle work of move and curnt in one fused kernel per species.  The
+ * particle work of move and curnt in one fused kernel per species
+ * (as em2g_move_curnt; particles are kept grouped by cell internally).  The
  * outputs refer to the last iteration (energies_out written only when the
  * last `it` is a multiple of isav). */
 int em2g_step(em2g_ctx *ctx, int nsteps, double *ake_out, double *energies_out,

@@ -226,6 +226,18 @@ int em2g_create(const em2g_params *p, em2g_ctx **out) {
   if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMemset"));
   rc = cg_init(c);
   if (rc) return bail(rc);
+  rc = sort_init(c);
+  if (rc) return bail(rc);
+  {
+    // the fast push writes one ake partial per block of 64 cells
+    const int64_t fast_blocks = (c->ncell * 4 + 255) / 256;
+    if (fast_blocks > c->red_blocks) {
+      cudaFree(c->red);
+      c->red_blocks = (int)fast_blocks;
+      e = cudaMalloc((void **)&c->red, sizeof(double) * c->red_blocks);
+      if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc red"));
+    }
+  }
   e = cudaMemset(c->cg.status, 0, sizeof(int) * 2);
   if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMemset"));
   e = cudaDeviceSynchronize();
@@ -251,6 +263,7 @@ int em2g_destroy(em2g_ctx *c) {
   cudaFree(c->dev_out);
   if (c->host_out) cudaFreeHost(c->host_out);
   cg_free(c);
+  sort_free(c);
   for (cudaEvent_t e : c->ev) cudaEventDestroy(e);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
@@ -370,6 +383,7 @@ int em2g_set_particles(em2g_ctx *c, int isp, int64_t n, const double *x, const d
     EM2G_CUDA(cudaGetLastError());
   }
   S.n = n;
+  S.sorted = false;
   EM2G_CUDA(cudaStreamSynchronize(c->stream));
   return EM2G_OK;
 }
@@ -410,6 +424,7 @@ int em2g_set_particles_device(em2g_ctx *c, int isp, int64_t n, const double *x,
     return fail(EM2G_ERR_RANGE, std::to_string(hb[0]) + " particles outside the grid");
   }
   S.n = n;
+  S.sorted = false;
   return EM2G_OK;
 }
 
@@ -459,13 +474,21 @@ int em2g_move(em2g_ctx *c, double *ake_out) {
   return finish_outputs(c, ake_out, nullptr, nullptr, false);
 }
 
+// one fused move + curnt of every species on the cell-sorted fast path
+static int fast_push_all(em2g_ctx *c) {
+  int rc;
+  for (int s = 0; s < c->P.nsp; ++s) {
+    if (!c->sp[s].sorted && (rc = sort_full(c, s))) return rc;
+    if ((rc = launch_prescale(c, s))) return rc;
+    if ((rc = launch_push_cells_f64(c, s))) return rc;
+  }
+  return EM2G_OK;
+}
+
 int em2g_move_curnt(em2g_ctx *c, double *ake_out) {
   int rc = check_ctx(c);
   if (rc) return rc;
-  for (int s = 0; s < c->P.nsp; ++s) {
-    if ((rc = launch_prescale(c, s))) return rc;
-    if ((rc = launch_push_f64(c, s, 3))) return rc;
-  }
+  if ((rc = fast_push_all(c))) return rc;
   return finish_outputs(c, ake_out, nullptr, nullptr, false);
 }
 
@@ -498,8 +521,10 @@ int em2g_reset_counters(em2g_ctx *c) {
 int em2g_curnt(em2g_ctx *c) {
   int rc = check_ctx(c);
   if (rc) return rc;
-  for (int s = 0; s < c->P.nsp; ++s)
+  for (int s = 0; s < c->P.nsp; ++s) {
     if ((rc = launch_push_f64(c, s, 2))) return rc;
+    c->sp[s].sorted = false;  // positions moved outside the fast path's bookkeeping
+  }
   EM2G_CUDA(cudaStreamSynchronize(c->stream));
   EM2G_CUDA(cudaGetLastError());
   return EM2G_OK;
@@ -530,10 +555,7 @@ int em2g_step(em2g_ctx *c, int nsteps, double *ake_out, double *energies_out,
   if (nsteps < 0) return fail(EM2G_ERR_INVALID, "nsteps < 0");
   EM2G_CUDA(cudaMemsetAsync(c->cg.status, 0, sizeof(int) * 2, c->stream));
   for (int k = 0; k < nsteps; ++k) {
-    for (int s = 0; s < c->P.nsp; ++s) {
-      if ((rc = launch_prescale(c, s))) return rc;
-      if ((rc = launch_push_f64(c, s, 3))) return rc;
-    }
+    if ((rc = fast_push_all(c))) return rc;
     c->it += 1;
     if ((rc = fields_f64(c, c->it, true, nullptr))) return rc;
   }

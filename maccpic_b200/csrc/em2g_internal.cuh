@@ -39,6 +39,15 @@ struct Species {
   int32_t *slot = nullptr;     // cap
   double *part_alt = nullptr;  // 6*cap, sort target
   int32_t *slot_alt = nullptr;
+  // Cell-sorted order of the fast path (push_fast_f64.cu, sort.cu): `part`
+  // holds the particles grouped by cell (row-major key iy*nx+ix), cell k's
+  // particles at [off[k], off[k+1]); cnt[k] counts the particles whose
+  // current position lies in cell k.  `sorted` is false until a full sort
+  // ran after the last change of positions outside the fast path.
+  int32_t *off = nullptr, *off_alt = nullptr;  // ncell+1 each
+  int32_t *cnt = nullptr, *cnt_alt = nullptr;  // ncell each
+  int32_t *cursor = nullptr;                   // ncell
+  bool sorted = false;
 };
 
 // Device workspace of the Poisson/cgm solve (pic/fields.f90:370-651).
@@ -75,6 +84,8 @@ struct em2g_ctx {
   // counters (em2g_get_counters): kernel launches, and when timing is on,
   // CUDA-event time of the particle-push launches
   int64_t launches = 0;
+  int32_t *scan_tmp = nullptr;  // block sums of the cell scans
+  int64_t ncell = 0;
   int timing = 0;
   std::vector<cudaEvent_t> ev;  // start/stop pairs of the pending push launches
   size_t ev_used = 0;
@@ -92,6 +103,13 @@ int launch_ake_finish(em2g_ctx *c, int isp, int nblocks_used);
 int fields_f64(em2g_ctx *c, int it, bool want_energies, int *cg_iters);
 int smooth2_f64(em2g_ctx *c, double *a);
 int cg_init(em2g_ctx *c);
+// cell sort of the fast path (sort.cu)
+int sort_init(em2g_ctx *c);
+void sort_free(em2g_ctx *c);
+int sort_full(em2g_ctx *c, int isp);
+int scan_cells(em2g_ctx *c, const int32_t *cnt, int32_t *off);
+// one fast-path push of species isp (push_fast_f64.cu)
+int launch_push_cells_f64(em2g_ctx *c, int isp);
 // bracket one push launch with events when timing is on (api.cu)
 int timing_begin(em2g_ctx *c);
 int timing_end(em2g_ctx *c);

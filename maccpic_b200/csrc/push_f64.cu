@@ -6,10 +6,12 @@
 // those of em2 (pic/move.f90, pic/curnt.f90).  Only the order in which the
 // contributions of different particles are summed into rho/J (atomics) and
 // into ake differs from the reference's serial loop.
-#include "em2g_internal.cuh"
+#include "push_common.cuh"
 
 namespace em2g {
 namespace {
+
+using namespace f64;
 
 constexpr int kThreads = 256;
 
@@ -23,94 +25,6 @@ struct PushArgs {
   double *ake_partial;
 };
 
-__device__ __forceinline__ double sq(double t) { return t * t; }
-
-// 9-point quadratic-spline weights of one staggering, in the reference's
-// naming: s2x/s2xp/s2xm along x, s2y/s2yp/s2ym along y.
-struct W9 {
-  double q, qxp, qxm, qyp, qxpyp, qxmyp, qym, qxpym, qxmym;
-};
-
-__device__ __forceinline__ W9 weights(double s2x, double s2xp, double s2xm, double s2y,
-                                      double s2yp, double s2ym) {
-  W9 w;
-  w.q = s2x * s2y;
-  w.qxp = s2xp * s2y;
-  w.qxm = s2xm * s2y;
-  w.qyp = s2x * s2yp;
-  w.qxpyp = s2xp * s2yp;
-  w.qxmyp = s2xm * s2yp;
-  w.qym = s2x * s2ym;
-  w.qxpym = s2xp * s2ym;
-  w.qxmym = s2xm * s2ym;
-  return w;
-}
-
-// pic/move.f90:95-97: sum in the reference's order
-// (ix,iy) (ix,iyp) (ix,iym) (ixp,iy) (ixp,iyp) (ixp,iym) (ixm,iy) (ixm,iyp) (ixm,iym)
-__device__ __forceinline__ double gather9(const double *__restrict__ A, int nxg, int ix,
-                                          int iy, const W9 &w) {
-  const double *r0 = A + (int64_t)iy * nxg;
-  const double *rp = r0 + nxg;
-  const double *rm = r0 - nxg;
-  return __ldg(r0 + ix) * w.q + __ldg(rp + ix) * w.qyp + __ldg(rm + ix) * w.qym +
-         __ldg(r0 + ix + 1) * w.qxp + __ldg(rp + ix + 1) * w.qxpyp +
-         __ldg(rm + ix + 1) * w.qxpym + __ldg(r0 + ix - 1) * w.qxm +
-         __ldg(rp + ix - 1) * w.qxmyp + __ldg(rm + ix - 1) * w.qxmym;
-}
-
-// pic/curnt.f90:72-80: A(i,j) += (s2x*s2y*qd) * v, nine points
-__device__ __forceinline__ void scatter9(double *A, int nxg, int ix, int iy, double s2x,
-                                         double s2xp, double s2xm, double s2y, double s2yp,
-                                         double s2ym, double qd, double v) {
-  double *r0 = A + (int64_t)iy * nxg;
-  double *rp = r0 + nxg;
-  double *rm = r0 - nxg;
-  atomicAdd(r0 + ix, s2x * s2y * qd * v);
-  atomicAdd(r0 + ix + 1, s2xp * s2y * qd * v);
-  atomicAdd(r0 + ix - 1, s2xm * s2y * qd * v);
-  atomicAdd(rp + ix, s2x * s2yp * qd * v);
-  atomicAdd(rp + ix + 1, s2xp * s2yp * qd * v);
-  atomicAdd(rp + ix - 1, s2xm * s2yp * qd * v);
-  atomicAdd(rm + ix, s2x * s2ym * qd * v);
-  atomicAdd(rm + ix + 1, s2xp * s2ym * qd * v);
-  atomicAdd(rm + ix - 1, s2xm * s2ym * qd * v);
-}
-
-// rho (pic/curnt.f90:208-225): same pattern without the velocity factor
-__device__ __forceinline__ void scatter9_rho(double *A, int nxg, int ix, int iy, double s2x,
-                                             double s2xp, double s2xm, double s2y,
-                                             double s2yp, double s2ym, double qd) {
-  double *r0 = A + (int64_t)iy * nxg;
-  double *rp = r0 + nxg;
-  double *rm = r0 - nxg;
-  atomicAdd(r0 + ix, s2x * s2y * qd);
-  atomicAdd(r0 + ix + 1, s2xp * s2y * qd);
-  atomicAdd(r0 + ix - 1, s2xm * s2y * qd);
-  atomicAdd(rp + ix, s2x * s2yp * qd);
-  atomicAdd(rp + ix + 1, s2xp * s2yp * qd);
-  atomicAdd(rp + ix - 1, s2xm * s2yp * qd);
-  atomicAdd(rm + ix, s2x * s2ym * qd);
-  atomicAdd(rm + ix + 1, s2xp * s2ym * qd);
-  atomicAdd(rm + ix - 1, s2xm * s2ym * qd);
-}
-
-// Quadratic weights of the two staggerings along one axis.
-// "half" (cell-centred node, index int(x+1)): pic/move.f90:76-81
-__device__ __forceinline__ void w_half(double x, int &i, double &s, double &sp, double &sm) {
-  i = (int)(x + 1.0);
-  s = 0.75 - sq(x + 0.5 - i);
-  sp = 0.5 * sq(1.0 + x - i);
-  sm = 0.5 * sq(-x + i);
-}
-// "node" (integer node, index int(x+1.5)): pic/move.f90:127-132
-__device__ __forceinline__ void w_node(double x, int &i, double &s, double &sp, double &sm) {
-  i = (int)(x + 1.5);
-  s = 0.75 - sq(x + 1.0 - i);
-  sp = 0.5 * sq(1.5 + x - i);
-  sm = 0.5 * sq(-0.5 - x + i);
-}
-
 template <int MODE>
 __global__ void __launch_bounds__(kThreads) k_push_f64(PushArgs a) {
   const int64_t j = (int64_t)blockIdx.x * kThreads + threadIdx.x;
@@ -122,91 +36,27 @@ __global__ void __launch_bounds__(kThreads) k_push_f64(PushArgs a) {
     double vxj = vx[j], vyj = vy[j], vzj = vz[j];
     const int nxg = a.nxg;
     if (MODE & 1) {
-      const double gj = gm[j];
-      const double *aex = a.s, *aey = a.s + a.w, *aez = a.s + 2 * a.w, *abx = a.s + 3 * a.w,
-                   *aby = a.s + 4 * a.w, *abz = a.s + 5 * a.w;
-      int ixh, ixn, iyh, iyn;
-      double sxh, sxhp, sxhm, sxn, sxnp, sxnm, syh, syhp, syhm, syn, synp, synm;
-      w_half(xj, ixh, sxh, sxhp, sxhm);
-      w_node(yj, iyn, syn, synp, synm);
-      // Ex, Bx: x half, y node (pic/move.f90:76-100)
-      W9 w = weights(sxh, sxhp, sxhm, syn, synp, synm);
-      const double aexpt = gather9(aex, nxg, ixh, iyn, w);
-      double abxpt = gather9(abx, nxg, ixh, iyn, w);
-      // Ez, Bz: half, half (pic/move.f90:103-124)
-      w_half(yj, iyh, syh, syhp, syhm);
-      w = weights(sxh, sxhp, sxhm, syh, syhp, syhm);
-      const double aezpt = gather9(aez, nxg, ixh, iyh, w);
-      double abzpt = gather9(abz, nxg, ixh, iyh, w);
-      // Ey, By: node, half (pic/move.f90:127-148)
-      w_node(xj, ixn, sxn, sxnp, sxnm);
-      w = weights(sxn, sxnp, sxnm, syh, syhp, syhm);
-      const double aeypt = gather9(aey, nxg, ixn, iyh, w);
-      double abypt = gather9(aby, nxg, ixn, iyh, w);
-      // relativistic Boris (pic/move.f90:176-203)
-      double gvxs = vxj * gj + aexpt;
-      double gvys = vyj * gj + aeypt;
-      double gvzs = vzj * gj + aezpt;
-      double g = sqrt(1.0 + gvxs * gvxs + gvys * gvys + gvzs * gvzs);
-      akel = g - 1.0;
-      const double dcg = 1.0 / (a.c * g);
-      abxpt = dcg * abxpt;
-      abypt = dcg * abypt;
-      abzpt = dcg * abzpt;
-      const double vvx = gvxs + gvys * abzpt - gvzs * abypt;
-      const double vvy = gvys + gvzs * abxpt - gvxs * abzpt;
-      const double vvz = gvzs + gvxs * abypt - gvys * abxpt;
-      const double f = 2.0 / (1.0 + abxpt * abxpt + abypt * abypt + abzpt * abzpt);
-      abxpt = f * abxpt;
-      abypt = f * abypt;
-      abzpt = f * abzpt;
-      gvxs = gvxs + vvy * abzpt - vvz * abypt + aexpt;
-      gvys = gvys + vvz * abxpt - vvx * abzpt + aeypt;
-      gvzs = gvzs + vvx * abypt - vvy * abxpt + aezpt;
-      g = sqrt(1.0 + gvxs * gvxs + gvys * gvys + gvzs * gvzs);
-      vxj = gvxs / g;
-      vyj = gvys / g;
-      vzj = gvzs / g;
-      gm[j] = g;
+      const Scaled S{a.s, a.s + a.w, a.s + 2 * a.w, a.s + 3 * a.w, a.s + 4 * a.w,
+                     a.s + 5 * a.w};
+      double gj = gm[j];
+      akel = gather_boris(S, nxg, a.c, xj, yj, vxj, vyj, vzj, gj) - 1.0;
+      gm[j] = gj;
       vx[j] = vxj;
       vy[j] = vyj;
       vz[j] = vzj;
     }
     if (MODE & 2) {
-      double *rho = a.fld + EM2G_RHO * a.w, *jxm = a.fld + EM2G_JXM * a.w,
-             *jxp = a.fld + EM2G_JXP * a.w, *jym = a.fld + EM2G_JYM * a.w,
-             *jyp = a.fld + EM2G_JYP * a.w, *jzm = a.fld + EM2G_JZM * a.w,
-             *jzp = a.fld + EM2G_JZP * a.w;
-      const double qd = a.qd;
-      int ixh, ixn, iyh, iyn;
-      double sxh, sxhp, sxhm, sxn, sxnp, sxnm, syh, syhp, syhm, syn, synp, synm;
-      // jm at the old position (pic/curnt.f90:53-132)
-      w_half(xj, ixh, sxh, sxhp, sxhm);
-      w_node(yj, iyn, syn, synp, synm);
-      scatter9(jxm, nxg, ixh, iyn, sxh, sxhp, sxhm, syn, synp, synm, qd, vxj);
-      w_half(yj, iyh, syh, syhp, syhm);
-      scatter9(jzm, nxg, ixh, iyh, sxh, sxhp, sxhm, syh, syhp, syhm, qd, vzj);
-      w_node(xj, ixn, sxn, sxnp, sxnm);
-      scatter9(jym, nxg, ixn, iyh, sxn, sxnp, sxnm, syh, syhp, syhm, qd, vyj);
-      // move and wrap (pic/curnt.f90:181-194)
-      xj = xj + vxj * a.dt / a.dx;
-      yj = yj + vyj * a.dt / a.dy;
-      if (xj < 0.0) xj = xj + a.xn;
-      if (xj >= a.xn) xj = xj - a.xn;
-      if (yj < 0.0) yj = yj + a.yn;
-      if (yj >= a.yn) yj = yj - a.yn;
+      double *rho = a.fld + EM2G_RHO * a.w;
+      // jm at the old position, move and wrap, rho and jp at the new one
+      // (pic/curnt.f90:53-303)
+      deposit_j_atomic(a.fld + EM2G_JXM * a.w, a.fld + EM2G_JYM * a.w, a.fld + EM2G_JZM * a.w,
+                       nxg, xj, yj, a.qd, vxj, vyj, vzj);
+      move_wrap(xj, yj, vxj, vyj, a.dt, a.dx, a.dy, a.xn, a.yn);
       x[j] = xj;
       y[j] = yj;
-      // rho at the new position (pic/curnt.f90:197-225)
-      w_node(xj, ixn, sxn, sxnp, sxnm);
-      w_node(yj, iyn, syn, synp, synm);
-      scatter9_rho(rho, nxg, ixn, iyn, sxn, sxnp, sxnm, syn, synp, synm, qd);
-      // jp at the new position (pic/curnt.f90:227-303)
-      w_half(xj, ixh, sxh, sxhp, sxhm);
-      scatter9(jxp, nxg, ixh, iyn, sxh, sxhp, sxhm, syn, synp, synm, qd, vxj);
-      w_half(yj, iyh, syh, syhp, syhm);
-      scatter9(jzp, nxg, ixh, iyh, sxh, sxhp, sxhm, syh, syhp, syhm, qd, vzj);
-      scatter9(jyp, nxg, ixn, iyh, sxn, sxnp, sxnm, syh, syhp, syhm, qd, vyj);
+      deposit_rho_atomic(rho, nxg, xj, yj, a.qd);
+      deposit_j_atomic(a.fld + EM2G_JXP * a.w, a.fld + EM2G_JYP * a.w, a.fld + EM2G_JZP * a.w,
+                       nxg, xj, yj, a.qd, vxj, vyj, vzj);
     }
   }
   if (MODE & 1) {
@@ -297,12 +147,15 @@ int launch_push_f64(em2g_ctx *c, int isp, int mode) {
   c->launches += 1;
   EM2G_CUDA(cudaGetLastError());
   if ((rc = timing_end(c))) return rc;
-  if (mode & 1) {
-    k_ake_finish<<<1, 256, 0, c->stream>>>(c->red, nb, c->P.am[isp], c->P.dn[isp],
-                                           c->dev_out + isp);
-    c->launches += 1;
-    EM2G_CUDA(cudaGetLastError());
-  }
+  if (mode & 1) return launch_ake_finish(c, isp, nb);
+  return EM2G_OK;
+}
+
+int launch_ake_finish(em2g_ctx *c, int isp, int nblocks_used) {
+  k_ake_finish<<<1, 1024, 0, c->stream>>>(c->red, nblocks_used, c->P.am[isp], c->P.dn[isp],
+                                          c->dev_out + isp);
+  c->launches += 1;
+  EM2G_CUDA(cudaGetLastError());
   return EM2G_OK;
 }
 
