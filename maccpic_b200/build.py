@@ -25,7 +25,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
           "-I", os.path.join(ROOT, "include"), "--expt-relaxed-constexpr"]
-NO_FMA = {"push_f64.cu", "fields_f64.cu", "smooth2_static.cu"}
+NO_FMA = {"push_f64.cu", "push_fast_f64.cu", "fields_f64.cu", "smooth2_static.cu"}
 
 
 def _headers():
