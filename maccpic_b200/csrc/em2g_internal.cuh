@@ -48,11 +48,15 @@ struct Species {
   int32_t *cnt = nullptr, *cnt_alt = nullptr;  // ncell each
   int32_t *cursor = nullptr;                   // ncell
   bool sorted = false;
+  // FP32 contexts: xr, yr (offsets in the cell of the particle's range),
+  // ux, uy, uz; 5*cap floats, always grouped by cell (push_fast_f32.cu)
+  float *p32 = nullptr, *p32_alt = nullptr;
 };
 
 // Device workspace of the Poisson/cgm solve (pic/fields.f90:370-651).
 struct CgWork {
-  double *u = nullptr, *r = nullptr, *p = nullptr, *ap = nullptr;  // nx*ny each
+  void *u = nullptr;           // u, r, p, Ap: 4 arrays of nx*ny elements
+  int elem = 0;                // element size (8 FP64, 4 FP32)
   double *partial = nullptr;   // 2 * max_blocks
   unsigned *bar = nullptr;     // barrier counter + generation
   int *status = nullptr;       // [0] timeout flag, [1] iterations
@@ -73,6 +77,8 @@ struct em2g_ctx {
   // per-species copies of E and B scaled by (q/m)dt/2 (pic/move.f90:52-64)
   double *scaled = nullptr;  // nsp * 6 * w
   double *smooth_tmp = nullptr;  // w, the `dummy` array of smooth2
+  // FP32 contexts use these instead of fld / scaled / smooth_tmp
+  float *fld32 = nullptr, *scaled32 = nullptr, *smooth_tmp32 = nullptr;
   em2g::Species sp[EM2G_MAX_SPECIES];
   em2g::CgWork cg;
   // reductions: ake partials per species, energy partials
@@ -110,6 +116,14 @@ int sort_full(em2g_ctx *c, int isp);
 int scan_cells(em2g_ctx *c, const int32_t *cnt, int32_t *off);
 // one fast-path push of species isp (push_fast_f64.cu)
 int launch_push_cells_f64(em2g_ctx *c, int isp);
+// mixed-precision path (push_fast_f32.cu, fields_f32.cu)
+int launch_prescale_f32(em2g_ctx *c, int isp);
+int launch_push_cells_f32(em2g_ctx *c, int isp);
+int upload_f32(em2g_ctx *c, int isp, const double *staging, int64_t n);
+int download_f32(em2g_ctx *c, int isp, double *staging);
+int smooth2_f32(em2g_ctx *c, float *a);
+int cg_init_f32(em2g_ctx *c);
+int fields_f32(em2g_ctx *c, int it, bool want_energies);
 // bracket one push launch with events when timing is on (api.cu)
 int timing_begin(em2g_ctx *c);
 int timing_end(em2g_ctx *c);

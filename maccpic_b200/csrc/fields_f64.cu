@@ -1,386 +1,18 @@
-// fields_f64.cu -- grid kernels of the FP64 drop-in path: the guard fold,
-// the Yee leapfrog, smooth2, the Poisson correction with its conjugate-
-// gradient solve, and the field energies (pic/fields.f90, pic/smooth.f90).
-//
-// Compiled with -fmad=false: each cell's arithmetic is rounded as em2's is,
-// so the stencil kernels are bitwise those of the reference; the CG's dot
-// products and the energies are FP64 tree sums (deterministic for a given
-// grid, but summed in another order than em2's serial loops).
-//
-// Every stencil sweep of the reference ends with guard copies, columns 0 and
-// nx+2 from nx and 2, then rows 0 and ny+2 from ny and 2
-// (pic/fields.f90:192-200).  Here the thread that computes a cell also
-// stores it into the guard positions that copy it, so no second pass is
-// needed and the values are the same.
-#include "em2g_internal.cuh"
+// fields_f64.cu -- the grid half of the FP64 drop-in path: fold, Yee,
+// smooth2, Poisson/CG and energies (pic/fields.f90, pic/smooth.f90) on the
+// FP64 field block.  Compiled with -fmad=false: every stencil cell is
+// rounded as em2 rounds it, so these sweeps are bitwise em2's for equal
+// inputs; the CG dot products and the energies are FP64 tree sums
+// (deterministic for a given grid, summed in another order than em2's loops).
+#include "fields_impl.cuh"
 
 namespace em2g {
-namespace {
-
-constexpr int TX = 32, TY = 8;
-
-struct G {
-  int nx, ny, nxg;
-  int64_t w;
-};
-
-__device__ __forceinline__ int64_t at(const G &g, int ix, int iy) {
-  return (int64_t)iy * g.nxg + ix;
-}
-
-// store v at (ix,iy), 1<=ix<=nx+1, 1<=iy<=ny+1, and at its guard copies
-__device__ __forceinline__ void store_with_guards(const G &g, double *a, int ix, int iy,
-                                                  double v) {
-  a[at(g, ix, iy)] = v;
-  const int mx = (ix == g.nx) ? 0 : ((ix == 2) ? g.nx + 2 : -1);
-  const int my = (iy == g.ny) ? 0 : ((iy == 2) ? g.ny + 2 : -1);
-  if (mx >= 0) a[at(g, mx, iy)] = v;
-  if (my >= 0) a[at(g, ix, my)] = v;
-  if (mx >= 0 && my >= 0) a[at(g, mx, my)] = v;
-}
-
-// ---- guard fold of rho and the 6 current arrays (pic/fields.f90:44-137)
-// x pass: one thread per (row iy in 0..ny+2, array)
-__global__ void k_fold_x(G g, double *fld) {
-  const int iy = blockIdx.x * blockDim.x + threadIdx.x;
-  const int k = blockIdx.y;  // 0..6 -> rho..jzp
-  if (iy > g.ny + 2) return;
-  double *a = fld + (EM2G_RHO + k) * g.w + (int64_t)iy * g.nxg;
-  const int nx = g.nx;
-  a[1] = a[1] + a[nx + 1];
-  a[2] = a[2] + a[nx + 2];
-  a[nx] = a[nx] + a[0];
-  a[nx + 1] = a[1];
-  a[nx + 2] = a[2];
-  a[0] = a[nx];
-}
-// y pass: one thread per (column ix in 0..nx+2, array)
-__global__ void k_fold_y(G g, double *fld) {
-  const int ix = blockIdx.x * blockDim.x + threadIdx.x;
-  const int k = blockIdx.y;
-  if (ix > g.nx + 2) return;
-  double *a = fld + (EM2G_RHO + k) * g.w + ix;
-  const int64_t s = g.nxg;
-  const int ny = g.ny;
-  a[1 * s] = a[1 * s] + a[(ny + 1) * s];
-  a[2 * s] = a[2 * s] + a[(ny + 2) * s];
-  a[ny * s] = a[ny * s] + a[0];
-  a[(ny + 1) * s] = a[1 * s];
-  a[(ny + 2) * s] = a[2 * s];
-  a[0] = a[ny * s];
-}
-
-// ---- Yee half step of B (pic/fields.f90:184-200, :231-247)
-__global__ void k_b_half(G g, double *fld, double ctxh, double ctyh) {
-  const int ix = 1 + blockIdx.x * TX + threadIdx.x;
-  const int iy = 1 + blockIdx.y * TY + threadIdx.y;
-  if (ix > g.nx + 1 || iy > g.ny + 1) return;
-  const double *ex = fld + EM2G_EX * g.w, *ey = fld + EM2G_EY * g.w, *ez = fld + EM2G_EZ * g.w;
-  double *bx = fld + EM2G_BX * g.w, *by = fld + EM2G_BY * g.w, *bz = fld + EM2G_BZ * g.w;
-  const int64_t c = at(g, ix, iy);
-  const double ezc = ez[c];
-  const double vbx = bx[c] - ctyh * (ezc - ez[c - g.nxg]);
-  const double vby = by[c] + ctxh * (ezc - ez[c - 1]);
-  const double vbz = bz[c] - ctxh * (ey[c + 1] - ey[c]) + ctyh * (ex[c + g.nxg] - ex[c]);
-  store_with_guards(g, bx, ix, iy, vbx);
-  store_with_guards(g, by, ix, iy, vby);
-  store_with_guards(g, bz, ix, iy, vbz);
-}
-
-// ---- Yee full step of E (pic/fields.f90:207-224)
-__global__ void k_e_full(G g, double *fld, double ctx, double cty, double tem) {
-  const int ix = 1 + blockIdx.x * TX + threadIdx.x;
-  const int iy = 1 + blockIdx.y * TY + threadIdx.y;
-  if (ix > g.nx + 1 || iy > g.ny + 1) return;
-  double *ex = fld + EM2G_EX * g.w, *ey = fld + EM2G_EY * g.w, *ez = fld + EM2G_EZ * g.w;
-  const double *bx = fld + EM2G_BX * g.w, *by = fld + EM2G_BY * g.w, *bz = fld + EM2G_BZ * g.w;
-  const double *jxm = fld + EM2G_JXM * g.w, *jxp = fld + EM2G_JXP * g.w,
-               *jym = fld + EM2G_JYM * g.w, *jyp = fld + EM2G_JYP * g.w,
-               *jzm = fld + EM2G_JZM * g.w, *jzp = fld + EM2G_JZP * g.w;
-  const int64_t c = at(g, ix, iy);
-  const double bzc = bz[c];
-  const double vex = ex[c] + cty * (bzc - bz[c - g.nxg]) - tem * (jxm[c] + jxp[c]);
-  const double vey = ey[c] - ctx * (bzc - bz[c - 1]) - tem * (jym[c] + jyp[c]);
-  const double vez = ez[c] + ctx * (by[c + 1] - by[c]) - cty * (bx[c + g.nxg] - bx[c]) -
-                     tem * (jzm[c] + jzp[c]);
-  store_with_guards(g, ex, ix, iy, vex);
-  store_with_guards(g, ey, ix, iy, vey);
-  store_with_guards(g, ez, ix, iy, vez);
-}
-
-// ---- smooth2 (pic/smooth.f90:143-177): binomial pass into `d`, then the
-// compensation pass back into `s`.
-__global__ void k_smooth_binomial(G g, const double *__restrict__ s, double *d) {
-  const int ix = 1 + blockIdx.x * TX + threadIdx.x;
-  const int iy = 1 + blockIdx.y * TY + threadIdx.y;
-  if (ix > g.nx + 1 || iy > g.ny + 1) return;
-  const int64_t c = at(g, ix, iy), n = g.nxg;
-  const double v = (4 * s[c] + 2 * (s[c - 1] + s[c + 1] + s[c - n] + s[c + n]) +
-                    s[c - 1 - n] + s[c - 1 + n] + s[c + 1 - n] + s[c + 1 + n]) /
-                   16.0;
-  store_with_guards(g, d, ix, iy, v);
-}
-__global__ void k_smooth_compensate(G g, const double *__restrict__ d, double *s) {
-  const int ix = 1 + blockIdx.x * TX + threadIdx.x;
-  const int iy = 1 + blockIdx.y * TY + threadIdx.y;
-  if (ix > g.nx + 1 || iy > g.ny + 1) return;
-  const int64_t c = at(g, ix, iy), n = g.nxg;
-  const double v = (20 * d[c] - d[c - 1] - d[c + 1] - d[c - n] - d[c + n] - d[c - 1 - n] -
-                    d[c - 1 + n] - d[c + 1 - n] - d[c + 1 + n]) /
-                   12.0;
-  store_with_guards(g, s, ix, iy, v);
-}
-
-// ---- Poisson right-hand side (pic/fields.f90:392-405): f = (div E - rho)
-// * dx * dx on the nx*ny periodic grid; written straight into r (u = 0, so
-// cgm's first residual r = f - L u is f) and p = r.
-__global__ void k_poisson_rhs(G g, const double *__restrict__ fld, double dx, double dy,
-                              double *r, double *p) {
-  const int ix = 1 + blockIdx.x * TX + threadIdx.x;
-  const int iy = 1 + blockIdx.y * TY + threadIdx.y;
-  if (ix > g.nx || iy > g.ny) return;
-  const double *ex = fld + EM2G_EX * g.w, *ey = fld + EM2G_EY * g.w, *rho = fld + EM2G_RHO * g.w;
-  const int ixm = (ix == 1) ? g.nx : ix - 1;
-  const double f = (ex[at(g, ix, iy)] - ex[at(g, ixm, iy)]) / dx +
-                   (ey[at(g, ix, iy)] - ey[at(g, ix, iy - 1)]) / dy - rho[at(g, ix, iy)];
-  const double fs = f * dx * dx;
-  const int64_t k = (int64_t)(iy - 1) * g.nx + (ix - 1);
-  r[k] = fs;
-  p[k] = fs;
-}
-
-// ---- E -= grad(phi) with periodic images and guards (pic/fields.f90:410-442)
-__device__ __forceinline__ void store_images(const G &g, double *a, int ix, int iy, double v) {
-  // (ix,iy) in 1..nx x 1..ny; its copies in 0..nx+2 x 0..ny+2
-  int xs[3], ys[3], nxs = 0, nys = 0;
-  xs[nxs++] = ix;
-  if (ix == 1) xs[nxs++] = g.nx + 1;
-  if (ix == g.nx) xs[nxs++] = 0;
-  if (ix == 2) xs[nxs++] = g.nx + 2;
-  ys[nys++] = iy;
-  if (iy == 1) ys[nys++] = g.ny + 1;
-  if (iy == g.ny) ys[nys++] = 0;
-  if (iy == 2) ys[nys++] = g.ny + 2;
-  for (int a1 = 0; a1 < nys; ++a1)
-    for (int a0 = 0; a0 < nxs; ++a0) a[at(g, xs[a0], ys[a1])] = v;
-}
-__global__ void k_poisson_correct(G g, double *fld, const double *__restrict__ u, double dx,
-                                  double dy) {
-  const int ix = 1 + blockIdx.x * TX + threadIdx.x;
-  const int iy = 1 + blockIdx.y * TY + threadIdx.y;
-  if (ix > g.nx || iy > g.ny) return;
-  double *ex = fld + EM2G_EX * g.w, *ey = fld + EM2G_EY * g.w;
-  const int64_t k = (int64_t)(iy - 1) * g.nx + (ix - 1);
-  const int64_t kxp = (int64_t)(iy - 1) * g.nx + (ix == g.nx ? 0 : ix);
-  const int64_t kyp = (int64_t)(iy == g.ny ? 0 : iy) * g.nx + (ix - 1);
-  const double uc = u[k];
-  const double vx = ex[at(g, ix, iy)] - (u[kxp] - uc) / dx;
-  const double vy = ey[at(g, ix, iy)] - (u[kyp] - uc) / dy;
-  store_images(g, ex, ix, iy, vx);
-  store_images(g, ey, ix, iy, vy);
-}
-
-// ---- conjugate gradient, one persistent launch (pic/fields.f90:508-651)
-//
-// All blocks are co-resident (cooperative launch).  Between phases they
-// meet at a software grid barrier whose wait is bounded: after kSpinLimit
-// polls a block records a timeout in status[0] and every block leaves.
-// Dot products: each block writes a partial; after the barrier every block
-// sums all partials in the same fixed order, so all blocks take the same
-// decisions on the same values.
-constexpr long kSpinLimit = 20000000;  // polls of ~100 ns: about 2 s
-
-__device__ bool grid_barrier(unsigned *bar, unsigned nblocks, int *status) {
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    volatile unsigned *gen = bar + 1;
-    const unsigned g0 = *gen;
-    __threadfence();
-    const unsigned arrived = atomicAdd(bar, 1u);
-    if (arrived == nblocks - 1) {
-      atomicExch(bar, 0u);
-      __threadfence();
-      atomicAdd(bar + 1, 1u);
-    } else {
-      long spins = 0;
-      while (*gen == g0) {
-        if (*(volatile int *)status != 0) break;
-        if (++spins > kSpinLimit) {
-          atomicExch(status, 1);
-          break;
-        }
-        __nanosleep(100);
-      }
-    }
-    __threadfence();
-  }
-  __syncthreads();
-  return *(volatile int *)status == 0;
-}
-
-// sum of nb partials in a fixed order; result valid in every thread
-__device__ double sum_partials(const double *partial, int nb, double *sh) {
-  if (threadIdx.x < 32) {
-    double v = 0.0;
-    for (int i = threadIdx.x; i < nb; i += 32) v += ((volatile const double *)partial)[i];
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    if (threadIdx.x == 0) sh[0] = v;
-  }
-  __syncthreads();
-  const double r = sh[0];
-  __syncthreads();
-  return r;
-}
-
-__device__ double block_sum(double v, double *sh) {
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
-  __syncthreads();
-  double r = 0.0;
-  if (threadIdx.x < 32) {
-    r = threadIdx.x < (int)(blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
-    for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
-  }
-  __syncthreads();
-  return r;  // valid in thread 0
-}
-
-struct CgArgs {
-  int nx, ny;
-  double *u, *r, *p, *ap;
-  double *partial;  // [2][gridDim.x]
-  unsigned *bar;
-  int *status;      // [0] timeout, [1] iterations
-  int maxits;
-  double eps;
-};
-
-__global__ void __launch_bounds__(256) k_cg(CgArgs a) {
-  __shared__ double sh[33];
-  const int64_t N = (int64_t)a.nx * a.ny;
-  const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  const unsigned nb = gridDim.x;
-  double *part0 = a.partial, *part1 = a.partial + nb;
-  // rr = sum r^2 for n = 1 (pic/fields.f90:546-556); u starts at 0
-  double loc = 0.0;
-  for (int64_t k = tid; k < N; k += stride) {
-    a.u[k] = 0.0;
-    loc += a.r[k] * a.r[k];
-  }
-  loc = block_sum(loc, sh);
-  if (threadIdx.x == 0) part0[blockIdx.x] = loc;
-  if (!grid_barrier(a.bar, nb, a.status)) return;
-  double rr = sum_partials(part0, nb, sh);
-  int n;
-  for (n = 1; n <= a.maxits; ++n) {
-    // ap = L p and pap = sum p*ap (pic/fields.f90:559-584)
-    loc = 0.0;
-    for (int64_t k = tid; k < N; k += stride) {
-      const int j = (int)(k % a.nx), l = (int)(k / a.nx);
-      const int64_t row = (int64_t)l * a.nx;
-      const int64_t kxp = row + (j == a.nx - 1 ? 0 : j + 1);
-      const int64_t kxm = row + (j == 0 ? a.nx - 1 : j - 1);
-      const int64_t kyp = (int64_t)(l == a.ny - 1 ? 0 : l + 1) * a.nx + j;
-      const int64_t kym = (int64_t)(l == 0 ? a.ny - 1 : l - 1) * a.nx + j;
-      // p was written by other threads before the barrier: read past L1
-      const double pc = __ldcg(a.p + k);
-      const double v = __ldcg(a.p + kxp) + __ldcg(a.p + kxm) + __ldcg(a.p + kyp) +
-                       __ldcg(a.p + kym) - 4.0 * pc;
-      a.ap[k] = v;
-      loc += pc * v;
-    }
-    loc = block_sum(loc, sh);
-    if (threadIdx.x == 0) part1[blockIdx.x] = loc;
-    if (!grid_barrier(a.bar, nb, a.status)) return;
-    const double pap = sum_partials(part1, nb, sh);
-    const double ak = rr / pap;
-    // u += ak p, r1 = r - ak ap, r_norm = sum r1^2 (pic/fields.f90:586-614)
-    loc = 0.0;
-    for (int64_t k = tid; k < N; k += stride) {
-      a.u[k] = a.u[k] + ak * a.p[k];
-      const double r1 = a.r[k] - ak * a.ap[k];
-      a.r[k] = r1;
-      loc += r1 * r1;
-    }
-    loc = block_sum(loc, sh);
-    if (threadIdx.x == 0) part0[blockIdx.x] = loc;
-    if (!grid_barrier(a.bar, nb, a.status)) return;
-    const double r_norm = sum_partials(part0, nb, sh);
-    if (r_norm / a.nx / a.ny < a.eps) break;  // pic/fields.f90:616
-    const double bk = r_norm / rr;            // pic/fields.f90:632
-    for (int64_t k = tid; k < N; k += stride) a.p[k] = a.r[k] + bk * a.p[k];
-    rr = r_norm;  // next pass's sum of r^2 over the same r, same order
-    if (!grid_barrier(a.bar, nb, a.status)) return;
-  }
-  if (blockIdx.x == 0 && threadIdx.x == 0) a.status[1] = n;
-}
-
-// ---- energies (pic/fields.f90:267-347): per-block partial sums of a^2 over
-// rows lo..hi, columns 1..nx of the six E/B arrays.
-__global__ void k_energy_partial(G g, const double *__restrict__ fld, int lo, int hi,
-                                 double *partial) {
-  __shared__ double sh[32];
-  const int k = blockIdx.y;  // field 0..5
-  const double *a = fld + k * g.w;
-  const int64_t ncols = g.nx, nrows = hi - lo + 1, N = ncols * nrows;
-  double loc = 0.0;
-  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < N;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    const int ix = 1 + (int)(t % ncols), iy = lo + (int)(t / ncols);
-    const double v = a[at(g, ix, iy)];
-    loc += v * v;
-  }
-  loc = block_sum(loc, sh);
-  if (threadIdx.x == 0) partial[k * gridDim.x + blockIdx.x] = loc;
-}
-__global__ void k_energy_finish(const double *__restrict__ partial, int nb, double anorml1,
-                                int rows_mode, int ny, double *out) {
-  __shared__ double sh[32];
-  const int k = blockIdx.x;
-  double v = 0.0;
-  for (int i = threadIdx.x; i < nb; i += blockDim.x) v += partial[k * nb + i];
-  v = block_sum(v, sh);
-  // pic/fields.f90:341: exe = exes*anorml1*ny/80.d0
-  if (threadIdx.x == 0) out[k] = rows_mode ? v * anorml1 * ny / 80.0 : v * anorml1;
-}
-
-G geom(const em2g_ctx *c) { return G{c->g.nx, c->g.ny, c->g.nxg, c->g.w}; }
-
-dim3 grid_for(int nxc, int nyc) { return dim3((nxc + TX - 1) / TX, (nyc + TY - 1) / TY); }
-
-}  // namespace
 
 int smooth2_f64(em2g_ctx *c, double *a) {
-  const G g = geom(c);
-  const dim3 grd = grid_for(g.nx + 1, g.ny + 1), blk(TX, TY);
-  k_smooth_binomial<<<grd, blk, 0, c->stream>>>(g, a, c->smooth_tmp);
-  k_smooth_compensate<<<grd, blk, 0, c->stream>>>(g, c->smooth_tmp, a);
-  c->launches += 2;
-  EM2G_CUDA(cudaGetLastError());
-  return EM2G_OK;
+  return grid::smooth2_t<double>(c, a, c->smooth_tmp);
 }
 
-int cg_init(em2g_ctx *c) {
-  CgWork &W = c->cg;
-  const int64_t N = (int64_t)c->g.nx * c->g.ny;
-  int per_sm = 0;
-  EM2G_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg, W.threads, 0));
-  if (per_sm < 1) return fail(EM2G_ERR_CUDA, "cg kernel cannot be resident");
-  int64_t want = (N + W.threads - 1) / W.threads;
-  int64_t maxb = (int64_t)per_sm * c->num_sms;
-  W.blocks = (int)(want < maxb ? want : maxb);
-  if (W.blocks < 1) W.blocks = 1;
-  EM2G_CUDA(cudaMalloc(&W.u, sizeof(double) * N * 4));
-  W.r = W.u + N;
-  W.p = W.u + 2 * N;
-  W.ap = W.u + 3 * N;
-  EM2G_CUDA(cudaMalloc(&W.partial, sizeof(double) * 2 * W.blocks));
-  EM2G_CUDA(cudaMalloc(&W.bar, sizeof(unsigned) * 2));
-  EM2G_CUDA(cudaMalloc(&W.status, sizeof(int) * 2));
-  EM2G_CUDA(cudaMemset(W.bar, 0, sizeof(unsigned) * 2));
-  return EM2G_OK;
-}
+int cg_init(em2g_ctx *c) { return grid::cg_init_t<double>(c); }
 
 void cg_free(em2g_ctx *c) {
   cudaFree(c->cg.u);
@@ -390,87 +22,9 @@ void cg_free(em2g_ctx *c) {
   c->cg = CgWork();
 }
 
-static int poisson_f64(em2g_ctx *c, int *iters) {
-  const G g = geom(c);
-  CgWork &W = c->cg;
-  const double dx = c->P.dx, dy = c->P.dy;
-  const dim3 blk(TX, TY);
-  k_poisson_rhs<<<grid_for(g.nx, g.ny), blk, 0, c->stream>>>(g, c->fld, dx, dy, W.r, W.p);
-  EM2G_CUDA(cudaGetLastError());
-  EM2G_CUDA(cudaMemsetAsync(W.bar, 0, sizeof(unsigned) * 2, c->stream));
-  CgArgs a;
-  a.nx = g.nx;
-  a.ny = g.ny;
-  a.u = W.u;
-  a.r = W.r;
-  a.p = W.p;
-  a.ap = W.ap;
-  a.partial = W.partial;
-  a.bar = W.bar;
-  a.status = W.status;
-  a.maxits = c->P.cg_maxits;
-  a.eps = c->P.cg_eps;
-  void *args[] = {&a};
-  EM2G_CUDA(cudaLaunchCooperativeKernel((const void *)k_cg, dim3(W.blocks), dim3(W.threads),
-                                        args, 0, c->stream));
-  k_poisson_correct<<<grid_for(g.nx, g.ny), blk, 0, c->stream>>>(g, c->fld, W.u, dx, dy);
-  c->launches += 3;
-  EM2G_CUDA(cudaGetLastError());
-  // status[0] (sticky timeout flag) and status[1] (iterations) are read by
-  // the caller after its last launch; no host synchronisation here.
-  (void)iters;
-  return EM2G_OK;
-}
-
-static int energies_f64(em2g_ctx *c) {
-  const G g = geom(c);
-  int lo = 1, hi = g.ny;
-  const double alx = c->P.dx * g.nx, aly = c->P.dy * g.ny;
-  const double t = c->P.qme / c->P.wpe / c->P.c;
-  const double rnmec2i = t * t / (alx * aly);  // pic/global.f90:112
-  const double anorml1 = 0.5 * c->P.dx * c->P.dy * rnmec2i;
-  if (c->P.energy_mode == 1) {
-    lo = 88;
-    hi = 168;
-  }
-  const int nb = kEnergyBlocks;
-  k_energy_partial<<<dim3(nb, 6), 256, 0, c->stream>>>(g, c->fld, lo, hi, c->red);
-  k_energy_finish<<<6, 256, 0, c->stream>>>(c->red, nb, anorml1, c->P.energy_mode == 1, g.ny,
-                                            c->dev_out + 4);
-  c->launches += 2;
-  EM2G_CUDA(cudaGetLastError());
-  return EM2G_OK;
-}
-
 int fields_f64(em2g_ctx *c, int it, bool want_energies, int *cg_iters) {
-  const G g = geom(c);
-  const dim3 blk(TX, TY);
-  // fold (pic/fields.f90:44-137)
-  k_fold_x<<<dim3((g.ny + 3 + 127) / 128, 7), 128, 0, c->stream>>>(g, c->fld);
-  k_fold_y<<<dim3((g.nx + 3 + 127) / 128, 7), 128, 0, c->stream>>>(g, c->fld);
-  // Yee (pic/fields.f90:184-247)
-  const double ctx = c->P.dt * c->P.c / c->P.dx, cty = c->P.dt * c->P.c / c->P.dy;
-  const double ctxh = ctx * 0.5, ctyh = cty * 0.5, tem = 0.5 * c->P.dt;
-  const dim3 grd = grid_for(g.nx + 1, g.ny + 1);
-  k_b_half<<<grd, blk, 0, c->stream>>>(g, c->fld, ctxh, ctyh);
-  k_e_full<<<grd, blk, 0, c->stream>>>(g, c->fld, ctx, cty, tem);
-  k_b_half<<<grd, blk, 0, c->stream>>>(g, c->fld, ctxh, ctyh);
-  c->launches += 5;
-  EM2G_CUDA(cudaGetLastError());
-  // filters (pic/fields.f90:252-260)
-  int rc = smooth2_f64(c, c->fld + EM2G_RHO * g.w);
-  if (rc) return rc;
-  if (it % c->P.isav == 0)
-    for (int k = EM2G_EX; k <= EM2G_BZ; ++k)
-      if ((rc = smooth2_f64(c, c->fld + k * g.w))) return rc;
-  // Poisson (pic/fields.f90:262)
-  if ((rc = poisson_f64(c, cg_iters))) return rc;
-  // energies (pic/fields.f90:267-347)
-  if (want_energies && it % c->P.isav == 0)
-    if ((rc = energies_f64(c))) return rc;
-  // reset rho and J (pic/fields.f90:353-365)
-  EM2G_CUDA(cudaMemsetAsync(c->fld + EM2G_RHO * g.w, 0, sizeof(double) * 7 * g.w, c->stream));
-  return EM2G_OK;
+  (void)cg_iters;  // read from cg.status by the caller after its last launch
+  return grid::fields_t<double>(c, c->fld, c->smooth_tmp, it, want_energies);
 }
 
 }  // namespace em2g

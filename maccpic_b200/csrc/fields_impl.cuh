@@ -1,0 +1,137 @@
+// fields_impl.cuh -- host side of fields (pic/fields.f90:2-367), smooth2
+// and the Poisson solve, templated on the storage type of the field block
+// (double: fields_f64.cu; float: fields_f32.cu).
+#pragma once
+#include "grid_kernels.cuh"
+
+namespace em2g {
+namespace grid {
+namespace {
+
+inline G geom(const em2g_ctx *c) { return G{c->g.nx, c->g.ny, c->g.nxg, c->g.w}; }
+
+inline dim3 grid_for(int nxc, int nyc) { return dim3((nxc + TX - 1) / TX, (nyc + TY - 1) / TY); }
+
+template <typename T>
+int smooth2_t(em2g_ctx *c, T *a, T *tmp) {
+  const G g = geom(c);
+  const dim3 grd = grid_for(g.nx + 1, g.ny + 1), blk(TX, TY);
+  k_smooth_binomial<T><<<grd, blk, 0, c->stream>>>(g, a, tmp);
+  k_smooth_compensate<T><<<grd, blk, 0, c->stream>>>(g, tmp, a);
+  c->launches += 2;
+  EM2G_CUDA(cudaGetLastError());
+  return EM2G_OK;
+}
+
+template <typename T>
+int cg_init_t(em2g_ctx *c) {
+  CgWork &W = c->cg;
+  const int64_t N = (int64_t)c->g.nx * c->g.ny;
+  int per_sm = 0;
+  EM2G_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg<T>, W.threads, 0));
+  if (per_sm < 1) return fail(EM2G_ERR_CUDA, "cg kernel cannot be resident");
+  const int64_t want = (N + W.threads - 1) / W.threads;
+  const int64_t maxb = (int64_t)per_sm * c->num_sms;
+  W.blocks = (int)(want < maxb ? want : maxb);
+  if (W.blocks < 1) W.blocks = 1;
+  EM2G_CUDA(cudaMalloc(&W.u, sizeof(T) * N * 4));
+  W.elem = sizeof(T);
+  EM2G_CUDA(cudaMalloc(&W.partial, sizeof(double) * 2 * W.blocks));
+  EM2G_CUDA(cudaMalloc(&W.bar, sizeof(unsigned) * 2));
+  EM2G_CUDA(cudaMalloc(&W.status, sizeof(int) * 2));
+  EM2G_CUDA(cudaMemset(W.bar, 0, sizeof(unsigned) * 2));
+  return EM2G_OK;
+}
+
+// pic/fields.f90:384-442 + cgm :508-651.  The CG's exit count and a sticky
+// timeout flag land in cg.status; the caller reads them after its last
+// launch (no host synchronisation here).
+template <typename T>
+int poisson_t(em2g_ctx *c, T *fld) {
+  const G g = geom(c);
+  CgWork &W = c->cg;
+  const int64_t N = (int64_t)g.nx * g.ny;
+  T *u = (T *)W.u, *r = u + N, *p = u + 2 * N, *ap = u + 3 * N;
+  const T dx = (T)c->P.dx, dy = (T)c->P.dy;
+  const dim3 blk(TX, TY);
+  k_poisson_rhs<T><<<grid_for(g.nx, g.ny), blk, 0, c->stream>>>(g, fld, dx, dy, r, p);
+  EM2G_CUDA(cudaGetLastError());
+  EM2G_CUDA(cudaMemsetAsync(W.bar, 0, sizeof(unsigned) * 2, c->stream));
+  CgArgs<T> a;
+  a.nx = g.nx;
+  a.ny = g.ny;
+  a.u = u;
+  a.r = r;
+  a.p = p;
+  a.ap = ap;
+  a.partial = W.partial;
+  a.bar = W.bar;
+  a.status = W.status;
+  a.maxits = c->P.cg_maxits;
+  a.eps = c->P.cg_eps;
+  void *args[] = {&a};
+  EM2G_CUDA(cudaLaunchCooperativeKernel((const void *)k_cg<T>, dim3(W.blocks),
+                                        dim3(W.threads), args, 0, c->stream));
+  k_poisson_correct<T><<<grid_for(g.nx, g.ny), blk, 0, c->stream>>>(g, fld, u, dx, dy);
+  c->launches += 3;
+  EM2G_CUDA(cudaGetLastError());
+  return EM2G_OK;
+}
+
+// pic/fields.f90:267-347 into dev_out[4..9]
+template <typename T>
+int energies_t(em2g_ctx *c, const T *fld) {
+  const G g = geom(c);
+  int lo = 1, hi = g.ny;
+  const double alx = c->P.dx * g.nx, aly = c->P.dy * g.ny;
+  const double t = c->P.qme / c->P.wpe / c->P.c;
+  const double rnmec2i = t * t / (alx * aly);  // pic/global.f90:112
+  const double anorml1 = 0.5 * c->P.dx * c->P.dy * rnmec2i;
+  if (c->P.energy_mode == 1) {
+    lo = 88;
+    hi = 168;
+  }
+  const int nb = kEnergyBlocks;
+  k_energy_partial<T><<<dim3(nb, 6), 256, 0, c->stream>>>(g, fld, lo, hi, c->red);
+  k_energy_finish<<<6, 256, 0, c->stream>>>(c->red, nb, anorml1, c->P.energy_mode == 1, g.ny,
+                                            c->dev_out + 4);
+  c->launches += 2;
+  EM2G_CUDA(cudaGetLastError());
+  return EM2G_OK;
+}
+
+template <typename T>
+int fields_t(em2g_ctx *c, T *fld, T *tmp, int it, bool want_energies) {
+  const G g = geom(c);
+  const dim3 blk(TX, TY);
+  // fold (pic/fields.f90:44-137)
+  k_fold_x<T><<<dim3((g.ny + 3 + 127) / 128, 7), 128, 0, c->stream>>>(g, fld);
+  k_fold_y<T><<<dim3((g.nx + 3 + 127) / 128, 7), 128, 0, c->stream>>>(g, fld);
+  // Yee (pic/fields.f90:184-247)
+  const double ctx = c->P.dt * c->P.c / c->P.dx, cty = c->P.dt * c->P.c / c->P.dy;
+  const double ctxh = ctx * 0.5, ctyh = cty * 0.5, tem = 0.5 * c->P.dt;
+  const dim3 grd = grid_for(g.nx + 1, g.ny + 1);
+  k_b_half<T><<<grd, blk, 0, c->stream>>>(g, fld, (T)ctxh, (T)ctyh);
+  k_e_full<T><<<grd, blk, 0, c->stream>>>(g, fld, (T)ctx, (T)cty, (T)tem);
+  k_b_half<T><<<grd, blk, 0, c->stream>>>(g, fld, (T)ctxh, (T)ctyh);
+  c->launches += 5;
+  EM2G_CUDA(cudaGetLastError());
+  // filters (pic/fields.f90:252-260)
+  int rc = smooth2_t<T>(c, fld + EM2G_RHO * g.w, tmp);
+  if (rc) return rc;
+  if (it % c->P.isav == 0)
+    for (int k = EM2G_EX; k <= EM2G_BZ; ++k)
+      if ((rc = smooth2_t<T>(c, fld + k * g.w, tmp))) return rc;
+  // Poisson (pic/fields.f90:262)
+  if ((rc = poisson_t<T>(c, fld))) return rc;
+  // energies (pic/fields.f90:267-347)
+  if (want_energies && it % c->P.isav == 0)
+    if ((rc = energies_t<T>(c, fld))) return rc;
+  // reset rho and J (pic/fields.f90:353-365)
+  EM2G_CUDA(cudaMemsetAsync(fld + EM2G_RHO * g.w, 0, sizeof(T) * 7 * g.w, c->stream));
+  return EM2G_OK;
+}
+
+}  // namespace
+}  // namespace grid
+}  // namespace em2g

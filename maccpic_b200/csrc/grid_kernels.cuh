@@ -1,0 +1,361 @@
+// grid_kernels.cuh -- the grid kernels of em2's fields / smooth2 / Poisson
+// (pic/fields.f90, pic/smooth.f90), templated on the storage type T:
+// double for the drop-in FP64 path (fields_f64.cu, compiled with
+// -fmad=false so each cell is rounded as em2 rounds it) and float for the
+// mixed path (fields_f32.cu).  Dot products and energies always accumulate
+// in FP64.
+//
+// Every stencil sweep of the reference ends with guard copies, columns 0 and
+// nx+2 from nx and 2, then rows 0 and ny+2 from ny and 2
+// (pic/fields.f90:192-200).  Here the thread that computes a cell also
+// stores it into the guard positions that copy it, so no second pass is
+// needed and the values are the same.
+#pragma once
+#include "em2g_internal.cuh"
+
+namespace em2g {
+namespace grid {
+namespace {
+
+constexpr int TX = 32, TY = 8;
+
+struct G {
+  int nx, ny, nxg;
+  int64_t w;
+};
+
+__device__ __forceinline__ int64_t at(const G &g, int ix, int iy) {
+  return (int64_t)iy * g.nxg + ix;
+}
+
+// store v at (ix,iy), 1<=ix<=nx+1, 1<=iy<=ny+1, and at its guard copies
+template <typename T>
+__device__ __forceinline__ void store_with_guards(const G &g, T *a, int ix, int iy, T v) {
+  a[at(g, ix, iy)] = v;
+  const int mx = (ix == g.nx) ? 0 : ((ix == 2) ? g.nx + 2 : -1);
+  const int my = (iy == g.ny) ? 0 : ((iy == 2) ? g.ny + 2 : -1);
+  if (mx >= 0) a[at(g, mx, iy)] = v;
+  if (my >= 0) a[at(g, ix, my)] = v;
+  if (mx >= 0 && my >= 0) a[at(g, mx, my)] = v;
+}
+
+// ---- guard fold of rho and the 6 current arrays (pic/fields.f90:44-137)
+// x pass: one thread per (row iy in 0..ny+2, array)
+template <typename T>
+__global__ void k_fold_x(G g, T *fld) {
+  const int iy = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = blockIdx.y;  // 0..6 -> rho..jzp
+  if (iy > g.ny + 2) return;
+  T *a = fld + (EM2G_RHO + k) * g.w + (int64_t)iy * g.nxg;
+  const int nx = g.nx;
+  a[1] = a[1] + a[nx + 1];
+  a[2] = a[2] + a[nx + 2];
+  a[nx] = a[nx] + a[0];
+  a[nx + 1] = a[1];
+  a[nx + 2] = a[2];
+  a[0] = a[nx];
+}
+// y pass: one thread per (column ix in 0..nx+2, array)
+template <typename T>
+__global__ void k_fold_y(G g, T *fld) {
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = blockIdx.y;
+  if (ix > g.nx + 2) return;
+  T *a = fld + (EM2G_RHO + k) * g.w + ix;
+  const int64_t s = g.nxg;
+  const int ny = g.ny;
+  a[1 * s] = a[1 * s] + a[(ny + 1) * s];
+  a[2 * s] = a[2 * s] + a[(ny + 2) * s];
+  a[ny * s] = a[ny * s] + a[0];
+  a[(ny + 1) * s] = a[1 * s];
+  a[(ny + 2) * s] = a[2 * s];
+  a[0] = a[ny * s];
+}
+
+// ---- Yee half step of B (pic/fields.f90:184-200, :231-247)
+template <typename T>
+__global__ void k_b_half(G g, T *fld, T ctxh, T ctyh) {
+  const int ix = 1 + blockIdx.x * TX + threadIdx.x;
+  const int iy = 1 + blockIdx.y * TY + threadIdx.y;
+  if (ix > g.nx + 1 || iy > g.ny + 1) return;
+  const T *ex = fld + EM2G_EX * g.w, *ey = fld + EM2G_EY * g.w, *ez = fld + EM2G_EZ * g.w;
+  T *bx = fld + EM2G_BX * g.w, *by = fld + EM2G_BY * g.w, *bz = fld + EM2G_BZ * g.w;
+  const int64_t c = at(g, ix, iy);
+  const T ezc = ez[c];
+  const T vbx = bx[c] - ctyh * (ezc - ez[c - g.nxg]);
+  const T vby = by[c] + ctxh * (ezc - ez[c - 1]);
+  const T vbz = bz[c] - ctxh * (ey[c + 1] - ey[c]) + ctyh * (ex[c + g.nxg] - ex[c]);
+  store_with_guards(g, bx, ix, iy, vbx);
+  store_with_guards(g, by, ix, iy, vby);
+  store_with_guards(g, bz, ix, iy, vbz);
+}
+
+// ---- Yee full step of E (pic/fields.f90:207-224)
+template <typename T>
+__global__ void k_e_full(G g, T *fld, T ctx, T cty, T tem) {
+  const int ix = 1 + blockIdx.x * TX + threadIdx.x;
+  const int iy = 1 + blockIdx.y * TY + threadIdx.y;
+  if (ix > g.nx + 1 || iy > g.ny + 1) return;
+  T *ex = fld + EM2G_EX * g.w, *ey = fld + EM2G_EY * g.w, *ez = fld + EM2G_EZ * g.w;
+  const T *bx = fld + EM2G_BX * g.w, *by = fld + EM2G_BY * g.w, *bz = fld + EM2G_BZ * g.w;
+  const T *jxm = fld + EM2G_JXM * g.w, *jxp = fld + EM2G_JXP * g.w,
+               *jym = fld + EM2G_JYM * g.w, *jyp = fld + EM2G_JYP * g.w,
+               *jzm = fld + EM2G_JZM * g.w, *jzp = fld + EM2G_JZP * g.w;
+  const int64_t c = at(g, ix, iy);
+  const T bzc = bz[c];
+  const T vex = ex[c] + cty * (bzc - bz[c - g.nxg]) - tem * (jxm[c] + jxp[c]);
+  const T vey = ey[c] - ctx * (bzc - bz[c - 1]) - tem * (jym[c] + jyp[c]);
+  const T vez = ez[c] + ctx * (by[c + 1] - by[c]) - cty * (bx[c + g.nxg] - bx[c]) -
+                     tem * (jzm[c] + jzp[c]);
+  store_with_guards(g, ex, ix, iy, vex);
+  store_with_guards(g, ey, ix, iy, vey);
+  store_with_guards(g, ez, ix, iy, vez);
+}
+
+// ---- smooth2 (pic/smooth.f90:143-177): binomial pass into `d`, then the
+// compensation pass back into `s`.
+template <typename T>
+__global__ void k_smooth_binomial(G g, const T *__restrict__ s, T *d) {
+  const int ix = 1 + blockIdx.x * TX + threadIdx.x;
+  const int iy = 1 + blockIdx.y * TY + threadIdx.y;
+  if (ix > g.nx + 1 || iy > g.ny + 1) return;
+  const int64_t c = at(g, ix, iy), n = g.nxg;
+  const T v = (4 * s[c] + 2 * (s[c - 1] + s[c + 1] + s[c - n] + s[c + n]) +
+                    s[c - 1 - n] + s[c - 1 + n] + s[c + 1 - n] + s[c + 1 + n]) /
+                   T(16.0);
+  store_with_guards(g, d, ix, iy, v);
+}
+template <typename T>
+__global__ void k_smooth_compensate(G g, const T *__restrict__ d, T *s) {
+  const int ix = 1 + blockIdx.x * TX + threadIdx.x;
+  const int iy = 1 + blockIdx.y * TY + threadIdx.y;
+  if (ix > g.nx + 1 || iy > g.ny + 1) return;
+  const int64_t c = at(g, ix, iy), n = g.nxg;
+  const T v = (20 * d[c] - d[c - 1] - d[c + 1] - d[c - n] - d[c + n] - d[c - 1 - n] -
+                    d[c - 1 + n] - d[c + 1 - n] - d[c + 1 + n]) /
+                   T(12.0);
+  store_with_guards(g, s, ix, iy, v);
+}
+
+// ---- Poisson right-hand side (pic/fields.f90:392-405): f = (div E - rho)
+// * dx * dx on the nx*ny periodic grid; written straight into r (u = 0, so
+// cgm's first residual r = f - L u is f) and p = r.
+template <typename T>
+__global__ void k_poisson_rhs(G g, const T *__restrict__ fld, T dx, T dy, T *r, T *p) {
+  const int ix = 1 + blockIdx.x * TX + threadIdx.x;
+  const int iy = 1 + blockIdx.y * TY + threadIdx.y;
+  if (ix > g.nx || iy > g.ny) return;
+  const T *ex = fld + EM2G_EX * g.w, *ey = fld + EM2G_EY * g.w, *rho = fld + EM2G_RHO * g.w;
+  const int ixm = (ix == 1) ? g.nx : ix - 1;
+  const T f = (ex[at(g, ix, iy)] - ex[at(g, ixm, iy)]) / dx +
+                   (ey[at(g, ix, iy)] - ey[at(g, ix, iy - 1)]) / dy - rho[at(g, ix, iy)];
+  const T fs = f * dx * dx;
+  const int64_t k = (int64_t)(iy - 1) * g.nx + (ix - 1);
+  r[k] = fs;
+  p[k] = fs;
+}
+
+// ---- E -= grad(phi) with periodic images and guards (pic/fields.f90:410-442)
+template <typename T>
+__device__ __forceinline__ void store_images(const G &g, T *a, int ix, int iy, T v) {
+  // (ix,iy) in 1..nx x 1..ny; its copies in 0..nx+2 x 0..ny+2
+  int xs[3], ys[3], nxs = 0, nys = 0;
+  xs[nxs++] = ix;
+  if (ix == 1) xs[nxs++] = g.nx + 1;
+  if (ix == g.nx) xs[nxs++] = 0;
+  if (ix == 2) xs[nxs++] = g.nx + 2;
+  ys[nys++] = iy;
+  if (iy == 1) ys[nys++] = g.ny + 1;
+  if (iy == g.ny) ys[nys++] = 0;
+  if (iy == 2) ys[nys++] = g.ny + 2;
+  for (int a1 = 0; a1 < nys; ++a1)
+    for (int a0 = 0; a0 < nxs; ++a0) a[at(g, xs[a0], ys[a1])] = v;
+}
+template <typename T>
+__global__ void k_poisson_correct(G g, T *fld, const T *__restrict__ u, T dx, T dy) {
+  const int ix = 1 + blockIdx.x * TX + threadIdx.x;
+  const int iy = 1 + blockIdx.y * TY + threadIdx.y;
+  if (ix > g.nx || iy > g.ny) return;
+  T *ex = fld + EM2G_EX * g.w, *ey = fld + EM2G_EY * g.w;
+  const int64_t k = (int64_t)(iy - 1) * g.nx + (ix - 1);
+  const int64_t kxp = (int64_t)(iy - 1) * g.nx + (ix == g.nx ? 0 : ix);
+  const int64_t kyp = (int64_t)(iy == g.ny ? 0 : iy) * g.nx + (ix - 1);
+  const T uc = u[k];
+  const T vx = ex[at(g, ix, iy)] - (u[kxp] - uc) / dx;
+  const T vy = ey[at(g, ix, iy)] - (u[kyp] - uc) / dy;
+  store_images(g, ex, ix, iy, vx);
+  store_images(g, ey, ix, iy, vy);
+}
+
+// ---- conjugate gradient, one persistent launch (pic/fields.f90:508-651)
+//
+// All blocks are co-resident (cooperative launch).  Between phases they
+// meet at a software grid barrier whose wait is bounded: after kSpinLimit
+// polls a block records a timeout in status[0] and every block leaves.
+// Dot products: each block writes a partial; after the barrier every block
+// sums all partials in the same fixed order, so all blocks take the same
+// decisions on the same values.
+constexpr long kSpinLimit = 20000000;  // polls of ~100 ns: about 2 s
+
+__device__ bool grid_barrier(unsigned *bar, unsigned nblocks, int *status) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned *gen = bar + 1;
+    const unsigned g0 = *gen;
+    __threadfence();
+    const unsigned arrived = atomicAdd(bar, 1u);
+    if (arrived == nblocks - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      long spins = 0;
+      while (*gen == g0) {
+        if (*(volatile int *)status != 0) break;
+        if (++spins > kSpinLimit) {
+          atomicExch(status, 1);
+          break;
+        }
+        __nanosleep(100);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return *(volatile int *)status == 0;
+}
+
+// sum of nb partials in a fixed order; result valid in every thread
+__device__ double sum_partials(const double *partial, int nb, double *sh) {
+  if (threadIdx.x < 32) {
+    double v = 0.0;
+    for (int i = threadIdx.x; i < nb; i += 32) v += ((volatile const double *)partial)[i];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (threadIdx.x == 0) sh[0] = v;
+  }
+  __syncthreads();
+  const double r = sh[0];
+  __syncthreads();
+  return r;
+}
+
+__device__ double block_sum(double v, double *sh) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (threadIdx.x < 32) {
+    r = threadIdx.x < (int)(blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
+  }
+  __syncthreads();
+  return r;  // valid in thread 0
+}
+
+template <typename T>
+struct CgArgs {
+  int nx, ny;
+  T *u, *r, *p, *ap;
+  double *partial;  // [2][gridDim.x]
+  unsigned *bar;
+  int *status;      // [0] timeout, [1] iterations
+  int maxits;
+  double eps;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_cg(CgArgs<T> a) {
+  __shared__ double sh[33];
+  const int64_t N = (int64_t)a.nx * a.ny;
+  const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const unsigned nb = gridDim.x;
+  double *part0 = a.partial, *part1 = a.partial + nb;
+  // rr = sum r^2 for n = 1 (pic/fields.f90:546-556); u starts at 0
+  double loc = 0.0;
+  for (int64_t k = tid; k < N; k += stride) {
+    a.u[k] = T(0);
+    loc += (double)a.r[k] * (double)a.r[k];
+  }
+  loc = block_sum(loc, sh);
+  if (threadIdx.x == 0) part0[blockIdx.x] = loc;
+  if (!grid_barrier(a.bar, nb, a.status)) return;
+  double rr = sum_partials(part0, nb, sh);
+  int n;
+  for (n = 1; n <= a.maxits; ++n) {
+    // ap = L p and pap = sum p*ap (pic/fields.f90:559-584)
+    loc = 0.0;
+    for (int64_t k = tid; k < N; k += stride) {
+      const int j = (int)(k % a.nx), l = (int)(k / a.nx);
+      const int64_t row = (int64_t)l * a.nx;
+      const int64_t kxp = row + (j == a.nx - 1 ? 0 : j + 1);
+      const int64_t kxm = row + (j == 0 ? a.nx - 1 : j - 1);
+      const int64_t kyp = (int64_t)(l == a.ny - 1 ? 0 : l + 1) * a.nx + j;
+      const int64_t kym = (int64_t)(l == 0 ? a.ny - 1 : l - 1) * a.nx + j;
+      // p was written by other threads before the barrier: read past L1
+      const T pc = __ldcg(a.p + k);
+      const T v = __ldcg(a.p + kxp) + __ldcg(a.p + kxm) + __ldcg(a.p + kyp) +
+                  __ldcg(a.p + kym) - T(4) * pc;
+      a.ap[k] = v;
+      loc += (double)pc * (double)v;
+    }
+    loc = block_sum(loc, sh);
+    if (threadIdx.x == 0) part1[blockIdx.x] = loc;
+    if (!grid_barrier(a.bar, nb, a.status)) return;
+    const double pap = sum_partials(part1, nb, sh);
+    const double ak = rr / pap;
+    // u += ak p, r1 = r - ak ap, r_norm = sum r1^2 (pic/fields.f90:586-614)
+    loc = 0.0;
+    for (int64_t k = tid; k < N; k += stride) {
+      a.u[k] = (T)(a.u[k] + ak * a.p[k]);
+      const T r1 = (T)(a.r[k] - ak * a.ap[k]);
+      a.r[k] = r1;
+      loc += (double)r1 * (double)r1;
+    }
+    loc = block_sum(loc, sh);
+    if (threadIdx.x == 0) part0[blockIdx.x] = loc;
+    if (!grid_barrier(a.bar, nb, a.status)) return;
+    const double r_norm = sum_partials(part0, nb, sh);
+    if (r_norm / a.nx / a.ny < a.eps) break;  // pic/fields.f90:616
+    const double bk = r_norm / rr;            // pic/fields.f90:632
+    for (int64_t k = tid; k < N; k += stride) a.p[k] = (T)(a.r[k] + bk * a.p[k]);
+    rr = r_norm;  // next pass's sum of r^2 over the same r, same order
+    if (!grid_barrier(a.bar, nb, a.status)) return;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) a.status[1] = n;
+}
+
+// ---- energies (pic/fields.f90:267-347): per-block partial sums of a^2 over
+// rows lo..hi, columns 1..nx of the six E/B arrays.
+template <typename T>
+__global__ void k_energy_partial(G g, const T *__restrict__ fld, int lo, int hi,
+                                 double *partial) {
+  __shared__ double sh[32];
+  const int k = blockIdx.y;  // field 0..5
+  const T *a = fld + k * g.w;
+  const int64_t ncols = g.nx, nrows = hi - lo + 1, N = ncols * nrows;
+  double loc = 0.0;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < N;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int ix = 1 + (int)(t % ncols), iy = lo + (int)(t / ncols);
+    const double v = (double)a[at(g, ix, iy)];
+    loc += v * v;
+  }
+  loc = block_sum(loc, sh);
+  if (threadIdx.x == 0) partial[k * gridDim.x + blockIdx.x] = loc;
+}
+__global__ void k_energy_finish(const double *__restrict__ partial, int nb, double anorml1,
+                                int rows_mode, int ny, double *out) {
+  __shared__ double sh[32];
+  const int k = blockIdx.x;
+  double v = 0.0;
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) v += partial[k * nb + i];
+  v = block_sum(v, sh);
+  // pic/fields.f90:341: exe = exes*anorml1*ny/80.d0
+  if (threadIdx.x == 0) out[k] = rows_mode ? v * anorml1 * ny / 80.0 : v * anorml1;
+}
+
+
+}  // namespace
+}  // namespace grid
+}  // namespace em2g
