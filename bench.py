@@ -7,10 +7,13 @@ One step is em2's main-loop pass move -> curnt -> it+1 -> fields
 particles), run through libem2g.  Prints one JSON line (rank 0).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--config NAME] [--precision fp64|fp32]
+                  [--config NAME] [--precision fp32|fp64]
 
 value : device-resident state, K steps of em2g_step timed with CUDA events on
-        the library's stream (inputs of 13-26 GB are far larger than L2).
+        the library's stream (inputs of 13-26 GB are far larger than L2), in
+        the mixed-precision form by default; the FP64 form is then run from
+        the same initial state for the same steps and reported beside it
+        ("mixed_vs_fp64": its speed and the field-energy error between them).
 e2e   : the same K steps through the drop-in entry points (em2g_move_curnt,
         em2g_fields) starting from the state in pinned host memory: the
         timed region includes the host->device upload of every field and
@@ -45,7 +48,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--config", default="harris_2048x1024_ppc64")
-    ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64")
+    ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp32")
+    ap.add_argument("--no-fp64-compare", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
@@ -227,35 +231,26 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def run_ours(args):
+def field_energy(fld, nx, ny):
+    """0.5 * mean over the interior of E^2 + B^2 (FP64, host)."""
     import numpy as np
+    a = fld[:6, 1:ny + 1, 1:nx + 1]
+    return 0.5 * float(np.sum(a * a)) / (nx * ny)
+
+
+def measure(args, cfg, precision, local, parts, fields, stream, ws):
+    """Device-resident run: warm-up, then K timed steps.  Returns timings,
+    counters and the final fields and kinetic energies."""
     import torch
-    from maccpic_b200 import build, loader
+    from maccpic_b200 import _lib
     from maccpic_b200.em2 import Em2Gpu
-
-    ws, rank, local = dist_init()
-    build.build()
-    cfg = loader.PRESETS[args.config]
-    rp = cfg.run_params(device=local)
-    stream = torch.cuda.current_stream()
-    fields = loader.initial_fields(cfg)
-    n = cfg.nx * cfg.ny * cfg.ppc
-    n_total = 2 * n
-    W = (cfg.nx + 3) * (cfg.ny + 3)
-
+    rp = cfg.run_params(device=local, precision=precision)
     g = Em2Gpu(rp)
     g.set_stream(stream)
     g.set_fields(fields)
-    parts = loader.sample_particles_torch(cfg, device=f"cuda:{local}")
     for s in range(2):
         g.set_particles_device(s, parts[s])
     torch.cuda.synchronize()
-    parts_host = None
-    if rank == 0 and not args.no_e2e:
-        parts_host = [p.cpu().pin_memory() for p in parts]
-    del parts
-    torch.cuda.empty_cache()
-
     for _ in range(args.warmup):
         g.step(1)
     g.reset_counters()
@@ -263,58 +258,108 @@ def run_ours(args):
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier(ws)
     torch.cuda.synchronize()
+    cg = []
     with Clocks(local) as clk:
         start.record(stream)
-        cg = []
         for _ in range(args.steps):
             r = g.step(1)
             cg.append(r["cg_iters"])
         stop.record(stream)
         torch.cuda.synchronize()
     barrier(ws)
-    ms = start.elapsed_time(stop)
-    ms = max_over_ranks(ws, ms)
+    ms = max_over_ranks(ws, start.elapsed_time(stop))
     cnt = g.counters()
     g.set_timing(False)
-    value = n_total * ws * args.steps / (ms / 1e3)
+    out = {"ms": ms, "counters": cnt, "cg": cg, "clocks": clk.summary(), "ake": r["ake"],
+           "fields": g.get_fields()}
+    g.close()
+    return out
 
-    # roofline of the dominant kernel (fused push): algorithmic bytes per
-    # launch = n * 96 B (x, y, vx, vy, vz, gamma read and written) + the grid
-    # arrays it touches: 6 scaled field arrays read and 7 deposit arrays
-    # read-modify-written, W * 8 * (6 + 14) B
-    bytes_launch = n * 96 + W * 8 * 20
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    from maccpic_b200 import build, loader, _lib
+
+    ws, rank, local = dist_init()
+    build.build()
+    cfg = loader.PRESETS[args.config]
+    fp32 = args.precision == "fp32"
+    stream = torch.cuda.current_stream()
+    fields = loader.initial_fields(cfg)
+    n = cfg.nx * cfg.ny * cfg.ppc
+    n_total = 2 * n
+    W = (cfg.nx + 3) * (cfg.ny + 3)
+    parts = loader.sample_particles_torch(cfg, device=f"cuda:{local}")
+    torch.cuda.synchronize()
+
+    main = measure(args, cfg, _lib.FP32 if fp32 else _lib.FP64, local, parts, fields, stream, ws)
+    ms = main["ms"]
+    value = n_total * ws * args.steps / (ms / 1e3)
+    # the other precision on the same initial state: speed and field-energy
+    # error of the mixed path against FP64 after the same W + K steps
+    compare = None
+    if fp32 and not args.no_fp64_compare:
+        ref = measure(args, cfg, _lib.FP64, local, parts, fields, stream, ws)
+        e32, e64 = (field_energy(m["fields"], cfg.nx, cfg.ny) for m in (main, ref))
+        k32, k64 = (float(np.sum(m["ake"])) for m in (main, ref))
+        compare = {"fp64_value": n_total * ws * args.steps / (ref["ms"] / 1e3),
+                   "fp64_ms_per_step": ref["ms"] / args.steps,
+                   "speedup_fp32_over_fp64": ref["ms"] / ms,
+                   "field_energy_rel_error": abs(e32 - e64) / abs(e64),
+                   "kinetic_energy_rel_error": abs(k32 - k64) / abs(k64),
+                   "after_steps": args.warmup + args.steps}
+    parts_host = None
+    if rank == 0 and (not args.no_e2e or not args.no_cpu_baseline):
+        parts_host = [p.cpu().pin_memory() for p in parts]
+    del parts
+    torch.cuda.empty_cache()
+
+    cnt = main["counters"]
+    # roofline of the dominant kernel (the fused push of one species):
+    # algorithmic bytes per launch = n * (particle state read + written) +
+    # the grid arrays it touches (6 scaled field arrays read, 7 deposit
+    # arrays read-modify-written) = W * word * (6 + 14)
+    word = 4 if fp32 else 8
+    per_particle = 48 if fp32 else 96
+    bytes_launch = n * per_particle + W * word * 20
     avg_ms = cnt["push_ms"] / max(cnt["push_launches_timed"], 1)
     achieved = bytes_launch / (avg_ms / 1e3) / 1e9
     peak, peak_kind = peaks()
-    traffic = profile_traffic(f"push_f64_{args.config}")
+    kernel = "k_push_cells_f32" if fp32 else "k_push_cells_f64"
+    traffic = profile_traffic(f"{kernel}_{args.config}")
 
     e2e = None
     if rank == 0 and not args.no_e2e:
+        rp = cfg.run_params(precision=_lib.FP32 if fp32 else _lib.FP64)
         e2e = run_e2e(args, cfg, rp, fields, parts_host)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(cfg, fields, [p.numpy() for p in parts_host]
-                           if parts_host is not None else
-                           [p.cpu().numpy() for p in loader.sample_particles_torch(cfg)])
-    g.close()
+        cpu = cpu_baseline(cfg, fields, [p.numpy() for p in parts_host])
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic (seeded double-Harris sampling, GPU Philox)",
+            "dtype": "f32" if fp32 else "f64",
+            "data": "synthetic (seeded double-Harris sampling, GPU Philox)",
             "config": {"workload": args.config, "grid": [cfg.nx, cfg.ny], "ppc": cfg.ppc,
                        "particles_per_gpu": n_total, "mass_ratio": cfg.mass_ratio,
-                       "precision": args.precision, "path": "em2g_step (fused push)",
-                       "l2": "inputs larger than L2 (particle state 25.8 GB)",
-                       "parallelism": f"replicas x{ws}", "cg_iters_mean":
-                           sum(cg) / len(cg)},
+                       "precision": ("mixed: FP32 push/deposit/Yee, FP64 reductions"
+                                     if fp32 else "FP64 (em2's arithmetic)"),
+                       "path": "em2g_step (fused push, cell-sorted)",
+                       "l2": f"inputs larger than L2 (particle state "
+                             f"{n_total * per_particle / 2 / 1e9:.1f} GB)",
+                       "parallelism": f"replicas x{ws}",
+                       "cg_iters_mean": sum(main["cg"]) / len(main["cg"])},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic,
-                         "kernel": "k_push_f64<3>", "peak_kind": peak_kind,
-                         "bytes_per_launch": bytes_launch, "avg_launch_ms": avg_ms},
+                         "frac": achieved / peak, "traffic": traffic, "kernel": kernel,
+                         "peak_kind": peak_kind, "bytes_per_launch": bytes_launch,
+                         "avg_launch_ms": avg_ms},
             "gpu_launches": cnt["kernel_launches"],
-            "clocks": clk.summary(),
+            "clocks": main["clocks"],
+            "mixed_vs_fp64": compare,
+            "adjoint_over_forward": None,
             "e2e": e2e,
             "cpu_baseline": cpu,
         }
@@ -327,7 +372,6 @@ def run_ours(args):
 def run_e2e(args, cfg, rp, fields, parts_host):
     """Drop-in path from host memory: upload, K steps of move_curnt + fields
     reading ake / CG count / energies back every step, download everything."""
-    import numpy as np
     import torch
     from maccpic_b200.em2 import Em2Gpu
 
@@ -354,7 +398,7 @@ def run_e2e(args, cfg, rp, fields, parts_host):
         g.fields(it)
     out_f[...] = g.get_fields()
     for s in range(2):
-        n = C_get_particles_into(g, s, out_p[s])
+        C_get_particles_into(g, s, out_p[s])
     el = time.perf_counter() - t
     g.close()
     n_total = sum(p.shape[1] for p in pnp)
@@ -363,7 +407,7 @@ def run_e2e(args, cfg, rp, fields, parts_host):
     return {"value": n_total * args.steps / el, "unit": METRIC,
             "h2d_bytes_per_step": state / args.steps,
             "d2h_bytes_per_step": (state + small * args.steps) / args.steps,
-            "path": "em2g_set_fields/em2g_set_particles (pinned host), K x "
+            "path": "em2g_set_fields/em2g_set_particles (pinned host, FP64 em2 layout), K x "
                     "(em2g_move_curnt, em2g_fields), em2g_get_fields/em2g_get_particles"}
 
 

@@ -88,6 +88,58 @@ __global__ void k_iota(int32_t *slot, int64_t n) {
   if (j < n) slot[j] = (int32_t)j;
 }
 
+__global__ void k_d2f(const double *__restrict__ a, float *b, int64_t n) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) b[k] = (float)a[k];
+}
+__global__ void k_f2d(const float *__restrict__ a, double *b, int64_t n) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) b[k] = (double)a[k];
+}
+
+bool is_fp32(const em2g_ctx *c) { return c->P.precision == EM2G_FP32; }
+
+// host FP64 arrays [first, first+count) of the field block -> device
+int put_fields_host(em2g_ctx *c, int first, int count, const double *host) {
+  const int64_t n = (int64_t)count * c->g.w;
+  for (int64_t k = 0; k < n; ++k)
+    if (!std::isfinite(host[k])) return fail(EM2G_ERR_NONFINITE, "non-finite field value");
+  if (is_fp32(c)) {
+    std::vector<float> tmp((size_t)n);
+    for (int64_t k = 0; k < n; ++k) tmp[k] = (float)host[k];
+    EM2G_CUDA(cudaMemcpyAsync(c->fld32 + first * c->g.w, tmp.data(), sizeof(float) * n,
+                              cudaMemcpyHostToDevice, c->stream));
+    EM2G_CUDA(cudaStreamSynchronize(c->stream));
+  } else {
+    EM2G_CUDA(cudaMemcpyAsync(c->fld + first * c->g.w, host, sizeof(double) * n,
+                              cudaMemcpyHostToDevice, c->stream));
+    EM2G_CUDA(cudaStreamSynchronize(c->stream));
+  }
+  return EM2G_OK;
+}
+
+int get_fields_host(em2g_ctx *c, int first, int count, double *host) {
+  const int64_t n = (int64_t)count * c->g.w;
+  if (is_fp32(c)) {
+    std::vector<float> tmp((size_t)n);
+    EM2G_CUDA(cudaMemcpyAsync(tmp.data(), c->fld32 + first * c->g.w, sizeof(float) * n,
+                              cudaMemcpyDeviceToHost, c->stream));
+    EM2G_CUDA(cudaStreamSynchronize(c->stream));
+    for (int64_t k = 0; k < n; ++k) host[k] = (double)tmp[k];
+  } else {
+    EM2G_CUDA(cudaMemcpyAsync(host, c->fld + first * c->g.w, sizeof(double) * n,
+                              cudaMemcpyDeviceToHost, c->stream));
+    EM2G_CUDA(cudaStreamSynchronize(c->stream));
+  }
+  return EM2G_OK;
+}
+
+// device staging of 6*n doubles (x, y, vx, vy, vz, gamma) for FP32 contexts
+struct Staging {
+  double *p = nullptr;
+  ~Staging() { cudaFree(p); }
+};
+
 int check_ctx(em2g_ctx *c) {
   if (!c) return fail(EM2G_ERR_INVALID, "null context");
   EM2G_CUDA(cudaSetDevice(c->device));
@@ -173,8 +225,6 @@ int em2g_create(const em2g_params *p, em2g_ctx **out) {
   *out = nullptr;
   int rc = validate(p);
   if (rc) return rc;
-  if (p->precision != EM2G_FP64)
-    return fail(EM2G_ERR_INVALID, "this entry point creates FP64 contexts");
   em2g_ctx *c = new (std::nothrow) em2g_ctx();
   if (!c) return fail(EM2G_ERR_NOMEM, "host allocation failed");
   c->P = *p;
@@ -200,16 +250,28 @@ int em2g_create(const em2g_params *p, em2g_ctx **out) {
     e = cudaMalloc((void **)&(ptr), (bytes));                        \
     if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc " #ptr)); \
   } while (0)
-  ALLOC(c->fld, sizeof(double) * EM2G_NFIELD * w);
-  ALLOC(c->scaled, sizeof(double) * 6 * w * p->nsp);
-  ALLOC(c->smooth_tmp, sizeof(double) * w);
+  const bool fp32 = p->precision == EM2G_FP32;
+  if (fp32) {
+    ALLOC(c->fld32, sizeof(float) * EM2G_NFIELD * w);
+    ALLOC(c->scaled32, sizeof(float) * 6 * w * p->nsp);
+    ALLOC(c->smooth_tmp32, sizeof(float) * w);
+  } else {
+    ALLOC(c->fld, sizeof(double) * EM2G_NFIELD * w);
+    ALLOC(c->scaled, sizeof(double) * 6 * w * p->nsp);
+    ALLOC(c->smooth_tmp, sizeof(double) * w);
+  }
   int64_t maxn = 0;
   for (int s = 0; s < p->nsp; ++s) {
     Species &S = c->sp[s];
     S.cap = p->np_max[s] > 0 ? p->np_max[s] : 1;
     if (S.cap > maxn) maxn = S.cap;
-    ALLOC(S.part, sizeof(double) * 6 * S.cap);
-    ALLOC(S.part_alt, sizeof(double) * 6 * S.cap);
+    if (fp32) {
+      ALLOC(S.p32, sizeof(float) * 5 * S.cap);
+      ALLOC(S.p32_alt, sizeof(float) * 5 * S.cap);
+    } else {
+      ALLOC(S.part, sizeof(double) * 6 * S.cap);
+      ALLOC(S.part_alt, sizeof(double) * 6 * S.cap);
+    }
     ALLOC(S.slot, sizeof(int32_t) * S.cap);
     ALLOC(S.slot_alt, sizeof(int32_t) * S.cap);
   }
@@ -220,17 +282,20 @@ int em2g_create(const em2g_params *p, em2g_ctx **out) {
 #undef ALLOC
   e = cudaMallocHost((void **)&c->host_out, sizeof(double) * 16);
   if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMallocHost"));
-  e = cudaMemset(c->fld, 0, sizeof(double) * EM2G_NFIELD * w);
+  if (fp32)
+    e = cudaMemset(c->fld32, 0, sizeof(float) * EM2G_NFIELD * w);
+  else
+    e = cudaMemset(c->fld, 0, sizeof(double) * EM2G_NFIELD * w);
   if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMemset"));
   e = cudaMemset(c->dev_out, 0, sizeof(double) * 16);
   if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMemset"));
-  rc = cg_init(c);
+  rc = fp32 ? cg_init_f32(c) : cg_init(c);
   if (rc) return bail(rc);
   rc = sort_init(c);
   if (rc) return bail(rc);
   {
-    // the fast push writes one ake partial per block of 64 cells
-    const int64_t fast_blocks = (c->ncell * 4 + 255) / 256;
+    // the fast pushes write one ake partial per block (64 or 32 cells)
+    const int64_t fast_blocks = (c->ncell * 8 + 255) / 256;
     if (fast_blocks > c->red_blocks) {
       cudaFree(c->red);
       c->red_blocks = (int)fast_blocks;
@@ -253,9 +318,14 @@ int em2g_destroy(em2g_ctx *c) {
   cudaFree(c->fld);
   cudaFree(c->scaled);
   cudaFree(c->smooth_tmp);
+  cudaFree(c->fld32);
+  cudaFree(c->scaled32);
+  cudaFree(c->smooth_tmp32);
   for (auto &S : c->sp) {
     cudaFree(S.part);
     cudaFree(S.part_alt);
+    cudaFree(S.p32);
+    cudaFree(S.p32_alt);
     cudaFree(S.slot);
     cudaFree(S.slot_alt);
   }
@@ -288,52 +358,42 @@ int em2g_set_field(em2g_ctx *c, int id, const double *host) {
   int rc = check_ctx(c);
   if (rc) return rc;
   if (id < 0 || id >= EM2G_NFIELD || !host) return fail(EM2G_ERR_INVALID, "bad field id or pointer");
-  for (int64_t k = 0; k < c->g.w; ++k)
-    if (!std::isfinite(host[k])) return fail(EM2G_ERR_NONFINITE, "non-finite field value");
-  EM2G_CUDA(cudaMemcpyAsync(c->fld + id * c->g.w, host, sizeof(double) * c->g.w,
-                            cudaMemcpyHostToDevice, c->stream));
-  EM2G_CUDA(cudaStreamSynchronize(c->stream));
-  return EM2G_OK;
+  return put_fields_host(c, id, 1, host);
 }
 
 int em2g_get_field(em2g_ctx *c, int id, double *host) {
   int rc = check_ctx(c);
   if (rc) return rc;
   if (id < 0 || id >= EM2G_NFIELD || !host) return fail(EM2G_ERR_INVALID, "bad field id or pointer");
-  EM2G_CUDA(cudaMemcpyAsync(host, c->fld + id * c->g.w, sizeof(double) * c->g.w,
-                            cudaMemcpyDeviceToHost, c->stream));
-  EM2G_CUDA(cudaStreamSynchronize(c->stream));
-  return EM2G_OK;
+  return get_fields_host(c, id, 1, host);
 }
 
 int em2g_set_fields(em2g_ctx *c, const double *host13) {
   int rc = check_ctx(c);
   if (rc) return rc;
   if (!host13) return fail(EM2G_ERR_INVALID, "null pointer");
-  const int64_t n = EM2G_NFIELD * c->g.w;
-  for (int64_t k = 0; k < n; ++k)
-    if (!std::isfinite(host13[k])) return fail(EM2G_ERR_NONFINITE, "non-finite field value");
-  EM2G_CUDA(cudaMemcpyAsync(c->fld, host13, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
-  EM2G_CUDA(cudaStreamSynchronize(c->stream));
-  return EM2G_OK;
+  return put_fields_host(c, 0, EM2G_NFIELD, host13);
 }
 
 int em2g_get_fields(em2g_ctx *c, double *host13) {
   int rc = check_ctx(c);
   if (rc) return rc;
   if (!host13) return fail(EM2G_ERR_INVALID, "null pointer");
-  EM2G_CUDA(cudaMemcpyAsync(host13, c->fld, sizeof(double) * EM2G_NFIELD * c->g.w,
-                            cudaMemcpyDeviceToHost, c->stream));
-  EM2G_CUDA(cudaStreamSynchronize(c->stream));
-  return EM2G_OK;
+  return get_fields_host(c, 0, EM2G_NFIELD, host13);
 }
 
 int em2g_set_fields_device(em2g_ctx *c, const double *dev13) {
   int rc = check_ctx(c);
   if (rc) return rc;
   if (!dev13) return fail(EM2G_ERR_INVALID, "null pointer");
-  EM2G_CUDA(cudaMemcpyAsync(c->fld, dev13, sizeof(double) * EM2G_NFIELD * c->g.w,
-                            cudaMemcpyDeviceToDevice, c->stream));
+  const int64_t n = EM2G_NFIELD * c->g.w;
+  if (is_fp32(c)) {
+    k_d2f<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(dev13, c->fld32, n);
+    EM2G_CUDA(cudaGetLastError());
+  } else {
+    EM2G_CUDA(cudaMemcpyAsync(c->fld, dev13, sizeof(double) * n, cudaMemcpyDeviceToDevice,
+                              c->stream));
+  }
   return EM2G_OK;
 }
 
@@ -341,8 +401,14 @@ int em2g_get_fields_device(em2g_ctx *c, double *dev13) {
   int rc = check_ctx(c);
   if (rc) return rc;
   if (!dev13) return fail(EM2G_ERR_INVALID, "null pointer");
-  EM2G_CUDA(cudaMemcpyAsync(dev13, c->fld, sizeof(double) * EM2G_NFIELD * c->g.w,
-                            cudaMemcpyDeviceToDevice, c->stream));
+  const int64_t n = EM2G_NFIELD * c->g.w;
+  if (is_fp32(c)) {
+    k_f2d<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(c->fld32, dev13, n);
+    EM2G_CUDA(cudaGetLastError());
+  } else {
+    EM2G_CUDA(cudaMemcpyAsync(dev13, c->fld, sizeof(double) * n, cudaMemcpyDeviceToDevice,
+                              c->stream));
+  }
   return EM2G_OK;
 }
 
@@ -350,7 +416,10 @@ int em2g_field_device_ptr(em2g_ctx *c, int id, void **dptr) {
   int rc = check_ctx(c);
   if (rc) return rc;
   if (id < 0 || id >= EM2G_NFIELD || !dptr) return fail(EM2G_ERR_INVALID, "bad field id or pointer");
-  *dptr = c->fld + id * c->g.w;
+  if (is_fp32(c))
+    *dptr = c->fld32 + id * c->g.w;
+  else
+    *dptr = c->fld + id * c->g.w;
   return EM2G_OK;
 }
 
@@ -374,6 +443,18 @@ int em2g_set_particles(em2g_ctx *c, int isp, int64_t n, const double *x, const d
       return fail(EM2G_ERR_RANGE, "particle outside the grid at slot " + std::to_string(j));
   }
   const double *src[6] = {x, y, vx, vy, vz, gamma};
+  if (is_fp32(c)) {
+    Staging st;
+    if (n > 0) {
+      EM2G_CUDA(cudaMalloc(&st.p, sizeof(double) * 6 * n));
+      for (int k = 0; k < 6; ++k)
+        EM2G_CUDA(cudaMemcpyAsync(st.p + k * n, src[k], sizeof(double) * n,
+                                  cudaMemcpyHostToDevice, c->stream));
+    }
+    if ((rc = upload_f32(c, isp, st.p, n))) return rc;
+    EM2G_CUDA(cudaStreamSynchronize(c->stream));
+    return EM2G_OK;
+  }
   for (int k = 0; k < 6; ++k)
     if (n > 0)
       EM2G_CUDA(cudaMemcpyAsync(S.part + k * S.cap, src[k], sizeof(double) * n,
@@ -402,15 +483,22 @@ int em2g_set_particles_device(em2g_ctx *c, int isp, int64_t n, const double *x,
   }
   if (!x || !y || !vx || !vy || !vz || !gamma) return fail(EM2G_ERR_INVALID, "null particle array");
   const double *src[6] = {x, y, vx, vy, vz, gamma};
+  Staging st;
+  double *dst = S.part;
+  int64_t ld = S.cap;
+  if (is_fp32(c)) {
+    EM2G_CUDA(cudaMalloc(&st.p, sizeof(double) * 6 * n));
+    dst = st.p;
+    ld = n;
+  }
   for (int k = 0; k < 6; ++k)
-    EM2G_CUDA(cudaMemcpyAsync(S.part + k * S.cap, src[k], sizeof(double) * n,
+    EM2G_CUDA(cudaMemcpyAsync(dst + k * ld, src[k], sizeof(double) * n,
                               cudaMemcpyDeviceToDevice, c->stream));
   unsigned long long *bad = (unsigned long long *)c->red;  // 2 counters
   EM2G_CUDA(cudaMemsetAsync(bad, 0, 2 * sizeof(unsigned long long), c->stream));
   const unsigned nb = (unsigned)((n + 255) / 256);
-  k_check_particles<<<nb, 256, 0, c->stream>>>(S.part, n, S.cap, c->P.nx + 0.5, c->P.ny + 0.5,
-                                                bad);
-  k_iota<<<nb, 256, 0, c->stream>>>(S.slot, n);
+  k_check_particles<<<nb, 256, 0, c->stream>>>(dst, n, ld, c->P.nx + 0.5, c->P.ny + 0.5, bad);
+  if (!is_fp32(c)) k_iota<<<nb, 256, 0, c->stream>>>(S.slot, n);
   EM2G_CUDA(cudaGetLastError());
   unsigned long long hb[2] = {0, 0};
   EM2G_CUDA(cudaMemcpyAsync(hb, bad, sizeof(hb), cudaMemcpyDeviceToHost, c->stream));
@@ -422,6 +510,11 @@ int em2g_set_particles_device(em2g_ctx *c, int isp, int64_t n, const double *x,
   if (hb[0]) {
     S.n = 0;
     return fail(EM2G_ERR_RANGE, std::to_string(hb[0]) + " particles outside the grid");
+  }
+  if (is_fp32(c)) {
+    if ((rc = upload_f32(c, isp, st.p, n))) return rc;
+    EM2G_CUDA(cudaStreamSynchronize(c->stream));
+    return EM2G_OK;
   }
   S.n = n;
   S.sorted = false;
@@ -438,6 +531,17 @@ int em2g_get_particles(em2g_ctx *c, int isp, int64_t *n, double *x, double *y, d
   if (S.n == 0) return EM2G_OK;
   if (!x && !y && !vx && !vy && !vz && !gamma) return EM2G_OK;  // count query
   if (!x || !y || !vx || !vy || !vz || !gamma) return fail(EM2G_ERR_INVALID, "null particle array");
+  if (is_fp32(c)) {
+    Staging st;
+    EM2G_CUDA(cudaMalloc(&st.p, sizeof(double) * 6 * S.n));
+    if ((rc = download_f32(c, isp, st.p))) return rc;
+    double *dst[6] = {x, y, vx, vy, vz, gamma};
+    for (int k = 0; k < 6; ++k)
+      EM2G_CUDA(cudaMemcpyAsync(dst[k], st.p + k * S.n, sizeof(double) * S.n,
+                                cudaMemcpyDeviceToHost, c->stream));
+    EM2G_CUDA(cudaStreamSynchronize(c->stream));
+    return EM2G_OK;
+  }
   k_unsort<<<(unsigned)((S.n + 255) / 256), 256, 0, c->stream>>>(S.part, S.slot, S.part_alt,
                                                                   S.n, S.cap);
   EM2G_CUDA(cudaGetLastError());
@@ -467,6 +571,9 @@ int em2g_get_step(em2g_ctx *c, int *it) {
 int em2g_move(em2g_ctx *c, double *ake_out) {
   int rc = check_ctx(c);
   if (rc) return rc;
+  if (is_fp32(c))
+    return fail(EM2G_ERR_INVALID,
+                "FP32 contexts run move and curnt fused: use em2g_move_curnt or em2g_step");
   for (int s = 0; s < c->P.nsp; ++s) {
     if ((rc = launch_prescale(c, s))) return rc;
     if ((rc = launch_push_f64(c, s, 1))) return rc;
@@ -478,6 +585,11 @@ int em2g_move(em2g_ctx *c, double *ake_out) {
 static int fast_push_all(em2g_ctx *c) {
   int rc;
   for (int s = 0; s < c->P.nsp; ++s) {
+    if (is_fp32(c)) {
+      if ((rc = launch_prescale_f32(c, s))) return rc;
+      if ((rc = launch_push_cells_f32(c, s))) return rc;
+      continue;
+    }
     if (!c->sp[s].sorted && (rc = sort_full(c, s))) return rc;
     if ((rc = launch_prescale(c, s))) return rc;
     if ((rc = launch_push_cells_f64(c, s))) return rc;
@@ -521,6 +633,9 @@ int em2g_reset_counters(em2g_ctx *c) {
 int em2g_curnt(em2g_ctx *c) {
   int rc = check_ctx(c);
   if (rc) return rc;
+  if (is_fp32(c))
+    return fail(EM2G_ERR_INVALID,
+                "FP32 contexts run move and curnt fused: use em2g_move_curnt or em2g_step");
   for (int s = 0; s < c->P.nsp; ++s) {
     if ((rc = launch_push_f64(c, s, 2))) return rc;
     c->sp[s].sorted = false;  // positions moved outside the fast path's bookkeeping
@@ -535,7 +650,8 @@ int em2g_fields(em2g_ctx *c, int it, double *energies_out, int *cg_iters_out) {
   if (rc) return rc;
   EM2G_CUDA(cudaMemsetAsync(c->cg.status, 0, sizeof(int) * 2, c->stream));
   c->it = it;
-  if ((rc = fields_f64(c, it, true, nullptr))) return rc;
+  rc = is_fp32(c) ? fields_f32(c, it, true) : fields_f64(c, it, true, nullptr);
+  if (rc) return rc;
   return finish_outputs(c, nullptr, energies_out, cg_iters_out, it % c->P.isav == 0);
 }
 
@@ -543,7 +659,9 @@ int em2g_smooth2(em2g_ctx *c, int id) {
   int rc = check_ctx(c);
   if (rc) return rc;
   if (id < 0 || id >= EM2G_NFIELD) return fail(EM2G_ERR_INVALID, "bad field id");
-  if ((rc = smooth2_f64(c, c->fld + id * c->g.w))) return rc;
+  rc = is_fp32(c) ? smooth2_f32(c, c->fld32 + id * c->g.w)
+                  : smooth2_f64(c, c->fld + id * c->g.w);
+  if (rc) return rc;
   EM2G_CUDA(cudaStreamSynchronize(c->stream));
   return EM2G_OK;
 }
@@ -557,7 +675,8 @@ int em2g_step(em2g_ctx *c, int nsteps, double *ake_out, double *energies_out,
   for (int k = 0; k < nsteps; ++k) {
     if ((rc = fast_push_all(c))) return rc;
     c->it += 1;
-    if ((rc = fields_f64(c, c->it, true, nullptr))) return rc;
+    rc = is_fp32(c) ? fields_f32(c, c->it, true) : fields_f64(c, c->it, true, nullptr);
+    if (rc) return rc;
   }
   return finish_outputs(c, ake_out, energies_out, cg_iters_out,
                         nsteps > 0 && c->it % c->P.isav == 0);
