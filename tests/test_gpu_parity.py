@@ -274,3 +274,34 @@ def test_drop_in_and_fast_paths_interleave(gpu, oracle_lib):
             assert rel(got[k], st.fld[k]) < TOL, k
         for s in range(2):
             assert rel(g.get_particles(s), st.parts[s]) < 1e-12
+
+
+def test_gpu_restart_through_em2_files(gpu, tmp_path, oracle_lib):
+    """Write em2's restart files from the GPU state after curnt, read them
+    into a new context, run fields as cont does and carry on: the result
+    matches the oracle's straight run within TOL."""
+    from maccpic_b200 import dumpio
+    op, rp, fld, parts = harris_case(nx=64, ny=32, ppc=8)
+    st = oracle_lib.State(op, fld, parts)
+    for it in range(1, 11):
+        st.move()
+        st.curnt()
+        st.fields(it)
+    with make_gpu(rp, fld, parts) as g:
+        for it in range(1, 5):
+            g.move_curnt()
+            g.fields(it)
+        g.move_curnt()
+        dumpio.save(g, str(tmp_path))
+    from maccpic_b200.em2 import Em2Gpu
+    with Em2Gpu(rp) as h:
+        dumpio.load(h, str(tmp_path), [p.shape[1] for p in parts])
+        h.fields(5)
+        for it in range(6, 11):
+            h.move_curnt()
+            h.fields(it)
+        got = h.get_fields()
+        for k in range(6):
+            assert rel(got[k], st.fld[k]) < TOL, k
+        for s in range(2):
+            assert rel(h.get_particles(s), st.parts[s]) < 1e-12
