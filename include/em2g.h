@@ -182,6 +182,19 @@ int em2g_step(em2g_ctx *ctx, int nsteps, double *ake_out, double *energies_out,
 #define EM2G_SMOOTH2_STATIC_MAX_POINTS (1 << 19)
 int em2g_smooth2_static(int nx, int ny, double *dev_array, void *cuda_stream);
 
+/* ---- diagnostics (no counterpart subroutine; FP64 on the GPU) --------
+ * out[0..6)  0.5 * mean over the interior of ex^2, ey^2, ez^2, bx^2, by^2,
+ *            bz^2 of the current fields (em2's exe..bze over the whole grid,
+ *            pic/fields.f90:267-347)
+ * out[6..8)  reconnected flux max(psi) - min(psi) along the centre row of
+ *            the sheet at ny/4 and at 3ny/4, psi = -integral of By dx
+ * out[8..10) mean r^2 of the last Poisson solve before and after the CG
+ *            (the charge-conservation residual (div E - rho)^2 dx^4, and the
+ *            level cgm stopped at, pic/fields.f90:616)
+ * nout values are written (at most EM2G_NDIAG). */
+#define EM2G_NDIAG 10
+int em2g_diagnostics(em2g_ctx *ctx, double *out, int nout);
+
 /* ---- instrumentation ------------------------------------------------- */
 /* kernel launches since the last reset; with timing on, the number of
  * particle-push launches timed with CUDA events and their summed time */

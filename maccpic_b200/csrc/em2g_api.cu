@@ -177,7 +177,7 @@ int validate(const em2g_params *p) {
 
 int finish_outputs(em2g_ctx *c, double *ake_out, double *energies_out, int *cg_iters_out,
                    bool energies_valid) {
-  EM2G_CUDA(cudaMemcpyAsync(c->host_out, c->dev_out, sizeof(double) * 16,
+  EM2G_CUDA(cudaMemcpyAsync(c->host_out, c->dev_out, sizeof(double) * kDevOut,
                             cudaMemcpyDeviceToHost, c->stream));
   int st[2] = {0, 0};
   EM2G_CUDA(cudaMemcpyAsync(st, c->cg.status, sizeof(st), cudaMemcpyDeviceToHost, c->stream));
@@ -278,16 +278,16 @@ int em2g_create(const em2g_params *p, em2g_ctx **out) {
   c->red_blocks = (int)((maxn + 255) / 256);
   if (c->red_blocks < 6 * kEnergyBlocks) c->red_blocks = 6 * kEnergyBlocks;
   ALLOC(c->red, sizeof(double) * c->red_blocks);
-  ALLOC(c->dev_out, sizeof(double) * 16);
+  ALLOC(c->dev_out, sizeof(double) * kDevOut);
 #undef ALLOC
-  e = cudaMallocHost((void **)&c->host_out, sizeof(double) * 16);
+  e = cudaMallocHost((void **)&c->host_out, sizeof(double) * kDevOut);
   if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMallocHost"));
   if (fp32)
     e = cudaMemset(c->fld32, 0, sizeof(float) * EM2G_NFIELD * w);
   else
     e = cudaMemset(c->fld, 0, sizeof(double) * EM2G_NFIELD * w);
   if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMemset"));
-  e = cudaMemset(c->dev_out, 0, sizeof(double) * 16);
+  e = cudaMemset(c->dev_out, 0, sizeof(double) * kDevOut);
   if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMemset"));
   rc = fp32 ? cg_init_f32(c) : cg_init(c);
   if (rc) return bail(rc);
@@ -653,6 +653,17 @@ int em2g_fields(em2g_ctx *c, int it, double *energies_out, int *cg_iters_out) {
   rc = is_fp32(c) ? fields_f32(c, it, true) : fields_f64(c, it, true, nullptr);
   if (rc) return rc;
   return finish_outputs(c, nullptr, energies_out, cg_iters_out, it % c->P.isav == 0);
+}
+
+int em2g_diagnostics(em2g_ctx *c, double *out, int nout) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!out || nout < 1) return fail(EM2G_ERR_INVALID, "null or empty output");
+  if ((rc = diagnostics(c))) return rc;
+  if ((rc = finish_outputs(c, nullptr, nullptr, nullptr, false))) return rc;
+  const int n = nout < EM2G_NDIAG ? nout : EM2G_NDIAG;
+  for (int k = 0; k < n; ++k) out[k] = c->host_out[10 + k];
+  return EM2G_OK;
 }
 
 int em2g_smooth2(em2g_ctx *c, int id) {

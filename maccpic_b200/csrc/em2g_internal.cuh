@@ -11,6 +11,11 @@
 namespace em2g {
 
 constexpr int kEnergyBlocks = 296;  // partial sums per field in the energy reduction
+// small device results, mirrored to pinned host memory after each call:
+// [0,4) ake per species, [4,10) energies at isav steps, [10,16) energies of
+// the current fields, [16,18) reconnected flux of the two sheets, [18,20)
+// mean r^2 of the last Poisson solve before and after the CG
+constexpr int kDevOut = 32;
 
 // Sets the per-thread error message and returns the status (api.cu).
 int fail(int status, const std::string &msg);
@@ -124,6 +129,8 @@ int download_f32(em2g_ctx *c, int isp, double *staging);
 int smooth2_f32(em2g_ctx *c, float *a);
 int cg_init_f32(em2g_ctx *c);
 int fields_f32(em2g_ctx *c, int it, bool want_energies);
+// em2g_diagnostics into dev_out[10..20) (diag.cu)
+int diagnostics(em2g_ctx *c);
 // bracket one push launch with events when timing is on (api.cu)
 int timing_begin(em2g_ctx *c);
 int timing_end(em2g_ctx *c);

@@ -67,6 +67,7 @@ int poisson_t(em2g_ctx *c, T *fld) {
   a.partial = W.partial;
   a.bar = W.bar;
   a.status = W.status;
+  a.res = c->dev_out + 18;
   a.maxits = c->P.cg_maxits;
   a.eps = c->P.cg_eps;
   void *args[] = {&a};

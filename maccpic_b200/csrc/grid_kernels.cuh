@@ -259,6 +259,7 @@ struct CgArgs {
   double *partial;  // [2][gridDim.x]
   unsigned *bar;
   int *status;      // [0] timeout, [1] iterations
+  double *res;      // [0] mean r^2 before the first iteration, [1] at exit
   int maxits;
   double eps;
 };
@@ -281,6 +282,8 @@ __global__ void __launch_bounds__(256) k_cg(CgArgs<T> a) {
   if (threadIdx.x == 0) part0[blockIdx.x] = loc;
   if (!grid_barrier(a.bar, nb, a.status)) return;
   double rr = sum_partials(part0, nb, sh);
+  if (blockIdx.x == 0 && threadIdx.x == 0) a.res[0] = rr / a.nx / a.ny;
+  double r_last = rr;
   int n;
   for (n = 1; n <= a.maxits; ++n) {
     // ap = L p and pap = sum p*ap (pic/fields.f90:559-584)
@@ -316,13 +319,17 @@ __global__ void __launch_bounds__(256) k_cg(CgArgs<T> a) {
     if (threadIdx.x == 0) part0[blockIdx.x] = loc;
     if (!grid_barrier(a.bar, nb, a.status)) return;
     const double r_norm = sum_partials(part0, nb, sh);
+    r_last = r_norm;
     if (r_norm / a.nx / a.ny < a.eps) break;  // pic/fields.f90:616
     const double bk = r_norm / rr;            // pic/fields.f90:632
     for (int64_t k = tid; k < N; k += stride) a.p[k] = (T)(a.r[k] + bk * a.p[k]);
     rr = r_norm;  // next pass's sum of r^2 over the same r, same order
     if (!grid_barrier(a.bar, nb, a.status)) return;
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) a.status[1] = n;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.status[1] = n;
+    a.res[1] = r_last / a.nx / a.ny;
+  }
 }
 
 // ---- energies (pic/fields.f90:267-347): per-block partial sums of a^2 over

@@ -217,6 +217,14 @@ class Em2Gpu:
         check(self._L.em2g_fields(self._h, int(it), _dp(e6), C.byref(n)))
         return n.value, (e6 if it % self.p.isav == 0 else None)
 
+    def diagnostics(self) -> dict:
+        """Field energies of the current fields, reconnected flux of both
+        sheets and the last Poisson residuals (FP64, computed on the GPU)."""
+        out = np.zeros(10)
+        check(self._L.em2g_diagnostics(self._h, _dp(out), 10))
+        return {"energies": out[:6].copy(), "flux": out[6:8].copy(),
+                "poisson_r2_before": out[8], "poisson_r2_after": out[9]}
+
     def smooth2(self, name: str) -> None:
         """pic/smooth.f90:95 on one resident field array."""
         check(self._L.em2g_smooth2(self._h, FIELD_ID[name]))
