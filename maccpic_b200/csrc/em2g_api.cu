@@ -151,6 +151,7 @@ int validate(const em2g_params *p) {
   if (p->struct_size != sizeof(em2g_params))
     return fail(EM2G_ERR_INVALID, "em2g_params.struct_size mismatch (header/library version)");
   if (p->nx < 4 || p->ny < 4) return fail(EM2G_ERR_INVALID, "nx and ny must be >= 4");
+  if (p->ny > 65535) return fail(EM2G_ERR_INVALID, "ny must be <= 65535");
   if ((int64_t)(p->nx + 3) * (p->ny + 3) > (int64_t)1 << 31)
     return fail(EM2G_ERR_INVALID, "grid too large");
   if (p->nsp < 1 || p->nsp > EM2G_MAX_SPECIES)
@@ -294,8 +295,11 @@ int em2g_create(const em2g_params *p, em2g_ctx **out) {
   rc = sort_init(c);
   if (rc) return bail(rc);
   {
-    // the fast pushes write one ake partial per block (64 or 32 cells)
-    const int64_t fast_blocks = (c->ncell * 8 + 255) / 256;
+    // the fast pushes write one ake partial per block of 64 cells (FP64) or
+    // per warp of a 32-cell row segment (FP32)
+    const int64_t f64_parts = (c->ncell * 4 + 255) / 256;
+    const int64_t f32_parts = (int64_t)((c->g.nx + 31) / 32) * c->g.ny * 4;
+    const int64_t fast_blocks = f64_parts > f32_parts ? f64_parts : f32_parts;
     if (fast_blocks > c->red_blocks) {
       cudaFree(c->red);
       c->red_blocks = (int)fast_blocks;

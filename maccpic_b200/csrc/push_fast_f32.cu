@@ -18,21 +18,37 @@
 //   integer nodes (x index cx+1+[f>=1/2]), h = f - [f>=1/2]:
 //                                      s = 3/4 - h^2, s+ = (1/2+h)^2/2,
 //                                      s- = (1/2-h)^2/2
-// and the relativistic Boris rotation on u.  The cell-group register
-// deposit and the fused counting sort are those of push_fast_f64.cu with
-// G = 8 lanes per cell (8 FP32 values = one 32-byte sector).
+// and the relativistic Boris rotation on u.
+//
+// Work layout.  A CTA of 128 threads owns a row segment of 32 cells; 4 lanes
+// own one cell and walk its particles 4 at a time.  The scaled fields the
+// segment's particles can touch (x nodes x0-1 .. x0+35, y nodes y0-1 ..
+// y0+4) are staged once in shared memory as (E, B) pairs of the three
+// staggerings, so a gather is 27 shared float2 loads.  A particle still in
+// the lane's cell adds its rho and J into a 49-value register block (Jx 4x3,
+// Jy 3x4, Jz 3x3, rho 4x4); one that left it deposits with atomics.  At the
+// end of the cell the four blocks are summed with two shuffle levels and added
+// to the arrays once.  Each particle is written to the other buffer grouped
+// by the cell it started the step in (one atomic per group and iteration for
+// the common in-cell case), and the cells of the new positions are counted
+// for the next step's offsets: the counting sort rides along with the push.
 #include "em2g_internal.cuh"
 #include "sort_common.cuh"
 
 namespace em2g {
 namespace {
 
-constexpr int kThreads = 256;
-constexpr int G = 8;
+constexpr int G = 4;               // lanes per cell
+constexpr int TCX = 32;            // cells per CTA (one row segment)
+constexpr int kThreads = TCX * G;  // 128
+constexpr int WX = TCX + 5;        // window columns: x0-1 .. x0+35
+constexpr int WY = 6;              // window rows: y0-1 .. y0+4
+constexpr int kWarps = kThreads / 32;
 
 struct Args32 {
-  const float *__restrict__ aex, *__restrict__ aey, *__restrict__ aez;
-  const float *__restrict__ abx, *__restrict__ aby, *__restrict__ abz;
+  const float2 *__restrict__ ebx;  // (a*Ex, a*Bx): x half, y node staggering
+  const float2 *__restrict__ ebz;  // (a*Ez, a*Bz): x half, y half
+  const float2 *__restrict__ eby;  // (a*Ey, a*By): x node, y half
   float *rho, *jx, *jy, *jz;
   const float *__restrict__ A;  // xr, yr, ux, uy, uz
   const int32_t *__restrict__ slotA;
@@ -48,8 +64,8 @@ struct Args32 {
 };
 
 struct Wts {
-  int i;           // array index of the middle node
-  float m, s, p;   // weights of nodes i-1, i, i+1
+  int i;          // array index of the middle node
+  float m, s, p;  // weights of nodes i-1, i, i+1
 };
 
 __device__ __forceinline__ Wts half_w(int c, float f) {
@@ -64,14 +80,19 @@ __device__ __forceinline__ Wts node_w(int c, float f) {
   return Wts{c + 1 + up, 0.5f * a * a, 0.75f - h * h, 0.5f * b * b};
 }
 
-__device__ __forceinline__ float gather9(const float *__restrict__ A, int nxg, const Wts &wx,
-                                         const Wts &wy) {
-  const float *r0 = A + (int64_t)wy.i * nxg + wx.i;
-  const float *rm = r0 - nxg, *rp = r0 + nxg;
-  const float row_m = __ldg(rm - 1) * wx.m + __ldg(rm) * wx.s + __ldg(rm + 1) * wx.p;
-  const float row_0 = __ldg(r0 - 1) * wx.m + __ldg(r0) * wx.s + __ldg(r0 + 1) * wx.p;
-  const float row_p = __ldg(rp - 1) * wx.m + __ldg(rp) * wx.s + __ldg(rp + 1) * wx.p;
-  return row_m * wy.m + row_0 * wy.s + row_p * wy.p;
+// 9-point gather of an (E, B) pair; base points at node (i-1, j-1) of the
+// stencil in an array of row pitch `pitch`
+__device__ __forceinline__ float2 gather_pair(const float2 *base, int pitch, const Wts &wx,
+                                              const Wts &wy) {
+  float2 r[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const float2 a = base[k * pitch], b = base[k * pitch + 1], c = base[k * pitch + 2];
+    r[k].x = a.x * wx.m + b.x * wx.s + c.x * wx.p;
+    r[k].y = a.y * wx.m + b.y * wx.s + c.y * wx.p;
+  }
+  return make_float2(r[0].x * wy.m + r[1].x * wy.s + r[2].x * wy.p,
+                     r[0].y * wy.m + r[1].y * wy.s + r[2].y * wy.p);
 }
 
 __device__ __forceinline__ void scatter9(float *A, int nxg, const Wts &wx, const Wts &wy,
@@ -103,9 +124,9 @@ __device__ __forceinline__ void spread4(const Wts &w, int c, float o[4]) {
 }
 
 // J of one particle at local offsets (fx, fy) of the group's cell (cx, cy)
-__device__ __forceinline__ void block_add_j(Block32 &b, int cx, int cy, float fx, float fy,
+__device__ __forceinline__ void block_add_j(Block32 &b, int cx, int cy, const Wts &hx,
+                                            const Wts &hy, const Wts &nxw, const Wts &nyw,
                                             float qx, float qy, float qz) {
-  const Wts hx = half_w(cx, fx), hy = half_w(cy, fy), nxw = node_w(cx, fx), nyw = node_w(cy, fy);
   float wxn[4], wyn[4];
   spread4(nxw, cx, wxn);
   spread4(nyw, cy, wyn);
@@ -126,11 +147,11 @@ __device__ __forceinline__ void block_add_j(Block32 &b, int cx, int cy, float fx
   }
 }
 
-__device__ __forceinline__ void block_add_rho(Block32 &b, int cx, int cy, float fx, float fy,
-                                              float q) {
+__device__ __forceinline__ void block_add_rho(Block32 &b, int cx, int cy, const Wts &nxw,
+                                              const Wts &nyw, float q) {
   float wxn[4], wyn[4];
-  spread4(node_w(cx, fx), cx, wxn);
-  spread4(node_w(cy, fy), cy, wyn);
+  spread4(nxw, cx, wxn);
+  spread4(nyw, cy, wyn);
 #pragma unroll
   for (int r = 0; r < 4; ++r) {
     const float t = wyn[r] * q;
@@ -139,39 +160,54 @@ __device__ __forceinline__ void block_add_rho(Block32 &b, int cx, int cy, float 
   }
 }
 
-__device__ __forceinline__ void deposit_j_atomic(const Args32 &a, int cx, int cy, float fx,
-                                                 float fy, float qx, float qy, float qz) {
-  const Wts hx = half_w(cx, fx), hy = half_w(cy, fy), nxw = node_w(cx, fx), nyw = node_w(cy, fy);
+__device__ __forceinline__ void deposit_j_atomic(const Args32 &a, const Wts &hx, const Wts &hy,
+                                                 const Wts &nxw, const Wts &nyw, float qx,
+                                                 float qy, float qz) {
   scatter9(a.jx, a.nxg, hx, nyw, qx);
   scatter9(a.jz, a.nxg, hx, hy, qz);
   scatter9(a.jy, a.nxg, nxw, hy, qy);
 }
 
 __device__ __forceinline__ float group_sum(float v) {
-#pragma unroll
-  for (int o = 1; o < G; o <<= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  v += __shfl_xor_sync(0xffffffffu, v, 1);
+  v += __shfl_xor_sync(0xffffffffu, v, 2);
   return v;
 }
 
 __device__ __forceinline__ void flush_one(float *A, int nxg, int ix, int iy, float v, int e,
                                           int gl) {
-  if ((e % G) == gl && v != 0.0f) atomicAdd(A + (int64_t)iy * nxg + ix, v);
+  if ((e & (G - 1)) == gl && v != 0.0f) atomicAdd(A + (int64_t)iy * nxg + ix, v);
 }
 
 __device__ __forceinline__ int floor_small(float f) { return f < 0.0f ? -1 : (f >= 1.0f ? 1 : 0); }
 
+__device__ __forceinline__ int wrap(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
+
 __global__ void __launch_bounds__(kThreads) k_push_cells_f32(Args32 a) {
-  const int lane = threadIdx.x & 31;
-  const int gl = lane & (G - 1);
-  const int64_t cell = ((int64_t)blockIdx.x * kThreads + threadIdx.x) / G;
-  const int64_t ncell = (int64_t)a.nx * a.ny;
-  const bool valid = cell < ncell;
-  const int kx = valid ? (int)(cell % a.nx) : 0;
-  const int ky = valid ? (int)(cell / a.nx) : 0;
+  __shared__ float2 win[3][WY][WX];
+  const int nx = a.nx, ny = a.ny, nxg = a.nxg;
+  const int x0 = blockIdx.x * TCX, y0 = blockIdx.y;
+  // stage the segment's (E, B) window: array indices x0-1.., y0-1..
+  for (int t = threadIdx.x; t < 3 * WY * WX; t += kThreads) {
+    const int comp = t / (WY * WX), r = (t / WX) % WY, col = t % WX;
+    const int gx = x0 - 1 + col, gy = y0 - 1 + r;
+    float2 v = make_float2(0.f, 0.f);
+    if (gx >= 0 && gx <= nx + 2 && gy >= 0 && gy <= ny + 2) {
+      const float2 *src = comp == 0 ? a.ebx : (comp == 1 ? a.ebz : a.eby);
+      v = src[(int64_t)gy * nxg + gx];
+    }
+    win[comp][r][col] = v;
+  }
+  __syncthreads();
+
+  const int lane = threadIdx.x & 31, gl = lane & (G - 1);
+  const int kx = x0 + (int)(threadIdx.x / G), ky = y0;
+  const bool valid = kx < nx;
+  const int64_t cell = (int64_t)ky * nx + kx;
   const int32_t beg = valid ? a.offA[cell] : 0;
   const int32_t end = valid ? a.offA[cell + 1] : 0;
   const int64_t cap = a.cap;
-  const int nxg = a.nxg, nx = a.nx, ny = a.ny;
+  const unsigned gmask = 0xFu << (lane & ~(G - 1));  // this lane's group in the warp
 
   Block32 b;
 #pragma unroll
@@ -184,34 +220,68 @@ __global__ void __launch_bounds__(kThreads) k_push_cells_f32(Args32 a) {
       if (r < 3 && k < 3) b.jz[r][k] = 0.0f;
     }
   double akel = 0.0;
+  int stay_new = 0;  // particles of this lane whose new position is in cell k
 
-  for (int32_t i = beg + gl;; i += G) {
+  // software pipeline: the next particle's state is loaded while this one runs
+  int32_t i = beg + gl;
+  float pxr = 0.f, pyr = 0.f, pux = 0.f, puy = 0.f, puz = 0.f;
+  int32_t pslot = 0;
+  if (i < end) {
+    pxr = a.A[i];
+    pyr = a.A[cap + i];
+    pux = a.A[2 * cap + i];
+    puy = a.A[3 * cap + i];
+    puz = a.A[4 * cap + i];
+    pslot = a.slotA[i];
+  }
+  for (;; i += G) {
     const bool active = i < end;
     const unsigned am = __ballot_sync(0xffffffffu, active);
     if (am == 0u) break;
+    const float xr = pxr, yr = pyr;
+    float ux = pux, uy = puy, uz = puz;
+    const int32_t slot = pslot;
+    const int32_t inext = i + G;
+    if (inext < end) {
+      pxr = a.A[inext];
+      pyr = a.A[cap + inext];
+      pux = a.A[2 * cap + inext];
+      puy = a.A[3 * cap + inext];
+      puz = a.A[4 * cap + inext];
+      pslot = a.slotA[inext];
+    }
+    bool in_cell_old = false;
+    int key_cur = 0;
     if (active) {
-      const float xr = a.A[i], yr = a.A[cap + i];
-      float ux = a.A[2 * cap + i], uy = a.A[3 * cap + i], uz = a.A[4 * cap + i];
-      const int32_t slot = a.slotA[i];
-      // the cell the particle is in now, and its offsets in that cell
+      // the cell the particle is in now (it may have left cell k last step)
       const int ox = floor_small(xr), oy = floor_small(yr);
-      int cx = kx + ox, cy = ky + oy;
-      cx = cx < 0 ? cx + nx : (cx >= nx ? cx - nx : cx);
-      cy = cy < 0 ? cy + ny : (cy >= ny ? cy - ny : cy);
+      const int cxu = kx + ox, cyu = ky + oy;  // unwrapped
+      const int cx = wrap(cxu, nx), cy = wrap(cyu, ny);
       const float fx = xr - (float)ox, fy = yr - (float)oy;
-      const int key_cur = cy * nx + cx;
-      // gather (pic/move.f90:76-148) with the scaled fields
+      key_cur = cy * nx + cx;
+      in_cell_old = (ox == 0) && (oy == 0);
       const Wts hx = half_w(cx, fx), hy = half_w(cy, fy), nxw = node_w(cx, fx),
                 nyw = node_w(cy, fy);
-      const float ex = gather9(a.aex, nxg, hx, nyw), bx = gather9(a.abx, nxg, hx, nyw);
-      const float ez = gather9(a.aez, nxg, hx, hy), bz = gather9(a.abz, nxg, hx, hy);
-      const float ey = gather9(a.aey, nxg, nxw, hy), by = gather9(a.aby, nxg, nxw, hy);
+      // gather from the shared window when the stencil is inside it (always,
+      // unless the particle wrapped around the box); else from global memory
+      float2 ebx, ebz, eby;
+      if (cxu == cx && cyu == cy && cx >= x0 - 1 && cx <= x0 + TCX && cy >= y0 - 1 &&
+          cy <= y0 + 1) {
+        const int c0 = cx - x0 + 1, r0 = cy - y0 + 1;  // window index of node (cx, cy)
+        ebx = gather_pair(&win[0][r0 + nyw.i - cy - 1][c0 + hx.i - cx - 1], WX, hx, nyw);
+        ebz = gather_pair(&win[1][r0 + hy.i - cy - 1][c0 + hx.i - cx - 1], WX, hx, hy);
+        eby = gather_pair(&win[2][r0 + hy.i - cy - 1][c0 + nxw.i - cx - 1], WX, nxw, hy);
+      } else {
+        ebx = gather_pair(a.ebx + (int64_t)(nyw.i - 1) * nxg + hx.i - 1, nxg, hx, nyw);
+        ebz = gather_pair(a.ebz + (int64_t)(hy.i - 1) * nxg + hx.i - 1, nxg, hx, hy);
+        eby = gather_pair(a.eby + (int64_t)(hy.i - 1) * nxg + nxw.i - 1, nxg, nxw, hy);
+      }
       // relativistic Boris on u (pic/move.f90:176-203)
-      float gx = ux + ex, gy = uy + ey, gz = uz + ez;
+      const float gx = ux + ebx.x, gy = uy + eby.x, gz = uz + ebz.x;
       const float gm = sqrtf(1.0f + gx * gx + gy * gy + gz * gz);
       akel += (double)gm - 1.0;
       const float dcg = 1.0f / (a.c * gm);
-      float tx = dcg * bx, ty = dcg * by, tz = dcg * bz;
+      float tx = dcg * ebx.y, ty = dcg * eby.y, tz = dcg * ebz.y;
       const float vvx = gx + gy * tz - gz * ty;
       const float vvy = gy + gz * tx - gx * tz;
       const float vvz = gz + gx * ty - gy * tx;
@@ -219,47 +289,59 @@ __global__ void __launch_bounds__(kThreads) k_push_cells_f32(Args32 a) {
       tx *= f2;
       ty *= f2;
       tz *= f2;
-      ux = gx + vvy * tz - vvz * ty + ex;
-      uy = gy + vvz * tx - vvx * tz + ey;
-      uz = gz + vvx * ty - vvy * tx + ez;
+      ux = gx + vvy * tz - vvz * ty + ebx.x;
+      uy = gy + vvz * tx - vvx * tz + eby.x;
+      uz = gz + vvx * ty - vvy * tx + ebz.x;
       const float ginv = 1.0f / sqrtf(1.0f + ux * ux + uy * uy + uz * uz);
       const float vx = ux * ginv, vy = uy * ginv, vz = uz * ginv;
       const float qx = a.qd * vx, qy = a.qd * vy, qz = a.qd * vz;
       // jm at the old position (pic/curnt.f90:53-132)
-      const bool in_old = (cx == kx) && (cy == ky);
-      if (in_old)
-        block_add_j(b, cx, cy, fx, fy, qx, qy, qz);
+      if (in_cell_old)
+        block_add_j(b, cx, cy, hx, hy, nxw, nyw, qx, qy, qz);
       else
-        deposit_j_atomic(a, cx, cy, fx, fy, qx, qy, qz);
+        deposit_j_atomic(a, hx, hy, nxw, nyw, qx, qy, qz);
       // move (pic/curnt.f90:181-194), relative to the start cell
       const float mx = fmaf(vx, a.dtdx, fx), my = fmaf(vy, a.dtdy, fy);
       const int nox = floor_small(mx), noy = floor_small(my);
-      int ncx = cx + nox, ncy = cy + noy;
-      ncx = ncx < 0 ? ncx + nx : (ncx >= nx ? ncx - nx : ncx);
-      ncy = ncy < 0 ? ncy + ny : (ncy >= ny ? ncy - ny : ncy);
+      const int ncx = wrap(cx + nox, nx), ncy = wrap(cy + noy, ny);
       const float nfx = mx - (float)nox, nfy = my - (float)noy;
+      const Wts nhx = half_w(ncx, nfx), nhy = half_w(ncy, nfy), nnx = node_w(ncx, nfx),
+                nny = node_w(ncy, nfy);
       // rho and jp at the new position (pic/curnt.f90:197-303)
-      const bool in_new = (ncx == kx) && (ncy == ky);
-      if (in_new) {
-        block_add_rho(b, ncx, ncy, nfx, nfy, a.qd);
-        block_add_j(b, ncx, ncy, nfx, nfy, qx, qy, qz);
+      if (ncx == kx && ncy == ky) {
+        block_add_rho(b, ncx, ncy, nnx, nny, a.qd);
+        block_add_j(b, ncx, ncy, nhx, nhy, nnx, nny, qx, qy, qz);
+        ++stay_new;
       } else {
-        const Wts nx2 = node_w(ncx, nfx), ny2 = node_w(ncy, nfy);
-        scatter9(a.rho, nxg, nx2, ny2, a.qd);
-        deposit_j_atomic(a, ncx, ncy, nfx, nfy, qx, qy, qz);
+        scatter9(a.rho, nxg, nnx, nny, a.qd);
+        deposit_j_atomic(a, nhx, nhy, nnx, nny, qx, qy, qz);
+        atomicAdd(a.cnt_next + ncy * nx + ncx, 1);
       }
-      // write back grouped by the start cell, position relative to it
-      const int64_t pos = (int64_t)a.offB[key_cur] + agg_atomic_add(a.cursor, key_cur, am);
+      // write back grouped by the start cell, position relative to it; the
+      // in-cell lanes of a group share one cursor update
+      const unsigned inm = __ballot_sync(am, in_cell_old) & gmask;
+      int64_t pos;
+      if (in_cell_old) {
+        const int leader = __ffs(inm) - 1;
+        int base = 0;
+        if (lane == leader) base = atomicAdd(a.cursor + key_cur, __popc(inm));
+        base = __shfl_sync(inm, base, leader);
+        pos = (int64_t)a.offB[key_cur] + base + __popc(inm & ((1u << lane) - 1u));
+      } else {
+        pos = (int64_t)a.offB[key_cur] + atomicAdd(a.cursor + key_cur, 1);
+      }
       a.B[pos] = mx;
       a.B[cap + pos] = my;
       a.B[2 * cap + pos] = ux;
       a.B[3 * cap + pos] = uy;
       a.B[4 * cap + pos] = uz;
       a.slotB[pos] = slot;
-      agg_atomic_add(a.cnt_next, ncy * nx + ncx, am);
     }
   }
 
+  // the group's new-position counts for cell k, and its register blocks
+  const int stay = group_sum((float)stay_new) + 0.5f;
+  if (valid && gl == 0 && stay > 0) atomicAdd(a.cnt_next + cell, stay);
   if (__any_sync(0xffffffffu, valid && end > beg)) {
     int e = 0;
 #pragma unroll
@@ -295,29 +377,21 @@ __global__ void __launch_bounds__(kThreads) k_push_cells_f32(Args32 a) {
         ++e;
       }
   }
-
-  __shared__ double red[kThreads / 32];
+  // per-warp partial of sum(gamma - 1); no block barrier at the end
   for (int o = 16; o > 0; o >>= 1) akel += __shfl_down_sync(0xffffffffu, akel, o);
-  if (lane == 0) red[threadIdx.x >> 5] = akel;
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    double v = threadIdx.x < kThreads / 32 ? red[threadIdx.x] : 0.0;
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    if (threadIdx.x == 0) a.ake_partial[blockIdx.x] = v;
-  }
+  const int64_t blk = (int64_t)blockIdx.y * gridDim.x + blockIdx.x;
+  if (lane == 0) a.ake_partial[blk * kWarps + (threadIdx.x >> 5)] = akel;
 }
 
-// E and B times ae = 0.5*qm*dt/c into FP32 copies (pic/move.f90:52-64)
-__global__ void k_prescale_f32(const float *__restrict__ fld, float *__restrict__ s, int64_t w,
+// E and B times ae = 0.5*qm*dt/c into (E, B) pairs of the three staggerings
+// (pic/move.f90:52-64)
+__global__ void k_prescale_f32(const float *__restrict__ fld, float2 *__restrict__ s, int64_t w,
                                float ae, float tx, float ty) {
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= w) return;
-  s[k] = ae * fld[EM2G_EX * w + k];
-  s[w + k] = ae * fld[EM2G_EY * w + k];
-  s[2 * w + k] = ae * fld[EM2G_EZ * w + k];
-  s[3 * w + k] = ae * fld[EM2G_BX * w + k] + tx;
-  s[4 * w + k] = ae * fld[EM2G_BY * w + k] + ty;
-  s[5 * w + k] = ae * fld[EM2G_BZ * w + k];
+  s[k] = make_float2(ae * fld[EM2G_EX * w + k], ae * fld[EM2G_BX * w + k] + tx);
+  s[w + k] = make_float2(ae * fld[EM2G_EZ * w + k], ae * fld[EM2G_BZ * w + k]);
+  s[2 * w + k] = make_float2(ae * fld[EM2G_EY * w + k], ae * fld[EM2G_BY * w + k] + ty);
 }
 
 // FP64 (x, y, vx, vy, vz, gamma) staging -> histogram of cells
@@ -384,8 +458,8 @@ int launch_prescale_f32(em2g_ctx *c, int isp) {
   const double ae = 0.5 * c->P.qm[isp] * c->P.dt / c->P.c;
   const int64_t w = c->g.w;
   k_prescale_f32<<<(unsigned)((w + 255) / 256), 256, 0, c->stream>>>(
-      c->fld32, c->scaled32 + (int64_t)isp * 6 * w, w, (float)ae, (float)c->P.tx[isp],
-      (float)c->P.ty[isp]);
+      c->fld32, reinterpret_cast<float2 *>(c->scaled32 + (int64_t)isp * 6 * w), w, (float)ae,
+      (float)c->P.tx[isp], (float)c->P.ty[isp]);
   c->launches += 1;
   EM2G_CUDA(cudaGetLastError());
   return EM2G_OK;
@@ -394,14 +468,11 @@ int launch_prescale_f32(em2g_ctx *c, int isp) {
 int launch_push_cells_f32(em2g_ctx *c, int isp) {
   Species &S = c->sp[isp];
   const int64_t w = c->g.w;
-  const float *sc = c->scaled32 + (int64_t)isp * 6 * w;
+  const float2 *sc = reinterpret_cast<const float2 *>(c->scaled32 + (int64_t)isp * 6 * w);
   Args32 a;
-  a.aex = sc;
-  a.aey = sc + w;
-  a.aez = sc + 2 * w;
-  a.abx = sc + 3 * w;
-  a.aby = sc + 4 * w;
-  a.abz = sc + 5 * w;
+  a.ebx = sc;
+  a.ebz = sc + w;
+  a.eby = sc + 2 * w;
   a.rho = c->fld32 + EM2G_RHO * w;
   a.jx = c->fld32 + EM2G_JXM * w;
   a.jy = c->fld32 + EM2G_JYM * w;
@@ -423,15 +494,16 @@ int launch_push_cells_f32(em2g_ctx *c, int isp) {
   a.dtdy = (float)(c->P.dt / c->P.dy);
   a.c = (float)c->P.c;
   a.ake_partial = c->red;
-  const int64_t nb64 = (c->ncell * G + kThreads - 1) / kThreads;
-  if (nb64 > c->red_blocks) return fail(EM2G_ERR_RANGE, "grid exceeds reduction scratch");
-  const int nb = (int)nb64;
+  const dim3 grid((unsigned)((c->g.nx + TCX - 1) / TCX), (unsigned)c->g.ny);
+  const int64_t nparts = (int64_t)grid.x * grid.y * kWarps;
+  if (nparts > c->red_blocks) return fail(EM2G_ERR_RANGE, "grid exceeds reduction scratch");
+  const int nb = (int)nparts;
   int rc = scan_cells(c, S.cnt, S.off_alt);
   if (rc) return rc;
   EM2G_CUDA(cudaMemsetAsync(S.cursor, 0, sizeof(int32_t) * c->ncell, c->stream));
   EM2G_CUDA(cudaMemsetAsync(S.cnt_alt, 0, sizeof(int32_t) * c->ncell, c->stream));
   if ((rc = timing_begin(c))) return rc;
-  k_push_cells_f32<<<nb, kThreads, 0, c->stream>>>(a);
+  k_push_cells_f32<<<grid, kThreads, 0, c->stream>>>(a);
   c->launches += 1;
   EM2G_CUDA(cudaGetLastError());
   if ((rc = timing_end(c))) return rc;

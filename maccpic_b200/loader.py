@@ -99,6 +99,8 @@ PRESETS = {
     "harris_256x128_ppc16": HarrisConfig(),
     "harris_2048x1024_ppc64": HarrisConfig(nx=2048, ny=1024, ppc=64, steps=1000),
     "harris_512x256_ppc32": HarrisConfig(nx=512, ny=256, ppc=32, steps=800),
+    # profiling size: particle buffers (0.4-0.8 GB) well above the 126 MB L2
+    "harris_1024x512_ppc32": HarrisConfig(nx=1024, ny=512, ppc=32, steps=100),
     "harris_4096x2048_ppc100": HarrisConfig(nx=4096, ny=2048, ppc=100, mass_ratio=100.0,
                                             dt=0.04, steps=2000),
 }
