@@ -297,7 +297,7 @@ int em2g_create(const em2g_params *p, em2g_ctx **out) {
   {
     // the fast pushes write one ake partial per block of 64 cells (FP64) or
     // per warp of a 32-cell row segment (FP32)
-    const int64_t f64_parts = (c->ncell * 4 + 255) / 256;
+    const int64_t f64_parts = (int64_t)((c->g.nx + 31) / 32) * c->g.ny * 4;
     const int64_t f32_parts = (int64_t)((c->g.nx + 31) / 32) * c->g.ny * 4;
     const int64_t fast_blocks = f64_parts > f32_parts ? f64_parts : f32_parts;
     if (fast_blocks > c->red_blocks) {
@@ -595,8 +595,7 @@ static int fast_push_all(em2g_ctx *c) {
       continue;
     }
     if (!c->sp[s].sorted && (rc = sort_full(c, s))) return rc;
-    if ((rc = launch_prescale(c, s))) return rc;
-    if ((rc = launch_push_cells_f64(c, s))) return rc;
+    if ((rc = launch_push_cells_f64(c, s))) return rc;  // prescales into pairs itself
   }
   return EM2G_OK;
 }

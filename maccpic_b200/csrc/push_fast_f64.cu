@@ -3,9 +3,10 @@
 //
 // Layout: each species' particles are ordered by the row-major key of the
 // cell they occupied when the previous step began; cell k's particles sit at
-// [off[k], off[k+1]) (sort.cu).  A group of G lanes owns one cell k and
-// walks its particles G at a time (adjacent lanes read adjacent particles,
-// adjacent groups adjacent cells).
+// [off[k], off[k+1]) (sort.cu).  A CTA of 128 threads owns a row segment of
+// 32 cells; a group of 4 lanes owns one cell and walks its particles 4 at a
+// time.  The scaled E and B the segment's particles can touch are staged once
+// in shared memory as (E, B) double pairs of the three staggerings.
 //
 // Per particle the arithmetic is the reference's (push_common.cuh, compiled
 // with -fmad=false): gather + Boris (pic/move.f90), jm at the old position,
@@ -31,11 +32,15 @@ namespace {
 
 using namespace f64;
 
-constexpr int kThreads = 256;
-constexpr int G = 4;  // lanes per cell
+constexpr int G = 4;               // lanes per cell
+constexpr int TCX = 32;            // cells per CTA (one row segment)
+constexpr int kThreads = TCX * G;  // 128
+constexpr int WX = TCX + 5;        // window columns: array x0-1 .. x0+35
+constexpr int WY = 6;              // window rows: array y0-1 .. y0+4
+constexpr int kWarps = kThreads / 32;
 
 struct FastArgs {
-  Scaled S;
+  const double2 *__restrict__ ebx, *__restrict__ ebz, *__restrict__ eby;
   double *rho, *jx, *jy, *jz;  // deposit targets (jx = jxm, ...)
   const double *__restrict__ A;
   const int32_t *__restrict__ slotA;
@@ -50,6 +55,21 @@ struct FastArgs {
   double c, qd, dt, dx, dy, xn, yn;
   double *ake_partial;
 };
+
+// pic/move.f90:95-97 on an (E, B) pair: the nine products summed in the
+// reference's order (ix,iy) (ix,iyp) (ix,iym) (ixp,iy) (ixp,iyp) (ixp,iym)
+// (ixm,iy) (ixm,iyp) (ixm,iym); `m` points at node (ix-1, iy-1)
+__device__ __forceinline__ double2 gather_pair(const double2 *m, int pitch, const W9 &w) {
+  const double2 *r0 = m + pitch + 1;  // (ix, iy)
+  const double2 a = r0[0], b = r0[pitch], c = r0[-pitch], d = r0[1], e = r0[pitch + 1],
+                f = r0[-pitch + 1], g = r0[-1], h = r0[pitch - 1], k = r0[-pitch - 1];
+  double2 o;
+  o.x = a.x * w.q + b.x * w.qyp + c.x * w.qym + d.x * w.qxp + e.x * w.qxpyp + f.x * w.qxpym +
+        g.x * w.qxm + h.x * w.qxmyp + k.x * w.qxmym;
+  o.y = a.y * w.q + b.y * w.qyp + c.y * w.qym + d.y * w.qxp + e.y * w.qxpyp + f.y * w.qxpym +
+        g.y * w.qxm + h.y * w.qxmyp + k.y * w.qxmym;
+  return o;
+}
 
 // 4-entry weight vector of a node-staggered axis relative to the cell:
 // offset o = i-1-cell in {0,1}; the three weights land at o, o+1, o+2.
@@ -116,29 +136,41 @@ __device__ __forceinline__ void block_add_rho(Block &b, double x, double y, int 
 }
 
 __device__ __forceinline__ double group_sum(double v) {
-#pragma unroll
-  for (int o = 1; o < G; o <<= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  v += __shfl_xor_sync(0xffffffffu, v, 1);
+  v += __shfl_xor_sync(0xffffffffu, v, 2);
   return v;
 }
 
 // flush entry e of the block (all lanes hold the group sum) if it is mine
 __device__ __forceinline__ void flush_one(double *A, int nxg, int ix, int iy, double v, int e,
                                           int gl) {
-  if ((e % G) == gl && v != 0.0) atomicAdd(A + (int64_t)iy * nxg + ix, v);
+  if ((e & (G - 1)) == gl && v != 0.0) atomicAdd(A + (int64_t)iy * nxg + ix, v);
 }
 
 __global__ void __launch_bounds__(kThreads) k_push_cells_f64(FastArgs a) {
-  const int lane = threadIdx.x & 31;
-  const int gl = lane & (G - 1);
-  const int64_t cell = ((int64_t)blockIdx.x * kThreads + threadIdx.x) / G;
-  const int64_t ncell = (int64_t)a.nx * a.ny;
-  const bool valid = cell < ncell;
-  const int cx = valid ? (int)(cell % a.nx) : 0;
-  const int cy = valid ? (int)(cell / a.nx) : 0;
+  __shared__ double2 win[3][WY][WX];
+  const int nx = a.nx, ny = a.ny, nxg = a.nxg;
+  const int x0 = blockIdx.x * TCX, y0 = blockIdx.y;
+  for (int t = threadIdx.x; t < 3 * WY * WX; t += kThreads) {
+    const int comp = t / (WY * WX), r = (t / WX) % WY, col = t % WX;
+    const int gx = x0 - 1 + col, gy = y0 - 1 + r;
+    double2 v = make_double2(0.0, 0.0);
+    if (gx >= 0 && gx <= nx + 2 && gy >= 0 && gy <= ny + 2) {
+      const double2 *src = comp == 0 ? a.ebx : (comp == 1 ? a.ebz : a.eby);
+      v = src[(int64_t)gy * nxg + gx];
+    }
+    win[comp][r][col] = v;
+  }
+  __syncthreads();
+
+  const int lane = threadIdx.x & 31, gl = lane & (G - 1);
+  const int cx = x0 + (int)(threadIdx.x / G), cy = y0;
+  const bool valid = cx < nx;
+  const int64_t cell = (int64_t)cy * nx + cx;
   const int32_t beg = valid ? a.offA[cell] : 0;
   const int32_t end = valid ? a.offA[cell + 1] : 0;
   const int64_t cap = a.cap;
-  const int nxg = a.nxg;
+  const unsigned gmask = 0xFu << (lane & ~(G - 1));
 
   Block b;
 #pragma unroll
@@ -151,49 +183,114 @@ __global__ void __launch_bounds__(kThreads) k_push_cells_f64(FastArgs a) {
       if (r < 3 && k < 3) b.jz[r][k] = 0.0;
     }
   double akel = 0.0;
+  int stay_new = 0;
 
   for (int32_t i = beg + gl;; i += G) {
     const bool active = i < end;
     const unsigned am = __ballot_sync(0xffffffffu, active);
     if (am == 0u) break;
     if (active) {
-    double x = a.A[i], y = a.A[cap + i];
-    double vx = a.A[2 * cap + i], vy = a.A[3 * cap + i], vz = a.A[4 * cap + i];
-    double g = a.A[5 * cap + i];
-    const int32_t slot = a.slotA[i];
-    const int key_cur = cell_key(x, y, a.nx, a.ny);
-    const bool in_old = ((int)x == cx) && ((int)y == cy);
-    akel += gather_boris(a.S, nxg, a.c, x, y, vx, vy, vz, g) - 1.0;
-    // jm at the old position
-    if (in_old)
-      block_add_j(b, x, y, cx, cy, a.qd, vx, vy, vz);
-    else
-      deposit_j_atomic(a.jx, a.jy, a.jz, nxg, x, y, a.qd, vx, vy, vz);
-    move_wrap(x, y, vx, vy, a.dt, a.dx, a.dy, a.xn, a.yn);
-    // rho and jp at the new position
-    const bool in_new = ((int)x == cx) && ((int)y == cy);
-    if (in_new) {
-      block_add_rho(b, x, y, cx, cy, a.qd);
-      block_add_j(b, x, y, cx, cy, a.qd, vx, vy, vz);
-    } else {
-      deposit_rho_atomic(a.rho, nxg, x, y, a.qd);
-      deposit_j_atomic(a.jx, a.jy, a.jz, nxg, x, y, a.qd, vx, vy, vz);
-    }
-    // write back, grouped by the cell of the start of this step
-    const int64_t pos = (int64_t)a.offB[key_cur] + agg_atomic_add(a.cursor, key_cur, am);
-    a.B[pos] = x;
-    a.B[cap + pos] = y;
-    a.B[2 * cap + pos] = vx;
-    a.B[3 * cap + pos] = vy;
-    a.B[4 * cap + pos] = vz;
-    a.B[5 * cap + pos] = g;
-    a.slotB[pos] = slot;
-    // counts of the cells the particles now occupy (next step's offsets)
-    agg_atomic_add(a.cnt_next, cell_key(x, y, a.nx, a.ny), am);
+      double x = a.A[i], y = a.A[cap + i];
+      double vx = a.A[2 * cap + i], vy = a.A[3 * cap + i], vz = a.A[4 * cap + i];
+      double g = a.A[5 * cap + i];
+      const int32_t slot = a.slotA[i];
+      const int key_cur = cell_key(x, y, nx, ny);
+      const int pcx = (int)x, pcy = (int)y;  // the particle's cell, unwrapped
+      const bool in_old = (pcx == cx) && (pcy == cy);
+      // gather + Boris (pic/move.f90:76-203), fields from the shared window
+      // when the stencil lies inside it, else from global memory
+      {
+        int ixh, ixn, iyh, iyn;
+        double sxh, sxhp, sxhm, sxn, sxnp, sxnm, syh, syhp, syhm, syn, synp, synm;
+        w_half(x, ixh, sxh, sxhp, sxhm);
+        w_node(y, iyn, syn, synp, synm);
+        w_half(y, iyh, syh, syhp, syhm);
+        w_node(x, ixn, sxn, sxnp, sxnm);
+        const W9 wxn = weights(sxh, sxhp, sxhm, syn, synp, synm);  // Ex, Bx
+        const W9 wzz = weights(sxh, sxhp, sxhm, syh, syhp, syhm);  // Ez, Bz
+        const W9 wyy = weights(sxn, sxnp, sxnm, syh, syhp, syhm);  // Ey, By
+        double2 pex, pez, pey;
+        if (pcx >= x0 - 1 && pcx <= x0 + TCX && pcy >= y0 - 1 && pcy <= y0 + 1) {
+          pex = gather_pair(&win[0][iyn - y0][ixh - x0], WX, wxn);
+          pez = gather_pair(&win[1][iyh - y0][ixh - x0], WX, wzz);
+          pey = gather_pair(&win[2][iyh - y0][ixn - x0], WX, wyy);
+        } else {
+          pex = gather_pair(a.ebx + (int64_t)(iyn - 1) * nxg + ixh - 1, nxg, wxn);
+          pez = gather_pair(a.ebz + (int64_t)(iyh - 1) * nxg + ixh - 1, nxg, wzz);
+          pey = gather_pair(a.eby + (int64_t)(iyh - 1) * nxg + ixn - 1, nxg, wyy);
+        }
+        const double aexpt = pex.x, aeypt = pey.x, aezpt = pez.x;
+        double abxpt = pex.y, abypt = pey.y, abzpt = pez.y;
+        double gvxs = vx * g + aexpt;
+        double gvys = vy * g + aeypt;
+        double gvzs = vz * g + aezpt;
+        double gm = sqrt(1.0 + gvxs * gvxs + gvys * gvys + gvzs * gvzs);
+        akel += gm - 1.0;
+        const double dcg = 1.0 / (a.c * gm);
+        abxpt = dcg * abxpt;
+        abypt = dcg * abypt;
+        abzpt = dcg * abzpt;
+        const double vvx = gvxs + gvys * abzpt - gvzs * abypt;
+        const double vvy = gvys + gvzs * abxpt - gvxs * abzpt;
+        const double vvz = gvzs + gvxs * abypt - gvys * abxpt;
+        const double f = 2.0 / (1.0 + abxpt * abxpt + abypt * abypt + abzpt * abzpt);
+        abxpt = f * abxpt;
+        abypt = f * abypt;
+        abzpt = f * abzpt;
+        gvxs = gvxs + vvy * abzpt - vvz * abypt + aexpt;
+        gvys = gvys + vvz * abxpt - vvx * abzpt + aeypt;
+        gvzs = gvzs + vvx * abypt - vvy * abxpt + aezpt;
+        gm = sqrt(1.0 + gvxs * gvxs + gvys * gvys + gvzs * gvzs);
+        g = gm;
+        vx = gvxs / gm;
+        vy = gvys / gm;
+        vz = gvzs / gm;
+      }
+      // jm at the old position
+      if (in_old)
+        block_add_j(b, x, y, cx, cy, a.qd, vx, vy, vz);
+      else
+        deposit_j_atomic(a.jx, a.jy, a.jz, nxg, x, y, a.qd, vx, vy, vz);
+      move_wrap(x, y, vx, vy, a.dt, a.dx, a.dy, a.xn, a.yn);
+      // rho and jp at the new position
+      if (((int)x == cx) && ((int)y == cy)) {
+        block_add_rho(b, x, y, cx, cy, a.qd);
+        block_add_j(b, x, y, cx, cy, a.qd, vx, vy, vz);
+        ++stay_new;
+      } else {
+        deposit_rho_atomic(a.rho, nxg, x, y, a.qd);
+        deposit_j_atomic(a.jx, a.jy, a.jz, nxg, x, y, a.qd, vx, vy, vz);
+        atomicAdd(a.cnt_next + cell_key(x, y, nx, ny), 1);
+      }
+      // write back grouped by the cell of the start of this step; the lanes
+      // of a group that started in cell k share one cursor update
+      const bool home = key_cur == (int)cell;
+      const unsigned inm = __ballot_sync(am, home) & gmask;
+      int64_t pos;
+      if (home) {
+        const int leader = __ffs(inm) - 1;
+        int base = 0;
+        if (lane == leader) base = atomicAdd(a.cursor + key_cur, __popc(inm));
+        base = __shfl_sync(inm, base, leader);
+        pos = (int64_t)a.offB[key_cur] + base + __popc(inm & ((1u << lane) - 1u));
+      } else {
+        pos = (int64_t)a.offB[key_cur] + atomicAdd(a.cursor + key_cur, 1);
+      }
+      a.B[pos] = x;
+      a.B[cap + pos] = y;
+      a.B[2 * cap + pos] = vx;
+      a.B[3 * cap + pos] = vy;
+      a.B[4 * cap + pos] = vz;
+      a.B[5 * cap + pos] = g;
+      a.slotB[pos] = slot;
     }
   }
 
-  // sum the group's blocks and add them to the arrays once
+  // this cell's count of new positions, then the register blocks
+  int stay = stay_new;
+  stay += __shfl_xor_sync(0xffffffffu, stay, 1);
+  stay += __shfl_xor_sync(0xffffffffu, stay, 2);
+  if (valid && gl == 0 && stay > 0) atomicAdd(a.cnt_next + cell, stay);
   if (__any_sync(0xffffffffu, valid && end > beg)) {
     int e = 0;
 #pragma unroll
@@ -229,17 +326,21 @@ __global__ void __launch_bounds__(kThreads) k_push_cells_f64(FastArgs a) {
         ++e;
       }
   }
-
-  // block sum of (gamma - 1) in a fixed order
-  __shared__ double red[kThreads / 32];
+  // per-warp partial of sum(gamma - 1); no block barrier at the end
   for (int o = 16; o > 0; o >>= 1) akel += __shfl_down_sync(0xffffffffu, akel, o);
-  if (lane == 0) red[threadIdx.x >> 5] = akel;
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    double v = threadIdx.x < kThreads / 32 ? red[threadIdx.x] : 0.0;
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    if (threadIdx.x == 0) a.ake_partial[blockIdx.x] = v;
-  }
+  const int64_t blk = (int64_t)blockIdx.y * gridDim.x + blockIdx.x;
+  if (lane == 0) a.ake_partial[blk * kWarps + (threadIdx.x >> 5)] = akel;
+}
+
+// pic/move.f90:52-64: E and B times ae = 0.5*qm*dt/c (plus tx/ty), stored
+// as (E, B) pairs of the three staggerings
+__global__ void k_prescale_pairs(const double *__restrict__ fld, double2 *__restrict__ s,
+                                 int64_t w, double ae, double tx, double ty) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= w) return;
+  s[k] = make_double2(ae * fld[EM2G_EX * w + k], ae * fld[EM2G_BX * w + k] + tx);
+  s[w + k] = make_double2(ae * fld[EM2G_EZ * w + k], ae * fld[EM2G_BZ * w + k]);
+  s[2 * w + k] = make_double2(ae * fld[EM2G_EY * w + k], ae * fld[EM2G_BY * w + k] + ty);
 }
 
 }  // namespace
@@ -247,9 +348,17 @@ __global__ void __launch_bounds__(kThreads) k_push_cells_f64(FastArgs a) {
 int launch_push_cells_f64(em2g_ctx *c, int isp) {
   Species &S = c->sp[isp];
   const int64_t w = c->g.w;
-  const double *sc = c->scaled + (int64_t)isp * 6 * w;
+  double2 *sc = reinterpret_cast<double2 *>(c->scaled + (int64_t)isp * 6 * w);
+  const double ae = 0.5 * c->P.qm[isp] * c->P.dt / c->P.c;  // pic/move.f90:42
+  k_prescale_pairs<<<(unsigned)((w + 255) / 256), 256, 0, c->stream>>>(c->fld, sc, w, ae,
+                                                                        c->P.tx[isp],
+                                                                        c->P.ty[isp]);
+  c->launches += 1;
+  EM2G_CUDA(cudaGetLastError());
   FastArgs a;
-  a.S = Scaled{sc, sc + w, sc + 2 * w, sc + 3 * w, sc + 4 * w, sc + 5 * w};
+  a.ebx = sc;
+  a.ebz = sc + w;
+  a.eby = sc + 2 * w;
   a.rho = c->fld + EM2G_RHO * w;
   a.jx = c->fld + EM2G_JXM * w;
   a.jy = c->fld + EM2G_JYM * w;
@@ -274,16 +383,16 @@ int launch_push_cells_f64(em2g_ctx *c, int isp) {
   a.xn = (double)c->P.nx;
   a.yn = (double)c->P.ny;
   a.ake_partial = c->red;
-  const int64_t nb64 = (c->ncell * G + kThreads - 1) / kThreads;
-  if (nb64 > c->red_blocks) return fail(EM2G_ERR_RANGE, "grid exceeds reduction scratch");
-  const int nb = (int)nb64;
+  const dim3 grid((unsigned)((c->g.nx + TCX - 1) / TCX), (unsigned)c->g.ny);
+  const int64_t nparts = (int64_t)grid.x * grid.y * kWarps;
+  if (nparts > c->red_blocks) return fail(EM2G_ERR_RANGE, "grid exceeds reduction scratch");
   // offsets of B from the counts of the current cells; fresh counters
   int rc = scan_cells(c, S.cnt, S.off_alt);
   if (rc) return rc;
   EM2G_CUDA(cudaMemsetAsync(S.cursor, 0, sizeof(int32_t) * c->ncell, c->stream));
   EM2G_CUDA(cudaMemsetAsync(S.cnt_alt, 0, sizeof(int32_t) * c->ncell, c->stream));
   if ((rc = timing_begin(c))) return rc;
-  k_push_cells_f64<<<nb, kThreads, 0, c->stream>>>(a);
+  k_push_cells_f64<<<grid, kThreads, 0, c->stream>>>(a);
   c->launches += 1;
   EM2G_CUDA(cudaGetLastError());
   if ((rc = timing_end(c))) return rc;
@@ -292,7 +401,7 @@ int launch_push_cells_f64(em2g_ctx *c, int isp) {
   std::swap(S.slot, S.slot_alt);
   std::swap(S.off, S.off_alt);
   std::swap(S.cnt, S.cnt_alt);
-  return launch_ake_finish(c, isp, nb);
+  return launch_ake_finish(c, isp, (int)nparts);
 }
 
 }  // namespace em2g
