@@ -195,6 +195,16 @@ int em2g_smooth2_static(int nx, int ny, double *dev_array, void *cuda_stream);
 #define EM2G_NDIAG 10
 int em2g_diagnostics(em2g_ctx *ctx, double *out, int nout);
 
+/* ---- kernel variants (no counterpart in the reference) ---------------
+ * The fast push comes in a few compiled variants -- cells per CTA (tile
+ * width) times the CTAs per SM the register allocation allows.  All give the
+ * same results; their speed depends on grid, density and GPU.
+ * maccpic_b200/autotune.py times them on the live state and keeps the best. */
+int em2g_num_variants(em2g_ctx *ctx, int *n);
+int em2g_set_variant(em2g_ctx *ctx, int variant);
+/* current variant and its name (name may be NULL) */
+int em2g_get_variant(em2g_ctx *ctx, int *variant, char *name, int name_len);
+
 /* ---- instrumentation ------------------------------------------------- */
 /* kernel launches since the last reset; with timing on, the number of
  * particle-push launches timed with CUDA events and their summed time */

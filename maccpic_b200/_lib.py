@@ -30,7 +30,8 @@ EXPORTS = [
     "em2g_get_fields_device", "em2g_field_device_ptr", "em2g_move", "em2g_curnt",
     "em2g_fields", "em2g_smooth2", "em2g_step", "em2g_set_particles_device",
     "em2g_move_curnt", "em2g_set_timing", "em2g_get_counters", "em2g_reset_counters",
-    "em2g_smooth2_static", "em2g_diagnostics",
+    "em2g_smooth2_static", "em2g_diagnostics", "em2g_num_variants", "em2g_set_variant",
+    "em2g_get_variant",
 ]
 
 
@@ -104,6 +105,9 @@ def lib() -> C.CDLL:
         "em2g_reset_counters": (C.c_int, [ctx]),
         "em2g_smooth2_static": (C.c_int, [C.c_int, C.c_int, vp, vp]),
         "em2g_diagnostics": (C.c_int, [ctx, dp, C.c_int]),
+        "em2g_num_variants": (C.c_int, [ctx, ip]),
+        "em2g_set_variant": (C.c_int, [ctx, C.c_int]),
+        "em2g_get_variant": (C.c_int, [ctx, ip, C.c_char_p, C.c_int]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

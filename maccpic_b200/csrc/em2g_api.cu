@@ -297,9 +297,8 @@ int em2g_create(const em2g_params *p, em2g_ctx **out) {
   {
     // the fast pushes write one ake partial per block of 64 cells (FP64) or
     // per warp of a 32-cell row segment (FP32)
-    const int64_t f64_parts = (int64_t)((c->g.nx + 31) / 32) * c->g.ny * 4;
-    const int64_t f32_parts = (int64_t)((c->g.nx + 31) / 32) * c->g.ny * 4;
-    const int64_t fast_blocks = f64_parts > f32_parts ? f64_parts : f32_parts;
+    // (ceil(nx/tcx) * ny CTAs of tcx*4/32 warps, tcx in {32, 64})
+    const int64_t fast_blocks = (int64_t)((c->g.nx + 31) / 32) * c->g.ny * 4 + 64;
     if (fast_blocks > c->red_blocks) {
       cudaFree(c->red);
       c->red_blocks = (int)fast_blocks;
@@ -605,6 +604,35 @@ int em2g_move_curnt(em2g_ctx *c, double *ake_out) {
   if (rc) return rc;
   if ((rc = fast_push_all(c))) return rc;
   return finish_outputs(c, ake_out, nullptr, nullptr, false);
+}
+
+int em2g_num_variants(em2g_ctx *c, int *n) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!n) return fail(EM2G_ERR_INVALID, "null pointer");
+  *n = is_fp32(c) ? num_variants_f32() : num_variants_f64();
+  return EM2G_OK;
+}
+
+int em2g_set_variant(em2g_ctx *c, int v) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  const int n = is_fp32(c) ? num_variants_f32() : num_variants_f64();
+  if (v < 0 || v >= n) return fail(EM2G_ERR_INVALID, "variant out of range");
+  c->variant = v;
+  return EM2G_OK;
+}
+
+int em2g_get_variant(em2g_ctx *c, int *v, char *name, int name_len) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (v) *v = c->variant;
+  if (name && name_len > 0) {
+    const char *s = is_fp32(c) ? variant_name_f32(c->variant) : variant_name_f64(c->variant);
+    std::strncpy(name, s, (size_t)name_len - 1);
+    name[name_len - 1] = '\0';
+  }
+  return EM2G_OK;
 }
 
 int em2g_set_timing(em2g_ctx *c, int on) {

@@ -96,6 +96,7 @@ struct em2g_ctx {
   // CUDA-event time of the particle-push launches
   int64_t launches = 0;
   int32_t *scan_tmp = nullptr;  // block sums of the cell scans
+  int variant = 0;              // fast-push kernel variant (em2g_set_variant)
   int64_t ncell = 0;
   int timing = 0;
   std::vector<cudaEvent_t> ev;  // start/stop pairs of the pending push launches
@@ -121,6 +122,11 @@ int sort_full(em2g_ctx *c, int isp);
 int scan_cells(em2g_ctx *c, const int32_t *cnt, int32_t *off);
 // one fast-path push of species isp (push_fast_f64.cu)
 int launch_push_cells_f64(em2g_ctx *c, int isp);
+// fast-push variants (tile width x occupancy) for the autotuner
+int num_variants_f64();
+const char *variant_name_f64(int v);
+int num_variants_f32();
+const char *variant_name_f32(int v);
 // mixed-precision path (push_fast_f32.cu, fields_f32.cu)
 int launch_prescale_f32(em2g_ctx *c, int isp);
 int launch_push_cells_f32(em2g_ctx *c, int isp);

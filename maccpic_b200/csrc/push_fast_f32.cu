@@ -29,8 +29,9 @@
 // Jy 3x4, Jz 3x3, rho 4x4); one that left it deposits with atomics.  At the
 // end of the cell the four blocks are summed with two shuffle levels and added
 // to the arrays once.  Each particle is written to the other buffer grouped
-// by the cell it started the step in (one atomic per group and iteration for
-// the common in-cell case), and the cells of the new positions are counted
+// by the cell it started the step in, its position relative to that cell
+// (front slots by a running count for the common in-cell case, back slots by
+// an atomic for the rest), and the cells of the new positions are counted
 // for the next step's offsets: the counting sort rides along with the push.
 #include "em2g_internal.cuh"
 #include "sort_common.cuh"
@@ -38,12 +39,8 @@
 namespace em2g {
 namespace {
 
-constexpr int G = 4;               // lanes per cell
-constexpr int TCX = 32;            // cells per CTA (one row segment)
-constexpr int kThreads = TCX * G;  // 128
-constexpr int WX = TCX + 5;        // window columns: x0-1 .. x0+35
-constexpr int WY = 6;              // window rows: y0-1 .. y0+4
-constexpr int kWarps = kThreads / 32;
+constexpr int G = 4;   // lanes per cell
+constexpr int WY = 6;  // window rows: y0-1 .. y0+4
 
 struct Args32 {
   const float2 *__restrict__ ebx;  // (a*Ex, a*Bx): x half, y node staggering
@@ -183,7 +180,12 @@ __device__ __forceinline__ int floor_small(float f) { return f < 0.0f ? -1 : (f 
 
 __device__ __forceinline__ int wrap(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
 
-__global__ void __launch_bounds__(kThreads) k_push_cells_f32(Args32 a) {
+// TCX cells per CTA (a row segment), MINB: CTAs per SM the register
+// allocation must allow (the autotuner's two knobs)
+template <int TCX, int MINB>
+__global__ void __launch_bounds__(TCX * G, MINB) k_push_cells_f32(Args32 a) {
+  constexpr int kThreads = TCX * G;
+  constexpr int WX = TCX + 5;  // window columns: x0-1 .. x0+TCX+3
   __shared__ float2 win[3][WY][WX];
   const int nx = a.nx, ny = a.ny, nxg = a.nxg;
   const int x0 = blockIdx.x * TCX, y0 = blockIdx.y;
@@ -221,6 +223,7 @@ __global__ void __launch_bounds__(kThreads) k_push_cells_f32(Args32 a) {
     }
   double akel = 0.0;
   int stay_new = 0;  // particles of this lane whose new position is in cell k
+  int home_count = 0;  // particles of this group written to the front of cell k
 
   // software pipeline: the next particle's state is loaded while this one runs
   int32_t i = beg + gl;
@@ -317,19 +320,17 @@ __global__ void __launch_bounds__(kThreads) k_push_cells_f32(Args32 a) {
         deposit_j_atomic(a, nhx, nhy, nnx, nny, qx, qy, qz);
         atomicAdd(a.cnt_next + ncy * nx + ncx, 1);
       }
-      // write back grouped by the start cell, position relative to it; the
-      // in-cell lanes of a group share one cursor update
+      // write back grouped by the cell of the start of this step: particles
+      // that started it in cell k take the next slots from the front of k's
+      // segment in processing order (a running count per group, no atomics);
+      // the few that came from another cell's range fill it from the back
       const unsigned inm = __ballot_sync(am, in_cell_old) & gmask;
       int64_t pos;
-      if (in_cell_old) {
-        const int leader = __ffs(inm) - 1;
-        int base = 0;
-        if (lane == leader) base = atomicAdd(a.cursor + key_cur, __popc(inm));
-        base = __shfl_sync(inm, base, leader);
-        pos = (int64_t)a.offB[key_cur] + base + __popc(inm & ((1u << lane) - 1u));
-      } else {
-        pos = (int64_t)a.offB[key_cur] + atomicAdd(a.cursor + key_cur, 1);
-      }
+      if (in_cell_old)
+        pos = (int64_t)a.offB[key_cur] + home_count + __popc(inm & ((1u << lane) - 1u));
+      else
+        pos = (int64_t)a.offB[key_cur + 1] - 1 - atomicAdd(a.cursor + key_cur, 1);
+      home_count += __popc(inm);
       a.B[pos] = mx;
       a.B[cap + pos] = my;
       a.B[2 * cap + pos] = ux;
@@ -380,8 +381,21 @@ __global__ void __launch_bounds__(kThreads) k_push_cells_f32(Args32 a) {
   // per-warp partial of sum(gamma - 1); no block barrier at the end
   for (int o = 16; o > 0; o >>= 1) akel += __shfl_down_sync(0xffffffffu, akel, o);
   const int64_t blk = (int64_t)blockIdx.y * gridDim.x + blockIdx.x;
-  if (lane == 0) a.ake_partial[blk * kWarps + (threadIdx.x >> 5)] = akel;
+  if (lane == 0) a.ake_partial[blk * (kThreads / 32) + (threadIdx.x >> 5)] = akel;
 }
+
+struct Variant32 {
+  const char *name;
+  int tcx;
+  void (*kernel)(Args32);
+};
+const Variant32 kVariants32[] = {
+    {"f32 tcx32 minb4", 32, k_push_cells_f32<32, 4>},
+    {"f32 tcx32 minb5", 32, k_push_cells_f32<32, 5>},
+    {"f32 tcx32 minb6", 32, k_push_cells_f32<32, 6>},
+    {"f32 tcx64 minb2", 64, k_push_cells_f32<64, 2>},
+    {"f32 tcx64 minb3", 64, k_push_cells_f32<64, 3>},
+};
 
 // E and B times ae = 0.5*qm*dt/c into (E, B) pairs of the three staggerings
 // (pic/move.f90:52-64)
@@ -454,6 +468,9 @@ __global__ void k_gather_from_f32(const float *__restrict__ P, const int32_t *__
 
 }  // namespace
 
+int num_variants_f32() { return (int)(sizeof(kVariants32) / sizeof(kVariants32[0])); }
+const char *variant_name_f32(int v) { return kVariants32[v].name; }
+
 int launch_prescale_f32(em2g_ctx *c, int isp) {
   const double ae = 0.5 * c->P.qm[isp] * c->P.dt / c->P.c;
   const int64_t w = c->g.w;
@@ -494,8 +511,10 @@ int launch_push_cells_f32(em2g_ctx *c, int isp) {
   a.dtdy = (float)(c->P.dt / c->P.dy);
   a.c = (float)c->P.c;
   a.ake_partial = c->red;
-  const dim3 grid((unsigned)((c->g.nx + TCX - 1) / TCX), (unsigned)c->g.ny);
-  const int64_t nparts = (int64_t)grid.x * grid.y * kWarps;
+  const Variant32 &V = kVariants32[c->variant < num_variants_f32() ? c->variant : 0];
+  const int threads = V.tcx * G;
+  const dim3 grid((unsigned)((c->g.nx + V.tcx - 1) / V.tcx), (unsigned)c->g.ny);
+  const int64_t nparts = (int64_t)grid.x * grid.y * (threads / 32);
   if (nparts > c->red_blocks) return fail(EM2G_ERR_RANGE, "grid exceeds reduction scratch");
   const int nb = (int)nparts;
   int rc = scan_cells(c, S.cnt, S.off_alt);
@@ -503,7 +522,7 @@ int launch_push_cells_f32(em2g_ctx *c, int isp) {
   EM2G_CUDA(cudaMemsetAsync(S.cursor, 0, sizeof(int32_t) * c->ncell, c->stream));
   EM2G_CUDA(cudaMemsetAsync(S.cnt_alt, 0, sizeof(int32_t) * c->ncell, c->stream));
   if ((rc = timing_begin(c))) return rc;
-  k_push_cells_f32<<<grid, kThreads, 0, c->stream>>>(a);
+  V.kernel<<<grid, threads, 0, c->stream>>>(a);
   c->launches += 1;
   EM2G_CUDA(cudaGetLastError());
   if ((rc = timing_end(c))) return rc;

@@ -32,12 +32,8 @@ namespace {
 
 using namespace f64;
 
-constexpr int G = 4;               // lanes per cell
-constexpr int TCX = 32;            // cells per CTA (one row segment)
-constexpr int kThreads = TCX * G;  // 128
-constexpr int WX = TCX + 5;        // window columns: array x0-1 .. x0+35
-constexpr int WY = 6;              // window rows: array y0-1 .. y0+4
-constexpr int kWarps = kThreads / 32;
+constexpr int G = 4;   // lanes per cell
+constexpr int WY = 6;  // window rows: array y0-1 .. y0+4
 
 struct FastArgs {
   const double2 *__restrict__ ebx, *__restrict__ ebz, *__restrict__ eby;
@@ -147,7 +143,12 @@ __device__ __forceinline__ void flush_one(double *A, int nxg, int ix, int iy, do
   if ((e & (G - 1)) == gl && v != 0.0) atomicAdd(A + (int64_t)iy * nxg + ix, v);
 }
 
-__global__ void __launch_bounds__(kThreads) k_push_cells_f64(FastArgs a) {
+// TCX cells per CTA (a row segment), MINB: CTAs per SM the register
+// allocation must allow (the autotuner's two knobs)
+template <int TCX, int MINB>
+__global__ void __launch_bounds__(TCX * G, MINB) k_push_cells_f64(FastArgs a) {
+  constexpr int kThreads = TCX * G;
+  constexpr int WX = TCX + 5;  // window columns: array x0-1 .. x0+TCX+3
   __shared__ double2 win[3][WY][WX];
   const int nx = a.nx, ny = a.ny, nxg = a.nxg;
   const int x0 = blockIdx.x * TCX, y0 = blockIdx.y;
@@ -184,6 +185,7 @@ __global__ void __launch_bounds__(kThreads) k_push_cells_f64(FastArgs a) {
     }
   double akel = 0.0;
   int stay_new = 0;
+  int home_count = 0;  // particles of this group written to the front of cell k
 
   for (int32_t i = beg + gl;; i += G) {
     const bool active = i < end;
@@ -262,20 +264,18 @@ __global__ void __launch_bounds__(kThreads) k_push_cells_f64(FastArgs a) {
         deposit_j_atomic(a.jx, a.jy, a.jz, nxg, x, y, a.qd, vx, vy, vz);
         atomicAdd(a.cnt_next + cell_key(x, y, nx, ny), 1);
       }
-      // write back grouped by the cell of the start of this step; the lanes
-      // of a group that started in cell k share one cursor update
       const bool home = key_cur == (int)cell;
+      // write back grouped by the cell of the start of this step: particles
+      // that started it in cell k take the next slots from the front of k's
+      // segment in processing order (a running count per group, no atomics);
+      // the few that came from another cell's range fill it from the back
       const unsigned inm = __ballot_sync(am, home) & gmask;
       int64_t pos;
-      if (home) {
-        const int leader = __ffs(inm) - 1;
-        int base = 0;
-        if (lane == leader) base = atomicAdd(a.cursor + key_cur, __popc(inm));
-        base = __shfl_sync(inm, base, leader);
-        pos = (int64_t)a.offB[key_cur] + base + __popc(inm & ((1u << lane) - 1u));
-      } else {
-        pos = (int64_t)a.offB[key_cur] + atomicAdd(a.cursor + key_cur, 1);
-      }
+      if (home)
+        pos = (int64_t)a.offB[key_cur] + home_count + __popc(inm & ((1u << lane) - 1u));
+      else
+        pos = (int64_t)a.offB[key_cur + 1] - 1 - atomicAdd(a.cursor + key_cur, 1);
+      home_count += __popc(inm);
       a.B[pos] = x;
       a.B[cap + pos] = y;
       a.B[2 * cap + pos] = vx;
@@ -329,8 +329,19 @@ __global__ void __launch_bounds__(kThreads) k_push_cells_f64(FastArgs a) {
   // per-warp partial of sum(gamma - 1); no block barrier at the end
   for (int o = 16; o > 0; o >>= 1) akel += __shfl_down_sync(0xffffffffu, akel, o);
   const int64_t blk = (int64_t)blockIdx.y * gridDim.x + blockIdx.x;
-  if (lane == 0) a.ake_partial[blk * kWarps + (threadIdx.x >> 5)] = akel;
+  if (lane == 0) a.ake_partial[blk * (kThreads / 32) + (threadIdx.x >> 5)] = akel;
 }
+
+struct Variant64 {
+  const char *name;
+  int tcx;
+  void (*kernel)(FastArgs);
+};
+const Variant64 kVariants64[] = {
+    {"f64 tcx32 minb1", 32, k_push_cells_f64<32, 1>},
+    {"f64 tcx32 minb2", 32, k_push_cells_f64<32, 2>},
+    {"f64 tcx64 minb1", 64, k_push_cells_f64<64, 1>},
+};
 
 // pic/move.f90:52-64: E and B times ae = 0.5*qm*dt/c (plus tx/ty), stored
 // as (E, B) pairs of the three staggerings
@@ -344,6 +355,9 @@ __global__ void k_prescale_pairs(const double *__restrict__ fld, double2 *__rest
 }
 
 }  // namespace
+
+int num_variants_f64() { return (int)(sizeof(kVariants64) / sizeof(kVariants64[0])); }
+const char *variant_name_f64(int v) { return kVariants64[v].name; }
 
 int launch_push_cells_f64(em2g_ctx *c, int isp) {
   Species &S = c->sp[isp];
@@ -383,8 +397,10 @@ int launch_push_cells_f64(em2g_ctx *c, int isp) {
   a.xn = (double)c->P.nx;
   a.yn = (double)c->P.ny;
   a.ake_partial = c->red;
-  const dim3 grid((unsigned)((c->g.nx + TCX - 1) / TCX), (unsigned)c->g.ny);
-  const int64_t nparts = (int64_t)grid.x * grid.y * kWarps;
+  const Variant64 &V = kVariants64[c->variant < num_variants_f64() ? c->variant : 0];
+  const int threads = V.tcx * G;
+  const dim3 grid((unsigned)((c->g.nx + V.tcx - 1) / V.tcx), (unsigned)c->g.ny);
+  const int64_t nparts = (int64_t)grid.x * grid.y * (threads / 32);
   if (nparts > c->red_blocks) return fail(EM2G_ERR_RANGE, "grid exceeds reduction scratch");
   // offsets of B from the counts of the current cells; fresh counters
   int rc = scan_cells(c, S.cnt, S.off_alt);
@@ -392,7 +408,7 @@ int launch_push_cells_f64(em2g_ctx *c, int isp) {
   EM2G_CUDA(cudaMemsetAsync(S.cursor, 0, sizeof(int32_t) * c->ncell, c->stream));
   EM2G_CUDA(cudaMemsetAsync(S.cnt_alt, 0, sizeof(int32_t) * c->ncell, c->stream));
   if ((rc = timing_begin(c))) return rc;
-  k_push_cells_f64<<<grid, kThreads, 0, c->stream>>>(a);
+  V.kernel<<<grid, threads, 0, c->stream>>>(a);
   c->launches += 1;
   EM2G_CUDA(cudaGetLastError());
   if ((rc = timing_end(c))) return rc;

@@ -162,6 +162,21 @@ class Em2Gpu:
         handle = getattr(stream, "cuda_stream", stream)
         check(self._L.em2g_set_stream(self._h, C.c_void_p(handle or 0)))
 
+    def num_variants(self) -> int:
+        n = C.c_int()
+        check(self._L.em2g_num_variants(self._h, C.byref(n)))
+        return n.value
+
+    def set_variant(self, v: int) -> None:
+        check(self._L.em2g_set_variant(self._h, int(v)))
+
+    def variant(self):
+        """(index, name) of the fast-push kernel variant in use."""
+        v = C.c_int()
+        buf = C.create_string_buffer(64)
+        check(self._L.em2g_get_variant(self._h, C.byref(v), buf, 64))
+        return v.value, buf.value.decode()
+
     def set_timing(self, on: bool) -> None:
         check(self._L.em2g_set_timing(self._h, int(bool(on))))
 

@@ -84,3 +84,25 @@ def test_fp32_rejects_split_move_curnt(gpu):
         with pytest.raises(Em2gError) as ei:
             g.move()
         assert ei.value.status == ERR_INVALID
+
+
+def test_fp32_variants_agree(gpu):
+    """All FP32 push variants give the same fields to FP32 rounding."""
+    from maccpic_b200.em2 import Em2Gpu
+    op, rp, fld, parts = harris(nx=128, ny=32, ppc=8)
+    outs = []
+    with Em2Gpu(rp) as probe:
+        n = probe.num_variants()
+    for v in range(n):
+        with Em2Gpu(rp) as g:
+            g.set_variant(v)
+            g.set_fields(fld)
+            for s, p in enumerate(parts):
+                g.set_particles(s, p)
+            for _ in range(5):
+                g.step(1)
+            outs.append(g.get_fields())
+    for v in range(1, n):
+        for k in range(6):
+            err = np.abs(outs[v][k] - outs[0][k]).max() / np.abs(outs[0][k]).max()
+            assert err < 1e-4, (v, k, err)

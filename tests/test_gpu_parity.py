@@ -305,3 +305,26 @@ def test_gpu_restart_through_em2_files(gpu, tmp_path, oracle_lib):
             assert rel(got[k], st.fld[k]) < TOL, k
         for s in range(2):
             assert rel(h.get_particles(s), st.parts[s]) < 1e-12
+
+
+def test_every_push_variant_matches_the_oracle(gpu, oracle_lib):
+    """The autotuner's kernel variants compute the same step."""
+    from maccpic_b200.em2 import Em2Gpu
+    op, rp, fld, parts = harris_case(nx=96, ny=32, ppc=8)
+    st = oracle_lib.State(op, fld, parts)
+    for _ in range(6):
+        st.step()
+    with Em2Gpu(rp) as probe:
+        n = probe.num_variants()
+    assert n >= 2
+    for v in range(n):
+        with make_gpu(rp, fld, parts) as g:
+            g.set_variant(v)
+            assert g.variant()[0] == v
+            for _ in range(6):
+                g.step(1)
+            got = g.get_fields()
+            for k in range(6):
+                assert rel(got[k], st.fld[k]) < TOL, (v, k)
+            for s in range(2):
+                assert rel(g.get_particles(s), st.parts[s]) < 1e-12, v
