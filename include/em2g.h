@@ -87,7 +87,10 @@ typedef struct em2g_params {
   double qme, wpe;       /* -1, 1 (pic/input.f90:43) */
   int32_t device;        /* CUDA device ordinal */
   int32_t sort_interval; /* reserved, set 0 (the fast path re-sorts every step) */
-  int32_t reserved[16];
+  int32_t smooth_current; /* 1: smooth2 each current array after the fold, every
+                             step (not in em2, which filters only rho and, every
+                             isav steps, E and B); 0 = em2 */
+  int32_t reserved[15];
 } em2g_params;
 
 typedef struct em2g_ctx em2g_ctx;

@@ -49,7 +49,7 @@ class Em2gParams(C.Structure):
         ("cg_maxits", C.c_int32), ("energy_mode", C.c_int32),
         ("cg_eps", C.c_double), ("qme", C.c_double), ("wpe", C.c_double),
         ("device", C.c_int32), ("sort_interval", C.c_int32),
-        ("reserved", C.c_int32 * 16),
+        ("smooth_current", C.c_int32), ("reserved", C.c_int32 * 15),
     ]
 
 

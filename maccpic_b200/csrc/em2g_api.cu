@@ -166,6 +166,8 @@ int validate(const em2g_params *p) {
   if (p->energy_mode == 1 && p->ny < 170)
     return fail(EM2G_ERR_INVALID, "energy_mode 1 reads rows 88..168 and needs ny >= 170");
   if (p->cg_maxits < 1) return fail(EM2G_ERR_INVALID, "cg_maxits must be >= 1");
+  if (p->smooth_current != 0 && p->smooth_current != 1)
+    return fail(EM2G_ERR_INVALID, "smooth_current must be 0 or 1");
   for (int s = 0; s < p->nsp; ++s) {
     if (p->np_max[s] < 0 || p->np_max[s] > ((int64_t)1 << 31) - 1)
       return fail(EM2G_ERR_INVALID, "np_max out of range");
@@ -361,6 +363,7 @@ int em2g_set_field(em2g_ctx *c, int id, const double *host) {
   int rc = check_ctx(c);
   if (rc) return rc;
   if (id < 0 || id >= EM2G_NFIELD || !host) return fail(EM2G_ERR_INVALID, "bad field id or pointer");
+  c->jp_live = true;
   return put_fields_host(c, id, 1, host);
 }
 
@@ -375,6 +378,7 @@ int em2g_set_fields(em2g_ctx *c, const double *host13) {
   int rc = check_ctx(c);
   if (rc) return rc;
   if (!host13) return fail(EM2G_ERR_INVALID, "null pointer");
+  c->jp_live = true;
   return put_fields_host(c, 0, EM2G_NFIELD, host13);
 }
 
@@ -389,6 +393,7 @@ int em2g_set_fields_device(em2g_ctx *c, const double *dev13) {
   int rc = check_ctx(c);
   if (rc) return rc;
   if (!dev13) return fail(EM2G_ERR_INVALID, "null pointer");
+  c->jp_live = true;
   const int64_t n = EM2G_NFIELD * c->g.w;
   if (is_fp32(c)) {
     k_d2f<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(dev13, c->fld32, n);
@@ -419,6 +424,7 @@ int em2g_field_device_ptr(em2g_ctx *c, int id, void **dptr) {
   int rc = check_ctx(c);
   if (rc) return rc;
   if (id < 0 || id >= EM2G_NFIELD || !dptr) return fail(EM2G_ERR_INVALID, "bad field id or pointer");
+  c->jp_live = true;  // the caller may write through the pointer
   if (is_fp32(c))
     *dptr = c->fld32 + id * c->g.w;
   else
@@ -667,6 +673,7 @@ int em2g_curnt(em2g_ctx *c) {
   if (is_fp32(c))
     return fail(EM2G_ERR_INVALID,
                 "FP32 contexts run move and curnt fused: use em2g_move_curnt or em2g_step");
+  c->jp_live = true;
   for (int s = 0; s < c->P.nsp; ++s) {
     if ((rc = launch_push_f64(c, s, 2))) return rc;
     c->sp[s].sorted = false;  // positions moved outside the fast path's bookkeeping

@@ -97,6 +97,9 @@ struct em2g_ctx {
   int64_t launches = 0;
   int32_t *scan_tmp = nullptr;  // block sums of the cell scans
   int variant = 0;              // fast-push kernel variant (em2g_set_variant)
+  // false while jxp, jyp, jzp are known to hold zeros (after fields, and
+  // the fast path deposits the whole current into jxm, jym, jzm)
+  bool jp_live = true;
   int64_t ncell = 0;
   int timing = 0;
   std::vector<cudaEvent_t> ev;  // start/stop pairs of the pending push launches

@@ -108,6 +108,15 @@ int fields_t(em2g_ctx *c, T *fld, T *tmp, int it, bool want_energies) {
   // fold (pic/fields.f90:44-137)
   k_fold_x<T><<<dim3((g.ny + 3 + 127) / 128, 7), 128, 0, c->stream>>>(g, fld);
   k_fold_y<T><<<dim3((g.nx + 3 + 127) / 128, 7), 128, 0, c->stream>>>(g, fld);
+  c->launches += 2;
+  // optional current filter (no em2 counterpart): smooth2 of each J array
+  if (c->P.smooth_current)
+    for (int k = EM2G_JXM; k <= EM2G_JZP; ++k) {
+      const bool is_jp = k == EM2G_JXP || k == EM2G_JYP || k == EM2G_JZP;
+      if (is_jp && !c->jp_live) continue;
+      const int rc = smooth2_t<T>(c, fld + k * g.w, tmp);
+      if (rc) return rc;
+    }
   // Yee (pic/fields.f90:184-247)
   const double ctx = c->P.dt * c->P.c / c->P.dx, cty = c->P.dt * c->P.c / c->P.dy;
   const double ctxh = ctx * 0.5, ctyh = cty * 0.5, tem = 0.5 * c->P.dt;
@@ -115,7 +124,7 @@ int fields_t(em2g_ctx *c, T *fld, T *tmp, int it, bool want_energies) {
   k_b_half<T><<<grd, blk, 0, c->stream>>>(g, fld, (T)ctxh, (T)ctyh);
   k_e_full<T><<<grd, blk, 0, c->stream>>>(g, fld, (T)ctx, (T)cty, (T)tem);
   k_b_half<T><<<grd, blk, 0, c->stream>>>(g, fld, (T)ctxh, (T)ctyh);
-  c->launches += 5;
+  c->launches += 3;
   EM2G_CUDA(cudaGetLastError());
   // filters (pic/fields.f90:252-260)
   int rc = smooth2_t<T>(c, fld + EM2G_RHO * g.w, tmp);
@@ -130,6 +139,7 @@ int fields_t(em2g_ctx *c, T *fld, T *tmp, int it, bool want_energies) {
     if ((rc = energies_t<T>(c, fld))) return rc;
   // reset rho and J (pic/fields.f90:353-365)
   EM2G_CUDA(cudaMemsetAsync(fld + EM2G_RHO * g.w, 0, sizeof(T) * 7 * g.w, c->stream));
+  c->jp_live = false;
   return EM2G_OK;
 }
 

@@ -57,6 +57,7 @@ class RunParams:
     precision: int = _lib.FP64
     device: int = 0
     sort_interval: int = 0
+    smooth_current: int = 0     # 1: smooth2 the current every step (not in em2)
 
     @property
     def shape(self):
@@ -67,7 +68,7 @@ class RunParams:
         check(_lib.lib().em2g_params_init(C.byref(P)))
         for name in ("nx", "ny", "nsp", "isav", "precision", "dx", "dy", "dt", "c",
                      "cg_maxits", "energy_mode", "cg_eps", "qme", "wpe", "device",
-                     "sort_interval"):
+                     "sort_interval", "smooth_current"):
             setattr(P, name, getattr(self, name))
         for name in ("qm", "q", "dn", "am", "tx", "ty"):
             arr = getattr(P, name)

@@ -50,6 +50,7 @@ class HarrisConfig:
     isav: int = 20
     steps: int = 2000
     seed: int = 0
+    smooth_current: int = 0     # binomial current filter every step (not in em2)
 
     @property
     def b0(self):
@@ -89,6 +90,7 @@ class HarrisConfig:
     def run_params(self, np_max=None, **kw) -> RunParams:
         qm, q, dn, am = self.species_constants()
         n = self.nx * self.ny * self.ppc
+        kw.setdefault("smooth_current", self.smooth_current)
         return RunParams(nx=self.nx, ny=self.ny, dx=self.dx, dy=self.dx, dt=self.dt,
                          qm=qm, q=q, dn=dn, am=am,
                          np_max=np_max or [n, n], isav=self.isav, **kw)
@@ -102,7 +104,7 @@ PRESETS = {
     # profiling size: particle buffers (0.4-0.8 GB) well above the 126 MB L2
     "harris_1024x512_ppc32": HarrisConfig(nx=1024, ny=512, ppc=32, steps=100),
     "harris_4096x2048_ppc100": HarrisConfig(nx=4096, ny=2048, ppc=100, mass_ratio=100.0,
-                                            dt=0.04, steps=2000),
+                                            dt=0.04, steps=2000, smooth_current=1),
 }
 
 

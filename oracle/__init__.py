@@ -36,6 +36,7 @@ class _Params(C.Structure):
         ("am", C.c_double * 4), ("tx", C.c_double * 4), ("ty", C.c_double * 4),
         ("cg_maxits", C.c_int32), ("energy_mode", C.c_int32),
         ("cg_eps", C.c_double), ("qme", C.c_double), ("wpe", C.c_double),
+        ("smooth_current", C.c_int32),
     ]
 
 
@@ -131,6 +132,7 @@ class Params:
     energy_mode: int = 0
     qme: float = -1.0
     wpe: float = 1.0
+    smooth_current: int = 0
 
     def ctype(self) -> _Params:
         P = _Params()
@@ -143,6 +145,7 @@ class Params:
                 arr[i] = float(vals[i])
         P.cg_maxits, P.energy_mode = self.cg_maxits, self.energy_mode
         P.cg_eps, P.qme, P.wpe = self.cg_eps, self.qme, self.wpe
+        P.smooth_current = self.smooth_current
         return P
 
     @property

@@ -535,6 +535,8 @@ int em2o_fields(const em2o_params *p, double *fld, int it, double *e6) {
    * neither feeds the step) */
   const int64_t w = W(p);
   em2o_fold(p, fld);
+  if (p->smooth_current)
+    for (int k = EM2O_RHO + 1; k < EM2O_NFIELD; ++k) em2o_smooth2(p, fld + k * w);
   em2o_yee(p, fld);
   em2o_smooth2(p, fld + EM2O_RHO * w);
   if (it % p->isav == 0)

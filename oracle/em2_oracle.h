@@ -48,6 +48,8 @@ typedef struct {
   int32_t energy_mode;
   double cg_eps;
   double qme, wpe;
+  int32_t smooth_current; /* 1: smooth2 each current array after the fold
+                             (an option of the GPU library, not of em2) */
 } em2o_params;
 
 /* move for one species (pic/move.f90:37-209): gathers E, B with quadratic

@@ -328,3 +328,33 @@ def test_every_push_variant_matches_the_oracle(gpu, oracle_lib):
                 assert rel(got[k], st.fld[k]) < TOL, (v, k)
             for s in range(2):
                 assert rel(g.get_particles(s), st.parts[s]) < 1e-12, v
+
+
+def test_current_filter_matches_the_oracle(gpu, oracle_lib):
+    """smooth_current = 1 (no em2 counterpart): the drop-in sequence, which
+    deposits jm and jp separately, and the fused path, which deposits their
+    sum, against the oracle with the same filter."""
+    import dataclasses
+    op, rp, fld, parts = harris_case(nx=64, ny=32, ppc=16)
+    op = dataclasses.replace(op, smooth_current=1)
+    rp = dataclasses.replace(rp, smooth_current=1)
+    st_a = oracle_lib.State(op, fld, parts)
+    st_b = st_a.copy()
+    with make_gpu(rp, fld, parts) as a, make_gpu(rp, fld, parts) as b:
+        for it in range(1, 31):
+            st_a.move()
+            st_a.curnt()
+            n_ref, _ = st_a.fields(it)
+            a.move()
+            a.curnt()
+            n, _ = a.fields(it)
+            assert n == n_ref, it
+            r_ref = st_b.step()
+            r = b.step(1)
+            assert r["cg_iters"] == r_ref["cg_iters"], it
+        for g, st in ((a, st_a), (b, st_b)):
+            got = g.get_fields()
+            for k in range(6):
+                assert rel(got[k], st.fld[k]) < TOL, k
+            for s in range(2):
+                assert rel(g.get_particles(s), st.parts[s]) < 1e-12

@@ -192,3 +192,30 @@ def test_yee_vacuum_standing_wave_dispersion(oracle_lib):
         ez = f[oracle_lib.EZ][2, 1:nx + 1]
         a = (ez * np.cos(k * xe[1:nx + 1])).sum() * 2 / nx
         assert a == pytest.approx(np.cos(w * n * dt), abs=1e-12), n
+
+
+def test_current_filter_known_answer(oracle_lib):
+    """smooth_current = 1 filters each current array after the fold: from
+    E = B = 0 and a single Fourier mode in jzm + jzp, Ez after fields is
+    -dt/2 * (jzm + jzp) times smooth2's transfer function (1 with the filter
+    off, as in em2).  Ez is untouched by the Poisson correction."""
+    from oracle import EZ, JZM, JZP
+    nx, ny = 32, 16
+    mx, my = 3, 2
+    kx, ky = 2 * np.pi * mx / nx, 2 * np.pi * my / ny
+    tb = (1 + np.cos(kx)) * (1 + np.cos(ky)) / 4
+    tc = (20 - 2 * np.cos(kx) - 2 * np.cos(ky) - 4 * np.cos(kx) * np.cos(ky)) / 12
+    ix = np.arange(nx + 3)[None, :]
+    iy = np.arange(ny + 3)[:, None]
+    mode = np.cos(kx * ix + ky * iy)
+    interior = (slice(1, ny + 1), slice(1, nx + 1))
+    for flag, t in [(0, 1.0), (1, tb * tc)]:
+        op = oracle_lib.Params(nx=nx, ny=ny, dx=0.5, dy=0.5, dt=0.05, qm=[-1.0], q=[-1.0],
+                               dn=[1.0], am=[1.0], nsp=1, isav=1000, smooth_current=flag)
+        fld = np.zeros((13, ny + 3, nx + 3))
+        fld[JZM][interior] = mode[interior]          # guards zero: the fold adds nothing
+        fld[JZP][interior] = 0.5 * mode[interior]
+        st = oracle_lib.State(op, fld, [np.zeros((6, 0))])
+        st.fields(1)
+        np.testing.assert_allclose(st.fld[EZ][interior], -0.5 * op.dt * 1.5 * t * mode[interior],
+                                   atol=1e-15)
