@@ -216,6 +216,54 @@ int em2g_get_counters(em2g_ctx *ctx, int64_t *kernel_launches,
                       int64_t *push_launches_timed, double *push_ms);
 int em2g_reset_counters(em2g_ctx *ctx);
 
+/* ---- ensembles (no counterpart in the reference) ----------------------
+ * Up to 128 independent runs -- each its own em2 run with its own grid,
+ * species constants and particles, as em2g_step would advance it -- that
+ * advance together: per step one scan of all runs' cell counts, one
+ * persistent push launch whose CTAs claim row segments of all runs from a
+ * shared counter, and em2's fields for all runs in one launch per stage
+ * (one cooperative launch for all runs' CG, each run stopping at its own
+ * tolerance).  The whole step is captured once into a CUDA graph and
+ * replayed; nothing in it waits on the host.
+ *
+ * Every run is FP32 (precision EM2G_FP32) with energy_mode 0, on one device;
+ * at most 160 (run, species) pairs, 2^31 - 1 particles and cells in all.
+ * A run holds exactly np_max[s] particles of species s, set (once, or again
+ * to replace them) by em2g_ens_set_particles* before the first step.
+ * Runs are indexed 0..nruns-1.  Results per run go to arrays of nruns
+ * entries: ake_out 4 per run (species 0..3, zero past nsp), energies_out 6
+ * per run (written for runs whose isav divides the step count reached),
+ * cg_iters_out 1 per run. */
+typedef struct em2g_ens em2g_ens;
+int em2g_ens_create(const em2g_params *runs, int nruns, em2g_ens **out);
+int em2g_ens_destroy(em2g_ens *ens);
+int em2g_ens_num_runs(em2g_ens *ens, int *nruns);
+int em2g_ens_set_stream(em2g_ens *ens, void *cuda_stream);
+/* 1 (default): replay a captured graph per step; 0: launch the kernels */
+int em2g_ens_set_graph(em2g_ens *ens, int on);
+/* one of the em2g_num_variants FP32 push variants */
+int em2g_ens_set_variant(em2g_ens *ens, int variant);
+/* one run's 13 arrays, as em2g_set_fields / em2g_get_fields */
+int em2g_ens_set_fields(em2g_ens *ens, int run, const double *host13);
+int em2g_ens_get_fields(em2g_ens *ens, int run, double *host13);
+int em2g_ens_set_particles(em2g_ens *ens, int run, int isp, int64_t n, const double *x,
+                           const double *y, const double *vx, const double *vy,
+                           const double *vz, const double *gamma);
+int em2g_ens_set_particles_device(em2g_ens *ens, int run, int isp, int64_t n,
+                                  const double *x, const double *y, const double *vx,
+                                  const double *vy, const double *vz, const double *gamma);
+int em2g_ens_get_particles(em2g_ens *ens, int run, int isp, int64_t *n, double *x, double *y,
+                           double *vx, double *vy, double *vz, double *gamma);
+int em2g_ens_step(em2g_ens *ens, int nsteps, double *ake_out, double *energies_out,
+                  int *cg_iters_out);
+int em2g_ens_get_step(em2g_ens *ens, int *it);
+/* em2g_diagnostics of one run */
+int em2g_ens_diagnostics(em2g_ens *ens, int run, double *out, int nout);
+/* kernels launched (graph replays counted by their kernel nodes), graph
+ * launches, and kernels per step */
+int em2g_ens_get_counters(em2g_ens *ens, int64_t *kernel_launches, int64_t *graph_launches,
+                          int64_t *kernels_per_step);
+
 #ifdef __cplusplus
 }
 #endif

@@ -32,6 +32,10 @@ EXPORTS = [
     "em2g_move_curnt", "em2g_set_timing", "em2g_get_counters", "em2g_reset_counters",
     "em2g_smooth2_static", "em2g_diagnostics", "em2g_num_variants", "em2g_set_variant",
     "em2g_get_variant",
+    "em2g_ens_create", "em2g_ens_destroy", "em2g_ens_num_runs", "em2g_ens_set_stream",
+    "em2g_ens_set_graph", "em2g_ens_set_variant", "em2g_ens_set_fields", "em2g_ens_get_fields",
+    "em2g_ens_set_particles", "em2g_ens_set_particles_device", "em2g_ens_get_particles",
+    "em2g_ens_step", "em2g_ens_get_step", "em2g_ens_diagnostics", "em2g_ens_get_counters",
 ]
 
 
@@ -108,6 +112,21 @@ def lib() -> C.CDLL:
         "em2g_num_variants": (C.c_int, [ctx, ip]),
         "em2g_set_variant": (C.c_int, [ctx, C.c_int]),
         "em2g_get_variant": (C.c_int, [ctx, ip, C.c_char_p, C.c_int]),
+        "em2g_ens_create": (C.c_int, [pp, C.c_int, C.POINTER(C.c_void_p)]),
+        "em2g_ens_destroy": (C.c_int, [ctx]),
+        "em2g_ens_num_runs": (C.c_int, [ctx, ip]),
+        "em2g_ens_set_stream": (C.c_int, [ctx, vp]),
+        "em2g_ens_set_graph": (C.c_int, [ctx, C.c_int]),
+        "em2g_ens_set_variant": (C.c_int, [ctx, C.c_int]),
+        "em2g_ens_set_fields": (C.c_int, [ctx, C.c_int, dp]),
+        "em2g_ens_get_fields": (C.c_int, [ctx, C.c_int, dp]),
+        "em2g_ens_set_particles": (C.c_int, [ctx, C.c_int, C.c_int, C.c_int64] + [dp] * 6),
+        "em2g_ens_set_particles_device": (C.c_int, [ctx, C.c_int, C.c_int, C.c_int64] + [vp] * 6),
+        "em2g_ens_get_particles": (C.c_int, [ctx, C.c_int, C.c_int, i64p] + [dp] * 6),
+        "em2g_ens_step": (C.c_int, [ctx, C.c_int, dp, dp, ip]),
+        "em2g_ens_get_step": (C.c_int, [ctx, ip]),
+        "em2g_ens_diagnostics": (C.c_int, [ctx, C.c_int, dp, C.c_int]),
+        "em2g_ens_get_counters": (C.c_int, [ctx, i64p, i64p, i64p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -85,21 +85,20 @@ __global__ void k_energy_now_finish(const double *__restrict__ partial, int nb, 
   out[k] = v * scale;
 }
 
+// out[0..6) energies, out[6..8) flux of the sheets at ny/4 and 3ny/4
 template <typename T>
-int diag_t(em2g_ctx *c, const T *fld) {
-  const int nx = c->g.nx, ny = c->g.ny, nxg = c->g.nxg;
-  const int64_t w = c->g.w;
+int diag_t(const T *fld, const Grid &g, double dx, double *red, double *out, cudaStream_t st) {
+  const int nx = g.nx, ny = g.ny, nxg = g.nxg;
+  const int64_t w = g.w;
   const int nb = kEnergyBlocks;
   // 0.5 * mean of E^2 + B^2 per component over the interior (pic/fields.f90:341
   // with the whole grid): anorml1 = 0.5*dx*dy/(Lx*Ly) = 0.5/(nx*ny)
   const double scale = 0.5 / ((double)nx * ny);
-  k_energy_now<T><<<dim3(nb, 6), 256, 0, c->stream>>>(fld, nx, ny, nxg, w, c->red);
-  k_energy_now_finish<<<1, 32, 0, c->stream>>>(c->red, nb, scale, c->dev_out + 10);
+  k_energy_now<T><<<dim3(nb, 6), 256, 0, st>>>(fld, nx, ny, nxg, w, red);
+  k_energy_now_finish<<<1, 32, 0, st>>>(red, nb, scale, out);
   const T *by = fld + EM2G_BY * w;
-  k_sheet_flux<T><<<1, 32, 0, c->stream>>>(by, nx, nxg, ny / 4, c->P.dx, c->dev_out + 16);
-  k_sheet_flux<T><<<1, 32, 0, c->stream>>>(by, nx, nxg, ny / 4 + ny / 2, c->P.dx,
-                                           c->dev_out + 17);
-  c->launches += 4;
+  k_sheet_flux<T><<<1, 32, 0, st>>>(by, nx, nxg, ny / 4, dx, out + 6);
+  k_sheet_flux<T><<<1, 32, 0, st>>>(by, nx, nxg, ny / 4 + ny / 2, dx, out + 7);
   EM2G_CUDA(cudaGetLastError());
   return EM2G_OK;
 }
@@ -107,8 +106,15 @@ int diag_t(em2g_ctx *c, const T *fld) {
 }  // namespace
 
 int diagnostics(em2g_ctx *c) {
-  if (c->P.precision == EM2G_FP32) return diag_t<float>(c, c->fld32);
-  return diag_t<double>(c, c->fld);
+  c->launches += 4;
+  if (c->P.precision == EM2G_FP32)
+    return diag_t<float>(c->fld32, c->g, c->P.dx, c->red, c->dev_out + 10, c->stream);
+  return diag_t<double>(c->fld, c->g, c->P.dx, c->red, c->dev_out + 10, c->stream);
+}
+
+int diag_fields_f32(const float *fld, const Grid &g, double dx, double *red, double *out,
+                    cudaStream_t st) {
+  return diag_t<float>(fld, g, dx, red, out, st);
 }
 
 }  // namespace em2g

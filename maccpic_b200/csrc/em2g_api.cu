@@ -198,6 +198,18 @@ int finish_outputs(em2g_ctx *c, double *ake_out, double *energies_out, int *cg_i
 }
 
 }  // namespace
+
+int validate_params(const em2g_params *p) { return validate(p); }
+
+int check_particles_device(const double *part, int64_t n, int64_t ld, double xlim, double ylim,
+                           unsigned long long *bad, cudaStream_t st) {
+  EM2G_CUDA(cudaMemsetAsync(bad, 0, 2 * sizeof(unsigned long long), st));
+  if (n > 0)
+    k_check_particles<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(part, n, ld, xlim, ylim, bad);
+  EM2G_CUDA(cudaGetLastError());
+  return EM2G_OK;
+}
+
 }  // namespace em2g
 
 using namespace em2g;
@@ -298,9 +310,8 @@ int em2g_create(const em2g_params *p, em2g_ctx **out) {
   if (rc) return bail(rc);
   {
     // the fast pushes write one ake partial per block of 64 cells (FP64) or
-    // per warp of a 32-cell row segment (FP32)
-    // (ceil(nx/tcx) * ny CTAs of tcx*4/32 warps, tcx in {32, 64})
-    const int64_t fast_blocks = (int64_t)((c->g.nx + 31) / 32) * c->g.ny * 4 + 64;
+    // per warp of a row segment (FP32)
+    const int64_t fast_blocks = push_partials(c->g.nx, c->g.ny) + 64;
     if (fast_blocks > c->red_blocks) {
       cudaFree(c->red);
       c->red_blocks = (int)fast_blocks;

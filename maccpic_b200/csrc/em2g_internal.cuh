@@ -10,7 +10,10 @@
 
 namespace em2g {
 
-constexpr int kEnergyBlocks = 296;  // partial sums per field in the energy reduction
+constexpr int kEnergyBlocks = 296;
+// ensembles (ensemble_api.cu): runs, and (run, species) pairs, per ensemble
+constexpr int kEnsMaxRuns = 128;
+constexpr int kEnsMaxPairs = 160;  // partial sums per field in the energy reduction
 // small device results, mirrored to pinned host memory after each call:
 // [0,4) ake per species, [4,10) energies at isav steps, [10,16) energies of
 // the current fields, [16,18) reconnected flux of the two sheets, [18,20)
@@ -144,5 +147,28 @@ int diagnostics(em2g_ctx *c);
 int timing_begin(em2g_ctx *c);
 int timing_end(em2g_ctx *c);
 void cg_free(em2g_ctx *c);
+// kinetic-energy partials one fast push of an nx x ny grid writes, for the
+// widest-writing variant: ceil(nx/tcx) * ny segments of tcx*4/32 warps, tcx
+// 32 or 64
+inline int64_t push_partials(int nx, int ny) {
+  const int64_t a = (int64_t)((nx + 31) / 32) * 4, b = (int64_t)((nx + 63) / 64) * 8;
+  return (a > b ? a : b) * ny;
+}
+// the checks em2g_create applies to a parameter block (api.cu)
+int validate_params(const em2g_params *p);
+// counts particles of a 6 x ld FP64 block outside [0, xlim) x [0, ylim)
+// into bad[0] and those with non-finite values into bad[1] (api.cu)
+int check_particles_device(const double *part, int64_t n, int64_t ld, double xlim, double ylim,
+                           unsigned long long *bad, cudaStream_t st);
+// energies of the current fields and the reconnected flux of both sheets
+// of one FP32 field block into out[0..8); red: 6*kEnergyBlocks doubles
+// (diag.cu)
+int diag_fields_f32(const float *fld, const Grid &g, double dx, double *red, double *out,
+                    cudaStream_t st);
+// exclusive scan of cnt[0..n) into off[0..n], plus `base`, on `stream`;
+// tmp holds scan_tmp_size(n) ints (sort.cu)
+int64_t scan_tmp_size(int64_t n);
+int scan_counts(const int32_t *cnt, int32_t *off, int64_t n, int32_t base, int32_t *tmp,
+                cudaStream_t stream);
 
 }  // namespace em2g

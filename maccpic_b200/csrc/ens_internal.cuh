@@ -1,0 +1,95 @@
+// ens_internal.cuh -- layout of an ensemble of independent FP32 runs that
+// advance together (ensemble_api.cu), and the launchers its step uses.
+// Not part of the public ABI.
+//
+// Device layout.  Every array kind of all runs lives in one allocation,
+// run after run:
+//   fld     13 arrays of w_r floats per run (enum em2g_field order)
+//   scaled  nsp_r * 6 * w_r floats per run ((E, B) pairs, push_fast_f32.cu)
+//   tmp     6 * w_r floats per run (smooth2 scratch of up to six arrays)
+//   cgv     4 * nx_r * ny_r floats per run (u, r, p, Ap of the CG)
+// Particles of all (run, species) pairs share one cell-grouped buffer pair
+// (p32/p32_alt, 5 * cap floats, and their slots): pair (r, s) owns the
+// slots base[r][s] .. base[r][s] + n[r][s] - 1, and its cells are the keys
+// cell0[r][s] .. cell0[r][s] + nx_r*ny_r - 1 of the shared count and
+// offset arrays.  Because every pair holds exactly n[r][s] particles, one
+// exclusive scan over all pairs' counts yields every pair's offsets.
+#pragma once
+#include "em2g_internal.cuh"
+
+namespace em2g {
+
+// per run: [0,4) ake of the last step, [4,10) energies of the last isav
+// step, [10,12) mean r^2 before and after the last CG
+constexpr int kEnsOut = 16;
+
+struct EnsRun {
+  em2g_params P;
+  Grid g;
+  int64_t fld_off = 0, sc_off = 0, tmp_off = 0, cg_off = 0;  // elements
+  int64_t cell0[EM2G_MAX_SPECIES] = {};
+  int64_t base[EM2G_MAX_SPECIES] = {};
+  int64_t n[EM2G_MAX_SPECIES] = {};
+  int64_t red_off[EM2G_MAX_SPECIES] = {};  // first ake partial of the pair
+  bool loaded[EM2G_MAX_SPECIES] = {};
+  int cg_block0 = 0, cg_blocks = 0;
+};
+
+}  // namespace em2g
+
+struct em2g_ens {
+  int device = 0;
+  int num_sms = 0;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  std::vector<em2g::EnsRun> runs;
+  int npairs = 0;
+  bool any_smooth_current = false;
+  // grids
+  float *fld = nullptr, *scaled = nullptr, *tmp = nullptr, *cgv = nullptr;
+  int64_t fld_n = 0, scaled_n = 0, tmp_n = 0, cgv_n = 0;
+  double *cg_partial = nullptr;  // 2 per CG block
+  unsigned *cg_bar = nullptr;    // 2 per run
+  int *cg_status = nullptr;      // 2 per run: timeout flag, iterations
+  int cg_blocks = 0;
+  double *red = nullptr;         // ake partials of all pairs
+  int64_t red_n = 0;
+  double *dev_out = nullptr;     // kEnsOut per run
+  double *host_out = nullptr;    // pinned mirror of dev_out
+  int *host_status = nullptr;    // pinned mirror of cg_status
+  // particles; parity 0: current = p32/slot/off/cnt, next = the _alt set
+  float *p32 = nullptr, *p32_alt = nullptr;
+  int32_t *slot = nullptr, *slot_alt = nullptr;
+  int32_t *off = nullptr, *off_alt = nullptr, *cnt = nullptr, *cnt_alt = nullptr;
+  int32_t *cursor = nullptr, *scan_tmp = nullptr;
+  int64_t cap = 0, ncell = 0;
+  int parity = 0;
+  double *staging = nullptr;  // 6 * staging_n doubles (uploads, downloads)
+  int64_t staging_n = 0;
+  int *counter = nullptr;     // the persistent push's segment counter
+  int *d_it = nullptr;        // the step counter as the field kernels read it
+  int it = 0;
+  int variant = 0;
+  // one captured graph per buffer parity; invalid after a change of
+  // variant or stream
+  bool use_graph = true;
+  cudaGraphExec_t exec[2] = {nullptr, nullptr};
+  int64_t kernels_per_step = 0;
+  int64_t launches = 0, graph_launches = 0;
+};
+
+namespace em2g {
+
+// push_fast_f32.cu
+int ens_push(em2g_ens *e, int parity);
+int ens_upload_pair(em2g_ens *e, int r, int s, const double *staging);
+int ens_download_pair(em2g_ens *e, int r, int s, double *staging);
+int ens_push_kernels_per_step(const em2g_ens *e);
+// fields_ens.cu
+int ens_cg_setup(em2g_ens *e);
+int ens_prescale(em2g_ens *e);
+int ens_tick(em2g_ens *e);
+int ens_fields(em2g_ens *e);
+int ens_fields_kernels(const em2g_ens *e);
+
+}  // namespace em2g

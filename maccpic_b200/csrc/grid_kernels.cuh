@@ -42,9 +42,7 @@ __device__ __forceinline__ void store_with_guards(const G &g, T *a, int ix, int 
 // ---- guard fold of rho and the 6 current arrays (pic/fields.f90:44-137)
 // x pass: one thread per (row iy in 0..ny+2, array)
 template <typename T>
-__global__ void k_fold_x(G g, T *fld) {
-  const int iy = blockIdx.x * blockDim.x + threadIdx.x;
-  const int k = blockIdx.y;  // 0..6 -> rho..jzp
+__device__ __forceinline__ void fold_x_at(const G &g, T *fld, int iy, int k) {
   if (iy > g.ny + 2) return;
   T *a = fld + (EM2G_RHO + k) * g.w + (int64_t)iy * g.nxg;
   const int nx = g.nx;
@@ -55,11 +53,13 @@ __global__ void k_fold_x(G g, T *fld) {
   a[nx + 2] = a[2];
   a[0] = a[nx];
 }
+template <typename T>
+__global__ void k_fold_x(G g, T *fld) {
+  fold_x_at(g, fld, (int)(blockIdx.x * blockDim.x + threadIdx.x), (int)blockIdx.y);
+}
 // y pass: one thread per (column ix in 0..nx+2, array)
 template <typename T>
-__global__ void k_fold_y(G g, T *fld) {
-  const int ix = blockIdx.x * blockDim.x + threadIdx.x;
-  const int k = blockIdx.y;
+__device__ __forceinline__ void fold_y_at(const G &g, T *fld, int ix, int k) {
   if (ix > g.nx + 2) return;
   T *a = fld + (EM2G_RHO + k) * g.w + ix;
   const int64_t s = g.nxg;
@@ -71,12 +71,16 @@ __global__ void k_fold_y(G g, T *fld) {
   a[(ny + 2) * s] = a[2 * s];
   a[0] = a[ny * s];
 }
+template <typename T>
+__global__ void k_fold_y(G g, T *fld) {
+  fold_y_at(g, fld, (int)(blockIdx.x * blockDim.x + threadIdx.x), (int)blockIdx.y);
+}
 
 // ---- Yee half step of B (pic/fields.f90:184-200, :231-247)
 template <typename T>
-__global__ void k_b_half(G g, T *fld, T ctxh, T ctyh) {
-  const int ix = 1 + blockIdx.x * TX + threadIdx.x;
-  const int iy = 1 + blockIdx.y * TY + threadIdx.y;
+__device__ __forceinline__ void b_half_at(const G &g, T *fld, T ctxh, T ctyh, int tbx, int tby) {
+  const int ix = 1 + tbx * TX + threadIdx.x;
+  const int iy = 1 + tby * TY + threadIdx.y;
   if (ix > g.nx + 1 || iy > g.ny + 1) return;
   const T *ex = fld + EM2G_EX * g.w, *ey = fld + EM2G_EY * g.w, *ez = fld + EM2G_EZ * g.w;
   T *bx = fld + EM2G_BX * g.w, *by = fld + EM2G_BY * g.w, *bz = fld + EM2G_BZ * g.w;
@@ -89,12 +93,17 @@ __global__ void k_b_half(G g, T *fld, T ctxh, T ctyh) {
   store_with_guards(g, by, ix, iy, vby);
   store_with_guards(g, bz, ix, iy, vbz);
 }
+template <typename T>
+__global__ void k_b_half(G g, T *fld, T ctxh, T ctyh) {
+  b_half_at(g, fld, ctxh, ctyh, (int)blockIdx.x, (int)blockIdx.y);
+}
 
 // ---- Yee full step of E (pic/fields.f90:207-224)
 template <typename T>
-__global__ void k_e_full(G g, T *fld, T ctx, T cty, T tem) {
-  const int ix = 1 + blockIdx.x * TX + threadIdx.x;
-  const int iy = 1 + blockIdx.y * TY + threadIdx.y;
+__device__ __forceinline__ void e_full_at(const G &g, T *fld, T ctx, T cty, T tem, int tbx,
+                                          int tby) {
+  const int ix = 1 + tbx * TX + threadIdx.x;
+  const int iy = 1 + tby * TY + threadIdx.y;
   if (ix > g.nx + 1 || iy > g.ny + 1) return;
   T *ex = fld + EM2G_EX * g.w, *ey = fld + EM2G_EY * g.w, *ez = fld + EM2G_EZ * g.w;
   const T *bx = fld + EM2G_BX * g.w, *by = fld + EM2G_BY * g.w, *bz = fld + EM2G_BZ * g.w;
@@ -111,13 +120,18 @@ __global__ void k_e_full(G g, T *fld, T ctx, T cty, T tem) {
   store_with_guards(g, ey, ix, iy, vey);
   store_with_guards(g, ez, ix, iy, vez);
 }
+template <typename T>
+__global__ void k_e_full(G g, T *fld, T ctx, T cty, T tem) {
+  e_full_at(g, fld, ctx, cty, tem, (int)blockIdx.x, (int)blockIdx.y);
+}
 
 // ---- smooth2 (pic/smooth.f90:143-177): binomial pass into `d`, then the
 // compensation pass back into `s`.
 template <typename T>
-__global__ void k_smooth_binomial(G g, const T *__restrict__ s, T *d) {
-  const int ix = 1 + blockIdx.x * TX + threadIdx.x;
-  const int iy = 1 + blockIdx.y * TY + threadIdx.y;
+__device__ __forceinline__ void smooth_binomial_at(const G &g, const T *__restrict__ s, T *d,
+                                                   int tbx, int tby) {
+  const int ix = 1 + tbx * TX + threadIdx.x;
+  const int iy = 1 + tby * TY + threadIdx.y;
   if (ix > g.nx + 1 || iy > g.ny + 1) return;
   const int64_t c = at(g, ix, iy), n = g.nxg;
   const T v = (4 * s[c] + 2 * (s[c - 1] + s[c + 1] + s[c - n] + s[c + n]) +
@@ -126,9 +140,14 @@ __global__ void k_smooth_binomial(G g, const T *__restrict__ s, T *d) {
   store_with_guards(g, d, ix, iy, v);
 }
 template <typename T>
-__global__ void k_smooth_compensate(G g, const T *__restrict__ d, T *s) {
-  const int ix = 1 + blockIdx.x * TX + threadIdx.x;
-  const int iy = 1 + blockIdx.y * TY + threadIdx.y;
+__global__ void k_smooth_binomial(G g, const T *__restrict__ s, T *d) {
+  smooth_binomial_at(g, s, d, (int)blockIdx.x, (int)blockIdx.y);
+}
+template <typename T>
+__device__ __forceinline__ void smooth_compensate_at(const G &g, const T *__restrict__ d, T *s,
+                                                     int tbx, int tby) {
+  const int ix = 1 + tbx * TX + threadIdx.x;
+  const int iy = 1 + tby * TY + threadIdx.y;
   if (ix > g.nx + 1 || iy > g.ny + 1) return;
   const int64_t c = at(g, ix, iy), n = g.nxg;
   const T v = (20 * d[c] - d[c - 1] - d[c + 1] - d[c - n] - d[c + n] - d[c - 1 - n] -
@@ -136,14 +155,19 @@ __global__ void k_smooth_compensate(G g, const T *__restrict__ d, T *s) {
                    T(12.0);
   store_with_guards(g, s, ix, iy, v);
 }
+template <typename T>
+__global__ void k_smooth_compensate(G g, const T *__restrict__ d, T *s) {
+  smooth_compensate_at(g, d, s, (int)blockIdx.x, (int)blockIdx.y);
+}
 
 // ---- Poisson right-hand side (pic/fields.f90:392-405): f = (div E - rho)
 // * dx * dx on the nx*ny periodic grid; written straight into r (u = 0, so
 // cgm's first residual r = f - L u is f) and p = r.
 template <typename T>
-__global__ void k_poisson_rhs(G g, const T *__restrict__ fld, T dx, T dy, T *r, T *p) {
-  const int ix = 1 + blockIdx.x * TX + threadIdx.x;
-  const int iy = 1 + blockIdx.y * TY + threadIdx.y;
+__device__ __forceinline__ void poisson_rhs_at(const G &g, const T *__restrict__ fld, T dx, T dy,
+                                               T *r, T *p, int tbx, int tby) {
+  const int ix = 1 + tbx * TX + threadIdx.x;
+  const int iy = 1 + tby * TY + threadIdx.y;
   if (ix > g.nx || iy > g.ny) return;
   const T *ex = fld + EM2G_EX * g.w, *ey = fld + EM2G_EY * g.w, *rho = fld + EM2G_RHO * g.w;
   const int ixm = (ix == 1) ? g.nx : ix - 1;
@@ -153,6 +177,10 @@ __global__ void k_poisson_rhs(G g, const T *__restrict__ fld, T dx, T dy, T *r, 
   const int64_t k = (int64_t)(iy - 1) * g.nx + (ix - 1);
   r[k] = fs;
   p[k] = fs;
+}
+template <typename T>
+__global__ void k_poisson_rhs(G g, const T *__restrict__ fld, T dx, T dy, T *r, T *p) {
+  poisson_rhs_at(g, fld, dx, dy, r, p, (int)blockIdx.x, (int)blockIdx.y);
 }
 
 // ---- E -= grad(phi) with periodic images and guards (pic/fields.f90:410-442)
@@ -172,9 +200,10 @@ __device__ __forceinline__ void store_images(const G &g, T *a, int ix, int iy, T
     for (int a0 = 0; a0 < nxs; ++a0) a[at(g, xs[a0], ys[a1])] = v;
 }
 template <typename T>
-__global__ void k_poisson_correct(G g, T *fld, const T *__restrict__ u, T dx, T dy) {
-  const int ix = 1 + blockIdx.x * TX + threadIdx.x;
-  const int iy = 1 + blockIdx.y * TY + threadIdx.y;
+__device__ __forceinline__ void poisson_correct_at(const G &g, T *fld, const T *__restrict__ u,
+                                                   T dx, T dy, int tbx, int tby) {
+  const int ix = 1 + tbx * TX + threadIdx.x;
+  const int iy = 1 + tby * TY + threadIdx.y;
   if (ix > g.nx || iy > g.ny) return;
   T *ex = fld + EM2G_EX * g.w, *ey = fld + EM2G_EY * g.w;
   const int64_t k = (int64_t)(iy - 1) * g.nx + (ix - 1);
@@ -185,6 +214,10 @@ __global__ void k_poisson_correct(G g, T *fld, const T *__restrict__ u, T dx, T 
   const T vy = ey[at(g, ix, iy)] - (u[kyp] - uc) / dy;
   store_images(g, ex, ix, iy, vx);
   store_images(g, ey, ix, iy, vy);
+}
+template <typename T>
+__global__ void k_poisson_correct(G g, T *fld, const T *__restrict__ u, T dx, T dy) {
+  poisson_correct_at(g, fld, u, dx, dy, (int)blockIdx.x, (int)blockIdx.y);
 }
 
 // ---- conjugate gradient, one persistent launch (pic/fields.f90:508-651)
@@ -264,13 +297,13 @@ struct CgArgs {
   double eps;
 };
 
+// The solve on blocks bidx = 0..nb-1 of a launch (all of them for one
+// system, or one run's share of an ensemble launch); sh: 33 doubles.
 template <typename T>
-__global__ void __launch_bounds__(256) k_cg(CgArgs<T> a) {
-  __shared__ double sh[33];
+__device__ __forceinline__ void cg_body(const CgArgs<T> &a, int bidx, unsigned nb, double *sh) {
   const int64_t N = (int64_t)a.nx * a.ny;
-  const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  const unsigned nb = gridDim.x;
+  const int64_t tid = (int64_t)bidx * blockDim.x + threadIdx.x;
+  const int64_t stride = (int64_t)nb * blockDim.x;
   double *part0 = a.partial, *part1 = a.partial + nb;
   // rr = sum r^2 for n = 1 (pic/fields.f90:546-556); u starts at 0
   double loc = 0.0;
@@ -279,10 +312,10 @@ __global__ void __launch_bounds__(256) k_cg(CgArgs<T> a) {
     loc += (double)a.r[k] * (double)a.r[k];
   }
   loc = block_sum(loc, sh);
-  if (threadIdx.x == 0) part0[blockIdx.x] = loc;
+  if (threadIdx.x == 0) part0[bidx] = loc;
   if (!grid_barrier(a.bar, nb, a.status)) return;
   double rr = sum_partials(part0, nb, sh);
-  if (blockIdx.x == 0 && threadIdx.x == 0) a.res[0] = rr / a.nx / a.ny;
+  if (bidx == 0 && threadIdx.x == 0) a.res[0] = rr / a.nx / a.ny;
   double r_last = rr;
   int n;
   for (n = 1; n <= a.maxits; ++n) {
@@ -303,7 +336,7 @@ __global__ void __launch_bounds__(256) k_cg(CgArgs<T> a) {
       loc += (double)pc * (double)v;
     }
     loc = block_sum(loc, sh);
-    if (threadIdx.x == 0) part1[blockIdx.x] = loc;
+    if (threadIdx.x == 0) part1[bidx] = loc;
     if (!grid_barrier(a.bar, nb, a.status)) return;
     const double pap = sum_partials(part1, nb, sh);
     const double ak = rr / pap;
@@ -316,7 +349,7 @@ __global__ void __launch_bounds__(256) k_cg(CgArgs<T> a) {
       loc += (double)r1 * (double)r1;
     }
     loc = block_sum(loc, sh);
-    if (threadIdx.x == 0) part0[blockIdx.x] = loc;
+    if (threadIdx.x == 0) part0[bidx] = loc;
     if (!grid_barrier(a.bar, nb, a.status)) return;
     const double r_norm = sum_partials(part0, nb, sh);
     r_last = r_norm;
@@ -326,10 +359,16 @@ __global__ void __launch_bounds__(256) k_cg(CgArgs<T> a) {
     rr = r_norm;  // next pass's sum of r^2 over the same r, same order
     if (!grid_barrier(a.bar, nb, a.status)) return;
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (bidx == 0 && threadIdx.x == 0) {
     a.status[1] = n;
     a.res[1] = r_last / a.nx / a.ny;
   }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_cg(CgArgs<T> a) {
+  __shared__ double sh[33];
+  cg_body(a, (int)blockIdx.x, gridDim.x, sh);
 }
 
 // ---- energies (pic/fields.f90:267-347): per-block partial sums of a^2 over

@@ -33,7 +33,10 @@
 // (front slots by a running count for the common in-cell case, back slots by
 // an atomic for the rest), and the cells of the new positions are counted
 // for the next step's offsets: the counting sort rides along with the push.
-#include "em2g_internal.cuh"
+#include <algorithm>
+#include <memory>
+
+#include "ens_internal.cuh"
 #include "sort_common.cuh"
 
 namespace em2g {
@@ -58,6 +61,15 @@ struct Args32 {
   int nx, ny, nxg;
   float qd, dtdx, dtdy, c;
   double *ake_partial;
+};
+
+// the pairs of one ensemble push (a __grid_constant__ kernel parameter)
+struct EnsPush32 {
+  int npairs, ntiles;
+  int *counter;  // next unclaimed segment, zeroed before the launch
+  int tile0[kEnsMaxPairs + 1];
+  int segs[kEnsMaxPairs];
+  Args32 pair[kEnsMaxPairs];
 };
 
 struct Wts {
@@ -180,15 +192,14 @@ __device__ __forceinline__ int floor_small(float f) { return f < 0.0f ? -1 : (f 
 
 __device__ __forceinline__ int wrap(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
 
-// TCX cells per CTA (a row segment), MINB: CTAs per SM the register
-// allocation must allow (the autotuner's two knobs)
-template <int TCX, int MINB>
-__global__ void __launch_bounds__(TCX * G, MINB) k_push_cells_f32(Args32 a) {
+// One row segment: cells x0 .. x0+TCX-1 of row y0, by a CTA of TCX*G
+// threads; `blk` numbers the segment for the kinetic-energy partials.
+template <int TCX>
+__device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, int64_t blk,
+                                             float2 (*win)[WY][TCX + 5]) {
   constexpr int kThreads = TCX * G;
   constexpr int WX = TCX + 5;  // window columns: x0-1 .. x0+TCX+3
-  __shared__ float2 win[3][WY][WX];
   const int nx = a.nx, ny = a.ny, nxg = a.nxg;
-  const int x0 = blockIdx.x * TCX, y0 = blockIdx.y;
   // stage the segment's (E, B) window: array indices x0-1.., y0-1..
   for (int t = threadIdx.x; t < 3 * WY * WX; t += kThreads) {
     const int comp = t / (WY * WX), r = (t / WX) % WY, col = t % WX;
@@ -380,22 +391,80 @@ __global__ void __launch_bounds__(TCX * G, MINB) k_push_cells_f32(Args32 a) {
   }
   // per-warp partial of sum(gamma - 1); no block barrier at the end
   for (int o = 16; o > 0; o >>= 1) akel += __shfl_down_sync(0xffffffffu, akel, o);
-  const int64_t blk = (int64_t)blockIdx.y * gridDim.x + blockIdx.x;
   if (lane == 0) a.ake_partial[blk * (kThreads / 32) + (threadIdx.x >> 5)] = akel;
+}
+
+// TCX cells per CTA (a row segment), MINB: CTAs per SM the register
+// allocation must allow (the autotuner's two knobs)
+template <int TCX, int MINB>
+__global__ void __launch_bounds__(TCX * G, MINB) k_push_cells_f32(Args32 a) {
+  __shared__ float2 win[3][WY][TCX + 5];
+  push_segment<TCX>(a, (int)blockIdx.x * TCX, (int)blockIdx.y,
+                    (int64_t)blockIdx.y * gridDim.x + blockIdx.x, win);
+}
+
+// Ensemble: every (run, species) pair of an ensemble in one persistent
+// launch.  The pairs' row segments are numbered one after the other
+// (tile0[p] .. tile0[p+1]-1 for pair p, row-major within the pair); each
+// CTA takes the next unclaimed segment from a counter until none is left,
+// so runs of unequal size and density share the SMs without a tail per run.
+template <int TCX, int MINB>
+__global__ void __launch_bounds__(TCX * G, MINB) k_ens_push_f32(const __grid_constant__ EnsPush32 e) {
+  __shared__ float2 win[3][WY][TCX + 5];
+  __shared__ int s_tile;
+  for (;;) {
+    if (threadIdx.x == 0) s_tile = atomicAdd(e.counter, 1);
+    __syncthreads();  // also: every thread is done with the last segment's window
+    const int t = s_tile;
+    if (t >= e.ntiles) break;
+    int lo = 0, hi = e.npairs - 1;  // last pair p with tile0[p] <= t
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (e.tile0[mid] <= t) lo = mid; else hi = mid - 1;
+    }
+    const int lt = t - e.tile0[lo];
+    const int segs = e.segs[lo];
+    const int row = lt / segs;
+    push_segment<TCX>(e.pair[lo], (lt - row * segs) * TCX, row, lt, win);
+  }
 }
 
 struct Variant32 {
   const char *name;
   int tcx;
   void (*kernel)(Args32);
+  void (*ens_kernel)(const EnsPush32);
 };
 const Variant32 kVariants32[] = {
-    {"f32 tcx32 minb4", 32, k_push_cells_f32<32, 4>},
-    {"f32 tcx32 minb5", 32, k_push_cells_f32<32, 5>},
-    {"f32 tcx32 minb6", 32, k_push_cells_f32<32, 6>},
-    {"f32 tcx64 minb2", 64, k_push_cells_f32<64, 2>},
-    {"f32 tcx64 minb3", 64, k_push_cells_f32<64, 3>},
+    {"f32 tcx32 minb4", 32, k_push_cells_f32<32, 4>, k_ens_push_f32<32, 4>},
+    {"f32 tcx32 minb5", 32, k_push_cells_f32<32, 5>, k_ens_push_f32<32, 5>},
+    {"f32 tcx32 minb6", 32, k_push_cells_f32<32, 6>, k_ens_push_f32<32, 6>},
+    {"f32 tcx64 minb2", 64, k_push_cells_f32<64, 2>, k_ens_push_f32<64, 2>},
+    {"f32 tcx64 minb3", 64, k_push_cells_f32<64, 3>, k_ens_push_f32<64, 3>},
 };
+
+// kinetic energy of every pair of an ensemble: block p sums pair p's
+// partials in a fixed order (pic/move.f90:183, :208)
+struct EnsAke {
+  const double *partial[kEnsMaxPairs];
+  int count[kEnsMaxPairs];
+  double scale[kEnsMaxPairs];  // am * dn
+  double *out[kEnsMaxPairs];
+};
+__global__ void __launch_bounds__(256) k_ens_ake(const __grid_constant__ EnsAke a) {
+  __shared__ double red[8];
+  const int p = blockIdx.x;
+  double v = 0.0;
+  for (int i = threadIdx.x; i < a.count[p]; i += blockDim.x) v += a.partial[p][i];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    v = threadIdx.x < 8 ? red[threadIdx.x] : 0.0;
+    for (int o = 4; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (threadIdx.x == 0) *a.out[p] = v * a.scale[p];
+  }
+}
 
 // E and B times ae = 0.5*qm*dt/c into (E, B) pairs of the three staggerings
 // (pic/move.f90:52-64)
@@ -567,5 +636,122 @@ int download_f32(em2g_ctx *c, int isp, double *staging) {
   EM2G_CUDA(cudaGetLastError());
   return EM2G_OK;
 }
+
+// ---- ensembles (ensemble_api.cu) ---------------------------------------
+
+// One push of every pair: offsets of the next grouping from the current
+// counts (one scan over all pairs), the persistent push, the kinetic
+// energies.  parity selects which buffer set is current.
+int ens_push(em2g_ens *e, int parity) {
+  float *A = parity ? e->p32_alt : e->p32, *B = parity ? e->p32 : e->p32_alt;
+  int32_t *slotA = parity ? e->slot_alt : e->slot, *slotB = parity ? e->slot : e->slot_alt;
+  int32_t *offA = parity ? e->off_alt : e->off, *offB = parity ? e->off : e->off_alt;
+  int32_t *cntA = parity ? e->cnt_alt : e->cnt, *cntB = parity ? e->cnt : e->cnt_alt;
+  const Variant32 &V = kVariants32[e->variant < num_variants_f32() ? e->variant : 0];
+  const int threads = V.tcx * G;
+  cudaStream_t st = e->stream;
+  int rc = scan_counts(cntA, offB, e->ncell, 0, e->scan_tmp, st);
+  if (rc) return rc;
+  EM2G_CUDA(cudaMemsetAsync(e->cursor, 0, sizeof(int32_t) * e->ncell, st));
+  EM2G_CUDA(cudaMemsetAsync(cntB, 0, sizeof(int32_t) * e->ncell, st));
+  EM2G_CUDA(cudaMemsetAsync(e->counter, 0, sizeof(int), st));
+  std::unique_ptr<EnsPush32> P(new EnsPush32());
+  std::unique_ptr<EnsAke> K(new EnsAke());
+  int p = 0, t = 0;
+  for (size_t r = 0; r < e->runs.size(); ++r) {
+    const EnsRun &R = e->runs[r];
+    const int64_t w = R.g.w;
+    float *fld = e->fld + R.fld_off;
+    for (int s = 0; s < R.P.nsp; ++s, ++p) {
+      Args32 &a = P->pair[p];
+      const float2 *sc = reinterpret_cast<const float2 *>(e->scaled + R.sc_off + (int64_t)s * 6 * w);
+      a.ebx = sc;
+      a.ebz = sc + w;
+      a.eby = sc + 2 * w;
+      a.rho = fld + EM2G_RHO * w;
+      a.jx = fld + EM2G_JXM * w;
+      a.jy = fld + EM2G_JYM * w;
+      a.jz = fld + EM2G_JZM * w;
+      a.A = A;
+      a.slotA = slotA;
+      a.B = B;
+      a.slotB = slotB;
+      a.offA = offA + R.cell0[s];
+      a.offB = offB + R.cell0[s];
+      a.cursor = e->cursor + R.cell0[s];
+      a.cnt_next = cntB + R.cell0[s];
+      a.cap = e->cap;
+      a.nx = R.g.nx;
+      a.ny = R.g.ny;
+      a.nxg = R.g.nxg;
+      a.qd = (float)(R.P.q[s] * R.P.dn[s] / (R.P.dx * R.P.dy));
+      a.dtdx = (float)(R.P.dt / R.P.dx);
+      a.dtdy = (float)(R.P.dt / R.P.dy);
+      a.c = (float)R.P.c;
+      a.ake_partial = e->red + R.red_off[s];
+      const int segs = (R.g.nx + V.tcx - 1) / V.tcx;
+      P->tile0[p] = t;
+      P->segs[p] = segs;
+      t += segs * R.g.ny;
+      K->partial[p] = a.ake_partial;
+      K->count[p] = segs * R.g.ny * (threads / 32);
+      K->scale[p] = R.P.am[s] * R.P.dn[s];
+      K->out[p] = e->dev_out + (int64_t)r * kEnsOut + s;
+    }
+  }
+  P->npairs = p;
+  P->ntiles = t;
+  P->tile0[p] = t;
+  P->counter = e->counter;
+  int per_sm = 0;
+  EM2G_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, V.ens_kernel, threads, 0));
+  if (per_sm < 1) return fail(EM2G_ERR_CUDA, "ensemble push kernel cannot be resident");
+  const int blocks = std::min(per_sm * e->num_sms, t);
+  V.ens_kernel<<<blocks, threads, 0, st>>>(*P);
+  k_ens_ake<<<p, 256, 0, st>>>(*K);
+  EM2G_CUDA(cudaGetLastError());
+  return EM2G_OK;
+}
+
+// pair (r, s) from FP64 staging (6*n doubles, slot order) into the current
+// buffers: histogram, this pair's offsets from its first slot, scatter
+int ens_upload_pair(em2g_ens *e, int r, int s, const double *staging) {
+  const EnsRun &R = e->runs[r];
+  const int64_t n = R.n[s], nc = (int64_t)R.g.nx * R.g.ny, c0 = R.cell0[s];
+  float *P = e->parity ? e->p32_alt : e->p32;
+  int32_t *slot = e->parity ? e->slot_alt : e->slot;
+  int32_t *off = e->parity ? e->off_alt : e->off;
+  int32_t *cnt = e->parity ? e->cnt_alt : e->cnt;
+  cudaStream_t st = e->stream;
+  EM2G_CUDA(cudaMemsetAsync(cnt + c0, 0, sizeof(int32_t) * nc, st));
+  EM2G_CUDA(cudaMemsetAsync(e->cursor + c0, 0, sizeof(int32_t) * nc, st));
+  const unsigned nb = (unsigned)((n + 255) / 256);
+  if (n > 0) k_hist64<<<nb, 256, 0, st>>>(staging, n, R.g.nx, R.g.ny, cnt + c0);
+  int rc = scan_counts(cnt + c0, off + c0, nc, (int32_t)R.base[s], e->scan_tmp, st);
+  if (rc) return rc;
+  if (n > 0)
+    k_scatter_to_f32<<<nb, 256, 0, st>>>(staging, n, R.g.nx, R.g.ny, off + c0, e->cursor + c0,
+                                         P, slot, e->cap);
+  EM2G_CUDA(cudaGetLastError());
+  return EM2G_OK;
+}
+
+// pair (r, s) from the current buffers to FP64 staging in slot order
+int ens_download_pair(em2g_ens *e, int r, int s, double *staging) {
+  const EnsRun &R = e->runs[r];
+  const int64_t n = R.n[s];
+  if (n == 0) return EM2G_OK;
+  const float *P = e->parity ? e->p32_alt : e->p32;
+  const int32_t *slot = e->parity ? e->slot_alt : e->slot;
+  const int32_t *off = e->parity ? e->off_alt : e->off;
+  const int64_t nb = ((int64_t)R.g.nx * R.g.ny * G + 255) / 256;
+  k_gather_from_f32<<<(unsigned)nb, 256, 0, e->stream>>>(P, slot, off + R.cell0[s], e->cap, R.g.nx,
+                                                          R.g.ny, staging, n);
+  EM2G_CUDA(cudaGetLastError());
+  return EM2G_OK;
+}
+
+// kernels one ens_push enqueues: scan (3), push, kinetic energies
+int ens_push_kernels_per_step(const em2g_ens *) { return 5; }
 
 }  // namespace em2g

@@ -77,10 +77,11 @@ __global__ void __launch_bounds__(kScanBlock) k_scan_sums(int32_t *bsum, int nb)
   if (threadIdx.x == 0) bsum[nb] = carry;
 }
 
-__global__ void k_scan_add(int32_t *out, int64_t n, const int32_t *__restrict__ bsum, int nb) {
+__global__ void k_scan_add(int32_t *out, int64_t n, const int32_t *__restrict__ bsum, int nb,
+                           int32_t base) {
   const int64_t i = (int64_t)blockIdx.x * kScanBlock + threadIdx.x;
-  if (i < n) out[i] += bsum[blockIdx.x];
-  if (i == 0) out[n] = bsum[nb];
+  if (i < n) out[i] += bsum[blockIdx.x] + base;
+  if (i == 0) out[n] = bsum[nb] + base;
 }
 
 // histogram of the particles' current cells
@@ -114,8 +115,7 @@ __global__ void k_scatter(const double *__restrict__ A, const int32_t *__restric
 int sort_init(em2g_ctx *c) {
   c->ncell = (int64_t)c->g.nx * c->g.ny;
   const int64_t nc = c->ncell;
-  const int64_t nb = (nc + kScanBlock - 1) / kScanBlock;
-  EM2G_CUDA(cudaMalloc(&c->scan_tmp, sizeof(int32_t) * (nb + 1)));
+  EM2G_CUDA(cudaMalloc(&c->scan_tmp, sizeof(int32_t) * scan_tmp_size(nc)));
   for (int s = 0; s < c->P.nsp; ++s) {
     Species &S = c->sp[s];
     EM2G_CUDA(cudaMalloc(&S.off, sizeof(int32_t) * (nc + 1)));
@@ -141,15 +141,21 @@ void sort_free(em2g_ctx *c) {
   }
 }
 
-int scan_cells(em2g_ctx *c, const int32_t *cnt, int32_t *off) {
-  const int64_t n = c->ncell;
+int64_t scan_tmp_size(int64_t n) { return (n + kScanBlock - 1) / kScanBlock + 1; }
+
+int scan_counts(const int32_t *cnt, int32_t *off, int64_t n, int32_t base, int32_t *tmp,
+                cudaStream_t stream) {
   const int nb = (int)((n + kScanBlock - 1) / kScanBlock);
-  k_scan_local<<<nb, kScanBlock, 0, c->stream>>>(cnt, off, n, c->scan_tmp);
-  k_scan_sums<<<1, kScanBlock, 0, c->stream>>>(c->scan_tmp, nb);
-  k_scan_add<<<nb, kScanBlock, 0, c->stream>>>(off, n, c->scan_tmp, nb);
-  c->launches += 3;
+  k_scan_local<<<nb, kScanBlock, 0, stream>>>(cnt, off, n, tmp);
+  k_scan_sums<<<1, kScanBlock, 0, stream>>>(tmp, nb);
+  k_scan_add<<<nb, kScanBlock, 0, stream>>>(off, n, tmp, nb, base);
   EM2G_CUDA(cudaGetLastError());
   return EM2G_OK;
+}
+
+int scan_cells(em2g_ctx *c, const int32_t *cnt, int32_t *off) {
+  c->launches += 3;
+  return scan_counts(cnt, off, c->ncell, 0, c->scan_tmp, c->stream);
 }
 
 int sort_full(em2g_ctx *c, int isp) {

@@ -55,3 +55,55 @@ def test_invalid_params_rejected_without_gpu():
     L.em2g_params_init(C.byref(P))
     P.struct_size = 12
     assert L.em2g_create(C.byref(P), C.byref(h)) == _lib.ERR_INVALID
+
+
+def test_invalid_ensembles_rejected_without_gpu():
+    """em2g_ens_create checks every run before any device call."""
+    from maccpic_b200 import _lib
+    L = _lib.lib()
+
+    def runs(n, **kw):
+        arr = (_lib.Em2gParams * n)()
+        for k in range(n):
+            L.em2g_params_init(C.byref(arr[k]))
+            arr[k].nx, arr[k].ny, arr[k].dx, arr[k].dy, arr[k].dt = 32, 16, 0.5, 0.5, 0.05
+            arr[k].precision = _lib.FP32
+            arr[k].np_max[0] = arr[k].np_max[1] = 100
+            for name, v in kw.items():
+                setattr(arr[k], name, v)
+        return arr
+
+    h = C.c_void_p()
+    assert L.em2g_ens_create(runs(1), 0, C.byref(h)) == _lib.ERR_INVALID
+    assert L.em2g_ens_create(runs(129), 129, C.byref(h)) == _lib.ERR_INVALID
+    assert L.em2g_ens_create(runs(2, precision=_lib.FP64), 2, C.byref(h)) == _lib.ERR_INVALID
+    assert b"FP32" in L.em2g_last_error()
+    assert L.em2g_ens_create(runs(2, energy_mode=1), 2, C.byref(h)) == _lib.ERR_INVALID
+    a = runs(2)
+    a[1].np_max[1] = 0
+    assert L.em2g_ens_create(a, 2, C.byref(h)) == _lib.ERR_INVALID
+    assert b"np_max" in L.em2g_last_error()
+    a = runs(2)
+    a[1].device = 1
+    assert L.em2g_ens_create(a, 2, C.byref(h)) == _lib.ERR_INVALID
+    # 81 runs of 2 species: 162 pairs
+    assert L.em2g_ens_create(runs(81), 81, C.byref(h)) == _lib.ERR_INVALID
+    assert b"pairs" in L.em2g_last_error()
+    a = runs(1)
+    a[0].np_max[0] = a[0].np_max[1] = 1 << 30
+    assert L.em2g_ens_create(a, 1, C.byref(h)) == _lib.ERR_RANGE
+    assert h.value is None
+
+
+def test_harris_ensemble_draws_the_uneven_batch():
+    from maccpic_b200.ensemble import harris_ensemble
+    cfgs = harris_ensemble(64, seed=0)
+    assert len(cfgs) == 64
+    assert all(128 <= c.nx <= 1024 and c.ny * 2 == c.nx and c.nx % 16 == 0 for c in cfgs)
+    assert all(16 <= c.ppc <= 64 for c in cfgs)
+    assert {c.mass_ratio for c in cfgs} == {25.0, 49.0, 100.0}
+    assert len({c.seed for c in cfgs}) == 64
+    assert len({c.psi0_over_b0di for c in cfgs}) == 64
+    # log-uniform: both ends of the range are populated
+    assert min(c.nx for c in cfgs) < 256 and max(c.nx for c in cfgs) > 512
+    assert harris_ensemble(64, seed=0) == cfgs

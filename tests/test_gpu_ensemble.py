@@ -1,0 +1,186 @@
+"""Ensembles (maccpic_b200/ensemble.py, em2g_ens_* of include/em2g.h).
+
+Each run of an ensemble must advance exactly as an ordinary FP32 context
+of the same parameters does: after one step the particles are bitwise
+equal (same arithmetic on the same fields), the fields differ only by the
+order of the FP32 deposit atomics; over many steps the two stay within
+FP32 round-off growth.  The graph replay and the direct launches do the
+same work.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _cfgs():
+    from maccpic_b200.loader import HarrisConfig
+    return [HarrisConfig(nx=64, ny=32, ppc=8, seed=1),
+            HarrisConfig(nx=96, ny=48, ppc=4, seed=2, mass_ratio=49.0, psi0_over_b0di=0.13),
+            HarrisConfig(nx=128, ny=64, ppc=6, seed=3, mass_ratio=100.0, isav=5)]
+
+
+def _state(cfg):
+    from maccpic_b200 import loader
+    return loader.initial_fields(cfg), loader.sample_particles(cfg)
+
+
+def _single(cfg, fld, parts):
+    from maccpic_b200 import _lib
+    from maccpic_b200.em2 import Em2Gpu
+    n = parts[0].shape[1]
+    g = Em2Gpu(cfg.run_params(np_max=[n, n], precision=_lib.FP32))
+    g.set_fields(fld)
+    for s, p in enumerate(parts):
+        g.set_particles(s, p)
+    return g
+
+
+def _ensemble(cfgs, states):
+    from maccpic_b200 import _lib
+    from maccpic_b200.ensemble import Em2Ensemble
+    runs = []
+    for c, (fld, parts) in zip(cfgs, states):
+        n = parts[0].shape[1]
+        runs.append(c.run_params(np_max=[n, n], precision=_lib.FP32))
+    e = Em2Ensemble(runs)
+    for r, (fld, parts) in enumerate(states):
+        e.set_fields(r, fld)
+        for s, p in enumerate(parts):
+            e.set_particles(r, s, p)
+    return e
+
+
+def rel(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-30)
+
+
+def test_particle_roundtrip(gpu):
+    cfgs = _cfgs()
+    states = [_state(c) for c in cfgs]
+    with _ensemble(cfgs, states) as e:
+        for r, (_, parts) in enumerate(states):
+            for s, p in enumerate(parts):
+                q = e.get_particles(r, s)
+                assert np.abs(q[:2] - p[:2]).max() < 1e-6
+                np.testing.assert_allclose(q[2:], p[2:], rtol=1e-6, atol=1e-9)
+
+
+def test_first_step_matches_single_runs(gpu):
+    cfgs = _cfgs()
+    states = [_state(c) for c in cfgs]
+    with _ensemble(cfgs, states) as e:
+        r_ens = e.step(1)
+        for r, c in enumerate(cfgs):
+            with _single(c, *states[r]) as g:
+                r1 = g.step(1)
+                assert r_ens["cg_iters"][r] == r1["cg_iters"]
+                np.testing.assert_allclose(r_ens["ake"][r, :2], r1["ake"], rtol=1e-12)
+                for s in range(2):
+                    np.testing.assert_array_equal(e.get_particles(r, s), g.get_particles(s))
+                fe, fg = e.get_fields(r), g.get_fields()
+                for k in range(6):
+                    assert rel(fe[k], fg[k]) < 1e-4, (r, k)
+
+
+def test_many_steps_track_single_runs(gpu):
+    """25 steps: every run crosses an isav step (filters and energies)."""
+    cfgs = _cfgs()
+    states = [_state(c) for c in cfgs]
+    with _ensemble(cfgs, states) as e:
+        out = None
+        for _ in range(25):
+            out = e.step(1)
+        assert e.it == 25
+        for r, c in enumerate(cfgs):
+            with _single(c, *states[r]) as g:
+                for _ in range(25):
+                    r1 = g.step(1)
+                np.testing.assert_allclose(out["ake"][r, :2], r1["ake"], rtol=1e-4)
+                if 25 % c.isav == 0:
+                    np.testing.assert_allclose(out["energies"][r], r1["energies"], rtol=1e-3,
+                                               atol=1e-12)
+                else:
+                    assert np.isnan(out["energies"][r]).all()
+                assert abs(int(out["cg_iters"][r]) - r1["cg_iters"]) <= 1
+                fe, fg = e.get_fields(r), g.get_fields()
+                for k in range(3, 6):
+                    assert rel(fe[k], fg[k]) < 1e-3, (r, k)
+                de, dg = e.diagnostics(r), g.diagnostics()
+                np.testing.assert_allclose(de["flux"], dg["flux"], rtol=1e-3)
+
+
+def test_graph_and_direct_launches_agree(gpu):
+    cfgs = _cfgs()
+    states = [_state(c) for c in cfgs]
+    with _ensemble(cfgs, states) as a, _ensemble(cfgs, states) as b:
+        b.set_graph(False)
+        for _ in range(6):
+            ra = a.step(1)
+            rb = b.step(1)
+        np.testing.assert_allclose(ra["ake"], rb["ake"], rtol=1e-4)
+        ca, cb = a.counters(), b.counters()
+        assert ca["graph_launches"] == 6 and cb["graph_launches"] == 0
+        # one scan (3), push, kinetic energies, prescale, tick, 14 field stages
+        assert ca["kernels_per_step"] == cb["kernels_per_step"] == 21
+        assert ca["kernel_launches"] == 6 * 21
+        for r in range(len(cfgs)):
+            fa, fb = a.get_fields(r), b.get_fields(r)
+            for k in range(3, 6):
+                assert rel(fa[k], fb[k]) < 1e-4
+
+
+def test_every_variant_runs(gpu):
+    from maccpic_b200 import _lib
+    cfgs = _cfgs()[:2]
+    states = [_state(c) for c in cfgs]
+    with _ensemble(cfgs, states) as ref:
+        ref.step(1)
+        want = [[ref.get_particles(r, s) for s in range(2)] for r in range(2)]
+        for v in range(1, 5):
+            with _ensemble(cfgs, states) as e:
+                e.set_variant(v)
+                e.step(1)
+                for r in range(2):
+                    for s in range(2):
+                        np.testing.assert_array_equal(e.get_particles(r, s), want[r][s])
+
+
+def test_current_filter_in_an_ensemble(gpu):
+    import dataclasses
+    cfgs = [dataclasses.replace(c, smooth_current=1) for c in _cfgs()[:2]]
+    states = [_state(c) for c in cfgs]
+    with _ensemble(cfgs, states) as e:
+        e.step(3)
+        assert e.counters()["kernels_per_step"] == 23
+        for r, c in enumerate(cfgs):
+            with _single(c, *states[r]) as g:
+                g.step(3)
+                fe, fg = e.get_fields(r), g.get_fields()
+                for k in range(6):
+                    assert rel(fe[k], fg[k]) < 1e-4, (r, k)
+
+
+def test_errors(gpu):
+    from maccpic_b200 import _lib
+    from maccpic_b200._lib import Em2gError
+    cfgs = _cfgs()[:2]
+    states = [_state(c) for c in cfgs]
+    e = _ensemble(cfgs, states)
+    with e:
+        with pytest.raises(Em2gError) as ei:
+            e.set_particles(0, 0, states[0][1][0][:, :10])
+        assert ei.value.status == _lib.ERR_RANGE
+        bad = states[0][1][0].copy()
+        bad[0, 3] = cfgs[0].nx + 1.0
+        with pytest.raises(Em2gError) as ei:
+            e.set_particles(0, 0, bad)
+        assert ei.value.status == _lib.ERR_RANGE
+        with pytest.raises(IndexError):
+            e.get_fields(5)
+    from maccpic_b200.ensemble import Em2Ensemble
+    n = states[0][1][0].shape[1]
+    with Em2Ensemble([cfgs[0].run_params(np_max=[n, n], precision=_lib.FP32)]) as f:
+        with pytest.raises(Em2gError) as ei:
+            f.step(1)
+        assert ei.value.status == _lib.ERR_INVALID
