@@ -54,6 +54,7 @@ def parse():
     ap.add_argument("--no-fp64-compare", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true")
     return ap.parse_args()
 
 
@@ -361,8 +362,12 @@ def run_ours(args):
 
     e2e = None
     if rank == 0 and not args.no_e2e:
-        rp = cfg.run_params(precision=_lib.FP32 if fp32 else _lib.FP64)
-        e2e = run_e2e(args, cfg, rp, fields, parts_host)
+        rp = cfg.run_params(precision=_lib.FP32 if fp32 else _lib.FP64,
+                            sort_interval=main["tuned"]["sort_interval"])
+        e2e = run_e2e(args, cfg, rp, fields, parts_host, main["tuned"]["variant"])
+    ens = None
+    if rank == 0 and ws == 1 and fp32 and not args.no_ensemble:
+        ens = run_ensemble(args, local)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(cfg, fields, [p.numpy() for p in parts_host])
@@ -385,7 +390,9 @@ def run_ours(args):
                                        if ws > 1 else "1 GPU"),
                        "cg_iters_mean": sum(main["cg"]) / len(main["cg"]),
                        "push_variant": main["tuned"]["name"],
-                       "variant_times_ms": main["tuned"]["times_ms"]},
+                       "variant_times_ms": main["tuned"]["times_ms"],
+                       "sort_interval": main["tuned"]["sort_interval"],
+                       "interval_step_ms": main["tuned"]["interval_ms"]},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "kernel": kernel,
                          "peak_kind": peak_kind, "bytes_per_launch": bytes_launch,
@@ -394,6 +401,7 @@ def run_ours(args):
             "clocks": main["clocks"],
             "mixed_vs_fp64": compare,
             "adjoint_over_forward": None,
+            "ensemble": ens,
             "e2e": e2e,
             "cpu_baseline": cpu,
         }
@@ -403,7 +411,37 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def run_e2e(args, cfg, rp, fields, parts_host):
+def run_ensemble(args, local):
+    """The uneven batch of double-Harris runs (64 runs, grids log-uniform
+    from 128x64 to 1024x512, 16-64 particles per cell, mass ratio 25/49/100)
+    as one ensemble: one graph launch per step."""
+    import torch
+    from maccpic_b200.ensemble import harris_ensemble, load_harris
+    cfgs = harris_ensemble(64, seed=0)
+    ens = load_harris(cfgs, device=f"cuda:{local}")
+    try:
+        ens.step(args.warmup)
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        start.record()
+        out = ens.step(args.steps)
+        stop.record()
+        torch.cuda.synchronize()
+        ms = start.elapsed_time(stop)
+        cnt = ens.counters()
+        n = ens.particles
+        return {"workload": "harris_ensemble_64runs", "runs": len(cfgs), "particles": n,
+                "grids": [min(c.nx for c in cfgs), max(c.nx for c in cfgs)],
+                "value": n * args.steps / (ms / 1e3), "unit": METRIC,
+                "ms_per_step": ms / args.steps, "graph": True,
+                "kernels_per_step": cnt["kernels_per_step"],
+                "cg_iters_max": int(out["cg_iters"].max())}
+    finally:
+        ens.close()
+        torch.cuda.empty_cache()
+
+
+def run_e2e(args, cfg, rp, fields, parts_host, variant=0):
     """Drop-in path from host memory: upload, K steps of move_curnt + fields
     reading ake / CG count / energies back every step, download everything."""
     import torch
@@ -413,6 +451,7 @@ def run_e2e(args, cfg, rp, fields, parts_host):
     fnp = fields_pin.numpy()
     pnp = [p.numpy() for p in parts_host]
     g = Em2Gpu(rp)
+    g.set_variant(variant)
     out_f = torch.empty_like(fields_pin).pin_memory().numpy()
     out_p = [torch.empty_like(p).pin_memory().numpy() for p in parts_host]
     # warm-up (not timed): one full pass

@@ -86,7 +86,9 @@ typedef struct em2g_params {
   double cg_eps;         /* 1e-9 in cgm (pic/fields.f90:519) */
   double qme, wpe;       /* -1, 1 (pic/input.f90:43) */
   int32_t device;        /* CUDA device ordinal */
-  int32_t sort_interval; /* reserved, set 0 (the fast path re-sorts every step) */
+  int32_t sort_interval; /* FP32 fast path: regroup particles by cell on every
+                            k-th push and update them in place in between
+                            (0 or 1: every push; k * c * dt < dx, dy) */
   int32_t smooth_current; /* 1: smooth2 each current array after the fold, every
                              step (not in em2, which filters only rho and, every
                              isav steps, E and B); 0 = em2 */
@@ -207,6 +209,8 @@ int em2g_num_variants(em2g_ctx *ctx, int *n);
 int em2g_set_variant(em2g_ctx *ctx, int variant);
 /* current variant and its name (name may be NULL) */
 int em2g_get_variant(em2g_ctx *ctx, int *variant, char *name, int name_len);
+/* em2g_params.sort_interval, changed between steps (same rules) */
+int em2g_set_sort_interval(em2g_ctx *ctx, int sort_interval);
 
 /* ---- instrumentation ------------------------------------------------- */
 /* kernel launches since the last reset; with timing on, the number of

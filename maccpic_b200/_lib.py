@@ -31,7 +31,7 @@ EXPORTS = [
     "em2g_fields", "em2g_smooth2", "em2g_step", "em2g_set_particles_device",
     "em2g_move_curnt", "em2g_set_timing", "em2g_get_counters", "em2g_reset_counters",
     "em2g_smooth2_static", "em2g_diagnostics", "em2g_num_variants", "em2g_set_variant",
-    "em2g_get_variant",
+    "em2g_get_variant", "em2g_set_sort_interval",
     "em2g_ens_create", "em2g_ens_destroy", "em2g_ens_num_runs", "em2g_ens_set_stream",
     "em2g_ens_set_graph", "em2g_ens_set_variant", "em2g_ens_set_fields", "em2g_ens_get_fields",
     "em2g_ens_set_particles", "em2g_ens_set_particles_device", "em2g_ens_get_particles",
@@ -112,6 +112,7 @@ def lib() -> C.CDLL:
         "em2g_num_variants": (C.c_int, [ctx, ip]),
         "em2g_set_variant": (C.c_int, [ctx, C.c_int]),
         "em2g_get_variant": (C.c_int, [ctx, ip, C.c_char_p, C.c_int]),
+        "em2g_set_sort_interval": (C.c_int, [ctx, C.c_int]),
         "em2g_ens_create": (C.c_int, [pp, C.c_int, C.POINTER(C.c_void_p)]),
         "em2g_ens_destroy": (C.c_int, [ctx]),
         "em2g_ens_num_runs": (C.c_int, [ctx, ip]),

@@ -1,11 +1,15 @@
-"""Autotuner for the fast push: picks the kernel variant (cells per CTA and
-CTAs per SM) by timing each one on the live state.
+"""Autotuner for the fast push: picks the kernel variant (cells per CTA =
+the tile width, and CTAs per SM, which sets the particles in flight per SM)
+and the sort interval by timing them on the live state.
 
 The variants are compiled into libem2g (em2g_num_variants); they compute the
-same step, so tuning simply advances the run by a few steps per variant.
-The particle sort is fused into the push and runs every step, so there is no
-sort interval left to tune.  The winner is remembered per GPU model, grid,
-particles per cell and precision in a small JSON cache.
+same step, so tuning simply advances the run by a few steps per candidate.
+The sort interval trades the regrouping work of the push (per-cell write
+positions, the scan of the cell counts) against the growing share of
+particles outside their group cell, which deposit with atomics: the
+interval is timed as whole steps over full regrouping cycles.  The winner is
+remembered per GPU model, grid, particles per cell and precision in a small
+JSON cache.
 """
 from __future__ import annotations
 
@@ -22,10 +26,23 @@ def _key(run, particles: int) -> str:
     return f"{dev}|{run.p.nx}x{run.p.ny}|ppc{ppc:.1f}|prec{run.p.precision}"
 
 
+def _step_ms(run, k: int, cycles: int) -> float:
+    """Mean wall time of a step at sort interval k over whole cycles."""
+    import time
+    run.set_sort_interval(k)
+    run.step(k)  # align to a regrouping
+    n = k * cycles
+    t = time.perf_counter()
+    run.step(n)
+    return (time.perf_counter() - t) * 1e3 / n
+
+
 def autotune(run, particles: int, steps: int = 2, warm: int = 1, cache: str | None = DEFAULT_CACHE,
-             use_cache: bool = True) -> dict:
-    """Time every variant on `run` (an Em2Gpu with its state loaded) and keep
-    the fastest.  Returns {"variant", "name", "times_ms", "from_cache"}."""
+             use_cache: bool = True, intervals=None) -> dict:
+    """Time every variant on `run` (an Em2Gpu with its state loaded), keep the
+    fastest, then time the sort intervals with it (FP32 only).  Returns
+    {"variant", "name", "times_ms", "sort_interval", "interval_ms",
+    "from_cache"}."""
     key = _key(run, particles)
     table = {}
     if cache and os.path.exists(cache):
@@ -34,9 +51,12 @@ def autotune(run, particles: int, steps: int = 2, warm: int = 1, cache: str | No
         except (OSError, ValueError):
             table = {}
     n = run.num_variants()
-    if use_cache and key in table and 0 <= table[key]["variant"] < n:
+    if (use_cache and key in table and 0 <= table[key]["variant"] < n
+            and "sort_interval" in table[key]):
         run.set_variant(table[key]["variant"])
+        run.set_sort_interval(table[key]["sort_interval"])
         return {**table[key], "from_cache": True}
+    run.set_sort_interval(1)
     times = []
     for v in range(n):
         run.set_variant(v)
@@ -51,8 +71,17 @@ def autotune(run, particles: int, steps: int = 2, warm: int = 1, cache: str | No
         times.append(c["push_ms"] / max(1, c["push_launches_timed"]))
     best = min(range(n), key=lambda v: times[v])
     run.set_variant(best)
+    kmax = run.max_sort_interval()
+    if intervals is None:
+        intervals = sorted({k for k in (1, 2, 3, 4, 6, kmax) if 1 <= k <= kmax})
+    interval_ms = {}
+    for k in intervals:
+        interval_ms[k] = _step_ms(run, k, cycles=max(1, 12 // k))
+    k_best = min(interval_ms, key=interval_ms.get)
+    run.set_sort_interval(k_best)
     run.reset_counters()
-    result = {"variant": best, "name": run.variant()[1], "times_ms": times}
+    result = {"variant": best, "name": run.variant()[1], "times_ms": times,
+              "sort_interval": k_best, "interval_ms": {str(k): v for k, v in interval_ms.items()}}
     if cache:
         table[key] = result
         try:

@@ -168,6 +168,15 @@ int validate(const em2g_params *p) {
   if (p->cg_maxits < 1) return fail(EM2G_ERR_INVALID, "cg_maxits must be >= 1");
   if (p->smooth_current != 0 && p->smooth_current != 1)
     return fail(EM2G_ERR_INVALID, "smooth_current must be 0 or 1");
+  if (p->sort_interval < 0) return fail(EM2G_ERR_INVALID, "sort_interval must be >= 0");
+  if (p->sort_interval > 1) {
+    if (p->precision != EM2G_FP32)
+      return fail(EM2G_ERR_INVALID, "sort_interval > 1 needs the FP32 path");
+    // positions drift from their group cell by < c*dt per step between
+    // regroupings and must stay within one cell of it
+    if (p->sort_interval * p->c * p->dt >= p->dx || p->sort_interval * p->c * p->dt >= p->dy)
+      return fail(EM2G_ERR_INVALID, "sort_interval * c * dt must be < dx and dy");
+  }
   for (int s = 0; s < p->nsp; ++s) {
     if (p->np_max[s] < 0 || p->np_max[s] > ((int64_t)1 << 31) - 1)
       return fail(EM2G_ERR_INVALID, "np_max out of range");
@@ -649,6 +658,16 @@ int em2g_get_variant(em2g_ctx *c, int *v, char *name, int name_len) {
     std::strncpy(name, s, (size_t)name_len - 1);
     name[name_len - 1] = '\0';
   }
+  return EM2G_OK;
+}
+
+int em2g_set_sort_interval(em2g_ctx *c, int k) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  em2g_params p = c->P;
+  p.sort_interval = k;
+  if ((rc = validate(&p))) return rc;
+  c->P.sort_interval = k;
   return EM2G_OK;
 }
 

@@ -59,6 +59,7 @@ struct Species {
   // FP32 contexts: xr, yr (offsets in the cell of the particle's range),
   // ux, uy, uz; 5*cap floats, always grouped by cell (push_fast_f32.cu)
   float *p32 = nullptr, *p32_alt = nullptr;
+  int since_sort = 0;  // FP32 pushes in place since the last regrouping
 };
 
 // Device workspace of the Poisson/cgm solve (pic/fields.f90:370-651).

@@ -108,6 +108,8 @@ int em2g_ens_create(const em2g_params *runs, int nruns, em2g_ens **out) {
     if (rc) return rc;
     if (P.precision != EM2G_FP32) return fail(EM2G_ERR_INVALID, "ensemble runs are FP32");
     if (P.energy_mode != 0) return fail(EM2G_ERR_INVALID, "ensemble runs use energy_mode 0");
+    if (P.sort_interval > 1)
+      return fail(EM2G_ERR_INVALID, "ensemble runs regroup every step (sort_interval 0 or 1)");
     if (P.device != runs[0].device) return fail(EM2G_ERR_INVALID, "runs on different devices");
     for (int s = 0; s < P.nsp; ++s) {
       if (P.np_max[s] < 1) return fail(EM2G_ERR_INVALID, "np_max must be the particle count");

@@ -194,7 +194,11 @@ __device__ __forceinline__ int wrap(int i, int n) { return i < 0 ? i + n : (i >=
 
 // One row segment: cells x0 .. x0+TCX-1 of row y0, by a CTA of TCX*G
 // threads; `blk` numbers the segment for the kinetic-energy partials.
-template <int TCX>
+// INPLACE: a step between regroupings -- every particle keeps its slot in
+// A (B == A) and its position stays relative to its group cell, so the
+// offsets drift by at most c*dt/dx per step (the interval is bounded so
+// that they stay in (-1, 2)); the counts of the new cells are still taken.
+template <int TCX, bool INPLACE>
 __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, int64_t blk,
                                              float2 (*win)[WY][TCX + 5]) {
   constexpr int kThreads = TCX * G;
@@ -331,6 +335,14 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
         deposit_j_atomic(a, nhx, nhy, nnx, nny, qx, qy, qz);
         atomicAdd(a.cnt_next + ncy * nx + ncx, 1);
       }
+      if (INPLACE) {
+        a.B[i] = mx + (float)ox;
+        a.B[cap + i] = my + (float)oy;
+        a.B[2 * cap + i] = ux;
+        a.B[3 * cap + i] = uy;
+        a.B[4 * cap + i] = uz;
+        continue;
+      }
       // write back grouped by the cell of the start of this step: particles
       // that started it in cell k take the next slots from the front of k's
       // segment in processing order (a running count per group, no atomics);
@@ -396,11 +408,11 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
 
 // TCX cells per CTA (a row segment), MINB: CTAs per SM the register
 // allocation must allow (the autotuner's two knobs)
-template <int TCX, int MINB>
+template <int TCX, int MINB, bool INPLACE>
 __global__ void __launch_bounds__(TCX * G, MINB) k_push_cells_f32(Args32 a) {
   __shared__ float2 win[3][WY][TCX + 5];
-  push_segment<TCX>(a, (int)blockIdx.x * TCX, (int)blockIdx.y,
-                    (int64_t)blockIdx.y * gridDim.x + blockIdx.x, win);
+  push_segment<TCX, INPLACE>(a, (int)blockIdx.x * TCX, (int)blockIdx.y,
+                             (int64_t)blockIdx.y * gridDim.x + blockIdx.x, win);
 }
 
 // Ensemble: every (run, species) pair of an ensemble in one persistent
@@ -425,7 +437,7 @@ __global__ void __launch_bounds__(TCX * G, MINB) k_ens_push_f32(const __grid_con
     const int lt = t - e.tile0[lo];
     const int segs = e.segs[lo];
     const int row = lt / segs;
-    push_segment<TCX>(e.pair[lo], (lt - row * segs) * TCX, row, lt, win);
+    push_segment<TCX, false>(e.pair[lo], (lt - row * segs) * TCX, row, lt, win);
   }
 }
 
@@ -433,15 +445,17 @@ struct Variant32 {
   const char *name;
   int tcx;
   void (*kernel)(Args32);
+  void (*kernel_inplace)(Args32);
   void (*ens_kernel)(const EnsPush32);
 };
+#define EM2G_VARIANT32(T, M)                                                          \
+  {"f32 tcx" #T " minb" #M, T, k_push_cells_f32<T, M, false>, k_push_cells_f32<T, M, true>, \
+   k_ens_push_f32<T, M>}
 const Variant32 kVariants32[] = {
-    {"f32 tcx32 minb4", 32, k_push_cells_f32<32, 4>, k_ens_push_f32<32, 4>},
-    {"f32 tcx32 minb5", 32, k_push_cells_f32<32, 5>, k_ens_push_f32<32, 5>},
-    {"f32 tcx32 minb6", 32, k_push_cells_f32<32, 6>, k_ens_push_f32<32, 6>},
-    {"f32 tcx64 minb2", 64, k_push_cells_f32<64, 2>, k_ens_push_f32<64, 2>},
-    {"f32 tcx64 minb3", 64, k_push_cells_f32<64, 3>, k_ens_push_f32<64, 3>},
+    EM2G_VARIANT32(32, 4), EM2G_VARIANT32(32, 5), EM2G_VARIANT32(32, 6),
+    EM2G_VARIANT32(64, 2), EM2G_VARIANT32(64, 3),
 };
+#undef EM2G_VARIANT32
 
 // kinetic energy of every pair of an ensemble: block p sums pair p's
 // partials in a fixed order (pic/move.f90:183, :208)
@@ -586,18 +600,29 @@ int launch_push_cells_f32(em2g_ctx *c, int isp) {
   const int64_t nparts = (int64_t)grid.x * grid.y * (threads / 32);
   if (nparts > c->red_blocks) return fail(EM2G_ERR_RANGE, "grid exceeds reduction scratch");
   const int nb = (int)nparts;
-  int rc = scan_cells(c, S.cnt, S.off_alt);
-  if (rc) return rc;
-  EM2G_CUDA(cudaMemsetAsync(S.cursor, 0, sizeof(int32_t) * c->ncell, c->stream));
+  // regroup on every sort_interval-th push (every push for 0 or 1); the
+  // pushes in between update the particles in place
+  const bool inplace = c->P.sort_interval > 1 && S.since_sort + 1 < c->P.sort_interval;
+  int rc;
+  if (inplace) {
+    a.B = S.p32;
+    ++S.since_sort;
+  } else {
+    if ((rc = scan_cells(c, S.cnt, S.off_alt))) return rc;
+    EM2G_CUDA(cudaMemsetAsync(S.cursor, 0, sizeof(int32_t) * c->ncell, c->stream));
+    S.since_sort = 0;
+  }
   EM2G_CUDA(cudaMemsetAsync(S.cnt_alt, 0, sizeof(int32_t) * c->ncell, c->stream));
   if ((rc = timing_begin(c))) return rc;
-  V.kernel<<<grid, threads, 0, c->stream>>>(a);
+  (inplace ? V.kernel_inplace : V.kernel)<<<grid, threads, 0, c->stream>>>(a);
   c->launches += 1;
   EM2G_CUDA(cudaGetLastError());
   if ((rc = timing_end(c))) return rc;
-  std::swap(S.p32, S.p32_alt);
-  std::swap(S.slot, S.slot_alt);
-  std::swap(S.off, S.off_alt);
+  if (!inplace) {
+    std::swap(S.p32, S.p32_alt);
+    std::swap(S.slot, S.slot_alt);
+    std::swap(S.off, S.off_alt);
+  }
   std::swap(S.cnt, S.cnt_alt);
   return launch_ake_finish(c, isp, nb);
 }
@@ -622,6 +647,7 @@ int upload_f32(em2g_ctx *c, int isp, const double *staging, int64_t n) {
   c->launches += 2;
   S.n = n;
   S.sorted = true;
+  S.since_sort = 0;
   return EM2G_OK;
 }
 

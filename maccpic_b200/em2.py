@@ -171,6 +171,19 @@ class Em2Gpu:
     def set_variant(self, v: int) -> None:
         check(self._L.em2g_set_variant(self._h, int(v)))
 
+    def set_sort_interval(self, k: int) -> None:
+        """Regroup particles by cell every k-th step (FP32; k*c*dt < dx, dy)."""
+        check(self._L.em2g_set_sort_interval(self._h, int(k)))
+        self.p.sort_interval = int(k)
+
+    def max_sort_interval(self) -> int:
+        """The largest interval the drift bound allows (1 for FP64)."""
+        if self.p.precision != _lib.FP32:
+            return 1
+        import math
+        step = self.p.c * self.p.dt / min(self.p.dx, self.p.dy)
+        return max(1, math.ceil(1.0 / step) - 1)
+
     def variant(self):
         """(index, name) of the fast-push kernel variant in use."""
         v = C.c_int()

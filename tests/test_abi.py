@@ -107,3 +107,21 @@ def test_harris_ensemble_draws_the_uneven_batch():
     # log-uniform: both ends of the range are populated
     assert min(c.nx for c in cfgs) < 256 and max(c.nx for c in cfgs) > 512
     assert harris_ensemble(64, seed=0) == cfgs
+
+
+def test_sort_interval_rules_without_gpu():
+    from maccpic_b200 import _lib
+    L = _lib.lib()
+    P = _lib.Em2gParams()
+    h = C.c_void_p()
+    L.em2g_params_init(C.byref(P))
+    P.nx, P.ny, P.dx, P.dy, P.dt = 32, 16, 0.5, 0.5, 0.05
+    P.sort_interval = 2                         # FP64 regroups every step
+    assert L.em2g_create(C.byref(P), C.byref(h)) == _lib.ERR_INVALID
+    assert b"FP32" in L.em2g_last_error()
+    P.precision = _lib.FP32
+    P.sort_interval = 10                        # 10 * c * dt = dx
+    assert L.em2g_create(C.byref(P), C.byref(h)) == _lib.ERR_INVALID
+    assert b"sort_interval" in L.em2g_last_error()
+    P.sort_interval = -1
+    assert L.em2g_create(C.byref(P), C.byref(h)) == _lib.ERR_INVALID

@@ -106,3 +106,65 @@ def test_fp32_variants_agree(gpu):
         for k in range(6):
             err = np.abs(outs[v][k] - outs[0][k]).max() / np.abs(outs[0][k]).max()
             assert err < 1e-4, (v, k, err)
+
+
+def _relativistic(nx=48, ny=32, n=6000, seed=4):
+    """Random fields and particles up to gamma ~ 5 (|v| up to 0.98 c): the
+    largest per-step drift the interval bound has to hold."""
+    from maccpic_b200 import _lib
+    from maccpic_b200.em2 import RunParams
+    rng = np.random.default_rng(seed)
+    fld = np.zeros((13, ny + 3, nx + 3))
+    f = rng.normal(scale=0.05, size=(6, ny, nx))
+    iy = (np.arange(ny + 3) - 1) % ny
+    ix = (np.arange(nx + 3) - 1) % nx
+    fld[:6] = f[:, iy][:, :, ix]
+    parts = []
+    for s in range(2):
+        u = rng.normal(size=(3, n)) * (2.5 if s == 0 else 0.3)
+        g = np.sqrt(1 + (u * u).sum(0))
+        parts.append(np.vstack([rng.random(n) * nx, rng.random(n) * ny, u / g, g]))
+    rp = RunParams(nx=nx, ny=ny, dx=0.5, dy=0.5, dt=0.05, qm=[-1.0, 1 / 25.0],
+                   q=[-0.01, 0.01], dn=[1.0, 1.0], am=[0.01, 0.25], np_max=[n, n],
+                   precision=_lib.FP32)
+    return rp, fld, parts
+
+
+@pytest.mark.parametrize("k", [2, 9])
+def test_sort_interval_matches_regrouping_every_step(gpu, k):
+    """In-place pushes between regroupings give the same run (to FP32
+    round-off) as regrouping every step, at the largest interval the drift
+    bound allows (9 at c dt / dx = 0.1) with particles near c."""
+    from maccpic_b200.em2 import Em2Gpu
+    rp, fld, parts = _relativistic()
+    with Em2Gpu(rp) as a, Em2Gpu(rp) as b:
+        assert b.max_sort_interval() == 9
+        for g in (a, b):
+            g.set_fields(fld)
+            for s, p in enumerate(parts):
+                g.set_particles(s, p)
+        b.set_sort_interval(k)
+        for _ in range(3 * k + 1):
+            ra, rb = a.step(1), b.step(1)
+            np.testing.assert_allclose(rb["ake"], ra["ake"], rtol=1e-5)
+        for s in range(2):
+            pa, pb = a.get_particles(s), b.get_particles(s)
+            d = np.abs(pa[:2] - pb[:2])
+            d = np.minimum(d, np.array([[rp.nx], [rp.ny]]) - d)
+            assert d.max() < 1e-4
+            np.testing.assert_allclose(pb[2:], pa[2:], rtol=1e-3, atol=1e-5)
+        fa, fb = a.get_fields(), b.get_fields()
+        for c in range(6):
+            assert np.abs(fa[c] - fb[c]).max() < 1e-4 * np.abs(fa[c]).max() + 1e-7
+
+
+def test_sort_interval_rejected_beyond_the_drift_bound(gpu):
+    from maccpic_b200 import _lib
+    from maccpic_b200._lib import Em2gError
+    from maccpic_b200.em2 import Em2Gpu
+    rp, fld, parts = _relativistic()
+    with Em2Gpu(rp) as g:
+        with pytest.raises(Em2gError) as ei:
+            g.set_sort_interval(10)
+        assert ei.value.status == _lib.ERR_INVALID
+        g.set_sort_interval(9)
