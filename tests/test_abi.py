@@ -4,6 +4,8 @@ import ctypes as C
 import os
 import re
 
+import pytest
+
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
@@ -125,3 +127,35 @@ def test_sort_interval_rules_without_gpu():
     assert b"sort_interval" in L.em2g_last_error()
     P.sort_interval = -1
     assert L.em2g_create(C.byref(P), C.byref(h)) == _lib.ERR_INVALID
+
+
+def _build_c_caller(tmp_path, cxx: bool):
+    import subprocess
+    from maccpic_b200 import build
+    build.build()
+    libdir = os.path.join(ROOT, "maccpic_b200")
+    exe = str(tmp_path / ("abi_smoke_cxx" if cxx else "abi_smoke_c"))
+    cc = ["g++", "-x", "c++", "-std=c++17"] if cxx else ["gcc", "-std=c11"]
+    cmd = cc + ["-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
+                os.path.join(ROOT, "tests", "abi_smoke.c"), "-o", exe,
+                "-L", libdir, "-Wl,-rpath," + libdir, "-l:libem2g.so", "-lm"]
+    subprocess.run(cmd, check=True)
+    return exe
+
+
+def test_c_and_cxx_callers_without_gpu(tmp_path):
+    """include/em2g.h compiles as C11 and C++17 and the library links from
+    both; the host-only checks run without a GPU."""
+    import subprocess
+    for cxx in (False, True):
+        exe = _build_c_caller(tmp_path, cxx)
+        out = subprocess.run([exe, "cpu"], capture_output=True, text=True)
+        assert out.returncode == 0 and out.stdout.strip() == "ok", out.stderr
+
+
+@pytest.mark.gpu
+def test_c_caller_runs_a_step(gpu, tmp_path):
+    import subprocess
+    exe = _build_c_caller(tmp_path, cxx=False)
+    out = subprocess.run([exe, "gpu"], capture_output=True, text=True)
+    assert out.returncode == 0 and out.stdout.strip() == "ok", out.stderr
