@@ -92,7 +92,10 @@ typedef struct em2g_params {
   int32_t smooth_current; /* 1: smooth2 each current array after the fold, every
                              step (not in em2, which filters only rho and, every
                              isav steps, E and B); 0 = em2 */
-  int32_t reserved[15];
+  int32_t poisson;       /* 0: em2's CG (cgm, stops at mean r^2 < cg_eps);
+                            1: exact solve by FFT (FP64; nx, ny powers of two
+                            <= 8192), a smooth map for the adjoint */
+  int32_t reserved[14];
 } em2g_params;
 
 typedef struct em2g_ctx em2g_ctx;
@@ -219,6 +222,42 @@ int em2g_set_timing(em2g_ctx *ctx, int on);
 int em2g_get_counters(em2g_ctx *ctx, int64_t *kernel_launches,
                       int64_t *push_launches_timed, double *push_ms);
 int em2g_reset_counters(em2g_ctx *ctx);
+
+/* ---- adjoint (no counterpart in the reference) ------------------------
+ * Reverse-mode derivative of the FP64 fast step (em2g_step) of a context
+ * with the exact Poisson solve (params.poisson = 1), for periodic states
+ * (guard cells equal to their periodic images, as em2g_step keeps them).
+ * The state it differentiates is the fields E, B and, per particle, the
+ * position (x, y) and u = gamma v (the quantity em2's Boris push advances,
+ * pic/move.f90:176-203).
+ *
+ * em2g_adj_forward advances the context nsteps, keeping E and B of every
+ * step and the particles every `checkpoint` steps.  After seeding the
+ * adjoint of the final state, em2g_adj_backward sweeps back to the state
+ * em2g_adj_forward started from: one kernel per step rebuilds the previous
+ * particle state by inverting the push (move, then the Boris rotation) and
+ * applies the transposed step -- gathers of the current and charge adjoints
+ * at the particles, the Boris rotation reversed, scatters of the force
+ * adjoint onto E and B -- and the kept checkpoints reset the rebuilt state
+ * every `checkpoint` steps.  Field adjoints use the periodic (ny, nx) layout
+ * (element [j][i] <-> em2 index (i+1, j+1)); particle adjoints are in slot
+ * order. */
+typedef struct em2g_adj em2g_adj;
+int em2g_adj_create(em2g_ctx *ctx, int max_steps, int checkpoint, em2g_adj **out);
+int em2g_adj_destroy(em2g_adj *adj);
+int em2g_adj_forward(em2g_adj *adj, int nsteps);
+/* adjoint of the final E, B: 6 arrays of ny*nx doubles (ex ey ez bx by bz),
+ * device memory; particles' final adjoints are zero */
+int em2g_adj_seed_fields_device(em2g_adj *adj, const double *dev6);
+int em2g_adj_backward(em2g_adj *adj);
+/* adjoints of the initial state (device memory) */
+int em2g_adj_get_fields_device(em2g_adj *adj, double *dev6);
+int em2g_adj_get_particles_device(em2g_adj *adj, int isp, double *lx, double *ly, double *lux,
+                                  double *luy, double *luz);
+/* the initial particles as the adjoint sees them: x, y, ux, uy, uz in slot
+ * order (device memory) */
+int em2g_adj_get_initial_particles_device(em2g_adj *adj, int isp, double *x, double *y,
+                                          double *ux, double *uy, double *uz);
 
 /* ---- ensembles (no counterpart in the reference) ----------------------
  * Up to 128 independent runs -- each its own em2 run with its own grid,

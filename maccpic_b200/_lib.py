@@ -32,6 +32,9 @@ EXPORTS = [
     "em2g_move_curnt", "em2g_set_timing", "em2g_get_counters", "em2g_reset_counters",
     "em2g_smooth2_static", "em2g_diagnostics", "em2g_num_variants", "em2g_set_variant",
     "em2g_get_variant", "em2g_set_sort_interval",
+    "em2g_adj_create", "em2g_adj_destroy", "em2g_adj_forward", "em2g_adj_seed_fields_device",
+    "em2g_adj_backward", "em2g_adj_get_fields_device", "em2g_adj_get_particles_device",
+    "em2g_adj_get_initial_particles_device",
     "em2g_ens_create", "em2g_ens_destroy", "em2g_ens_num_runs", "em2g_ens_set_stream",
     "em2g_ens_set_graph", "em2g_ens_set_variant", "em2g_ens_set_fields", "em2g_ens_get_fields",
     "em2g_ens_set_particles", "em2g_ens_set_particles_device", "em2g_ens_get_particles",
@@ -53,7 +56,7 @@ class Em2gParams(C.Structure):
         ("cg_maxits", C.c_int32), ("energy_mode", C.c_int32),
         ("cg_eps", C.c_double), ("qme", C.c_double), ("wpe", C.c_double),
         ("device", C.c_int32), ("sort_interval", C.c_int32),
-        ("smooth_current", C.c_int32), ("reserved", C.c_int32 * 15),
+        ("smooth_current", C.c_int32), ("poisson", C.c_int32), ("reserved", C.c_int32 * 14),
     ]
 
 
@@ -113,6 +116,14 @@ def lib() -> C.CDLL:
         "em2g_set_variant": (C.c_int, [ctx, C.c_int]),
         "em2g_get_variant": (C.c_int, [ctx, ip, C.c_char_p, C.c_int]),
         "em2g_set_sort_interval": (C.c_int, [ctx, C.c_int]),
+        "em2g_adj_create": (C.c_int, [ctx, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+        "em2g_adj_destroy": (C.c_int, [ctx]),
+        "em2g_adj_forward": (C.c_int, [ctx, C.c_int]),
+        "em2g_adj_seed_fields_device": (C.c_int, [ctx, vp]),
+        "em2g_adj_backward": (C.c_int, [ctx]),
+        "em2g_adj_get_fields_device": (C.c_int, [ctx, vp]),
+        "em2g_adj_get_particles_device": (C.c_int, [ctx, C.c_int] + [vp] * 5),
+        "em2g_adj_get_initial_particles_device": (C.c_int, [ctx, C.c_int] + [vp] * 5),
         "em2g_ens_create": (C.c_int, [pp, C.c_int, C.POINTER(C.c_void_p)]),
         "em2g_ens_destroy": (C.c_int, [ctx]),
         "em2g_ens_num_runs": (C.c_int, [ctx, ip]),

@@ -665,3 +665,143 @@ def flux_of_theta(cfg, theta, steps: int, draws, device="cpu"):
     E0, B0, P0 = initial_state_torch(cfg, (th[0], th[1], th[2]), draws)
     E, B, P = run_forward(E0, B0, P0, k, steps)
     return float(flux(B, k))
+
+
+# ---------------------------------------------------------------------------
+# the same derivative through the CUDA step (libem2g: em2g_adj_*)
+# ---------------------------------------------------------------------------
+def _guarded_block(E, B):
+    """(13, ny+3, nx+3) em2 field block on the device from periodic E, B:
+    index (ix, iy) holds periodic node (ix-1, iy-1); rho and J zero."""
+    ny, nx = E[0].shape
+    iy = (torch.arange(ny + 3, device=E[0].device) - 1) % ny
+    ix = (torch.arange(nx + 3, device=E[0].device) - 1) % nx
+    out = torch.zeros((13, ny + 3, nx + 3), dtype=torch.float64, device=E[0].device)
+    for k, a in enumerate(list(E) + list(B)):
+        out[k] = a[iy][:, ix]
+    return out
+
+
+class CudaAdjoint:
+    """One FP64 em2g context with the exact Poisson solve and its adjoint:
+    forward(T) advances the state keeping what the reverse sweep needs,
+    backward(seed) returns the adjoints of the state forward started from.
+    The state enters as (E, B, parts) in this module's periodic, u = gamma v
+    form; its first step number is it0."""
+
+    def __init__(self, k: StepConst, E, B, parts, max_steps: int, checkpoint: int,
+                 isav: int, smooth_current: int = 0, it0: int = 0):
+        import ctypes as C
+        from . import _lib
+        from ._lib import check
+        from .em2 import Em2Gpu, RunParams
+        self.k, self.nsp = k, len(parts)
+        self._L = _lib.lib()
+        n = [int(p[0].numel()) for p in parts]
+        # em2's species constants from StepConst: q*dn/(dx dy) = qd with dn = 1
+        rp = RunParams(nx=k.nx, ny=k.ny, dx=k.dx, dy=k.dx, dt=k.dt, c=k.c, nsp=self.nsp,
+                       qm=list(k.qm), q=[qd * k.dx * k.dx for qd in k.qd],
+                       dn=[1.0] * self.nsp, am=[1.0] * self.nsp, np_max=n, isav=isav,
+                       precision=_lib.FP64, poisson=1, smooth_current=smooth_current)
+        self.g = Em2Gpu(rp)
+        dev = E[0].device
+        # the library works on torch's stream: uploads follow their producers
+        self.g.set_stream(torch.cuda.current_stream(dev))
+        fld = _guarded_block([e.detach() for e in E], [b.detach() for b in B]).contiguous()
+        check(self._L.em2g_set_fields_device(self.g._h, C.c_void_p(fld.data_ptr())))
+        for s, (x, y, ux, uy, uz) in enumerate(parts):
+            u = torch.stack([ux, uy, uz]).detach()
+            gam = torch.sqrt(1.0 + (u * u).sum(0))
+            st = torch.stack([x.detach(), y.detach(), u[0] / gam, u[1] / gam, u[2] / gam,
+                              gam]).contiguous()
+            self.g.set_particles_device(s, st)
+        self.g.it = it0
+        torch.cuda.synchronize(dev)
+        h = C.c_void_p()
+        check(self._L.em2g_adj_create(self.g._h, int(max_steps), int(checkpoint), C.byref(h)))
+        self._h = h
+        self.dev = dev
+        self.n = n
+
+    def close(self):
+        from ._lib import check
+        if getattr(self, "_h", None) is not None and self._h.value:
+            check(self._L.em2g_adj_destroy(self._h))
+            self._h = None
+        if getattr(self, "g", None) is not None:
+            self.g.close()
+            self.g = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def forward(self, steps: int):
+        from ._lib import check
+        check(self._L.em2g_adj_forward(self._h, int(steps)))
+
+    def final_B(self):
+        """Periodic B of the current state (device tensors)."""
+        import ctypes as C
+        from ._lib import check
+        k = self.k
+        out = torch.empty((13, k.ny + 3, k.nx + 3), dtype=torch.float64, device=self.dev)
+        check(self._L.em2g_get_fields_device(self.g._h, C.c_void_p(out.data_ptr())))
+        torch.cuda.synchronize(self.dev)
+        return tuple(out[3 + c, 1:k.ny + 1, 1:k.nx + 1].clone() for c in range(3))
+
+    def backward(self, lE, lB):
+        """Adjoints of the initial state from those of the final E, B
+        (periodic tensors); the final particles' adjoints are zero."""
+        import ctypes as C
+        from ._lib import check
+        k = self.k
+        seed = torch.stack([t.to(torch.float64) for t in list(lE) + list(lB)]).contiguous()
+        check(self._L.em2g_adj_seed_fields_device(self._h, C.c_void_p(seed.data_ptr())))
+        check(self._L.em2g_adj_backward(self._h))
+        out = torch.empty((6, k.ny, k.nx), dtype=torch.float64, device=self.dev)
+        check(self._L.em2g_adj_get_fields_device(self._h, C.c_void_p(out.data_ptr())))
+        parts = []
+        for s in range(self.nsp):
+            lp = torch.empty((5, self.n[s]), dtype=torch.float64, device=self.dev)
+            check(self._L.em2g_adj_get_particles_device(
+                self._h, s, *[C.c_void_p(lp[c].data_ptr()) for c in range(5)]))
+            parts.append(tuple(lp[c] for c in range(5)))
+        return tuple(out[:3]), tuple(out[3:]), parts
+
+
+def theta_gradient_cuda(cfg, theta, steps: int, checkpoint: int = 50, draws=None,
+                        device="cuda"):
+    """flux(T) and d flux(T) / d theta with the CUDA step and its adjoint
+    (exact Poisson solve); autograd only through the initial-state map."""
+    draws = draws or make_draws(cfg, device=device)
+    k = step_const(cfg)
+    th = torch.tensor(theta, dtype=torch.float64, device=device, requires_grad=True)
+    with torch.enable_grad():
+        E0, B0, P0 = initial_state_torch(cfg, (th[0], th[1], th[2]), draws)
+        flat0 = _flatten(E0, B0, P0)
+    with CudaAdjoint(k, E0, B0, P0, steps, checkpoint, cfg.isav, cfg.smooth_current) as adj:
+        adj.forward(steps)
+        Bf = [b.requires_grad_(True) for b in adj.final_B()]
+        with torch.enable_grad():
+            F = flux(Bf, k)
+            gB = torch.autograd.grad(F, Bf, allow_unused=True)
+        gB = [g if g is not None else torch.zeros_like(b) for g, b in zip(gB, Bf)]
+        lE, lB, lP = adj.backward([torch.zeros_like(b) for b in Bf], gB)
+    lam = _flatten(lE, lB, lP)
+    used = [(t, l) for t, l in zip(flat0, lam) if t.requires_grad]
+    g = torch.autograd.grad([t for t, _ in used], th, grad_outputs=[l for _, l in used],
+                            allow_unused=True)[0]
+    return float(F.detach()), g.detach().cpu().numpy()
+
+
+def flux_of_theta_cuda(cfg, theta, steps: int, draws, device="cuda"):
+    """flux(T) by the CUDA FP64 step with the exact Poisson solve."""
+    k = step_const(cfg)
+    th = torch.tensor(theta, dtype=torch.float64, device=device)
+    E0, B0, P0 = initial_state_torch(cfg, (th[0], th[1], th[2]), draws)
+    with CudaAdjoint(k, E0, B0, P0, 1, 1, cfg.isav, cfg.smooth_current) as adj:
+        adj.g.step(steps)
+        return float(flux(adj.final_B(), k))

@@ -1,0 +1,873 @@
+// adjoint.cu -- reverse-mode derivative of the FP64 fast step (em2g_step
+// with the exact Poisson solve) for periodic states.  em2 has no adjoint;
+// the transposes follow the step's structure (pic/move.f90, pic/curnt.f90,
+// pic/fields.f90):
+//
+//   fields, in reverse: the Poisson projection E <- E - grad L^-1 dx^2
+//   (div E - rho) is self-adjoint in E and gives rho the adjoint
+//   -L^-1 dx^2 div(lambda_E); smooth2 is a symmetric stencil, its own
+//   transpose; the Yee half steps transpose into negated transposed curls;
+//   J's adjoint is -dt/2 lambda_E.
+//   particles, in reverse: the deposits' transpose is a gather of the
+//   current and charge adjoints at the particles (with the derivative of
+//   the quadratic weights for the positions), the gather's transpose a
+//   scatter of the force adjoint onto E and B, and the Boris rotation is
+//   reversed stage by stage.
+//
+// Memory.  The forward sweep keeps E and B before every step (6 periodic
+// arrays per step) and the particles every K steps.  The reverse sweep does
+// not recompute segments: the push is invertible, so one kernel per step
+// rebuilds the previous particle state from the current one (x -= v dt/dx
+// with u's velocity, then the Boris rotation about the same t by the
+// opposite angle) and applies the transposed step to it.  Round-off of the
+// rebuild grows for at most K steps: at every checkpoint the kept exact
+// state replaces it.
+//
+// Layout.  Field adjoints are periodic (ny, nx) arrays, element [j][i]
+// holding em2's node (i+1, j+1).  Particles and their adjoints travel
+// together in one working set per species (x, y, ux, uy, uz, and the five
+// adjoints), grouped by cell and regrouped every few steps as the rebuilt
+// positions drift; a CTA owns a row segment of 32 cells, 4 lanes per cell,
+// with the (E, B) pairs, the current and charge adjoints it gathers, and
+// the E and B adjoints it scatters, in shared-memory windows.
+#include <algorithm>
+#include <cmath>
+#include <new>
+#include <vector>
+
+#include "em2g_internal.cuh"
+#include "sort_common.cuh"
+
+struct em2g_adj {
+  em2g_ctx *ctx = nullptr;
+  int nx = 0, ny = 0, nsp = 0;
+  int64_t N = 0;  // nx*ny
+  int max_steps = 0, K = 1;
+  int steps = 0, it0 = 0;
+  double dx = 0, dy = 0, dt = 0, c = 1;
+  double ae[EM2G_MAX_SPECIES] = {}, qd[EM2G_MAX_SPECIES] = {};
+  int64_t n[EM2G_MAX_SPECIES] = {}, pb[EM2G_MAX_SPECIES] = {};  // particles, first index
+  int64_t ptot = 0;
+  double *hist = nullptr;   // max_steps x 6 x N
+  double *ckpt = nullptr;   // nck x 5 x ptot (per species 5 x n, slot order)
+  int nck = 0;
+  double *fin = nullptr;    // 5 x ptot, the state after the last recorded step
+  double *work = nullptr, *work_alt = nullptr;  // 10 x ptot (per species 10 x n)
+  int32_t *slot = nullptr, *slot_alt = nullptr;
+  int32_t *off = nullptr;   // per species ncell+1
+  int32_t *cnt = nullptr, *cursor = nullptr, *scan_tmp = nullptr;
+  double *g = nullptr;      // lE(3N) lB(3N) lJ(3N) lrho(N) w(N) tmp(6N)
+  double2 *spec = nullptr, *scaled = nullptr;  // N, nsp x 3 x N
+  bool seeded = false, swept = false;
+};
+
+namespace em2g {
+namespace {
+
+constexpr int TCX = 32, G = 4, WY = 6, WX = TCX + 5;
+constexpr int kRegroup = 8;  // reverse steps between regroupings
+
+__device__ __forceinline__ int wrapi(int i, int n) {
+  i %= n;
+  return i < 0 ? i + n : i;
+}
+
+// quadratic weights (pic/move.f90:76-148) with their x-derivatives; `i` is
+// em2's index of the middle node
+struct W3 {
+  int i;
+  double m, s, p, dm, ds, dp;
+};
+__device__ __forceinline__ W3 w_half(double x) {
+  const int ix = (int)(x + 1.0);
+  const double d = x + 0.5 - ix, e = 1.0 + x - ix, f = ix - x;
+  return W3{ix, 0.5 * f * f, 0.75 - d * d, 0.5 * e * e, -f, -2.0 * d, e};
+}
+__device__ __forceinline__ W3 w_node(double x) {
+  const int ix = (int)(x + 1.5);
+  const double d = x + 1.0 - ix, e = 1.5 + x - ix, f = -0.5 - x + ix;
+  return W3{ix, 0.5 * f * f, 0.75 - d * d, 0.5 * e * e, -f, -2.0 * d, e};
+}
+
+// where a 3x3 stencil sits: window coordinates (col, row of node i-1, j-1)
+// or, outside the window, periodic array indices of its three columns/rows
+struct Sten {
+  bool win;
+  int c0, r0;
+  int gx[3], gy[3];
+  W3 wx, wy;
+};
+
+struct Seg {
+  int x0, y0, kx, ky, nx, ny;
+};
+
+// em2 node index i of a particle whose wrapped cell is cx, seen from the
+// group cell kx: the same node unwrapped next to the group
+__device__ __forceinline__ int unwrap_shift(int cx, int kx, int n) {
+  const int d = cx - kx;
+  return d > n / 2 ? -n : (d < -n / 2 ? n : 0);
+}
+
+__device__ __forceinline__ Sten make_sten(const Seg &s, const W3 &wx, const W3 &wy, int shx,
+                                          int shy) {
+  Sten t;
+  t.wx = wx;
+  t.wy = wy;
+  t.c0 = wx.i - 1 + shx - (s.x0 - 1);
+  t.r0 = wy.i - 1 + shy - (s.y0 - 1);
+  t.win = t.c0 >= 0 && t.c0 + 2 < WX && t.r0 >= 0 && t.r0 + 2 < WY;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    t.gx[a] = wrapi(wx.i - 2 + a, s.nx);  // periodic index of em2 node i-1+a
+    t.gy[a] = wrapi(wy.i - 2 + a, s.ny);
+  }
+  return t;
+}
+
+struct Grad {
+  double v, gx, gy;
+};
+struct Grad2 {
+  double2 v, gx, gy;
+};
+
+__device__ __forceinline__ Grad gather_g(const double *glob, const double (*win)[WX],
+                                         const Sten &t, int nx) {
+  const double wx[3] = {t.wx.m, t.wx.s, t.wx.p}, dwx[3] = {t.wx.dm, t.wx.ds, t.wx.dp};
+  const double wy[3] = {t.wy.m, t.wy.s, t.wy.p}, dwy[3] = {t.wy.dm, t.wy.ds, t.wy.dp};
+  Grad r{0.0, 0.0, 0.0};
+#pragma unroll
+  for (int b = 0; b < 3; ++b) {
+    double sv = 0.0, sd = 0.0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const double f = t.win ? win[t.r0 + b][t.c0 + a] : glob[(int64_t)t.gy[b] * nx + t.gx[a]];
+      sv += f * wx[a];
+      sd += f * dwx[a];
+    }
+    r.v += sv * wy[b];
+    r.gx += sd * wy[b];
+    r.gy += sv * dwy[b];
+  }
+  return r;
+}
+
+__device__ __forceinline__ Grad2 gather_g2(const double2 *glob, const double2 (*win)[WX],
+                                           const Sten &t, int nx) {
+  const double wx[3] = {t.wx.m, t.wx.s, t.wx.p}, dwx[3] = {t.wx.dm, t.wx.ds, t.wx.dp};
+  const double wy[3] = {t.wy.m, t.wy.s, t.wy.p}, dwy[3] = {t.wy.dm, t.wy.ds, t.wy.dp};
+  Grad2 r;
+  r.v = r.gx = r.gy = make_double2(0.0, 0.0);
+#pragma unroll
+  for (int b = 0; b < 3; ++b) {
+    double2 sv = make_double2(0.0, 0.0), sd = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const double2 f =
+          t.win ? win[t.r0 + b][t.c0 + a] : glob[(int64_t)t.gy[b] * nx + t.gx[a]];
+      sv.x += f.x * wx[a];
+      sv.y += f.y * wx[a];
+      sd.x += f.x * dwx[a];
+      sd.y += f.y * dwx[a];
+    }
+    r.v.x += sv.x * wy[b];
+    r.v.y += sv.y * wy[b];
+    r.gx.x += sd.x * wy[b];
+    r.gx.y += sd.y * wy[b];
+    r.gy.x += sv.x * dwy[b];
+    r.gy.y += sv.y * dwy[b];
+  }
+  return r;
+}
+
+__device__ __forceinline__ void scatter_w(double *glob, double (*win)[WX], const Sten &t, int nx,
+                                          double q) {
+  const double wx[3] = {t.wx.m, t.wx.s, t.wx.p}, wy[3] = {t.wy.m, t.wy.s, t.wy.p};
+#pragma unroll
+  for (int b = 0; b < 3; ++b)
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const double v = q * wy[b] * wx[a];
+      if (t.win)
+        atomicAdd(&win[t.r0 + b][t.c0 + a], v);
+      else
+        atomicAdd(glob + (int64_t)t.gy[b] * nx + t.gx[a], v);
+    }
+}
+
+__device__ __forceinline__ double3 cross3(double3 a, double3 b) {
+  return make_double3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ double dot3(double3 a, double3 b) {
+  return a.x * b.x + a.y * b.y + a.z * b.z;
+}
+__device__ __forceinline__ double3 add3(double3 a, double3 b) {
+  return make_double3(a.x + b.x, a.y + b.y, a.z + b.z);
+}
+__device__ __forceinline__ double3 sub3(double3 a, double3 b) {
+  return make_double3(a.x - b.x, a.y - b.y, a.z - b.z);
+}
+__device__ __forceinline__ double3 mul3(double k, double3 a) {
+  return make_double3(k * a.x, k * a.y, k * a.z);
+}
+
+struct RevArgs {
+  const double2 *ebx, *ebz, *eby;        // (ae E, ae B) pairs, periodic
+  const double *ljx, *ljy, *ljz, *lrho;  // current and charge adjoints
+  double *lE[3], *lB[3];                 // E and B adjoints (accumulated)
+  double *P;                             // working set, 10 x n
+  int64_t n;
+  const int32_t *off;
+  int nx, ny;
+  double ae, qd, dtdx, dtdy, c;
+};
+
+// One reverse step of one species: rebuild each particle's state before the
+// step, then the transposed move + curnt.  Staggerings: Ex, Bx, Jx (half, node);
+// Ey, By, Jy (node, half); Ez, Bz, Jz (half, half); rho (node, node).
+__global__ void __launch_bounds__(TCX *G) k_adj_push(RevArgs a) {
+  __shared__ double2 w_eb[3][WY][WX];  // 0: (E,B)x, 1: (E,B)z, 2: (E,B)y
+  __shared__ double w_lj[3][WY][WX];   // lJx, lJy, lJz
+  __shared__ double w_lr[WY][WX];
+  __shared__ double w_acc[6][WY][WX];  // lEx lEy lEz lBx lBy lBz
+  const int nx = a.nx, ny = a.ny;
+  const Seg seg{(int)blockIdx.x * TCX, (int)blockIdx.y, 0, 0, nx, ny};
+  for (int t = threadIdx.x; t < WY * WX; t += blockDim.x) {
+    const int r = t / WX, col = t % WX;
+    // window node (em2 index x0-1+col, y0-1+r) -> periodic (index-1)
+    const int64_t k = (int64_t)wrapi(seg.y0 - 2 + r, ny) * nx + wrapi(seg.x0 - 2 + col, nx);
+    w_eb[0][r][col] = a.ebx[k];
+    w_eb[1][r][col] = a.ebz[k];
+    w_eb[2][r][col] = a.eby[k];
+    w_lj[0][r][col] = a.ljx[k];
+    w_lj[1][r][col] = a.ljy[k];
+    w_lj[2][r][col] = a.ljz[k];
+    w_lr[r][col] = a.lrho[k];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) w_acc[q][r][col] = 0.0;
+  }
+  __syncthreads();
+
+  const int gl = threadIdx.x & (G - 1);
+  const int kx = seg.x0 + (int)(threadIdx.x / G), ky = seg.y0;
+  const int64_t n = a.n;
+  double *P = a.P;
+  if (kx < nx) {
+    const int64_t cell = (int64_t)ky * nx + kx;
+    const int32_t beg = a.off[cell], end = a.off[cell + 1];
+    const double q = a.qd;
+    for (int32_t i = beg + gl; i < end; i += G) {
+      // the state after the step and its adjoints
+      const double x1 = P[i], y1 = P[n + i];
+      const double3 u1 = make_double3(P[2 * n + i], P[3 * n + i], P[4 * n + i]);
+      double lx1 = P[5 * n + i], ly1 = P[6 * n + i];
+      const double3 lu1 = make_double3(P[7 * n + i], P[8 * n + i], P[9 * n + i]);
+      const double g1 = sqrt(1.0 + dot3(u1, u1));
+      const double3 v = mul3(1.0 / g1, u1);
+      // rebuild the position before the move (pic/curnt.f90:181-194)
+      double x0 = x1 - v.x * a.dtdx, y0 = y1 - v.y * a.dtdy;
+      if (x0 < 0.0) x0 += nx; else if (x0 >= nx) x0 -= nx;
+      if (y0 < 0.0) y0 += ny; else if (y0 >= ny) y0 -= ny;
+      const int sx0 = unwrap_shift((int)x0, kx, nx), sy0 = unwrap_shift((int)y0, ky, ny);
+      const int sx1 = unwrap_shift((int)x1, kx, nx), sy1 = unwrap_shift((int)y1, ky, ny);
+      const W3 hx0 = w_half(x0), nx0 = w_node(x0), hy0 = w_half(y0), ny0 = w_node(y0);
+      const W3 hx1 = w_half(x1), nx1 = w_node(x1), hy1 = w_half(y1), ny1 = w_node(y1);
+      const Sten s_hn0 = make_sten(seg, hx0, ny0, sx0, sy0);  // x staggering
+      const Sten s_nh0 = make_sten(seg, nx0, hy0, sx0, sy0);  // y staggering
+      const Sten s_hh0 = make_sten(seg, hx0, hy0, sx0, sy0);  // z staggering
+      // scaled fields before the step at the old position, with gradients
+      const Grad2 gbx = gather_g2(a.ebx, w_eb[0], s_hn0, nx);
+      const Grad2 gbz = gather_g2(a.ebz, w_eb[1], s_hh0, nx);
+      const Grad2 gby = gather_g2(a.eby, w_eb[2], s_nh0, nx);
+      const double3 aE = make_double3(gbx.v.x, gby.v.x, gbz.v.x);
+      const double3 aB = make_double3(gbx.v.y, gby.v.y, gbz.v.y);
+      // rebuild u before the Boris rotation (pic/move.f90:176-203): the
+      // rotation about t by the opposite angle
+      const double3 upl_b = sub3(u1, aE);
+      const double3 tb = mul3(1.0 / (a.c * sqrt(1.0 + dot3(upl_b, upl_b))), aB);
+      const double3 up_b = sub3(upl_b, cross3(upl_b, tb));
+      const double3 sb = mul3(2.0 / (1.0 + dot3(tb, tb)), tb);
+      const double3 u0 = sub3(sub3(upl_b, cross3(up_b, sb)), aE);
+      // the forward intermediates from the rebuilt state
+      const double3 um = add3(u0, aE);
+      const double gm = sqrt(1.0 + dot3(um, um));
+      const double3 t = mul3(1.0 / (a.c * gm), aB);
+      const double3 up = add3(um, cross3(um, t));
+      const double f = 2.0 / (1.0 + dot3(t, t));
+      const double3 s = mul3(f, t);
+      // transposed deposits: rho and jp at the new position, jm at the old
+      const Sten s_nn1 = make_sten(seg, nx1, ny1, sx1, sy1);
+      const Grad gr = gather_g(a.lrho, w_lr, s_nn1, nx);
+      double lxn = lx1 + q * gr.gx, lyn = ly1 + q * gr.gy;
+      double lx = 0.0, ly = 0.0;
+      double lv[3];
+      const Sten s1[3] = {make_sten(seg, hx1, ny1, sx1, sy1), make_sten(seg, nx1, hy1, sx1, sy1),
+                          make_sten(seg, hx1, hy1, sx1, sy1)};
+      const Sten *s0[3] = {&s_hn0, &s_nh0, &s_hh0};
+      const double vv[3] = {v.x, v.y, v.z};
+      const double *ljg[3] = {a.ljx, a.ljy, a.ljz};
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const Grad j1 = gather_g(ljg[c], w_lj[c], s1[c], nx);
+        const Grad j0 = gather_g(ljg[c], w_lj[c], *s0[c], nx);
+        lv[c] = q * (j1.v + j0.v);
+        lxn += q * vv[c] * j1.gx;
+        lyn += q * vv[c] * j1.gy;
+        lx += q * vv[c] * j0.gx;
+        ly += q * vv[c] * j0.gy;
+      }
+      // move: x1 = x0 + v dt/dx
+      lx += lxn;
+      ly += lyn;
+      lv[0] += lxn * a.dtdx;
+      lv[1] += lyn * a.dtdy;
+      // v = u1 / gamma(u1)
+      const double3 lvv = make_double3(lv[0], lv[1], lv[2]);
+      const double dt_ = dot3(lvv, u1);
+      double3 lun = sub3(mul3(1.0 / g1, lvv), mul3(dt_ / (g1 * g1 * g1), u1));
+      lun = add3(lun, lu1);
+      // Boris, reversed stage by stage
+      double3 laE = lun;
+      double3 lum = lun;
+      const double3 lup = cross3(s, lun);
+      const double3 ls = cross3(lun, up);
+      double3 lt = mul3(f, ls);
+      const double lf = dot3(ls, t);
+      lt = sub3(lt, mul3(f * f * lf, t));
+      lum = add3(add3(lum, lup), cross3(t, lup));
+      lt = add3(lt, cross3(lup, um));
+      const double3 laB = mul3(1.0 / (a.c * gm), lt);
+      const double lg = -dot3(lt, t) / gm;
+      lum = add3(lum, mul3(lg / gm, um));
+      laE = add3(laE, lum);
+      // transposed gather: the force adjoint onto E and B
+      scatter_w(a.lE[0], w_acc[0], s_hn0, nx, a.ae * laE.x);
+      scatter_w(a.lE[1], w_acc[1], s_nh0, nx, a.ae * laE.y);
+      scatter_w(a.lE[2], w_acc[2], s_hh0, nx, a.ae * laE.z);
+      scatter_w(a.lB[0], w_acc[3], s_hn0, nx, a.ae * laB.x);
+      scatter_w(a.lB[1], w_acc[4], s_nh0, nx, a.ae * laB.y);
+      scatter_w(a.lB[2], w_acc[5], s_hh0, nx, a.ae * laB.z);
+      lx += laE.x * gbx.gx.x + laB.x * gbx.gx.y + laE.y * gby.gx.x + laB.y * gby.gx.y +
+            laE.z * gbz.gx.x + laB.z * gbz.gx.y;
+      ly += laE.x * gbx.gy.x + laB.x * gbx.gy.y + laE.y * gby.gy.x + laB.y * gby.gy.y +
+            laE.z * gbz.gy.x + laB.z * gbz.gy.y;
+      // the state before the step and its adjoints, in place
+      P[i] = x0;
+      P[n + i] = y0;
+      P[2 * n + i] = u0.x;
+      P[3 * n + i] = u0.y;
+      P[4 * n + i] = u0.z;
+      P[5 * n + i] = lx;
+      P[6 * n + i] = ly;
+      P[7 * n + i] = lum.x;
+      P[8 * n + i] = lum.y;
+      P[9 * n + i] = lum.z;
+    }
+  }
+  __syncthreads();
+  // the window's E and B adjoints into the arrays (windows of neighbouring
+  // segments overlap)
+  for (int t = threadIdx.x; t < WY * WX; t += blockDim.x) {
+    const int r = t / WX, col = t % WX;
+    const int64_t k = (int64_t)wrapi(seg.y0 - 2 + r, ny) * nx + wrapi(seg.x0 - 2 + col, nx);
+#pragma unroll
+    for (int qq = 0; qq < 6; ++qq) {
+      const double v = w_acc[qq][r][col];
+      if (v != 0.0) atomicAdd((qq < 3 ? a.lE[qq] : a.lB[qq - 3]) + k, v);
+    }
+  }
+}
+
+// ---- periodic grid transposes (k = j*nx + i) -------------------------------
+struct PG {
+  int nx, ny;
+};
+__device__ __forceinline__ int64_t xm(const PG &p, int64_t k) {
+  const int i = (int)(k % p.nx);
+  return i == 0 ? k + p.nx - 1 : k - 1;
+}
+__device__ __forceinline__ int64_t xp(const PG &p, int64_t k) {
+  const int i = (int)(k % p.nx);
+  return i == p.nx - 1 ? k - (p.nx - 1) : k + 1;
+}
+__device__ __forceinline__ int64_t ym(const PG &p, int64_t k) {
+  return k < p.nx ? k + (int64_t)(p.ny - 1) * p.nx : k - p.nx;
+}
+__device__ __forceinline__ int64_t yp(const PG &p, int64_t k) {
+  return k >= (int64_t)(p.ny - 1) * p.nx ? k - (int64_t)(p.ny - 1) * p.nx : k + p.nx;
+}
+
+#define PG_LOOP(N) \
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < (N); k += (int64_t)gridDim.x * blockDim.x)
+
+// rhs = dx^2 div(lE) (backward differences)
+__global__ void k_adj_div(PG p, const double *lex, const double *ley, double dx, double dy,
+                          double *rhs) {
+  PG_LOOP((int64_t)p.nx * p.ny) {
+    rhs[k] = ((lex[k] - lex[xm(p, k)]) / dx + (ley[k] - ley[ym(p, k)]) / dy) * dx * dx;
+  }
+}
+// lE -= grad w (forward differences); lrho = -w
+__global__ void k_adj_grad(PG p, double *lex, double *ley, const double *w, double dx,
+                           double dy, double *lrho) {
+  PG_LOOP((int64_t)p.nx * p.ny) {
+    const double wc = w[k];
+    lex[k] -= (w[xp(p, k)] - wc) / dx;
+    ley[k] -= (w[yp(p, k)] - wc) / dy;
+    lrho[k] = -wc;
+  }
+}
+// periodic smooth2 (pic/smooth.f90:143-177) of arrays a.p[blockIdx.y], with
+// scratch tmp + blockIdx.y * N
+struct Ptr6 {
+  double *p[6];
+};
+__global__ void k_adj_smooth_b(PG p, Ptr6 a, double *tmp, int64_t N) {
+  const double *s = a.p[blockIdx.y];
+  double *d = tmp + blockIdx.y * N;
+  PG_LOOP(N) {
+    const int64_t l = xm(p, k), r = xp(p, k);
+    d[k] = (4 * s[k] + 2 * (s[l] + s[r] + s[ym(p, k)] + s[yp(p, k)]) + s[ym(p, l)] +
+            s[yp(p, l)] + s[ym(p, r)] + s[yp(p, r)]) /
+           16.0;
+  }
+}
+__global__ void k_adj_smooth_c(PG p, Ptr6 a, const double *tmp, int64_t N) {
+  double *s = a.p[blockIdx.y];
+  const double *d = tmp + blockIdx.y * N;
+  PG_LOOP(N) {
+    const int64_t l = xm(p, k), r = xp(p, k);
+    s[k] = (20 * d[k] - d[l] - d[r] - d[ym(p, k)] - d[yp(p, k)] - d[ym(p, l)] - d[yp(p, l)] -
+            d[ym(p, r)] - d[yp(p, r)]) /
+           12.0;
+  }
+}
+// transpose of B += curl E half step: lE += curl^T lB (lB passes through)
+__global__ void k_adj_bhalf(PG p, double *lex, double *ley, double *lez, const double *lbx,
+                            const double *lby, const double *lbz, double ctxh, double ctyh) {
+  PG_LOOP((int64_t)p.nx * p.ny) {
+    lez[k] += -ctyh * (lbx[k] - lbx[yp(p, k)]) + ctxh * (lby[k] - lby[xp(p, k)]);
+    ley[k] -= ctxh * (lbz[xm(p, k)] - lbz[k]);
+    lex[k] += ctyh * (lbz[ym(p, k)] - lbz[k]);
+  }
+}
+// transpose of E += curl B - tem J: lB += curl^T lE, lJ = -tem lE
+__global__ void k_adj_efull(PG p, const double *lex, const double *ley, const double *lez,
+                            double *lbx, double *lby, double *lbz, double ctx, double cty,
+                            double tem, double *ljx, double *ljy, double *ljz) {
+  PG_LOOP((int64_t)p.nx * p.ny) {
+    lbz[k] += cty * (lex[k] - lex[yp(p, k)]) - ctx * (ley[k] - ley[xp(p, k)]);
+    lby[k] += ctx * (lez[xm(p, k)] - lez[k]);
+    lbx[k] -= cty * (lez[ym(p, k)] - lez[k]);
+    ljx[k] = -tem * lex[k];
+    ljy[k] = -tem * ley[k];
+    ljz[k] = -tem * lez[k];
+  }
+}
+// (ae E, ae B) pairs of the three staggerings from periodic E, B (6 x N)
+__global__ void k_adj_prescale(const double *eb, int64_t N, double ae, double2 *out) {
+  PG_LOOP(N) {
+    out[k] = make_double2(ae * eb[k], ae * eb[3 * N + k]);               // x
+    out[N + k] = make_double2(ae * eb[2 * N + k], ae * eb[5 * N + k]);   // z
+    out[2 * N + k] = make_double2(ae * eb[N + k], ae * eb[4 * N + k]);   // y
+  }
+}
+// periodic E, B from the context's guarded FP64 block
+__global__ void k_adj_record_fields(const double *fld, int nx, int ny, int64_t w, double *out) {
+  const int64_t N = (int64_t)nx * ny;
+  PG_LOOP(6 * N) {
+    const int c = (int)(k / N);
+    const int64_t e = k - c * N;
+    const int i = (int)(e % nx), j = (int)(e / nx);
+    out[k] = fld[c * w + (int64_t)(j + 1) * (nx + 3) + (i + 1)];
+  }
+}
+// context particles (6 x cap, grouped, with slots) -> x, y, u (5 x n, slot order)
+__global__ void k_adj_record_parts(const double *part, const int32_t *slot, int64_t n,
+                                   int64_t cap, double *out) {
+  PG_LOOP(n) {
+    const int64_t s = slot[k];
+    const double g = part[5 * cap + k];
+    out[s] = part[k];
+    out[n + s] = part[cap + k];
+    out[2 * n + s] = part[2 * cap + k] * g;  // u = v gamma (pic/move.f90:176-178)
+    out[3 * n + s] = part[3 * cap + k] * g;
+    out[4 * n + s] = part[4 * cap + k] * g;
+  }
+}
+// working set from a slot-order state: slot = index, adjoints zero
+__global__ void k_adj_load(const double *st, int64_t n, double *P, int32_t *slot) {
+  PG_LOOP(n) {
+    for (int c = 0; c < 5; ++c) P[c * n + k] = st[c * n + k];
+    for (int c = 5; c < 10; ++c) P[c * n + k] = 0.0;
+    slot[k] = (int32_t)k;
+  }
+}
+// the kept exact state replaces the rebuilt one
+__global__ void k_adj_restore(const double *st, int64_t n, double *P, const int32_t *slot) {
+  PG_LOOP(n) {
+    const int64_t s = slot[k];
+    for (int c = 0; c < 5; ++c) P[c * n + k] = st[c * n + s];
+  }
+}
+__global__ void k_adj_hist(const double *P, int64_t n, int nx, int ny, int32_t *cnt) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool active = k < n;
+  const unsigned am = __ballot_sync(0xffffffffu, active);
+  if (!active) return;
+  agg_atomic_add(cnt, cell_key(P[k], P[n + k], nx, ny), am);
+}
+__global__ void k_adj_scatter(const double *P, const int32_t *slot, int64_t n, int nx, int ny,
+                              const int32_t *off, int32_t *cursor, double *Q, int32_t *qslot) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool active = k < n;
+  const unsigned am = __ballot_sync(0xffffffffu, active);
+  if (!active) return;
+  const int key = cell_key(P[k], P[n + k], nx, ny);
+  const int64_t pos = (int64_t)off[key] + agg_atomic_add(cursor, key, am);
+  for (int c = 0; c < 10; ++c) Q[c * n + pos] = P[c * n + k];
+  qslot[pos] = slot[k];
+}
+// adjoints (or the state) of the working set back to slot order
+__global__ void k_adj_unsort(const double *P, const int32_t *slot, int64_t n, int first,
+                             double *o0, double *o1, double *o2, double *o3, double *o4) {
+  PG_LOOP(n) {
+    const int64_t s = slot[k];
+    o0[s] = P[(first + 0) * n + k];
+    o1[s] = P[(first + 1) * n + k];
+    o2[s] = P[(first + 2) * n + k];
+    o3[s] = P[(first + 3) * n + k];
+    o4[s] = P[(first + 4) * n + k];
+  }
+}
+
+unsigned blocks_for(int64_t n) {
+  const int64_t b = (n + 255) / 256;
+  return (unsigned)(b < 8192 ? (b < 1 ? 1 : b) : 8192);
+}
+
+int check_adj(em2g_adj *a) {
+  if (!a || !a->ctx) return fail(EM2G_ERR_INVALID, "null adjoint");
+  EM2G_CUDA(cudaSetDevice(a->ctx->device));
+  return EM2G_OK;
+}
+
+double *lE(em2g_adj *a, int c) { return a->g + c * a->N; }
+double *lB(em2g_adj *a, int c) { return a->g + (3 + c) * a->N; }
+double *lJ(em2g_adj *a, int c) { return a->g + (6 + c) * a->N; }
+double *lrho(em2g_adj *a) { return a->g + 9 * a->N; }
+double *wbuf(em2g_adj *a) { return a->g + 10 * a->N; }
+double *tmp6(em2g_adj *a) { return a->g + 11 * a->N; }
+
+// sort every species' working set by the cell of its current position
+int regroup(em2g_adj *a, cudaStream_t st) {
+  const int64_t nc = a->N;
+  for (int s = 0; s < a->nsp; ++s) {
+    const int64_t n = a->n[s];
+    double *P = a->work + 10 * a->pb[s], *Q = a->work_alt + 10 * a->pb[s];
+    int32_t *sl = a->slot + a->pb[s], *ql = a->slot_alt + a->pb[s];
+    int32_t *off = a->off + s * (nc + 1);
+    EM2G_CUDA(cudaMemsetAsync(a->cnt, 0, sizeof(int32_t) * nc, st));
+    EM2G_CUDA(cudaMemsetAsync(a->cursor, 0, sizeof(int32_t) * nc, st));
+    const unsigned nb = (unsigned)((n + 255) / 256);
+    if (n > 0) k_adj_hist<<<nb, 256, 0, st>>>(P, n, a->nx, a->ny, a->cnt);
+    int rc = scan_counts(a->cnt, off, nc, 0, a->scan_tmp, st);
+    if (rc) return rc;
+    if (n > 0) k_adj_scatter<<<nb, 256, 0, st>>>(P, sl, n, a->nx, a->ny, off, a->cursor, Q, ql);
+    EM2G_CUDA(cudaGetLastError());
+    EM2G_CUDA(cudaMemcpyAsync(P, Q, sizeof(double) * 10 * n, cudaMemcpyDeviceToDevice, st));
+    EM2G_CUDA(cudaMemcpyAsync(sl, ql, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, st));
+  }
+  return EM2G_OK;
+}
+
+int smooth_T(em2g_adj *a, const Ptr6 &arr, int count, cudaStream_t st) {
+  const PG p{a->nx, a->ny};
+  const dim3 grid(blocks_for(a->N), count);
+  k_adj_smooth_b<<<grid, 256, 0, st>>>(p, arr, tmp6(a), a->N);
+  k_adj_smooth_c<<<grid, 256, 0, st>>>(p, arr, tmp6(a), a->N);
+  EM2G_CUDA(cudaGetLastError());
+  return EM2G_OK;
+}
+
+// transposed fields(it) (pic/fields.f90:2-366 in reverse): lE, lB of the
+// state after the step -> of the state before it, plus lJ and lrho
+int fields_T(em2g_adj *a, int it, cudaStream_t st) {
+  const PG p{a->nx, a->ny};
+  const unsigned nb = blocks_for(a->N);
+  const em2g_params &P = a->ctx->P;
+  // Poisson: the projection is self-adjoint in E; rho's adjoint is -w,
+  // w = L^-1 dx^2 div(lE)
+  k_adj_div<<<nb, 256, 0, st>>>(p, lE(a, 0), lE(a, 1), a->dx, a->dy, wbuf(a));
+  int rc = spectral_solve(wbuf(a), wbuf(a), a->nx, a->ny, a->spec, st);
+  if (rc) return rc;
+  k_adj_grad<<<nb, 256, 0, st>>>(p, lE(a, 0), lE(a, 1), wbuf(a), a->dx, a->dy, lrho(a));
+  // filters (pic/fields.f90:252-260); smooth2 is its own transpose
+  if (it % P.isav == 0) {
+    Ptr6 eb{{lE(a, 0), lE(a, 1), lE(a, 2), lB(a, 0), lB(a, 1), lB(a, 2)}};
+    if ((rc = smooth_T(a, eb, 6, st))) return rc;
+  }
+  Ptr6 r{{lrho(a), nullptr, nullptr, nullptr, nullptr, nullptr}};
+  if ((rc = smooth_T(a, r, 1, st))) return rc;
+  // Yee in reverse: B/2, E, B/2 (pic/fields.f90:184-247)
+  const double ctx = P.dt * P.c / P.dx, cty = P.dt * P.c / P.dy, tem = 0.5 * P.dt;
+  k_adj_bhalf<<<nb, 256, 0, st>>>(p, lE(a, 0), lE(a, 1), lE(a, 2), lB(a, 0), lB(a, 1),
+                                  lB(a, 2), 0.5 * ctx, 0.5 * cty);
+  k_adj_efull<<<nb, 256, 0, st>>>(p, lE(a, 0), lE(a, 1), lE(a, 2), lB(a, 0), lB(a, 1), lB(a, 2),
+                                  ctx, cty, tem, lJ(a, 0), lJ(a, 1), lJ(a, 2));
+  k_adj_bhalf<<<nb, 256, 0, st>>>(p, lE(a, 0), lE(a, 1), lE(a, 2), lB(a, 0), lB(a, 1),
+                                  lB(a, 2), 0.5 * ctx, 0.5 * cty);
+  EM2G_CUDA(cudaGetLastError());
+  // the optional current filter after the fold (no em2 counterpart)
+  if (P.smooth_current) {
+    Ptr6 j{{lJ(a, 0), lJ(a, 1), lJ(a, 2), nullptr, nullptr, nullptr}};
+    if ((rc = smooth_T(a, j, 3, st))) return rc;
+  }
+  return EM2G_OK;
+}
+
+}  // namespace
+}  // namespace em2g
+
+using namespace em2g;
+
+extern "C" {
+
+int em2g_adj_create(em2g_ctx *ctx, int max_steps, int checkpoint, em2g_adj **out) {
+  if (!out) return fail(EM2G_ERR_INVALID, "null output pointer");
+  *out = nullptr;
+  if (!ctx) return fail(EM2G_ERR_INVALID, "null context");
+  const em2g_params &P = ctx->P;
+  if (P.precision != EM2G_FP64 || P.poisson != 1)
+    return fail(EM2G_ERR_INVALID, "the adjoint needs an FP64 context with poisson = 1");
+  if (max_steps < 1 || checkpoint < 1) return fail(EM2G_ERR_INVALID, "max_steps, checkpoint >= 1");
+  for (int s = 0; s < P.nsp; ++s)
+    if (P.tx[s] != 0.0 || P.ty[s] != 0.0)
+      return fail(EM2G_ERR_INVALID, "the adjoint assumes tx = ty = 0 (as em2 runs)");
+  if (std::fabs(P.dx - P.dy) > 1e-12 * P.dx)
+    return fail(EM2G_ERR_INVALID, "the adjoint assumes dx = dy (as cgm does)");
+  em2g_adj *a = new (std::nothrow) em2g_adj();
+  if (!a) return fail(EM2G_ERR_NOMEM, "host allocation failed");
+  auto bail = [&](int code) {
+    em2g_adj_destroy(a);
+    return code;
+  };
+  a->ctx = ctx;
+  a->nx = P.nx;
+  a->ny = P.ny;
+  a->nsp = P.nsp;
+  a->N = (int64_t)P.nx * P.ny;
+  a->max_steps = max_steps;
+  a->K = checkpoint;
+  a->dx = P.dx;
+  a->dy = P.dy;
+  a->dt = P.dt;
+  a->c = P.c;
+  for (int s = 0; s < P.nsp; ++s) {
+    a->ae[s] = 0.5 * P.qm[s] * P.dt / P.c;
+    a->qd[s] = P.q[s] * P.dn[s] / (P.dx * P.dy);
+    a->n[s] = ctx->sp[s].n;
+    a->pb[s] = a->ptot;
+    a->ptot += a->n[s];
+  }
+  a->nck = (max_steps + checkpoint - 1) / checkpoint;
+  const int64_t N = a->N, pt = a->ptot > 0 ? a->ptot : 1;
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return bail(cuda_fail(e, "cudaSetDevice"));
+#define ALLOC(ptr, bytes)                                                  \
+  do {                                                                     \
+    e = cudaMalloc((void **)&(ptr), (bytes));                              \
+    if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc " #ptr));   \
+  } while (0)
+  ALLOC(a->hist, sizeof(double) * 6 * N * max_steps);
+  ALLOC(a->ckpt, sizeof(double) * 5 * pt * a->nck);
+  ALLOC(a->fin, sizeof(double) * 5 * pt);
+  ALLOC(a->work, sizeof(double) * 10 * pt);
+  ALLOC(a->work_alt, sizeof(double) * 10 * pt);
+  ALLOC(a->slot, sizeof(int32_t) * pt);
+  ALLOC(a->slot_alt, sizeof(int32_t) * pt);
+  ALLOC(a->off, sizeof(int32_t) * (N + 1) * P.nsp);
+  ALLOC(a->cnt, sizeof(int32_t) * N);
+  ALLOC(a->cursor, sizeof(int32_t) * N);
+  ALLOC(a->scan_tmp, sizeof(int32_t) * scan_tmp_size(N));
+  ALLOC(a->g, sizeof(double) * 17 * N);
+  ALLOC(a->spec, sizeof(double2) * N);
+  ALLOC(a->scaled, sizeof(double2) * 3 * N * P.nsp);
+#undef ALLOC
+  int rc = spectral_prepare();
+  if (rc) return bail(rc);
+  *out = a;
+  return EM2G_OK;
+}
+
+int em2g_adj_destroy(em2g_adj *a) {
+  if (!a) return EM2G_OK;
+  if (a->ctx) cudaSetDevice(a->ctx->device);
+  void *bufs[] = {a->hist, a->ckpt,  a->fin, a->work,     a->work_alt, a->slot, a->slot_alt,
+                  a->off,  a->cnt,   a->cursor, a->scan_tmp, a->g,    a->spec, a->scaled};
+  for (void *p : bufs) cudaFree(p);
+  delete a;
+  return EM2G_OK;
+}
+
+static int record_parts(em2g_adj *a, double *dst, cudaStream_t st) {
+  for (int s = 0; s < a->nsp; ++s) {
+    const Species &S = a->ctx->sp[s];
+    if (S.n != a->n[s]) return fail(EM2G_ERR_INVALID, "particle count changed since em2g_adj_create");
+    if (S.n > 0)
+      k_adj_record_parts<<<blocks_for(S.n), 256, 0, st>>>(S.part, S.slot, S.n, S.cap,
+                                                          dst + 5 * a->pb[s]);
+  }
+  EM2G_CUDA(cudaGetLastError());
+  return EM2G_OK;
+}
+
+int em2g_adj_forward(em2g_adj *a, int nsteps) {
+  int rc = check_adj(a);
+  if (rc) return rc;
+  if (nsteps < 1 || nsteps > a->max_steps) return fail(EM2G_ERR_RANGE, "nsteps outside 1..max_steps");
+  em2g_ctx *c = a->ctx;
+  a->steps = 0;
+  a->seeded = a->swept = false;
+  a->it0 = c->it;
+  for (int k = 0; k < nsteps; ++k) {
+    cudaStream_t st = c->stream;
+    k_adj_record_fields<<<blocks_for(6 * a->N), 256, 0, st>>>(c->fld, a->nx, a->ny, c->g.w,
+                                                             a->hist + 6 * a->N * k);
+    EM2G_CUDA(cudaGetLastError());
+    if (k % a->K == 0 && (rc = record_parts(a, a->ckpt + 5 * a->ptot * (k / a->K), st)))
+      return rc;
+    if ((rc = em2g_step(c, 1, nullptr, nullptr, nullptr))) return rc;
+    // em2g_step runs the fast path only: the stored particles are its own
+    a->steps = k + 1;
+  }
+  if ((rc = record_parts(a, a->fin, c->stream))) return rc;
+  EM2G_CUDA(cudaStreamSynchronize(c->stream));
+  return EM2G_OK;
+}
+
+int em2g_adj_seed_fields_device(em2g_adj *a, const double *dev6) {
+  int rc = check_adj(a);
+  if (rc) return rc;
+  if (!dev6) return fail(EM2G_ERR_INVALID, "null pointer");
+  cudaStream_t st = a->ctx->stream;
+  EM2G_CUDA(cudaMemcpyAsync(a->g, dev6, sizeof(double) * 6 * a->N, cudaMemcpyDeviceToDevice, st));
+  EM2G_CUDA(cudaMemsetAsync(a->g + 6 * a->N, 0, sizeof(double) * 11 * a->N, st));
+  a->seeded = true;
+  return EM2G_OK;
+}
+
+int em2g_adj_backward(em2g_adj *a) {
+  int rc = check_adj(a);
+  if (rc) return rc;
+  if (a->steps < 1) return fail(EM2G_ERR_INVALID, "run em2g_adj_forward first");
+  if (!a->seeded) return fail(EM2G_ERR_INVALID, "seed the final adjoint first");
+  cudaStream_t st = a->ctx->stream;
+  for (int s = 0; s < a->nsp; ++s)
+    if (a->n[s] > 0)
+      k_adj_load<<<blocks_for(a->n[s]), 256, 0, st>>>(a->fin + 5 * a->pb[s], a->n[s],
+                                                      a->work + 10 * a->pb[s], a->slot + a->pb[s]);
+  EM2G_CUDA(cudaGetLastError());
+  if ((rc = regroup(a, st))) return rc;
+  int since = 0;
+  for (int k = a->steps - 1; k >= 0; --k) {
+    if (since == kRegroup) {
+      if ((rc = regroup(a, st))) return rc;
+      since = 0;
+    }
+    if ((rc = fields_T(a, a->it0 + k + 1, st))) return rc;
+    const double *eb = a->hist + 6 * a->N * k;
+    for (int s = 0; s < a->nsp; ++s) {
+      double2 *sc = a->scaled + 3 * a->N * s;
+      k_adj_prescale<<<blocks_for(a->N), 256, 0, st>>>(eb, a->N, a->ae[s], sc);
+      RevArgs r;
+      r.ebx = sc;
+      r.ebz = sc + a->N;
+      r.eby = sc + 2 * a->N;
+      r.ljx = lJ(a, 0);
+      r.ljy = lJ(a, 1);
+      r.ljz = lJ(a, 2);
+      r.lrho = lrho(a);
+      for (int q = 0; q < 3; ++q) {
+        r.lE[q] = lE(a, q);
+        r.lB[q] = lB(a, q);
+      }
+      r.P = a->work + 10 * a->pb[s];
+      r.n = a->n[s];
+      r.off = a->off + s * (a->N + 1);
+      r.nx = a->nx;
+      r.ny = a->ny;
+      r.ae = a->ae[s];
+      r.qd = a->qd[s];
+      r.dtdx = a->dt / a->dx;
+      r.dtdy = a->dt / a->dy;
+      r.c = a->c;
+      if (r.n > 0) {
+        const dim3 grid((unsigned)((a->nx + TCX - 1) / TCX), (unsigned)a->ny);
+        k_adj_push<<<grid, TCX * G, 0, st>>>(r);
+      }
+      // at a checkpoint the kept exact state replaces the rebuilt one
+      if (k % a->K == 0 && r.n > 0)
+        k_adj_restore<<<blocks_for(r.n), 256, 0, st>>>(a->ckpt + 5 * a->ptot * (k / a->K) +
+                                                           5 * a->pb[s],
+                                                       r.n, r.P, a->slot + a->pb[s]);
+    }
+    EM2G_CUDA(cudaGetLastError());
+    ++since;
+  }
+  EM2G_CUDA(cudaStreamSynchronize(st));
+  a->swept = true;
+  return EM2G_OK;
+}
+
+int em2g_adj_get_fields_device(em2g_adj *a, double *dev6) {
+  int rc = check_adj(a);
+  if (rc) return rc;
+  if (!dev6) return fail(EM2G_ERR_INVALID, "null pointer");
+  if (!a->swept) return fail(EM2G_ERR_INVALID, "run em2g_adj_backward first");
+  EM2G_CUDA(cudaMemcpyAsync(dev6, a->g, sizeof(double) * 6 * a->N, cudaMemcpyDeviceToDevice,
+                            a->ctx->stream));
+  EM2G_CUDA(cudaStreamSynchronize(a->ctx->stream));
+  return EM2G_OK;
+}
+
+static int unsort_out(em2g_adj *a, int isp, int first, double *o0, double *o1, double *o2,
+                      double *o3, double *o4) {
+  if (isp < 0 || isp >= a->nsp) return fail(EM2G_ERR_INVALID, "bad species index");
+  if (!o0 || !o1 || !o2 || !o3 || !o4) return fail(EM2G_ERR_INVALID, "null pointer");
+  const int64_t n = a->n[isp];
+  if (n > 0)
+    k_adj_unsort<<<blocks_for(n), 256, 0, a->ctx->stream>>>(
+        a->work + 10 * a->pb[isp], a->slot + a->pb[isp], n, first, o0, o1, o2, o3, o4);
+  EM2G_CUDA(cudaGetLastError());
+  EM2G_CUDA(cudaStreamSynchronize(a->ctx->stream));
+  return EM2G_OK;
+}
+
+int em2g_adj_get_particles_device(em2g_adj *a, int isp, double *lx, double *ly, double *lux,
+                                  double *luy, double *luz) {
+  int rc = check_adj(a);
+  if (rc) return rc;
+  if (!a->swept) return fail(EM2G_ERR_INVALID, "run em2g_adj_backward first");
+  return unsort_out(a, isp, 5, lx, ly, lux, luy, luz);
+}
+
+int em2g_adj_get_initial_particles_device(em2g_adj *a, int isp, double *x, double *y,
+                                          double *ux, double *uy, double *uz) {
+  int rc = check_adj(a);
+  if (rc) return rc;
+  if (a->steps < 1) return fail(EM2G_ERR_INVALID, "run em2g_adj_forward first");
+  if (isp < 0 || isp >= a->nsp) return fail(EM2G_ERR_INVALID, "bad species index");
+  if (!x || !y || !ux || !uy || !uz) return fail(EM2G_ERR_INVALID, "null pointer");
+  const int64_t n = a->n[isp];
+  const double *src = a->ckpt + 5 * a->pb[isp];
+  double *dst[5] = {x, y, ux, uy, uz};
+  for (int k = 0; k < 5; ++k)
+    EM2G_CUDA(cudaMemcpyAsync(dst[k], src + k * n, sizeof(double) * n, cudaMemcpyDeviceToDevice,
+                              a->ctx->stream));
+  EM2G_CUDA(cudaStreamSynchronize(a->ctx->stream));
+  return EM2G_OK;
+}
+
+}  // extern "C"

@@ -169,6 +169,10 @@ int validate(const em2g_params *p) {
   if (p->smooth_current != 0 && p->smooth_current != 1)
     return fail(EM2G_ERR_INVALID, "smooth_current must be 0 or 1");
   if (p->sort_interval < 0) return fail(EM2G_ERR_INVALID, "sort_interval must be >= 0");
+  if (p->poisson != 0 && p->poisson != 1) return fail(EM2G_ERR_INVALID, "poisson must be 0 or 1");
+  if (p->poisson == 1 && (p->precision != EM2G_FP64 || !spectral_size_ok(p->nx, p->ny)))
+    return fail(EM2G_ERR_INVALID,
+                "poisson 1 (spectral) needs FP64 and power-of-two nx, ny <= 8192");
   if (p->sort_interval > 1) {
     if (p->precision != EM2G_FP32)
       return fail(EM2G_ERR_INVALID, "sort_interval > 1 needs the FP32 path");
@@ -315,6 +319,11 @@ int em2g_create(const em2g_params *p, em2g_ctx **out) {
   if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMemset"));
   rc = fp32 ? cg_init_f32(c) : cg_init(c);
   if (rc) return bail(rc);
+  if (p->poisson == 1) {
+    e = cudaMalloc((void **)&c->spec, sizeof(double2) * (int64_t)p->nx * p->ny);
+    if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc spec"));
+    if ((rc = spectral_prepare())) return bail(rc);
+  }
   rc = sort_init(c);
   if (rc) return bail(rc);
   {
@@ -355,6 +364,7 @@ int em2g_destroy(em2g_ctx *c) {
     cudaFree(S.slot_alt);
   }
   cudaFree(c->red);
+  cudaFree(c->spec);
   cudaFree(c->dev_out);
   if (c->host_out) cudaFreeHost(c->host_out);
   cg_free(c);

@@ -104,6 +104,7 @@ struct em2g_ctx {
   // false while jxp, jyp, jzp are known to hold zeros (after fields, and
   // the fast path deposits the whole current into jxm, jym, jzm)
   bool jp_live = true;
+  double2 *spec = nullptr;  // nx*ny complex work of the spectral Poisson solve
   int64_t ncell = 0;
   int timing = 0;
   std::vector<cudaEvent_t> ev;  // start/stop pairs of the pending push launches
@@ -155,6 +156,10 @@ inline int64_t push_partials(int nx, int ny) {
   const int64_t a = (int64_t)((nx + 31) / 32) * 4, b = (int64_t)((nx + 63) / 64) * 8;
   return (a > b ? a : b) * ny;
 }
+// exact periodic Poisson solve by FFT (spectral.cu)
+bool spectral_size_ok(int nx, int ny);
+int spectral_prepare();
+int spectral_solve(const double *f, double *u, int nx, int ny, double2 *work, cudaStream_t st);
 // the checks em2g_create applies to a parameter block (api.cu)
 int validate_params(const em2g_params *p);
 // counts particles of a 6 x ld FP64 block outside [0, xlim) x [0, ylim)

@@ -56,6 +56,16 @@ int poisson_t(em2g_ctx *c, T *fld) {
   const dim3 blk(TX, TY);
   k_poisson_rhs<T><<<grid_for(g.nx, g.ny), blk, 0, c->stream>>>(g, fld, dx, dy, r, p);
   EM2G_CUDA(cudaGetLastError());
+  if constexpr (sizeof(T) == sizeof(double)) {
+    if (c->P.poisson == 1) {  // exact solve instead of cgm
+      int rc = spectral_solve(r, u, g.nx, g.ny, c->spec, c->stream);
+      if (rc) return rc;
+      k_poisson_correct<T><<<grid_for(g.nx, g.ny), blk, 0, c->stream>>>(g, fld, u, dx, dy);
+      c->launches += 7;
+      EM2G_CUDA(cudaGetLastError());
+      return EM2G_OK;
+    }
+  }
   EM2G_CUDA(cudaMemsetAsync(W.bar, 0, sizeof(unsigned) * 2, c->stream));
   CgArgs<T> a;
   a.nx = g.nx;

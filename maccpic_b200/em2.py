@@ -58,6 +58,7 @@ class RunParams:
     device: int = 0
     sort_interval: int = 0
     smooth_current: int = 0     # 1: smooth2 the current every step (not in em2)
+    poisson: int = 0            # 0: em2's CG; 1: exact spectral solve (FP64, 2^k sides)
 
     @property
     def shape(self):
@@ -68,7 +69,7 @@ class RunParams:
         check(_lib.lib().em2g_params_init(C.byref(P)))
         for name in ("nx", "ny", "nsp", "isav", "precision", "dx", "dy", "dt", "c",
                      "cg_maxits", "energy_mode", "cg_eps", "qme", "wpe", "device",
-                     "sort_interval", "smooth_current"):
+                     "sort_interval", "smooth_current", "poisson"):
             setattr(P, name, getattr(self, name))
         for name in ("qm", "q", "dn", "am", "tx", "ty"):
             arr = getattr(P, name)
@@ -83,6 +84,20 @@ class RunParams:
 
 def _dp(a: np.ndarray):
     return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+CUDA_STREAM_LEGACY = 1  # cudaStreamLegacy: the legacy default stream's handle
+
+
+def stream_handle(stream) -> C.c_void_p:
+    """The cudaStream_t to hand to the library: None -> NULL (the library's
+    own stream); a torch stream or an int handle as is, except the default
+    stream (handle 0, which the library would read as NULL) -> the legacy
+    default stream's explicit handle."""
+    if stream is None:
+        return C.c_void_p(0)
+    handle = getattr(stream, "cuda_stream", stream)
+    return C.c_void_p(handle if handle else CUDA_STREAM_LEGACY)
 
 
 class Em2Gpu:
@@ -160,8 +175,7 @@ class Em2Gpu:
     def set_stream(self, stream) -> None:
         """Enqueue further work on this cudaStream_t (int handle, or a torch
         stream); None returns to the context's own stream."""
-        handle = getattr(stream, "cuda_stream", stream)
-        check(self._L.em2g_set_stream(self._h, C.c_void_p(handle or 0)))
+        check(self._L.em2g_set_stream(self._h, stream_handle(stream)))
 
     def num_variants(self) -> int:
         n = C.c_int()

@@ -22,7 +22,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import NFIELD, check
-from .em2 import RunParams, _dp
+from .em2 import RunParams, _dp, stream_handle
 
 
 class Em2Ensemble:
@@ -125,8 +125,8 @@ class Em2Ensemble:
         check(self._L.em2g_ens_set_variant(self._h, int(v)))
 
     def set_stream(self, stream) -> None:
-        handle = getattr(stream, "cuda_stream", stream)
-        check(self._L.em2g_ens_set_stream(self._h, C.c_void_p(handle or 0)))
+        """As Em2Gpu.set_stream."""
+        check(self._L.em2g_ens_set_stream(self._h, stream_handle(stream)))
 
     def counters(self) -> dict:
         k, g, per = C.c_int64(), C.c_int64(), C.c_int64()

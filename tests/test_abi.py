@@ -159,3 +159,19 @@ def test_c_caller_runs_a_step(gpu, tmp_path):
     exe = _build_c_caller(tmp_path, cxx=False)
     out = subprocess.run([exe, "gpu"], capture_output=True, text=True)
     assert out.returncode == 0 and out.stdout.strip() == "ok", out.stderr
+
+
+def test_stream_handles_for_the_library():
+    """torch's default stream has handle 0, which the library reads as "its
+    own stream"; the wrappers hand over the legacy default stream's explicit
+    handle instead, so that work really is ordered on torch's stream."""
+    from maccpic_b200.em2 import CUDA_STREAM_LEGACY, stream_handle
+
+    class FakeStream:
+        def __init__(self, h):
+            self.cuda_stream = h
+
+    assert stream_handle(None).value is None
+    assert stream_handle(FakeStream(0)).value == CUDA_STREAM_LEGACY
+    assert stream_handle(FakeStream(0x1234)).value == 0x1234
+    assert stream_handle(0x5678).value == 0x5678

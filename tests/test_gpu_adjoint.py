@@ -1,0 +1,115 @@
+"""The CUDA adjoint (em2g_adj_*, maccpic_b200/adjoint.py CudaAdjoint).
+
+* the FP64 CUDA step with the exact Poisson solve is the PyTorch step of
+  maccpic_b200/adjoint.py (to round-off);
+* one reverse step equals the hand-written PyTorch reverse step_T, itself
+  checked against autograd (tests/test_adjoint.py);
+* the whole sweep (rebuilt states, checkpoints, regrouping) gives the
+  PyTorch adjoint's d flux / d theta;
+* d flux / d theta agrees with central differences of the CUDA forward
+  (common random numbers, h = 1e-3) to within 1 %.
+"""
+import numpy as np
+import pytest
+import torch
+
+from maccpic_b200 import adjoint as A
+from maccpic_b200 import loader
+
+pytestmark = pytest.mark.gpu
+
+THETA = (0.1, 0.0, 0.5)
+
+
+def _cfg(**kw):
+    base = dict(nx=32, ny=32, ppc=4, seed=3, isav=2)
+    base.update(kw)
+    return loader.HarrisConfig(**base)
+
+
+def _state(cfg):
+    d = A.make_draws(cfg, device="cuda")
+    k = A.step_const(cfg)
+    E, B, P = A.initial_state_torch(cfg, THETA, d)
+    return k, E, B, P
+
+
+def rel(a, b):
+    return float((a - b).abs().max()) / max(float(b.abs().max()), 1e-300)
+
+
+def test_spectral_step_matches_torch_step(gpu):
+    cfg = _cfg()
+    k, E, B, P = _state(cfg)
+    with A.CudaAdjoint(k, E, B, P, 1, 1, cfg.isav) as adj:
+        for it in range(1, 5):
+            E, B, P = A.step(E, B, P, k, it)
+            adj.g.step(1)
+        fld = adj.g.get_fields()
+        for c, a in enumerate(list(E) + list(B)):
+            got = torch.from_numpy(fld[c, 1:k.ny + 1, 1:k.nx + 1]).to(a.device)
+            assert rel(got, a) < 1e-10, c
+        for s, (x, y, ux, uy, uz) in enumerate(P):
+            q = torch.from_numpy(adj.g.get_particles(s)).to(x.device)
+            dx = (q[0] - x).abs()
+            assert float(torch.minimum(dx, k.nx - dx).max()) < 1e-11
+            dy = (q[1] - y).abs()
+            assert float(torch.minimum(dy, k.ny - dy).max()) < 1e-11
+            for c, u in enumerate((ux, uy, uz)):
+                assert float((q[2 + c] * q[5] - u).abs().max()) < 1e-11
+
+
+@pytest.mark.parametrize("isav", [1, 2])   # it = 1: with and without the E/B filter
+def test_one_reverse_step_matches_step_T(gpu, isav):
+    cfg = _cfg(isav=isav)
+    k, E, B, P = _state(cfg)
+    with torch.no_grad():
+        E, B, P = A.step(E, B, P, k, 1)      # a state with particles off the lattice
+    gen = torch.Generator(device="cuda").manual_seed(7)
+    lE2 = tuple(torch.randn(e.shape, generator=gen, dtype=e.dtype, device=e.device) for e in E)
+    lB2 = tuple(torch.randn(b.shape, generator=gen, dtype=b.dtype, device=b.device) for b in B)
+    zero = [tuple(torch.zeros_like(t) for t in p) for p in P]
+    import ctypes as C
+    from maccpic_b200._lib import check
+    with A.CudaAdjoint(k, E, B, P, 1, 1, isav, it0=1) as adj:
+        adj.forward(1)
+        # the state as the CUDA adjoint saw it (u = (u/gamma) gamma)
+        P_cuda = []
+        for s in range(len(P)):
+            x = torch.empty((5, adj.n[s]), dtype=torch.float64, device="cuda")
+            check(adj._L.em2g_adj_get_initial_particles_device(
+                adj._h, s, *[C.c_void_p(x[c].data_ptr()) for c in range(5)]))
+            P_cuda.append(tuple(x[c] for c in range(5)))
+        lE, lB, lP = adj.backward(lE2, lB2)
+    with torch.no_grad():
+        rE, rB, rP = A.step_T(E, B, P_cuda, lE2, lB2, zero, k, 2)
+    for a, b in zip(list(lE) + list(lB), list(rE) + list(rB)):
+        assert rel(a, b) < 1e-9
+    for s in range(len(P)):
+        for a, b in zip(lP[s], rP[s]):
+            assert rel(a, b) < 1e-8
+
+
+def test_sweep_matches_torch_gradient(gpu):
+    cfg = _cfg()
+    d = A.make_draws(cfg, device="cuda")
+    steps = 12
+    F_t, g_t = A.theta_gradient(cfg, THETA, steps, checkpoint=5, draws=d, device="cuda")
+    F_c, g_c = A.theta_gradient_cuda(cfg, THETA, steps, checkpoint=5, draws=d)
+    assert F_c == pytest.approx(F_t, rel=1e-10)
+    np.testing.assert_allclose(g_c, g_t, rtol=1e-7, atol=1e-12)
+
+
+def test_cuda_gradient_matches_central_differences(gpu):
+    cfg = _cfg(nx=64, ny=64, ppc=8, seed=11, isav=20)
+    d = A.make_draws(cfg, device="cuda")
+    steps, h = 30, 1e-3
+    F, g = A.theta_gradient_cuda(cfg, THETA, steps, checkpoint=10, draws=d)
+    assert F == pytest.approx(A.flux_of_theta_cuda(cfg, THETA, steps, d), rel=1e-12)
+    for i in range(3):
+        tp, tm = list(THETA), list(THETA)
+        tp[i] += h
+        tm[i] -= h
+        fd = (A.flux_of_theta_cuda(cfg, tp, steps, d)
+              - A.flux_of_theta_cuda(cfg, tm, steps, d)) / (2 * h)
+        assert abs(g[i] - fd) <= 0.01 * abs(fd) + 1e-9, (i, g[i], fd)
