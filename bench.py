@@ -55,6 +55,11 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--only-adjoint", action="store_true",
+                    help="run only the adjoint leg and print its JSON")
+    ap.add_argument("--adjoint-steps", type=int, default=40)
+    ap.add_argument("--adjoint-checkpoint", type=int, default=20)
     return ap.parse_args()
 
 
@@ -368,6 +373,9 @@ def run_ours(args):
     ens = None
     if rank == 0 and ws == 1 and fp32 and not args.no_ensemble:
         ens = run_ensemble(args, local)
+    adj = None
+    if rank == 0 and ws == 1 and not args.no_adjoint:
+        adj = run_adjoint(args, local)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(cfg, fields, [p.numpy() for p in parts_host])
@@ -400,7 +408,8 @@ def run_ours(args):
             "gpu_launches": cnt["kernel_launches"],
             "clocks": main["clocks"],
             "mixed_vs_fp64": compare,
-            "adjoint_over_forward": None,
+            "adjoint_over_forward": adj["gradient_over_forward"] if adj else None,
+            "adjoint": adj,
             "ensemble": ens,
             "e2e": e2e,
             "cpu_baseline": cpu,
@@ -409,6 +418,49 @@ def run_ours(args):
     if ws > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def run_adjoint(args, local):
+    """d(reconnected flux after T steps)/d(psi0, guide field, sheet
+    thickness) on the 512x256, 32-ppc double-Harris workload: the FP64 CUDA
+    step with the exact Poisson solve, T forward steps timed alone, then the
+    whole gradient (recording forward sweep, reverse sweep, the initial-state
+    map) timed the same way."""
+    import torch
+    from maccpic_b200 import adjoint as A, loader
+    cfg = loader.PRESETS["harris_512x256_ppc32"]
+    T, K = args.adjoint_steps, args.adjoint_checkpoint
+    theta = (cfg.psi0_over_b0di, cfg.guide_over_b0, cfg.l_over_di)
+    dev = f"cuda:{local}"
+    d = A.make_draws(cfg, device=dev)
+    k = A.step_const(cfg)
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        out = fn()
+        torch.cuda.synchronize()
+        return time.perf_counter() - t, out
+
+    with A.CudaAdjoint(k, *A.initial_state_torch(cfg, theta, d), T, K, cfg.isav) as adj:
+        adj.g.step(2)
+        t_fwd, _ = timed(lambda: adj.g.step(T))
+    A.theta_gradient_cuda(cfg, theta, min(T, 4), checkpoint=K, draws=d)  # warm-up
+    t_grad, (F, g) = timed(lambda: A.theta_gradient_cuda(cfg, theta, T, checkpoint=K, draws=d))
+    with A.CudaAdjoint(k, *A.initial_state_torch(cfg, theta, d), T, K, cfg.isav) as adj:
+        t_rec, _ = timed(lambda: adj.forward(T))
+        Bf = adj.final_B()
+        t_rev, _ = timed(lambda: adj.backward([torch.zeros_like(b) for b in Bf],
+                                              [torch.ones_like(b) * 1e-3 for b in Bf]))
+    torch.cuda.empty_cache()
+    return {"workload": "harris_512x256_ppc32", "particles": 2 * cfg.nx * cfg.ny * cfg.ppc,
+            "steps": T, "checkpoint": K, "flux": F, "dflux_dtheta": [float(x) for x in g],
+            "forward_ms_per_step": t_fwd * 1e3 / T,
+            "recording_forward_ms_per_step": t_rec * 1e3 / T,
+            "reverse_ms_per_step": t_rev * 1e3 / T,
+            "gradient_ms": t_grad * 1e3,
+            "gradient_over_forward": t_grad / t_fwd,
+            "forward": "em2g_step FP64, exact (spectral) Poisson solve"}
 
 
 def run_ensemble(args, local):
@@ -495,6 +547,11 @@ def C_get_particles_into(g, s, out):
 
 def main():
     args = parse()
+    if args.only_adjoint:
+        from maccpic_b200 import build
+        build.build()
+        print(json.dumps({"adjoint": run_adjoint(args, 0)}), flush=True)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:
