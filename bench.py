@@ -58,8 +58,9 @@ def parse():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--only-adjoint", action="store_true",
                     help="run only the adjoint leg and print its JSON")
-    ap.add_argument("--adjoint-steps", type=int, default=40)
-    ap.add_argument("--adjoint-checkpoint", type=int, default=20)
+    # the 512x256 workload's adjoint: 800 steps, checkpoints every 50
+    ap.add_argument("--adjoint-steps", type=int, default=800)
+    ap.add_argument("--adjoint-checkpoint", type=int, default=50)
     return ap.parse_args()
 
 

@@ -67,7 +67,12 @@ namespace {
 constexpr int TCX = 32, G = 4, WY = 6, WX = TCX + 5;
 constexpr int kRegroup = 8;  // reverse steps between regroupings
 
+// periodic wrap of an index within one period of [0, n)
 __device__ __forceinline__ int wrapi(int i, int n) {
+  return i < 0 ? i + n : (i >= n ? i - n : i);
+}
+// periodic wrap of any index (the window may be wider than the grid)
+__device__ __forceinline__ int wrapm(int i, int n) {
   i %= n;
   return i < 0 ? i + n : i;
 }
@@ -89,17 +94,17 @@ __device__ __forceinline__ W3 w_node(double x) {
   return W3{ix, 0.5 * f * f, 0.75 - d * d, 0.5 * e * e, -f, -2.0 * d, e};
 }
 
-// where a 3x3 stencil sits: window coordinates (col, row of node i-1, j-1)
-// or, outside the window, periodic array indices of its three columns/rows
+// where a 3x3 stencil sits: in the window (column, row of its first node)
+// or, outside it, em2's indices of its middle node (periodic wrap applied at
+// use).  The weights travel separately.
 struct Sten {
   bool win;
-  int c0, r0;
-  int gx[3], gy[3];
-  W3 wx, wy;
+  int c0, r0;  // window column and row of em2 node (i-1, j-1)
+  int i, j;    // em2 node indices of the middle node
 };
 
 struct Seg {
-  int x0, y0, kx, ky, nx, ny;
+  int x0, y0, nx, ny;
 };
 
 // em2 node index i of a particle whose wrapped cell is cx, seen from the
@@ -109,42 +114,52 @@ __device__ __forceinline__ int unwrap_shift(int cx, int kx, int n) {
   return d > n / 2 ? -n : (d < -n / 2 ? n : 0);
 }
 
-__device__ __forceinline__ Sten make_sten(const Seg &s, const W3 &wx, const W3 &wy, int shx,
-                                          int shy) {
+__device__ __forceinline__ Sten make_sten(const Seg &s, int i, int j, int shx, int shy) {
   Sten t;
-  t.wx = wx;
-  t.wy = wy;
-  t.c0 = wx.i - 1 + shx - (s.x0 - 1);
-  t.r0 = wy.i - 1 + shy - (s.y0 - 1);
+  t.i = i;
+  t.j = j;
+  t.c0 = i - 1 + shx - (s.x0 - 1);
+  t.r0 = j - 1 + shy - (s.y0 - 1);
   t.win = t.c0 >= 0 && t.c0 + 2 < WX && t.r0 >= 0 && t.r0 + 2 < WY;
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    t.gx[a] = wrapi(wx.i - 2 + a, s.nx);  // periodic index of em2 node i-1+a
-    t.gy[a] = wrapi(wy.i - 2 + a, s.ny);
-  }
   return t;
+}
+
+// periodic array index of stencil node (a, b), a, b in 0..2 (em2 node
+// (i-1+a, j-1+b) is periodic node (i-2+a, j-2+b))
+__device__ __forceinline__ int64_t gidx(const Sten &t, int a, int b, int nx, int ny) {
+  return (int64_t)wrapi(t.j - 2 + b, ny) * nx + wrapi(t.i - 2 + a, nx);
 }
 
 struct Grad {
   double v, gx, gy;
 };
-struct Grad2 {
-  double2 v, gx, gy;
-};
 
+// value and x-, y-derivatives of sum F w_x w_y over the stencil
 __device__ __forceinline__ Grad gather_g(const double *glob, const double (*win)[WX],
-                                         const Sten &t, int nx) {
-  const double wx[3] = {t.wx.m, t.wx.s, t.wx.p}, dwx[3] = {t.wx.dm, t.wx.ds, t.wx.dp};
-  const double wy[3] = {t.wy.m, t.wy.s, t.wy.p}, dwy[3] = {t.wy.dm, t.wy.ds, t.wy.dp};
+                                         const Sten &t, const W3 &X, const W3 &Y, int nx,
+                                         int ny) {
+  const double wx[3] = {X.m, X.s, X.p}, dwx[3] = {X.dm, X.ds, X.dp};
+  const double wy[3] = {Y.m, Y.s, Y.p}, dwy[3] = {Y.dm, Y.ds, Y.dp};
+  double F[3][3];
+  if (t.win) {
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+#pragma unroll
+      for (int q = 0; q < 3; ++q) F[b][q] = win[t.r0 + b][t.c0 + q];
+  } else {
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+#pragma unroll
+      for (int q = 0; q < 3; ++q) F[b][q] = glob[gidx(t, q, b, nx, ny)];
+  }
   Grad r{0.0, 0.0, 0.0};
 #pragma unroll
   for (int b = 0; b < 3; ++b) {
     double sv = 0.0, sd = 0.0;
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      const double f = t.win ? win[t.r0 + b][t.c0 + a] : glob[(int64_t)t.gy[b] * nx + t.gx[a]];
-      sv += f * wx[a];
-      sd += f * dwx[a];
+    for (int q = 0; q < 3; ++q) {
+      sv += F[b][q] * wx[q];
+      sd += F[b][q] * dwx[q];
     }
     r.v += sv * wy[b];
     r.gx += sd * wy[b];
@@ -153,47 +168,113 @@ __device__ __forceinline__ Grad gather_g(const double *glob, const double (*win)
   return r;
 }
 
-__device__ __forceinline__ Grad2 gather_g2(const double2 *glob, const double2 (*win)[WX],
-                                           const Sten &t, int nx) {
-  const double wx[3] = {t.wx.m, t.wx.s, t.wx.p}, dwx[3] = {t.wx.dm, t.wx.ds, t.wx.dp};
-  const double wy[3] = {t.wy.m, t.wy.s, t.wy.p}, dwy[3] = {t.wy.dm, t.wy.ds, t.wy.dp};
-  Grad2 r;
-  r.v = r.gx = r.gy = make_double2(0.0, 0.0);
+// value of sum (E, B) w_x w_y over the stencil
+__device__ __forceinline__ double2 gather_v2(const double2 *glob, const double2 (*win)[WX],
+                                             const Sten &t, const W3 &X, const W3 &Y, int nx,
+                                             int ny) {
+  const double wx[3] = {X.m, X.s, X.p}, wy[3] = {Y.m, Y.s, Y.p};
+  double2 F[3][3];
+  if (t.win) {
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+#pragma unroll
+      for (int q = 0; q < 3; ++q) F[b][q] = win[t.r0 + b][t.c0 + q];
+  } else {
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+#pragma unroll
+      for (int q = 0; q < 3; ++q) F[b][q] = glob[gidx(t, q, b, nx, ny)];
+  }
+  double2 r = make_double2(0.0, 0.0);
 #pragma unroll
   for (int b = 0; b < 3; ++b) {
-    double2 sv = make_double2(0.0, 0.0), sd = make_double2(0.0, 0.0);
+    double2 sv = make_double2(0.0, 0.0);
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      const double2 f =
-          t.win ? win[t.r0 + b][t.c0 + a] : glob[(int64_t)t.gy[b] * nx + t.gx[a]];
-      sv.x += f.x * wx[a];
-      sv.y += f.y * wx[a];
-      sd.x += f.x * dwx[a];
-      sd.y += f.y * dwx[a];
+    for (int q = 0; q < 3; ++q) {
+      const double2 f = F[b][q];
+      sv.x += f.x * wx[q];
+      sv.y += f.y * wx[q];
     }
-    r.v.x += sv.x * wy[b];
-    r.v.y += sv.y * wy[b];
-    r.gx.x += sd.x * wy[b];
-    r.gx.y += sd.y * wy[b];
-    r.gy.x += sv.x * dwy[b];
-    r.gy.y += sv.y * dwy[b];
+    r.x += sv.x * wy[b];
+    r.y += sv.y * wy[b];
   }
   return r;
 }
 
-__device__ __forceinline__ void scatter_w(double *glob, double (*win)[WX], const Sten &t, int nx,
-                                          double q) {
-  const double wx[3] = {t.wx.m, t.wx.s, t.wx.p}, wy[3] = {t.wy.m, t.wy.s, t.wy.p};
+// Per-lane accumulators of the E and B adjoints a lane's cell can receive
+// from its in-cell particles, every stencil position covered: nodes
+// (kx .. kx+3, ky .. ky+3) in em2 indices; x staggering (half, node) 3x4,
+// y staggering (node, half) 4x3, z staggering (half, half) 3x3, for E then B.
+// Stored entry-major, lane-minor ([kBlk][threads]): no bank conflicts, no
+// atomics.
+constexpr int kBlk = 66;
+// first entry of component c (lEx lEy lEz lBx lBy lBz) and entries per row
+__host__ __device__ constexpr int blk_off(int c) {
+  return c == 0 ? 0 : c == 1 ? 12 : c == 2 ? 24 : c == 3 ? 33 : c == 4 ? 45 : 57;
+}
+__host__ __device__ constexpr int blk_w(int c) { return c % 3 == 1 ? 4 : 3; }
+
+// The gather's transpose and its position derivative in one pass over an
+// (E, B) stencil of staggering c: add sc (qe, qb) w_x w_y to the E and B
+// adjoints -- into this lane's block when the particle is in the lane's
+// cell (block row rr, column cc of the stencil's first node), else into the
+// arrays with atomics -- and return (qe dE/dx + qb dB/dx, qe dE/dy + qb
+// dB/dy) of the gathered pair.
+__device__ __forceinline__ double2 scatter_grad2(const double2 *glob, const double2 (*win)[WX],
+                                                 double *ge, double *gb, double *blk, int c,
+                                                 bool incell, int rr, int cc, const Sten &t,
+                                                 const W3 &X, const W3 &Y, int nx, int ny,
+                                                 double qe, double qb, double sc) {
+  const double wx[3] = {X.m, X.s, X.p}, dwx[3] = {X.dm, X.ds, X.dp};
+  const double wy[3] = {Y.m, Y.s, Y.p}, dwy[3] = {Y.dm, Y.ds, Y.dp};
+  constexpr int kLanes = TCX * G;
+  const int bw = blk_w(c);
+  double *be = blk + (int64_t)(blk_off(c) + rr * bw + cc) * kLanes;
+  double *bb = blk + (int64_t)(blk_off(c + 3) + rr * bw + cc) * kLanes;
+  double gx = 0.0, gy = 0.0;
+  const double se = sc * qe, sb = sc * qb;
+  double2 F[3][3];
+  if (t.win) {
 #pragma unroll
-  for (int b = 0; b < 3; ++b)
+    for (int b = 0; b < 3; ++b)
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      const double v = q * wy[b] * wx[a];
-      if (t.win)
-        atomicAdd(&win[t.r0 + b][t.c0 + a], v);
-      else
-        atomicAdd(glob + (int64_t)t.gy[b] * nx + t.gx[a], v);
+      for (int q = 0; q < 3; ++q) F[b][q] = win[t.r0 + b][t.c0 + q];
+  } else {
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+#pragma unroll
+      for (int q = 0; q < 3; ++q) F[b][q] = glob[gidx(t, q, b, nx, ny)];
+  }
+#pragma unroll
+  for (int b = 0; b < 3; ++b) {
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      const double h = qe * F[b][q].x + qb * F[b][q].y;
+      gx += h * dwx[q] * wy[b];
+      gy += h * wx[q] * dwy[b];
     }
+  }
+  if (incell) {
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        const double w = wx[q] * wy[b];
+        be[(b * bw + q) * kLanes] += se * w;
+        bb[(b * bw + q) * kLanes] += sb * w;
+      }
+  } else {
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        const double w = wx[q] * wy[b];
+        const int64_t k = gidx(t, q, b, nx, ny);
+        atomicAdd(ge + k, se * w);
+        atomicAdd(gb + k, sb * w);
+      }
+  }
+  return make_double2(gx, gy);
 }
 
 __device__ __forceinline__ double3 cross3(double3 a, double3 b) {
@@ -223,6 +304,8 @@ struct RevArgs {
   double ae, qd, dtdx, dtdy, c;
 };
 
+constexpr int kBlkBytes = kBlk * TCX * G * (int)sizeof(double);
+
 // One reverse step of one species: rebuild each particle's state before the
 // step, then the transposed move + curnt.  Staggerings: Ex, Bx, Jx (half, node);
 // Ey, By, Jy (node, half); Ez, Bz, Jz (half, half); rho (node, node).
@@ -230,13 +313,13 @@ __global__ void __launch_bounds__(TCX *G) k_adj_push(RevArgs a) {
   __shared__ double2 w_eb[3][WY][WX];  // 0: (E,B)x, 1: (E,B)z, 2: (E,B)y
   __shared__ double w_lj[3][WY][WX];   // lJx, lJy, lJz
   __shared__ double w_lr[WY][WX];
-  __shared__ double w_acc[6][WY][WX];  // lEx lEy lEz lBx lBy lBz
+  extern __shared__ double blk[];      // kBlk x (TCX*G): per-lane E and B adjoints
   const int nx = a.nx, ny = a.ny;
-  const Seg seg{(int)blockIdx.x * TCX, (int)blockIdx.y, 0, 0, nx, ny};
+  const Seg seg{(int)blockIdx.x * TCX, (int)blockIdx.y, nx, ny};
   for (int t = threadIdx.x; t < WY * WX; t += blockDim.x) {
     const int r = t / WX, col = t % WX;
     // window node (em2 index x0-1+col, y0-1+r) -> periodic (index-1)
-    const int64_t k = (int64_t)wrapi(seg.y0 - 2 + r, ny) * nx + wrapi(seg.x0 - 2 + col, nx);
+    const int64_t k = (int64_t)wrapm(seg.y0 - 2 + r, ny) * nx + wrapm(seg.x0 - 2 + col, nx);
     w_eb[0][r][col] = a.ebx[k];
     w_eb[1][r][col] = a.ebz[k];
     w_eb[2][r][col] = a.eby[k];
@@ -244,9 +327,8 @@ __global__ void __launch_bounds__(TCX *G) k_adj_push(RevArgs a) {
     w_lj[1][r][col] = a.ljy[k];
     w_lj[2][r][col] = a.ljz[k];
     w_lr[r][col] = a.lrho[k];
-#pragma unroll
-    for (int q = 0; q < 6; ++q) w_acc[q][r][col] = 0.0;
   }
+  for (int e = 0; e < kBlk; ++e) blk[e * (TCX * G) + threadIdx.x] = 0.0;
   __syncthreads();
 
   const int gl = threadIdx.x & (G - 1);
@@ -258,11 +340,9 @@ __global__ void __launch_bounds__(TCX *G) k_adj_push(RevArgs a) {
     const int32_t beg = a.off[cell], end = a.off[cell + 1];
     const double q = a.qd;
     for (int32_t i = beg + gl; i < end; i += G) {
-      // the state after the step and its adjoints
+      // the state after the step
       const double x1 = P[i], y1 = P[n + i];
       const double3 u1 = make_double3(P[2 * n + i], P[3 * n + i], P[4 * n + i]);
-      double lx1 = P[5 * n + i], ly1 = P[6 * n + i];
-      const double3 lu1 = make_double3(P[7 * n + i], P[8 * n + i], P[9 * n + i]);
       const double g1 = sqrt(1.0 + dot3(u1, u1));
       const double3 v = mul3(1.0 / g1, u1);
       // rebuild the position before the move (pic/curnt.f90:181-194)
@@ -270,63 +350,78 @@ __global__ void __launch_bounds__(TCX *G) k_adj_push(RevArgs a) {
       if (x0 < 0.0) x0 += nx; else if (x0 >= nx) x0 -= nx;
       if (y0 < 0.0) y0 += ny; else if (y0 >= ny) y0 -= ny;
       const int sx0 = unwrap_shift((int)x0, kx, nx), sy0 = unwrap_shift((int)y0, ky, ny);
-      const int sx1 = unwrap_shift((int)x1, kx, nx), sy1 = unwrap_shift((int)y1, ky, ny);
       const W3 hx0 = w_half(x0), nx0 = w_node(x0), hy0 = w_half(y0), ny0 = w_node(y0);
-      const W3 hx1 = w_half(x1), nx1 = w_node(x1), hy1 = w_half(y1), ny1 = w_node(y1);
-      const Sten s_hn0 = make_sten(seg, hx0, ny0, sx0, sy0);  // x staggering
-      const Sten s_nh0 = make_sten(seg, nx0, hy0, sx0, sy0);  // y staggering
-      const Sten s_hh0 = make_sten(seg, hx0, hy0, sx0, sy0);  // z staggering
-      // scaled fields before the step at the old position, with gradients
-      const Grad2 gbx = gather_g2(a.ebx, w_eb[0], s_hn0, nx);
-      const Grad2 gbz = gather_g2(a.ebz, w_eb[1], s_hh0, nx);
-      const Grad2 gby = gather_g2(a.eby, w_eb[2], s_nh0, nx);
-      const double3 aE = make_double3(gbx.v.x, gby.v.x, gbz.v.x);
-      const double3 aB = make_double3(gbx.v.y, gby.v.y, gbz.v.y);
+      const Sten s_x0 = make_sten(seg, hx0.i, ny0.i, sx0, sy0);  // x staggering (half, node)
+      const Sten s_y0 = make_sten(seg, nx0.i, hy0.i, sx0, sy0);  // y staggering (node, half)
+      const Sten s_z0 = make_sten(seg, hx0.i, hy0.i, sx0, sy0);  // z staggering (half, half)
+      // scaled fields before the step at the old position
+      const double2 ebx = gather_v2(a.ebx, w_eb[0], s_x0, hx0, ny0, nx, ny);
+      const double2 ebz = gather_v2(a.ebz, w_eb[1], s_z0, hx0, hy0, nx, ny);
+      const double2 eby = gather_v2(a.eby, w_eb[2], s_y0, nx0, hy0, nx, ny);
+      const double3 aE = make_double3(ebx.x, eby.x, ebz.x);
+      const double3 aB = make_double3(ebx.y, eby.y, ebz.y);
       // rebuild u before the Boris rotation (pic/move.f90:176-203): the
       // rotation about t by the opposite angle
-      const double3 upl_b = sub3(u1, aE);
-      const double3 tb = mul3(1.0 / (a.c * sqrt(1.0 + dot3(upl_b, upl_b))), aB);
-      const double3 up_b = sub3(upl_b, cross3(upl_b, tb));
-      const double3 sb = mul3(2.0 / (1.0 + dot3(tb, tb)), tb);
-      const double3 u0 = sub3(sub3(upl_b, cross3(up_b, sb)), aE);
-      // the forward intermediates from the rebuilt state
-      const double3 um = add3(u0, aE);
-      const double gm = sqrt(1.0 + dot3(um, um));
-      const double3 t = mul3(1.0 / (a.c * gm), aB);
-      const double3 up = add3(um, cross3(um, t));
-      const double f = 2.0 / (1.0 + dot3(t, t));
-      const double3 s = mul3(f, t);
-      // transposed deposits: rho and jp at the new position, jm at the old
-      const Sten s_nn1 = make_sten(seg, nx1, ny1, sx1, sy1);
-      const Grad gr = gather_g(a.lrho, w_lr, s_nn1, nx);
-      double lxn = lx1 + q * gr.gx, lyn = ly1 + q * gr.gy;
-      double lx = 0.0, ly = 0.0;
-      double lv[3];
-      const Sten s1[3] = {make_sten(seg, hx1, ny1, sx1, sy1), make_sten(seg, nx1, hy1, sx1, sy1),
-                          make_sten(seg, hx1, hy1, sx1, sy1)};
-      const Sten *s0[3] = {&s_hn0, &s_nh0, &s_hh0};
-      const double vv[3] = {v.x, v.y, v.z};
-      const double *ljg[3] = {a.ljx, a.ljy, a.ljz};
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const Grad j1 = gather_g(ljg[c], w_lj[c], s1[c], nx);
-        const Grad j0 = gather_g(ljg[c], w_lj[c], *s0[c], nx);
-        lv[c] = q * (j1.v + j0.v);
-        lxn += q * vv[c] * j1.gx;
-        lyn += q * vv[c] * j1.gy;
-        lx += q * vv[c] * j0.gx;
-        ly += q * vv[c] * j0.gy;
+      double3 um, t, up, s;
+      double gm, f;
+      {
+        const double3 upl_b = sub3(u1, aE);
+        const double3 tb = mul3(1.0 / (a.c * sqrt(1.0 + dot3(upl_b, upl_b))), aB);
+        const double3 up_b = sub3(upl_b, cross3(upl_b, tb));
+        const double3 sb = mul3(2.0 / (1.0 + dot3(tb, tb)), tb);
+        const double3 u0 = sub3(sub3(upl_b, cross3(up_b, sb)), aE);
+        // the forward intermediates from the rebuilt state
+        um = add3(u0, aE);
+        gm = sqrt(1.0 + dot3(um, um));
+        t = mul3(1.0 / (a.c * gm), aB);
+        up = add3(um, cross3(um, t));
+        f = 2.0 / (1.0 + dot3(t, t));
+        s = mul3(f, t);
+        P[2 * n + i] = u0.x;
+        P[3 * n + i] = u0.y;
+        P[4 * n + i] = u0.z;
       }
-      // move: x1 = x0 + v dt/dx
-      lx += lxn;
-      ly += lyn;
-      lv[0] += lxn * a.dtdx;
-      lv[1] += lyn * a.dtdy;
+      const double vv[3] = {v.x, v.y, v.z};
+      double lv[3] = {0.0, 0.0, 0.0};
+      double lx, ly;
+      {  // transposed deposits at the new position: rho and jp
+        const int sx1 = unwrap_shift((int)x1, kx, nx), sy1 = unwrap_shift((int)y1, ky, ny);
+        const W3 hx1 = w_half(x1), nx1 = w_node(x1), hy1 = w_half(y1), ny1 = w_node(y1);
+        const Grad gr = gather_g(a.lrho, w_lr, make_sten(seg, nx1.i, ny1.i, sx1, sy1), nx1, ny1,
+                                 nx, ny);
+        double lxn = P[5 * n + i] + q * gr.gx, lyn = P[6 * n + i] + q * gr.gy;
+        const Grad jx = gather_g(a.ljx, w_lj[0], make_sten(seg, hx1.i, ny1.i, sx1, sy1), hx1,
+                                 ny1, nx, ny);
+        const Grad jy = gather_g(a.ljy, w_lj[1], make_sten(seg, nx1.i, hy1.i, sx1, sy1), nx1,
+                                 hy1, nx, ny);
+        const Grad jz = gather_g(a.ljz, w_lj[2], make_sten(seg, hx1.i, hy1.i, sx1, sy1), hx1,
+                                 hy1, nx, ny);
+        lv[0] = q * jx.v;
+        lv[1] = q * jy.v;
+        lv[2] = q * jz.v;
+        lxn += q * (vv[0] * jx.gx + vv[1] * jy.gx + vv[2] * jz.gx);
+        lyn += q * (vv[0] * jx.gy + vv[1] * jy.gy + vv[2] * jz.gy);
+        // move: x1 = x0 + v dt/dx
+        lx = lxn;
+        ly = lyn;
+        lv[0] += lxn * a.dtdx;
+        lv[1] += lyn * a.dtdy;
+      }
+      {  // jm at the old position
+        const Grad jx = gather_g(a.ljx, w_lj[0], s_x0, hx0, ny0, nx, ny);
+        const Grad jy = gather_g(a.ljy, w_lj[1], s_y0, nx0, hy0, nx, ny);
+        const Grad jz = gather_g(a.ljz, w_lj[2], s_z0, hx0, hy0, nx, ny);
+        lv[0] += q * jx.v;
+        lv[1] += q * jy.v;
+        lv[2] += q * jz.v;
+        lx += q * (vv[0] * jx.gx + vv[1] * jy.gx + vv[2] * jz.gx);
+        ly += q * (vv[0] * jx.gy + vv[1] * jy.gy + vv[2] * jz.gy);
+      }
       // v = u1 / gamma(u1)
       const double3 lvv = make_double3(lv[0], lv[1], lv[2]);
       const double dt_ = dot3(lvv, u1);
       double3 lun = sub3(mul3(1.0 / g1, lvv), mul3(dt_ / (g1 * g1 * g1), u1));
-      lun = add3(lun, lu1);
+      lun = add3(lun, make_double3(P[7 * n + i], P[8 * n + i], P[9 * n + i]));
       // Boris, reversed stage by stage
       double3 laE = lun;
       double3 lum = lun;
@@ -341,23 +436,29 @@ __global__ void __launch_bounds__(TCX *G) k_adj_push(RevArgs a) {
       const double lg = -dot3(lt, t) / gm;
       lum = add3(lum, mul3(lg / gm, um));
       laE = add3(laE, lum);
-      // transposed gather: the force adjoint onto E and B
-      scatter_w(a.lE[0], w_acc[0], s_hn0, nx, a.ae * laE.x);
-      scatter_w(a.lE[1], w_acc[1], s_nh0, nx, a.ae * laE.y);
-      scatter_w(a.lE[2], w_acc[2], s_hh0, nx, a.ae * laE.z);
-      scatter_w(a.lB[0], w_acc[3], s_hn0, nx, a.ae * laB.x);
-      scatter_w(a.lB[1], w_acc[4], s_nh0, nx, a.ae * laB.y);
-      scatter_w(a.lB[2], w_acc[5], s_hh0, nx, a.ae * laB.z);
-      lx += laE.x * gbx.gx.x + laB.x * gbx.gx.y + laE.y * gby.gx.x + laB.y * gby.gx.y +
-            laE.z * gbz.gx.x + laB.z * gbz.gx.y;
-      ly += laE.x * gbx.gy.x + laB.x * gbx.gy.y + laE.y * gby.gy.x + laB.y * gby.gy.y +
-            laE.z * gbz.gy.x + laB.z * gbz.gy.y;
+      // transposed gather: the force adjoint onto E and B, and the gathered
+      // fields' position derivatives
+      const double ae = a.ae;
+      // in the lane's cell: half-staggered stencils start at the cell's node,
+      // node-staggered ones at it or the next
+      const bool incell = (int)x0 == kx && (int)y0 == ky;
+      const int ch = hx0.i - 1 - kx, cn = nx0.i - 1 - kx;
+      const int rh = hy0.i - 1 - ky, rn = ny0.i - 1 - ky;
+      double2 d = scatter_grad2(a.ebx, w_eb[0], a.lE[0], a.lB[0], blk + threadIdx.x, 0, incell,
+                                rn, ch, s_x0, hx0, ny0, nx, ny, laE.x, laB.x, ae);
+      lx += d.x;
+      ly += d.y;
+      d = scatter_grad2(a.eby, w_eb[2], a.lE[1], a.lB[1], blk + threadIdx.x, 1, incell, rh, cn,
+                        s_y0, nx0, hy0, nx, ny, laE.y, laB.y, ae);
+      lx += d.x;
+      ly += d.y;
+      d = scatter_grad2(a.ebz, w_eb[1], a.lE[2], a.lB[2], blk + threadIdx.x, 2, incell, rh, ch,
+                        s_z0, hx0, hy0, nx, ny, laE.z, laB.z, ae);
+      lx += d.x;
+      ly += d.y;
       // the state before the step and its adjoints, in place
       P[i] = x0;
       P[n + i] = y0;
-      P[2 * n + i] = u0.x;
-      P[3 * n + i] = u0.y;
-      P[4 * n + i] = u0.z;
       P[5 * n + i] = lx;
       P[6 * n + i] = ly;
       P[7 * n + i] = lum.x;
@@ -366,16 +467,23 @@ __global__ void __launch_bounds__(TCX *G) k_adj_push(RevArgs a) {
     }
   }
   __syncthreads();
-  // the window's E and B adjoints into the arrays (windows of neighbouring
-  // segments overlap)
-  for (int t = threadIdx.x; t < WY * WX; t += blockDim.x) {
-    const int r = t / WX, col = t % WX;
-    const int64_t k = (int64_t)wrapi(seg.y0 - 2 + r, ny) * nx + wrapi(seg.x0 - 2 + col, nx);
+  // every cell's four lane blocks summed and added to the arrays once
+  // (blocks of neighbouring cells and segments overlap: atomics)
+  for (int t = threadIdx.x; t < TCX * kBlk; t += blockDim.x) {
+    const int cl = t / kBlk, e = t - cl * kBlk;
+    const int cx = seg.x0 + cl;
+    if (cx >= nx) continue;
+    double v = 0.0;
 #pragma unroll
-    for (int qq = 0; qq < 6; ++qq) {
-      const double v = w_acc[qq][r][col];
-      if (v != 0.0) atomicAdd((qq < 3 ? a.lE[qq] : a.lB[qq - 3]) + k, v);
-    }
+    for (int l = 0; l < G; ++l) v += blk[e * (TCX * G) + cl * G + l];
+    if (v == 0.0) continue;
+    const int comp = e < 12 ? 0 : e < 24 ? 1 : e < 33 ? 2 : e < 45 ? 3 : e < 57 ? 4 : 5;
+    const int w = blk_w(comp), f = e - blk_off(comp);
+    const int row = f / w, col = f - row * w;
+    // em2 node (cx + col, seg.y0 + row) -> periodic (index - 1)
+    const int64_t k =
+        (int64_t)wrapi(seg.y0 + row - 1, ny) * nx + wrapi(cx + col - 1, nx);
+    atomicAdd((comp < 3 ? a.lE[comp] : a.lB[comp - 3]) + k, v);
   }
 }
 
@@ -697,6 +805,8 @@ int em2g_adj_create(em2g_ctx *ctx, int max_steps, int checkpoint, em2g_adj **out
 #undef ALLOC
   int rc = spectral_prepare();
   if (rc) return bail(rc);
+  e = cudaFuncSetAttribute(k_adj_push, cudaFuncAttributeMaxDynamicSharedMemorySize, kBlkBytes);
+  if (e != cudaSuccess) return bail(cuda_fail(e, "cudaFuncSetAttribute"));
   *out = a;
   return EM2G_OK;
 }
@@ -805,7 +915,7 @@ int em2g_adj_backward(em2g_adj *a) {
       r.c = a->c;
       if (r.n > 0) {
         const dim3 grid((unsigned)((a->nx + TCX - 1) / TCX), (unsigned)a->ny);
-        k_adj_push<<<grid, TCX * G, 0, st>>>(r);
+        k_adj_push<<<grid, TCX * G, kBlkBytes, st>>>(r);
       }
       // at a checkpoint the kept exact state replaces the rebuilt one
       if (k % a->K == 0 && r.n > 0)
