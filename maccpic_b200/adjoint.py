@@ -687,7 +687,9 @@ class CudaAdjoint:
     forward(T) advances the state keeping what the reverse sweep needs,
     backward(seed) returns the adjoints of the state forward started from.
     The state enters as (E, B, parts) in this module's periodic, u = gamma v
-    form; its first step number is it0."""
+    form; its first step number is it0.  load() replaces the state, so one
+    object (and its device buffers: E, B of every step and the checkpointed
+    particles) serves many gradients of runs of the same shape."""
 
     def __init__(self, k: StepConst, E, B, parts, max_steps: int, checkpoint: int,
                  isav: int, smooth_current: int = 0, it0: int = 0):
@@ -704,9 +706,24 @@ class CudaAdjoint:
                        dn=[1.0] * self.nsp, am=[1.0] * self.nsp, np_max=n, isav=isav,
                        precision=_lib.FP64, poisson=1, smooth_current=smooth_current)
         self.g = Em2Gpu(rp)
-        dev = E[0].device
+        self.dev = E[0].device
+        self.n = n
+        self.max_steps, self.checkpoint, self.isav = int(max_steps), int(checkpoint), isav
+        self.smooth_current = smooth_current
         # the library works on torch's stream: uploads follow their producers
-        self.g.set_stream(torch.cuda.current_stream(dev))
+        self.g.set_stream(torch.cuda.current_stream(self.dev))
+        self.load(E, B, parts, it0)
+        h = C.c_void_p()
+        check(self._L.em2g_adj_create(self.g._h, self.max_steps, self.checkpoint, C.byref(h)))
+        self._h = h
+
+    def load(self, E, B, parts, it0: int = 0):
+        """Replace the context's state (same grid and particle counts)."""
+        import ctypes as C
+        from ._lib import check
+        if [int(p[0].numel()) for p in parts] != self.n or tuple(E[0].shape) != (self.k.ny,
+                                                                                 self.k.nx):
+            raise ValueError("state of another shape than this adjoint's")
         fld = _guarded_block([e.detach() for e in E], [b.detach() for b in B]).contiguous()
         check(self._L.em2g_set_fields_device(self.g._h, C.c_void_p(fld.data_ptr())))
         for s, (x, y, ux, uy, uz) in enumerate(parts):
@@ -716,12 +733,7 @@ class CudaAdjoint:
                               gam]).contiguous()
             self.g.set_particles_device(s, st)
         self.g.it = it0
-        torch.cuda.synchronize(dev)
-        h = C.c_void_p()
-        check(self._L.em2g_adj_create(self.g._h, int(max_steps), int(checkpoint), C.byref(h)))
-        self._h = h
-        self.dev = dev
-        self.n = n
+        torch.cuda.synchronize(self.dev)
 
     def close(self):
         from ._lib import check
@@ -773,16 +785,26 @@ class CudaAdjoint:
 
 
 def theta_gradient_cuda(cfg, theta, steps: int, checkpoint: int = 50, draws=None,
-                        device="cuda"):
+                        device="cuda", workspace: "CudaAdjoint | None" = None):
     """flux(T) and d flux(T) / d theta with the CUDA step and its adjoint
-    (exact Poisson solve); autograd only through the initial-state map."""
+    (exact Poisson solve); autograd only through the initial-state map.
+    `workspace`: a CudaAdjoint of this config's shape with max_steps >= steps
+    and this checkpoint interval, reused instead of allocating a new one."""
+    import contextlib
     draws = draws or make_draws(cfg, device=device)
     k = step_const(cfg)
     th = torch.tensor(theta, dtype=torch.float64, device=device, requires_grad=True)
     with torch.enable_grad():
         E0, B0, P0 = initial_state_torch(cfg, (th[0], th[1], th[2]), draws)
         flat0 = _flatten(E0, B0, P0)
-    with CudaAdjoint(k, E0, B0, P0, steps, checkpoint, cfg.isav, cfg.smooth_current) as adj:
+    if workspace is not None:
+        if workspace.max_steps < steps or workspace.checkpoint != checkpoint:
+            raise ValueError("workspace made for fewer steps or another checkpoint interval")
+        workspace.load(E0, B0, P0)
+        ctx = contextlib.nullcontext(workspace)
+    else:
+        ctx = CudaAdjoint(k, E0, B0, P0, steps, checkpoint, cfg.isav, cfg.smooth_current)
+    with ctx as adj:
         adj.forward(steps)
         Bf = [b.requires_grad_(True) for b in adj.final_B()]
         with torch.enable_grad():

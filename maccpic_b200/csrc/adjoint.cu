@@ -339,10 +339,22 @@ __global__ void __launch_bounds__(TCX *G) k_adj_push(RevArgs a) {
     const int64_t cell = (int64_t)ky * nx + kx;
     const int32_t beg = a.off[cell], end = a.off[cell + 1];
     const double q = a.qd;
+    // software pipeline: the next particle's state and adjoints are loaded
+    // while this one runs
+    double nx_[10];
+    if (beg + gl < end)
+#pragma unroll
+      for (int c = 0; c < 10; ++c) nx_[c] = P[c * n + beg + gl];
     for (int32_t i = beg + gl; i < end; i += G) {
+      double cur[10];
+#pragma unroll
+      for (int c = 0; c < 10; ++c) cur[c] = nx_[c];
+      if (i + G < end)
+#pragma unroll
+        for (int c = 0; c < 10; ++c) nx_[c] = P[c * n + i + G];
       // the state after the step
-      const double x1 = P[i], y1 = P[n + i];
-      const double3 u1 = make_double3(P[2 * n + i], P[3 * n + i], P[4 * n + i]);
+      const double x1 = cur[0], y1 = cur[1];
+      const double3 u1 = make_double3(cur[2], cur[3], cur[4]);
       const double g1 = sqrt(1.0 + dot3(u1, u1));
       const double3 v = mul3(1.0 / g1, u1);
       // rebuild the position before the move (pic/curnt.f90:181-194)
@@ -389,7 +401,7 @@ __global__ void __launch_bounds__(TCX *G) k_adj_push(RevArgs a) {
         const W3 hx1 = w_half(x1), nx1 = w_node(x1), hy1 = w_half(y1), ny1 = w_node(y1);
         const Grad gr = gather_g(a.lrho, w_lr, make_sten(seg, nx1.i, ny1.i, sx1, sy1), nx1, ny1,
                                  nx, ny);
-        double lxn = P[5 * n + i] + q * gr.gx, lyn = P[6 * n + i] + q * gr.gy;
+        double lxn = cur[5] + q * gr.gx, lyn = cur[6] + q * gr.gy;
         const Grad jx = gather_g(a.ljx, w_lj[0], make_sten(seg, hx1.i, ny1.i, sx1, sy1), hx1,
                                  ny1, nx, ny);
         const Grad jy = gather_g(a.ljy, w_lj[1], make_sten(seg, nx1.i, hy1.i, sx1, sy1), nx1,
@@ -421,7 +433,7 @@ __global__ void __launch_bounds__(TCX *G) k_adj_push(RevArgs a) {
       const double3 lvv = make_double3(lv[0], lv[1], lv[2]);
       const double dt_ = dot3(lvv, u1);
       double3 lun = sub3(mul3(1.0 / g1, lvv), mul3(dt_ / (g1 * g1 * g1), u1));
-      lun = add3(lun, make_double3(P[7 * n + i], P[8 * n + i], P[9 * n + i]));
+      lun = add3(lun, make_double3(cur[7], cur[8], cur[9]));
       // Boris, reversed stage by stage
       double3 laE = lun;
       double3 lum = lun;
@@ -684,9 +696,10 @@ int regroup(em2g_adj *a, cudaStream_t st) {
     if (rc) return rc;
     if (n > 0) k_adj_scatter<<<nb, 256, 0, st>>>(P, sl, n, a->nx, a->ny, off, a->cursor, Q, ql);
     EM2G_CUDA(cudaGetLastError());
-    EM2G_CUDA(cudaMemcpyAsync(P, Q, sizeof(double) * 10 * n, cudaMemcpyDeviceToDevice, st));
-    EM2G_CUDA(cudaMemcpyAsync(sl, ql, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, st));
   }
+  // every species was regrouped into the other buffers
+  std::swap(a->work, a->work_alt);
+  std::swap(a->slot, a->slot_alt);
   return EM2G_OK;
 }
 
@@ -848,12 +861,14 @@ int em2g_adj_forward(em2g_adj *a, int nsteps) {
     EM2G_CUDA(cudaGetLastError());
     if (k % a->K == 0 && (rc = record_parts(a, a->ckpt + 5 * a->ptot * (k / a->K), st)))
       return rc;
-    if ((rc = em2g_step(c, 1, nullptr, nullptr, nullptr))) return rc;
-    // em2g_step runs the fast path only: the stored particles are its own
+    // em2g_step's pass (the fast path: the stored particles are its own),
+    // enqueued without waiting for it
+    if ((rc = step_enqueue(c))) return rc;
     a->steps = k + 1;
   }
   if ((rc = record_parts(a, a->fin, c->stream))) return rc;
   EM2G_CUDA(cudaStreamSynchronize(c->stream));
+  EM2G_CUDA(cudaGetLastError());
   return EM2G_OK;
 }
 

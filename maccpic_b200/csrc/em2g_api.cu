@@ -772,3 +772,16 @@ int em2g_step(em2g_ctx *c, int nsteps, double *ake_out, double *energies_out,
 }
 
 }  // extern "C"
+
+namespace em2g {
+
+// one pass of em2g_step enqueued on the context's stream, without reading
+// its outputs back or waiting for it
+int step_enqueue(em2g_ctx *c) {
+  int rc = fast_push_all(c);
+  if (rc) return rc;
+  c->it += 1;
+  return is_fp32(c) ? fields_f32(c, c->it, true) : fields_f64(c, c->it, true, nullptr);
+}
+
+}  // namespace em2g

@@ -160,6 +160,8 @@ inline int64_t push_partials(int nx, int ny) {
 bool spectral_size_ok(int nx, int ny);
 int spectral_prepare();
 int spectral_solve(const double *f, double *u, int nx, int ny, double2 *work, cudaStream_t st);
+// one em2g_step pass enqueued without host synchronisation (api.cu)
+int step_enqueue(em2g_ctx *c);
 // the checks em2g_create applies to a parameter block (api.cu)
 int validate_params(const em2g_params *p);
 // counts particles of a 6 x ld FP64 block outside [0, xlim) x [0, ylim)

@@ -113,3 +113,17 @@ def test_cuda_gradient_matches_central_differences(gpu):
         fd = (A.flux_of_theta_cuda(cfg, tp, steps, d)
               - A.flux_of_theta_cuda(cfg, tm, steps, d)) / (2 * h)
         assert abs(g[i] - fd) <= 0.01 * abs(fd) + 1e-9, (i, g[i], fd)
+
+
+def test_reused_workspace_gives_the_same_gradient(gpu):
+    cfg = _cfg()
+    d = A.make_draws(cfg, device="cuda")
+    k = A.step_const(cfg)
+    F0, g0 = A.theta_gradient_cuda(cfg, THETA, 8, checkpoint=4, draws=d)
+    with A.CudaAdjoint(k, *A.initial_state_torch(cfg, THETA, d), 10, 4, cfg.isav) as ws:
+        for theta in (THETA, (0.12, 0.05, 0.55), THETA):
+            F, g = A.theta_gradient_cuda(cfg, theta, 8, checkpoint=4, draws=d, workspace=ws)
+        assert F == pytest.approx(F0, rel=1e-13)
+        np.testing.assert_allclose(g, g0, rtol=1e-9, atol=1e-13)
+        with pytest.raises(ValueError):
+            A.theta_gradient_cuda(cfg, THETA, 12, checkpoint=4, draws=d, workspace=ws)
