@@ -89,19 +89,41 @@ __device__ __forceinline__ Wts node_w(int c, float f) {
   return Wts{c + 1 + up, 0.5f * a * a, 0.75f - h * h, 0.5f * b * b};
 }
 
+// Packed FP32 pairs (sm_100a's f32x2 arithmetic): one instruction for the
+// two lanes of a pair, each rounded as its scalar FMA / multiply would be.
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
+  float2 r;
+  asm("{ .reg .b64 pa, pb, pc, pd;\n\t"
+      "mov.b64 pa, {%2, %3};\n\tmov.b64 pb, {%4, %5};\n\tmov.b64 pc, {%6, %7};\n\t"
+      "fma.rn.f32x2 pd, pa, pb, pc;\n\tmov.b64 {%0, %1}, pd; }"
+      : "=f"(r.x), "=f"(r.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+  return r;
+}
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) {
+  float2 r;
+  asm("{ .reg .b64 pa, pb, pd;\n\t"
+      "mov.b64 pa, {%2, %3};\n\tmov.b64 pb, {%4, %5};\n\t"
+      "mul.rn.f32x2 pd, pa, pb;\n\tmov.b64 {%0, %1}, pd; }"
+      : "=f"(r.x), "=f"(r.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+}
+__device__ __forceinline__ float2 bc2(float v) { return make_float2(v, v); }
+
 // 9-point gather of an (E, B) pair; base points at node (i-1, j-1) of the
-// stencil in an array of row pitch `pitch`
+// stencil in an array of row pitch `pitch`.  Both members of the pair go
+// through one packed instruction per weight: (a m + b s) + c p per row,
+// then the rows combined the same way.
 __device__ __forceinline__ float2 gather_pair(const float2 *base, int pitch, const Wts &wx,
                                               const Wts &wy) {
   float2 r[3];
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
     const float2 a = base[k * pitch], b = base[k * pitch + 1], c = base[k * pitch + 2];
-    r[k].x = a.x * wx.m + b.x * wx.s + c.x * wx.p;
-    r[k].y = a.y * wx.m + b.y * wx.s + c.y * wx.p;
+    r[k] = fma2(c, bc2(wx.p), fma2(b, bc2(wx.s), mul2(a, bc2(wx.m))));
   }
-  return make_float2(r[0].x * wy.m + r[1].x * wy.s + r[2].x * wy.p,
-                     r[0].y * wy.m + r[1].y * wy.s + r[2].y * wy.p);
+  return fma2(r[2], bc2(wy.p), fma2(r[1], bc2(wy.s), mul2(r[0], bc2(wy.m))));
 }
 
 __device__ __forceinline__ void scatter9(float *A, int nxg, const Wts &wx, const Wts &wy,
@@ -120,9 +142,20 @@ __device__ __forceinline__ void scatter9(float *A, int nxg, const Wts &wx, const
   atomicAdd(rp + 1, wx.p * qp);
 }
 
+// The 49-value register block, kept as pairs where rows allow so that packed
+// FMAs update two values at once: Jx rows 4 x (2 + 1), Jy rows 3 x (2 + 2),
+// Jz rows 3 x (2 + 1), rho rows 4 x (2 + 2).
 struct Block32 {
-  float jx[4][3], jy[3][4], jz[3][3], rho[4][4];
+  float2 jx01[4], jy01[3], jy23[3], jz01[3], rho01[4], rho23[4];
+  float jx2[4], jz2[3];
 };
+// element (r, k) of each array of the block (r, k compile-time constants)
+__device__ __forceinline__ float pick4(const float2 &lo, const float2 &hi, int k) {
+  return k == 0 ? lo.x : k == 1 ? lo.y : k == 2 ? hi.x : hi.y;
+}
+__device__ __forceinline__ float pick3(const float2 &lo, float last, int k) {
+  return k == 0 ? lo.x : k == 1 ? lo.y : last;
+}
 
 __device__ __forceinline__ void spread4(const Wts &w, int c, float o[4]) {
   const bool lo = (w.i == c + 1);
@@ -140,19 +173,21 @@ __device__ __forceinline__ void block_add_j(Block32 &b, int cx, int cy, const Wt
   spread4(nxw, cx, wxn);
   spread4(nyw, cy, wyn);
   const float wxh[3] = {hx.m, hx.s, hx.p}, wyh[3] = {hy.m, hy.s, hy.p};
+  const float2 h01 = make_float2(wxh[0], wxh[1]);
+  const float2 n01 = make_float2(wxn[0], wxn[1]), n23 = make_float2(wxn[2], wxn[3]);
 #pragma unroll
   for (int r = 0; r < 4; ++r) {
     const float t = wyn[r] * qx;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) b.jx[r][k] = fmaf(wxh[k], t, b.jx[r][k]);
+    b.jx01[r] = fma2(h01, bc2(t), b.jx01[r]);
+    b.jx2[r] = fmaf(wxh[2], t, b.jx2[r]);
   }
 #pragma unroll
   for (int r = 0; r < 3; ++r) {
     const float ty = wyh[r] * qy, tz = wyh[r] * qz;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) b.jy[r][k] = fmaf(wxn[k], ty, b.jy[r][k]);
-#pragma unroll
-    for (int k = 0; k < 3; ++k) b.jz[r][k] = fmaf(wxh[k], tz, b.jz[r][k]);
+    b.jy01[r] = fma2(n01, bc2(ty), b.jy01[r]);
+    b.jy23[r] = fma2(n23, bc2(ty), b.jy23[r]);
+    b.jz01[r] = fma2(h01, bc2(tz), b.jz01[r]);
+    b.jz2[r] = fmaf(wxh[2], tz, b.jz2[r]);
   }
 }
 
@@ -161,11 +196,12 @@ __device__ __forceinline__ void block_add_rho(Block32 &b, int cx, int cy, const 
   float wxn[4], wyn[4];
   spread4(nxw, cx, wxn);
   spread4(nyw, cy, wyn);
+  const float2 n01 = make_float2(wxn[0], wxn[1]), n23 = make_float2(wxn[2], wxn[3]);
 #pragma unroll
   for (int r = 0; r < 4; ++r) {
     const float t = wyn[r] * q;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) b.rho[r][k] = fmaf(wxn[k], t, b.rho[r][k]);
+    b.rho01[r] = fma2(n01, bc2(t), b.rho01[r]);
+    b.rho23[r] = fma2(n23, bc2(t), b.rho23[r]);
   }
 }
 
@@ -227,15 +263,16 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
   const unsigned gmask = 0xFu << (lane & ~(G - 1));  // this lane's group in the warp
 
   Block32 b;
+  const float2 z2 = make_float2(0.0f, 0.0f);
 #pragma unroll
-  for (int r = 0; r < 4; ++r)
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      b.rho[r][k] = 0.0f;
-      if (k < 3) b.jx[r][k] = 0.0f;
-      if (r < 3) b.jy[r][k] = 0.0f;
-      if (r < 3 && k < 3) b.jz[r][k] = 0.0f;
+  for (int r = 0; r < 4; ++r) {
+    b.rho01[r] = b.rho23[r] = b.jx01[r] = z2;
+    b.jx2[r] = 0.0f;
+    if (r < 3) {
+      b.jy01[r] = b.jy23[r] = b.jz01[r] = z2;
+      b.jz2[r] = 0.0f;
     }
+  }
   double akel = 0.0;
   int stay_new = 0;  // particles of this lane whose new position is in cell k
   int home_count = 0;  // particles of this group written to the front of cell k
@@ -372,7 +409,7 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
     for (int r = 0; r < 4; ++r)
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
-        const float v = group_sum(b.rho[r][k]);
+        const float v = group_sum(pick4(b.rho01[r], b.rho23[r], k));
         if (valid) flush_one(a.rho, nxg, kx + k, ky + r, v, e, gl);
         ++e;
       }
@@ -380,7 +417,7 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
     for (int r = 0; r < 4; ++r)
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
-        const float v = group_sum(b.jx[r][k]);
+        const float v = group_sum(pick3(b.jx01[r], b.jx2[r], k));
         if (valid) flush_one(a.jx, nxg, kx + k, ky + r, v, e, gl);
         ++e;
       }
@@ -388,7 +425,7 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
     for (int r = 0; r < 3; ++r)
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
-        const float v = group_sum(b.jy[r][k]);
+        const float v = group_sum(pick4(b.jy01[r], b.jy23[r], k));
         if (valid) flush_one(a.jy, nxg, kx + k, ky + r, v, e, gl);
         ++e;
       }
@@ -396,7 +433,7 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
     for (int r = 0; r < 3; ++r)
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
-        const float v = group_sum(b.jz[r][k]);
+        const float v = group_sum(pick3(b.jz01[r], b.jz2[r], k));
         if (valid) flush_one(a.jz, nxg, kx + k, ky + r, v, e, gl);
         ++e;
       }
