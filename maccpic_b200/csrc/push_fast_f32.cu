@@ -77,18 +77,6 @@ struct Wts {
   float m, s, p;  // weights of nodes i-1, i, i+1
 };
 
-__device__ __forceinline__ Wts half_w(int c, float f) {
-  const float d = f - 0.5f;
-  const float e = 1.0f - f;
-  return Wts{c + 1, 0.5f * e * e, 0.75f - d * d, 0.5f * f * f};
-}
-__device__ __forceinline__ Wts node_w(int c, float f) {
-  const int up = f >= 0.5f ? 1 : 0;
-  const float h = f - (float)up;
-  const float a = 0.5f - h, b = 0.5f + h;
-  return Wts{c + 1 + up, 0.5f * a * a, 0.75f - h * h, 0.5f * b * b};
-}
-
 // Packed FP32 pairs (sm_100a's f32x2 arithmetic): one instruction for the
 // two lanes of a pair, each rounded as its scalar FMA / multiply would be.
 __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
@@ -110,6 +98,36 @@ __device__ __forceinline__ float2 mul2(float2 a, float2 b) {
   return r;
 }
 __device__ __forceinline__ float2 bc2(float v) { return make_float2(v, v); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) {
+  float2 r;
+  asm("{ .reg .b64 pa, pb, pd;\n\t"
+      "mov.b64 pa, {%2, %3};\n\tmov.b64 pb, {%4, %5};\n\t"
+      "add.rn.f32x2 pd, pa, pb;\n\tmov.b64 {%0, %1}, pd; }"
+      : "=f"(r.x), "=f"(r.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+}
+
+// The quadratic weights of both axes at once for offsets f = (fx, fy) in
+// cell (cx, cy) (the forms of the file header): cell-centred nodes, middle
+// index c+1: (1-f)^2/2, 3/4 - (f-1/2)^2, f^2/2; integer nodes, middle index
+// c+1+u with u = [f >= 1/2], h = f - u: (1/2-h)^2/2, 3/4 - h^2, (1/2+h)^2/2.
+__device__ __forceinline__ void weights2(int cx, int cy, float2 f, Wts &hx, Wts &hy, Wts &nx,
+                                         Wts &ny) {
+  const float2 half = bc2(0.5f);
+  const float2 d = add2(f, bc2(-0.5f)), e = add2(bc2(1.0f), make_float2(-f.x, -f.y));
+  const float2 hm = mul2(mul2(half, e), e), hp = mul2(mul2(half, f), f);
+  const float2 hs = fma2(make_float2(-d.x, -d.y), d, bc2(0.75f));
+  hx = Wts{cx + 1, hm.x, hs.x, hp.x};
+  hy = Wts{cy + 1, hm.y, hs.y, hp.y};
+  const int ux = f.x >= 0.5f ? 1 : 0, uy = f.y >= 0.5f ? 1 : 0;
+  const float2 h = add2(f, make_float2(-(float)ux, -(float)uy));
+  const float2 am = add2(half, make_float2(-h.x, -h.y)), bp = add2(half, h);
+  const float2 nm = mul2(mul2(half, am), am), np = mul2(mul2(half, bp), bp);
+  const float2 ns = fma2(make_float2(-h.x, -h.y), h, bc2(0.75f));
+  nx = Wts{cx + 1 + ux, nm.x, ns.x, np.x};
+  ny = Wts{cy + 1 + uy, nm.y, ns.y, np.y};
+}
 
 // 9-point gather of an (E, B) pair; base points at node (i-1, j-1) of the
 // stencil in an array of row pitch `pitch`.  Both members of the pair go
@@ -315,8 +333,8 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
       const float fx = xr - (float)ox, fy = yr - (float)oy;
       key_cur = cy * nx + cx;
       in_cell_old = (ox == 0) && (oy == 0);
-      const Wts hx = half_w(cx, fx), hy = half_w(cy, fy), nxw = node_w(cx, fx),
-                nyw = node_w(cy, fy);
+      Wts hx, hy, nxw, nyw;
+      weights2(cx, cy, make_float2(fx, fy), hx, hy, nxw, nyw);
       // gather from the shared window when the stencil is inside it (always,
       // unless the particle wrapped around the box); else from global memory
       float2 ebx, ebz, eby;
@@ -356,12 +374,14 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
       else
         deposit_j_atomic(a, hx, hy, nxw, nyw, qx, qy, qz);
       // move (pic/curnt.f90:181-194), relative to the start cell
-      const float mx = fmaf(vx, a.dtdx, fx), my = fmaf(vy, a.dtdy, fy);
+      const float2 mv = fma2(make_float2(vx, vy), make_float2(a.dtdx, a.dtdy),
+                             make_float2(fx, fy));
+      const float mx = mv.x, my = mv.y;
       const int nox = floor_small(mx), noy = floor_small(my);
       const int ncx = wrap(cx + nox, nx), ncy = wrap(cy + noy, ny);
       const float nfx = mx - (float)nox, nfy = my - (float)noy;
-      const Wts nhx = half_w(ncx, nfx), nhy = half_w(ncy, nfy), nnx = node_w(ncx, nfx),
-                nny = node_w(ncy, nfy);
+      Wts nhx, nhy, nnx, nny;
+      weights2(ncx, ncy, make_float2(nfx, nfy), nhx, nhy, nnx, nny);
       // rho and jp at the new position (pic/curnt.f90:197-303)
       if (ncx == kx && ncy == ky) {
         block_add_rho(b, ncx, ncy, nnx, nny, a.qd);
