@@ -56,6 +56,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--variant", type=int, default=None,
+                    help="push variant to use instead of running the autotuner")
+    ap.add_argument("--sort-interval", type=int, default=1,
+                    help="sort interval to use with --variant")
     ap.add_argument("--only-adjoint", action="store_true",
                     help="run only the adjoint leg and print its JSON")
     # the 512x256 workload's adjoint: 800 steps, checkpoints every 50
@@ -266,10 +270,17 @@ def measure(args, cfg, precision, local, parts, fields, stream, ws):
     for s in range(2):
         g.set_particles_device(s, parts[s])
     torch.cuda.synchronize()
-    # the project's autotuner picks the push variant on this state (its
-    # steps are part of the warm-up)
+    # the project's autotuner picks the push variant and the sort interval on
+    # this state (its steps are part of the warm-up), unless they are given
     from maccpic_b200 import autotune
-    tuned = autotune.autotune(g, particles=parts[0].shape[1], use_cache=False, cache=None)
+    if args.variant is None:
+        tuned = autotune.autotune(g, particles=parts[0].shape[1], use_cache=False, cache=None)
+    else:
+        k = min(args.sort_interval, g.max_sort_interval())
+        g.set_variant(args.variant)
+        g.set_sort_interval(k)
+        tuned = {"variant": args.variant, "name": g.variant()[1], "times_ms": None,
+                 "sort_interval": k, "interval_ms": None}
     # back to the initial state, so that every measured run starts from it
     g.set_fields(fields)
     for s in range(2):
