@@ -246,6 +246,32 @@ __device__ __forceinline__ int floor_small(float f) { return f < 0.0f ? -1 : (f 
 
 __device__ __forceinline__ int wrap(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
 
+// Deposits of particles outside their lane's cell go to global memory with
+// atomics.  Done where they arise, they would run with the one or two lanes
+// that need them while the rest of the warp waits; instead each warp stacks
+// them in shared memory and does 32 at a time, one per lane.  An entry is a
+// cell, the offsets in it and the charge-weighted velocity; kind 0 deposits
+// J (jm at the old position), kind 1 rho, J (jp) and the cell count at the
+// new position.
+constexpr int kQCap = 96;  // < 32 left after a drain + at most 2 per lane
+struct DepQ {
+  int cx[kQCap], cy[kQCap];
+  float2 f[kQCap];
+  float4 q[kQCap];  // q*vx, q*vy, q*vz, kind
+};
+
+__device__ __forceinline__ void drain_entry(const Args32 &a, const DepQ &Q, int e) {
+  const int cx = Q.cx[e], cy = Q.cy[e];
+  const float4 qq = Q.q[e];
+  Wts hx, hy, nxw, nyw;
+  weights2(cx, cy, Q.f[e], hx, hy, nxw, nyw);
+  deposit_j_atomic(a, hx, hy, nxw, nyw, qq.x, qq.y, qq.z);
+  if (qq.w != 0.0f) {
+    scatter9(a.rho, a.nxg, nxw, nyw, a.qd);
+    atomicAdd(a.cnt_next + cy * a.nx + cx, 1);
+  }
+}
+
 // One row segment: cells x0 .. x0+TCX-1 of row y0, by a CTA of TCX*G
 // threads; `blk` numbers the segment for the kinetic-energy partials.
 // INPLACE: a step between regroupings -- every particle keeps its slot in
@@ -254,7 +280,7 @@ __device__ __forceinline__ int wrap(int i, int n) { return i < 0 ? i + n : (i >=
 // that they stay in (-1, 2)); the counts of the new cells are still taken.
 template <int TCX, bool INPLACE>
 __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, int64_t blk,
-                                             float2 (*win)[WY][TCX + 5]) {
+                                             float2 (*win)[WY][TCX + 5], DepQ *dq) {
   constexpr int kThreads = TCX * G;
   constexpr int WX = TCX + 5;  // window columns: x0-1 .. x0+TCX+3
   const int nx = a.nx, ny = a.ny, nxg = a.nxg;
@@ -294,6 +320,9 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
   double akel = 0.0;
   int stay_new = 0;  // particles of this lane whose new position is in cell k
   int home_count = 0;  // particles of this group written to the front of cell k
+  DepQ &Q = dq[threadIdx.x >> 5];
+  int qn = 0;  // entries on this warp's stack (the same in every lane)
+  const unsigned lt = (1u << lane) - 1u;
 
   // software pipeline: the next particle's state is loaded while this one runs
   int32_t i = beg + gl;
@@ -325,6 +354,9 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
     }
     bool in_cell_old = false;
     int key_cur = 0;
+    bool need_old = false, need_new = false;  // deposits for the warp's stack
+    int q_cx = 0, q_cy = 0, q_ncx = 0, q_ncy = 0;
+    float q_fx = 0.f, q_fy = 0.f, q_nfx = 0.f, q_nfy = 0.f, q_x = 0.f, q_y = 0.f, q_z = 0.f;
     if (active) {
       // the cell the particle is in now (it may have left cell k last step)
       const int ox = floor_small(xr), oy = floor_small(yr);
@@ -369,10 +401,18 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
       const float vx = ux * ginv, vy = uy * ginv, vz = uz * ginv;
       const float qx = a.qd * vx, qy = a.qd * vy, qz = a.qd * vz;
       // jm at the old position (pic/curnt.f90:53-132)
-      if (in_cell_old)
+      q_x = qx;
+      q_y = qy;
+      q_z = qz;
+      if (in_cell_old) {
         block_add_j(b, cx, cy, hx, hy, nxw, nyw, qx, qy, qz);
-      else
-        deposit_j_atomic(a, hx, hy, nxw, nyw, qx, qy, qz);
+      } else {
+        need_old = true;
+        q_cx = cx;
+        q_cy = cy;
+        q_fx = fx;
+        q_fy = fy;
+      }
       // move (pic/curnt.f90:181-194), relative to the start cell
       const float2 mv = fma2(make_float2(vx, vy), make_float2(a.dtdx, a.dtdy),
                              make_float2(fx, fy));
@@ -388,9 +428,11 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
         block_add_j(b, ncx, ncy, nhx, nhy, nnx, nny, qx, qy, qz);
         ++stay_new;
       } else {
-        scatter9(a.rho, nxg, nnx, nny, a.qd);
-        deposit_j_atomic(a, nhx, nhy, nnx, nny, qx, qy, qz);
-        atomicAdd(a.cnt_next + ncy * nx + ncx, 1);
+        need_new = true;
+        q_ncx = ncx;
+        q_ncy = ncy;
+        q_nfx = nfx;
+        q_nfy = nfy;
       }
       if (INPLACE) {
         a.B[i] = mx + (float)ox;
@@ -398,28 +440,58 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
         a.B[2 * cap + i] = ux;
         a.B[3 * cap + i] = uy;
         a.B[4 * cap + i] = uz;
-        continue;
+      } else {
+        // write back grouped by the cell of the start of this step: particles
+        // that started it in cell k take the next slots from the front of k's
+        // segment in processing order (a running count per group, no
+        // atomics); the few that came from another cell's range fill it from
+        // the back
+        const unsigned inm = __ballot_sync(am, in_cell_old) & gmask;
+        int64_t pos;
+        if (in_cell_old)
+          pos = (int64_t)a.offB[key_cur] + home_count + __popc(inm & lt);
+        else
+          pos = (int64_t)a.offB[key_cur + 1] - 1 - atomicAdd(a.cursor + key_cur, 1);
+        home_count += __popc(inm);
+        a.B[pos] = mx;
+        a.B[cap + pos] = my;
+        a.B[2 * cap + pos] = ux;
+        a.B[3 * cap + pos] = uy;
+        a.B[4 * cap + pos] = uz;
+        a.slotB[pos] = slot;
       }
-      // write back grouped by the cell of the start of this step: particles
-      // that started it in cell k take the next slots from the front of k's
-      // segment in processing order (a running count per group, no atomics);
-      // the few that came from another cell's range fill it from the back
-      const unsigned inm = __ballot_sync(am, in_cell_old) & gmask;
-      int64_t pos;
-      if (in_cell_old)
-        pos = (int64_t)a.offB[key_cur] + home_count + __popc(inm & ((1u << lane) - 1u));
-      else
-        pos = (int64_t)a.offB[key_cur + 1] - 1 - atomicAdd(a.cursor + key_cur, 1);
-      home_count += __popc(inm);
-      a.B[pos] = mx;
-      a.B[cap + pos] = my;
-      a.B[2 * cap + pos] = ux;
-      a.B[3 * cap + pos] = uy;
-      a.B[4 * cap + pos] = uz;
-      a.slotB[pos] = slot;
+    }
+    // this iteration's out-of-cell deposits onto the warp's stack; whole
+    // warps of them done at once
+    const unsigned m_old = __ballot_sync(0xffffffffu, need_old);
+    const unsigned m_new = __ballot_sync(0xffffffffu, need_new);
+    if (m_old | m_new) {
+      if (need_old) {
+        const int p = qn + __popc(m_old & lt);
+        Q.cx[p] = q_cx;
+        Q.cy[p] = q_cy;
+        Q.f[p] = make_float2(q_fx, q_fy);
+        Q.q[p] = make_float4(q_x, q_y, q_z, 0.0f);
+      }
+      const int qn1 = qn + __popc(m_old);
+      if (need_new) {
+        const int p = qn1 + __popc(m_new & lt);
+        Q.cx[p] = q_ncx;
+        Q.cy[p] = q_ncy;
+        Q.f[p] = make_float2(q_nfx, q_nfy);
+        Q.q[p] = make_float4(q_x, q_y, q_z, 1.0f);
+      }
+      qn = qn1 + __popc(m_new);
+      __syncwarp();
+      while (qn >= 32) {
+        qn -= 32;
+        drain_entry(a, Q, qn + lane);
+        __syncwarp();
+      }
     }
   }
 
+  if (lane < qn) drain_entry(a, Q, lane);
   // the group's new-position counts for cell k, and its register blocks
   const int stay = group_sum((float)stay_new) + 0.5f;
   if (valid && gl == 0 && stay > 0) atomicAdd(a.cnt_next + cell, stay);
@@ -468,8 +540,9 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
 template <int TCX, int MINB, bool INPLACE>
 __global__ void __launch_bounds__(TCX * G, MINB) k_push_cells_f32(Args32 a) {
   __shared__ float2 win[3][WY][TCX + 5];
+  __shared__ DepQ dq[TCX * G / 32];
   push_segment<TCX, INPLACE>(a, (int)blockIdx.x * TCX, (int)blockIdx.y,
-                             (int64_t)blockIdx.y * gridDim.x + blockIdx.x, win);
+                             (int64_t)blockIdx.y * gridDim.x + blockIdx.x, win, dq);
 }
 
 // Ensemble: every (run, species) pair of an ensemble in one persistent
@@ -480,6 +553,7 @@ __global__ void __launch_bounds__(TCX * G, MINB) k_push_cells_f32(Args32 a) {
 template <int TCX, int MINB>
 __global__ void __launch_bounds__(TCX * G, MINB) k_ens_push_f32(const __grid_constant__ EnsPush32 e) {
   __shared__ float2 win[3][WY][TCX + 5];
+  __shared__ DepQ dq[TCX * G / 32];
   __shared__ int s_tile;
   for (;;) {
     if (threadIdx.x == 0) s_tile = atomicAdd(e.counter, 1);
@@ -494,7 +568,7 @@ __global__ void __launch_bounds__(TCX * G, MINB) k_ens_push_f32(const __grid_con
     const int lt = t - e.tile0[lo];
     const int segs = e.segs[lo];
     const int row = lt / segs;
-    push_segment<TCX, false>(e.pair[lo], (lt - row * segs) * TCX, row, lt, win);
+    push_segment<TCX, false>(e.pair[lo], (lt - row * segs) * TCX, row, lt, win, dq);
   }
 }
 
