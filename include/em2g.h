@@ -120,7 +120,11 @@ int em2g_get_field(em2g_ctx *ctx, int field_id, double *host);
 /* all 13 arrays back to back in enum em2g_field order */
 int em2g_set_fields(em2g_ctx *ctx, const double *host13);
 int em2g_get_fields(em2g_ctx *ctx, double *host13);
-/* n particles of species isp (0-based), in slot order j = 0..n-1 */
+/* n particles of species isp (0-based), in slot order j = 0..n-1.  Input
+ * is checked on the device (finite values, 0 <= x < nx+0.5, 0 <= y <
+ * ny+0.5) before it replaces anything.  Host copies are staged through one
+ * FP64 device buffer, kept until em2g_destroy: the field arrays copied and,
+ * in FP32 contexts, 6 x the largest particle count copied, in doubles. */
 int em2g_set_particles(em2g_ctx *ctx, int isp, int64_t n, const double *x,
                        const double *y, const double *vx, const double *vy,
                        const double *vz, const double *gamma);

@@ -100,32 +100,68 @@ __global__ void k_f2d(const float *__restrict__ a, double *b, int64_t n) {
 bool is_fp32(const em2g_ctx *c) { return c->P.precision == EM2G_FP32; }
 
 // host FP64 arrays [first, first+count) of the field block -> device
+// The context's FP64 staging buffer on the device (particles: 6*n doubles
+// x, y, vx, vy, vz, gamma; fields: FP64 arrays), grown on demand and kept
+// until em2g_destroy so that repeated copies allocate nothing.
+int ensure_staging(em2g_ctx *c, int64_t ndoubles) {
+  if (ndoubles <= c->staging_n) return EM2G_OK;
+  EM2G_CUDA(cudaStreamSynchronize(c->stream));  // the old buffer may still be read
+  cudaFree(c->staging);
+  c->staging = nullptr;
+  c->staging_n = 0;
+  EM2G_CUDA(cudaMalloc((void **)&c->staging, sizeof(double) * ndoubles));
+  c->staging_n = ndoubles;
+  return EM2G_OK;
+}
+
+__global__ void k_count_nonfinite(const double *__restrict__ a, int64_t n,
+                                  unsigned long long *bad) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool nf = k < n && !isfinite(a[k]);
+  const unsigned m = __ballot_sync(0xffffffffu, nf);
+  if ((threadIdx.x & 31) == 0 && m) atomicAdd(bad, (unsigned long long)__popc(m));
+}
+
+// host FP64 arrays [first, first+count) of the field block -> device: copied
+// as FP64 to the device, checked there, then converted (FP32) or moved into
+// the block; non-finite input leaves the block as it was
 int put_fields_host(em2g_ctx *c, int first, int count, const double *host) {
   const int64_t n = (int64_t)count * c->g.w;
-  for (int64_t k = 0; k < n; ++k)
-    if (!std::isfinite(host[k])) return fail(EM2G_ERR_NONFINITE, "non-finite field value");
+  int rc = ensure_staging(c, n);
+  if (rc) return rc;
+  double *st = c->staging;
+  EM2G_CUDA(cudaMemcpyAsync(st, host, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+  unsigned long long *bad = (unsigned long long *)c->red;
+  EM2G_CUDA(cudaMemsetAsync(bad, 0, sizeof(unsigned long long), c->stream));
+  const unsigned nb = (unsigned)((n + 255) / 256);
+  k_count_nonfinite<<<nb, 256, 0, c->stream>>>(st, n, bad);
+  EM2G_CUDA(cudaGetLastError());
+  unsigned long long hb = 0;
+  EM2G_CUDA(cudaMemcpyAsync(&hb, bad, sizeof(hb), cudaMemcpyDeviceToHost, c->stream));
+  EM2G_CUDA(cudaStreamSynchronize(c->stream));
+  if (hb) return fail(EM2G_ERR_NONFINITE, std::to_string(hb) + " non-finite field values");
   if (is_fp32(c)) {
-    std::vector<float> tmp((size_t)n);
-    for (int64_t k = 0; k < n; ++k) tmp[k] = (float)host[k];
-    EM2G_CUDA(cudaMemcpyAsync(c->fld32 + first * c->g.w, tmp.data(), sizeof(float) * n,
-                              cudaMemcpyHostToDevice, c->stream));
-    EM2G_CUDA(cudaStreamSynchronize(c->stream));
+    k_d2f<<<nb, 256, 0, c->stream>>>(st, c->fld32 + first * c->g.w, n);
+    EM2G_CUDA(cudaGetLastError());
   } else {
-    EM2G_CUDA(cudaMemcpyAsync(c->fld + first * c->g.w, host, sizeof(double) * n,
-                              cudaMemcpyHostToDevice, c->stream));
-    EM2G_CUDA(cudaStreamSynchronize(c->stream));
+    EM2G_CUDA(cudaMemcpyAsync(c->fld + first * c->g.w, st, sizeof(double) * n,
+                              cudaMemcpyDeviceToDevice, c->stream));
   }
+  EM2G_CUDA(cudaStreamSynchronize(c->stream));
   return EM2G_OK;
 }
 
 int get_fields_host(em2g_ctx *c, int first, int count, double *host) {
   const int64_t n = (int64_t)count * c->g.w;
   if (is_fp32(c)) {
-    std::vector<float> tmp((size_t)n);
-    EM2G_CUDA(cudaMemcpyAsync(tmp.data(), c->fld32 + first * c->g.w, sizeof(float) * n,
-                              cudaMemcpyDeviceToHost, c->stream));
+    int rc = ensure_staging(c, n);
+    if (rc) return rc;
+    k_f2d<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(c->fld32 + first * c->g.w,
+                                                               c->staging, n);
+    EM2G_CUDA(cudaGetLastError());
+    EM2G_CUDA(cudaMemcpyAsync(host, c->staging, sizeof(double) * n, cudaMemcpyDeviceToHost,
+                              c->stream));
     EM2G_CUDA(cudaStreamSynchronize(c->stream));
-    for (int64_t k = 0; k < n; ++k) host[k] = (double)tmp[k];
   } else {
     EM2G_CUDA(cudaMemcpyAsync(host, c->fld + first * c->g.w, sizeof(double) * n,
                               cudaMemcpyDeviceToHost, c->stream));
@@ -133,12 +169,6 @@ int get_fields_host(em2g_ctx *c, int first, int count, double *host) {
   }
   return EM2G_OK;
 }
-
-// device staging of 6*n doubles (x, y, vx, vy, vz, gamma) for FP32 contexts
-struct Staging {
-  double *p = nullptr;
-  ~Staging() { cudaFree(p); }
-};
 
 int check_ctx(em2g_ctx *c) {
   if (!c) return fail(EM2G_ERR_INVALID, "null context");
@@ -365,6 +395,7 @@ int em2g_destroy(em2g_ctx *c) {
   }
   cudaFree(c->red);
   cudaFree(c->spec);
+  cudaFree(c->staging);
   cudaFree(c->dev_out);
   if (c->host_out) cudaFreeHost(c->host_out);
   cg_free(c);
@@ -462,50 +493,62 @@ int em2g_field_device_ptr(em2g_ctx *c, int id, void **dptr) {
   return EM2G_OK;
 }
 
+// n particles of species isp from six arrays (host or device memory, as
+// `kind` says): copied to a staging area on the device -- the FP64 reorder
+// target, or a temporary buffer for FP32 -- and checked there (positions in
+// [0, n+0.5), every value finite: em2 would read outside its arrays
+// otherwise); only input that passes replaces the species' particles.
+static int load_particles(em2g_ctx *c, int isp, int64_t n, const double *const *src,
+                          cudaMemcpyKind kind) {
+  Species &S = c->sp[isp];
+  if (n < 0 || n > S.cap) return fail(EM2G_ERR_RANGE, "particle count exceeds np_max");
+  if (n == 0) {
+    S.n = 0;
+    S.sorted = false;
+    if (is_fp32(c)) return upload_f32(c, isp, nullptr, 0);
+    return EM2G_OK;
+  }
+  for (int k = 0; k < 6; ++k)
+    if (!src[k]) return fail(EM2G_ERR_INVALID, "null particle array");
+  double *dst = S.part_alt;
+  int64_t ld = S.cap;
+  if (is_fp32(c)) {
+    const int rs = ensure_staging(c, 6 * n);
+    if (rs) return rs;
+    dst = c->staging;
+    ld = n;
+  }
+  for (int k = 0; k < 6; ++k)
+    EM2G_CUDA(cudaMemcpyAsync(dst + k * ld, src[k], sizeof(double) * n, kind, c->stream));
+  unsigned long long *bad = (unsigned long long *)c->red;  // 2 counters
+  int rc = check_particles_device(dst, n, ld, c->P.nx + 0.5, c->P.ny + 0.5, bad, c->stream);
+  if (rc) return rc;
+  unsigned long long hb[2] = {0, 0};
+  EM2G_CUDA(cudaMemcpyAsync(hb, bad, sizeof(hb), cudaMemcpyDeviceToHost, c->stream));
+  EM2G_CUDA(cudaStreamSynchronize(c->stream));
+  if (hb[1]) return fail(EM2G_ERR_NONFINITE, std::to_string(hb[1]) + " particles with non-finite values");
+  if (hb[0]) return fail(EM2G_ERR_RANGE, std::to_string(hb[0]) + " particles outside the grid");
+  if (is_fp32(c)) {
+    if ((rc = upload_f32(c, isp, dst, n))) return rc;
+  } else {
+    std::swap(S.part, S.part_alt);
+    k_iota<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(S.slot, n);
+    EM2G_CUDA(cudaGetLastError());
+    S.n = n;
+    S.sorted = false;
+  }
+  EM2G_CUDA(cudaStreamSynchronize(c->stream));
+  return EM2G_OK;
+}
+
 int em2g_set_particles(em2g_ctx *c, int isp, int64_t n, const double *x, const double *y,
                        const double *vx, const double *vy, const double *vz,
                        const double *gamma) {
   int rc = check_ctx(c);
   if (rc) return rc;
   if (isp < 0 || isp >= c->P.nsp) return fail(EM2G_ERR_INVALID, "bad species index");
-  Species &S = c->sp[isp];
-  if (n < 0 || n > S.cap) return fail(EM2G_ERR_RANGE, "particle count exceeds np_max");
-  if (n > 0 && (!x || !y || !vx || !vy || !vz || !gamma))
-    return fail(EM2G_ERR_INVALID, "null particle array");
-  // Positions must keep every stencil inside the (0:n+2) arrays: 0 <= x < n+0.5
-  const double xlim = c->P.nx + 0.5, ylim = c->P.ny + 0.5;
-  for (int64_t j = 0; j < n; ++j) {
-    if (!std::isfinite(x[j]) || !std::isfinite(y[j]) || !std::isfinite(vx[j]) ||
-        !std::isfinite(vy[j]) || !std::isfinite(vz[j]) || !std::isfinite(gamma[j]))
-      return fail(EM2G_ERR_NONFINITE, "non-finite particle value at slot " + std::to_string(j));
-    if (!(x[j] >= 0.0 && x[j] < xlim && y[j] >= 0.0 && y[j] < ylim))
-      return fail(EM2G_ERR_RANGE, "particle outside the grid at slot " + std::to_string(j));
-  }
   const double *src[6] = {x, y, vx, vy, vz, gamma};
-  if (is_fp32(c)) {
-    Staging st;
-    if (n > 0) {
-      EM2G_CUDA(cudaMalloc(&st.p, sizeof(double) * 6 * n));
-      for (int k = 0; k < 6; ++k)
-        EM2G_CUDA(cudaMemcpyAsync(st.p + k * n, src[k], sizeof(double) * n,
-                                  cudaMemcpyHostToDevice, c->stream));
-    }
-    if ((rc = upload_f32(c, isp, st.p, n))) return rc;
-    EM2G_CUDA(cudaStreamSynchronize(c->stream));
-    return EM2G_OK;
-  }
-  for (int k = 0; k < 6; ++k)
-    if (n > 0)
-      EM2G_CUDA(cudaMemcpyAsync(S.part + k * S.cap, src[k], sizeof(double) * n,
-                                cudaMemcpyHostToDevice, c->stream));
-  if (n > 0) {
-    k_iota<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(S.slot, n);
-    EM2G_CUDA(cudaGetLastError());
-  }
-  S.n = n;
-  S.sorted = false;
-  EM2G_CUDA(cudaStreamSynchronize(c->stream));
-  return EM2G_OK;
+  return load_particles(c, isp, n, src, cudaMemcpyHostToDevice);
 }
 
 int em2g_set_particles_device(em2g_ctx *c, int isp, int64_t n, const double *x,
@@ -514,50 +557,8 @@ int em2g_set_particles_device(em2g_ctx *c, int isp, int64_t n, const double *x,
   int rc = check_ctx(c);
   if (rc) return rc;
   if (isp < 0 || isp >= c->P.nsp) return fail(EM2G_ERR_INVALID, "bad species index");
-  Species &S = c->sp[isp];
-  if (n < 0 || n > S.cap) return fail(EM2G_ERR_RANGE, "particle count exceeds np_max");
-  if (n == 0) {
-    S.n = 0;
-    return EM2G_OK;
-  }
-  if (!x || !y || !vx || !vy || !vz || !gamma) return fail(EM2G_ERR_INVALID, "null particle array");
   const double *src[6] = {x, y, vx, vy, vz, gamma};
-  Staging st;
-  double *dst = S.part;
-  int64_t ld = S.cap;
-  if (is_fp32(c)) {
-    EM2G_CUDA(cudaMalloc(&st.p, sizeof(double) * 6 * n));
-    dst = st.p;
-    ld = n;
-  }
-  for (int k = 0; k < 6; ++k)
-    EM2G_CUDA(cudaMemcpyAsync(dst + k * ld, src[k], sizeof(double) * n,
-                              cudaMemcpyDeviceToDevice, c->stream));
-  unsigned long long *bad = (unsigned long long *)c->red;  // 2 counters
-  EM2G_CUDA(cudaMemsetAsync(bad, 0, 2 * sizeof(unsigned long long), c->stream));
-  const unsigned nb = (unsigned)((n + 255) / 256);
-  k_check_particles<<<nb, 256, 0, c->stream>>>(dst, n, ld, c->P.nx + 0.5, c->P.ny + 0.5, bad);
-  if (!is_fp32(c)) k_iota<<<nb, 256, 0, c->stream>>>(S.slot, n);
-  EM2G_CUDA(cudaGetLastError());
-  unsigned long long hb[2] = {0, 0};
-  EM2G_CUDA(cudaMemcpyAsync(hb, bad, sizeof(hb), cudaMemcpyDeviceToHost, c->stream));
-  EM2G_CUDA(cudaStreamSynchronize(c->stream));
-  if (hb[1]) {
-    S.n = 0;
-    return fail(EM2G_ERR_NONFINITE, std::to_string(hb[1]) + " particles with non-finite values");
-  }
-  if (hb[0]) {
-    S.n = 0;
-    return fail(EM2G_ERR_RANGE, std::to_string(hb[0]) + " particles outside the grid");
-  }
-  if (is_fp32(c)) {
-    if ((rc = upload_f32(c, isp, st.p, n))) return rc;
-    EM2G_CUDA(cudaStreamSynchronize(c->stream));
-    return EM2G_OK;
-  }
-  S.n = n;
-  S.sorted = false;
-  return EM2G_OK;
+  return load_particles(c, isp, n, src, cudaMemcpyDeviceToDevice);
 }
 
 int em2g_get_particles(em2g_ctx *c, int isp, int64_t *n, double *x, double *y, double *vx,
@@ -571,12 +572,11 @@ int em2g_get_particles(em2g_ctx *c, int isp, int64_t *n, double *x, double *y, d
   if (!x && !y && !vx && !vy && !vz && !gamma) return EM2G_OK;  // count query
   if (!x || !y || !vx || !vy || !vz || !gamma) return fail(EM2G_ERR_INVALID, "null particle array");
   if (is_fp32(c)) {
-    Staging st;
-    EM2G_CUDA(cudaMalloc(&st.p, sizeof(double) * 6 * S.n));
-    if ((rc = download_f32(c, isp, st.p))) return rc;
+    if ((rc = ensure_staging(c, 6 * S.n))) return rc;
+    if ((rc = download_f32(c, isp, c->staging))) return rc;
     double *dst[6] = {x, y, vx, vy, vz, gamma};
     for (int k = 0; k < 6; ++k)
-      EM2G_CUDA(cudaMemcpyAsync(dst[k], st.p + k * S.n, sizeof(double) * S.n,
+      EM2G_CUDA(cudaMemcpyAsync(dst[k], c->staging + k * S.n, sizeof(double) * S.n,
                                 cudaMemcpyDeviceToHost, c->stream));
     EM2G_CUDA(cudaStreamSynchronize(c->stream));
     return EM2G_OK;

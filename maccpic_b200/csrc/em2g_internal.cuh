@@ -105,6 +105,8 @@ struct em2g_ctx {
   // the fast path deposits the whole current into jxm, jym, jzm)
   bool jp_live = true;
   double2 *spec = nullptr;  // nx*ny complex work of the spectral Poisson solve
+  double *staging = nullptr;  // FP64 staging of host copies (grown on demand)
+  int64_t staging_n = 0;
   int64_t ncell = 0;
   int timing = 0;
   std::vector<cudaEvent_t> ev;  // start/stop pairs of the pending push launches

@@ -384,3 +384,27 @@ def test_species_moments_after_100_steps(gpu, oracle_lib):
             m_ref = species_moments(st.parts[s], op.nx, op.ny, rp.am[s])
             for k in range(5):
                 assert rel(m_gpu[k], m_ref[k]) < 1e-10, (s, k)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_invalid_fields_leave_the_state(gpu, precision):
+    """Field uploads are checked on the device before they replace anything:
+    a non-finite value is refused and the fields stay as they were."""
+    from maccpic_b200 import _lib
+    from maccpic_b200._lib import Em2gError, ERR_NONFINITE
+    import dataclasses
+    op, rp, fld, parts = random_case(n=100)
+    rp = dataclasses.replace(rp, precision=_lib.FP32 if precision == "fp32" else _lib.FP64)
+    with make_gpu(rp, fld, parts) as g:
+        before = g.get_fields()
+        bad = fld.copy()
+        bad[4, 3, 5] = np.inf
+        with pytest.raises(Em2gError) as ei:
+            g.set_fields(bad)
+        assert ei.value.status == ERR_NONFINITE
+        np.testing.assert_array_equal(g.get_fields(), before)
+        bad = parts[1].copy()
+        bad[2, 9] = np.nan
+        with pytest.raises(Em2gError):
+            g.set_particles(1, bad)
+        g.step(1)
