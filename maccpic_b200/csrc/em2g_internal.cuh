@@ -152,12 +152,10 @@ int timing_begin(em2g_ctx *c);
 int timing_end(em2g_ctx *c);
 void cg_free(em2g_ctx *c);
 // kinetic-energy partials one fast push of an nx x ny grid writes, for the
-// widest-writing variant: ceil(nx/tcx) * ny segments of tcx*4/32 warps, tcx
-// 32 or 64
-inline int64_t push_partials(int nx, int ny) {
-  const int64_t a = (int64_t)((nx + 31) / 32) * 4, b = (int64_t)((nx + 63) / 64) * 8;
-  return (a > b ? a : b) * ny;
-}
+// widest-writing variant: ceil(nx/tcx) * ny segments of tcx*g/32 warps, with
+// tcx 32 or 64 cells and g <= 8 lanes per cell -- at most 8 warps per 32
+// cells
+inline int64_t push_partials(int nx, int ny) { return (int64_t)((nx + 31) / 32) * 8 * ny; }
 // exact periodic Poisson solve by FFT (spectral.cu)
 bool spectral_size_ok(int nx, int ny);
 int spectral_prepare();

@@ -42,7 +42,7 @@
 namespace em2g {
 namespace {
 
-constexpr int G = 4;   // lanes per cell
+constexpr int kCopyLanes = 4;  // lanes per cell of the download gather
 constexpr int WY = 6;  // window rows: y0-1 .. y0+4
 
 struct Args32 {
@@ -231,12 +231,16 @@ __device__ __forceinline__ void deposit_j_atomic(const Args32 &a, const Wts &hx,
   scatter9(a.jy, a.nxg, nxw, hy, qy);
 }
 
+// sum over the G lanes of a cell's group (G a power of two)
+template <int G>
 __device__ __forceinline__ float group_sum(float v) {
-  v += __shfl_xor_sync(0xffffffffu, v, 1);
-  v += __shfl_xor_sync(0xffffffffu, v, 2);
+#pragma unroll
+  for (int o = 1; o < G; o <<= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
 
+// element e of a group's block goes to the array from lane e mod G
+template <int G>
 __device__ __forceinline__ void flush_one(float *A, int nxg, int ix, int iy, float v, int e,
                                           int gl) {
   if ((e & (G - 1)) == gl && v != 0.0f) atomicAdd(A + (int64_t)iy * nxg + ix, v);
@@ -278,7 +282,7 @@ __device__ __forceinline__ void drain_entry(const Args32 &a, const DepQ &Q, int 
 // A (B == A) and its position stays relative to its group cell, so the
 // offsets drift by at most c*dt/dx per step (the interval is bounded so
 // that they stay in (-1, 2)); the counts of the new cells are still taken.
-template <int TCX, bool INPLACE>
+template <int TCX, int G, bool INPLACE>
 __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, int64_t blk,
                                              float2 (*win)[WY][TCX + 5], DepQ *dq) {
   constexpr int kThreads = TCX * G;
@@ -304,7 +308,7 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
   const int32_t beg = valid ? a.offA[cell] : 0;
   const int32_t end = valid ? a.offA[cell + 1] : 0;
   const int64_t cap = a.cap;
-  const unsigned gmask = 0xFu << (lane & ~(G - 1));  // this lane's group in the warp
+  const unsigned gmask = ((1u << G) - 1u) << (lane & ~(G - 1));  // this lane's group
 
   Block32 b;
   const float2 z2 = make_float2(0.0f, 0.0f);
@@ -493,7 +497,7 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
 
   if (lane < qn) drain_entry(a, Q, lane);
   // the group's new-position counts for cell k, and its register blocks
-  const int stay = group_sum((float)stay_new) + 0.5f;
+  const int stay = group_sum<G>((float)stay_new) + 0.5f;
   if (valid && gl == 0 && stay > 0) atomicAdd(a.cnt_next + cell, stay);
   if (__any_sync(0xffffffffu, valid && end > beg)) {
     int e = 0;
@@ -501,32 +505,32 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
     for (int r = 0; r < 4; ++r)
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
-        const float v = group_sum(pick4(b.rho01[r], b.rho23[r], k));
-        if (valid) flush_one(a.rho, nxg, kx + k, ky + r, v, e, gl);
+        const float v = group_sum<G>(pick4(b.rho01[r], b.rho23[r], k));
+        if (valid) flush_one<G>(a.rho, nxg, kx + k, ky + r, v, e, gl);
         ++e;
       }
 #pragma unroll
     for (int r = 0; r < 4; ++r)
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
-        const float v = group_sum(pick3(b.jx01[r], b.jx2[r], k));
-        if (valid) flush_one(a.jx, nxg, kx + k, ky + r, v, e, gl);
+        const float v = group_sum<G>(pick3(b.jx01[r], b.jx2[r], k));
+        if (valid) flush_one<G>(a.jx, nxg, kx + k, ky + r, v, e, gl);
         ++e;
       }
 #pragma unroll
     for (int r = 0; r < 3; ++r)
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
-        const float v = group_sum(pick4(b.jy01[r], b.jy23[r], k));
-        if (valid) flush_one(a.jy, nxg, kx + k, ky + r, v, e, gl);
+        const float v = group_sum<G>(pick4(b.jy01[r], b.jy23[r], k));
+        if (valid) flush_one<G>(a.jy, nxg, kx + k, ky + r, v, e, gl);
         ++e;
       }
 #pragma unroll
     for (int r = 0; r < 3; ++r)
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
-        const float v = group_sum(pick3(b.jz01[r], b.jz2[r], k));
-        if (valid) flush_one(a.jz, nxg, kx + k, ky + r, v, e, gl);
+        const float v = group_sum<G>(pick3(b.jz01[r], b.jz2[r], k));
+        if (valid) flush_one<G>(a.jz, nxg, kx + k, ky + r, v, e, gl);
         ++e;
       }
   }
@@ -535,13 +539,14 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
   if (lane == 0) a.ake_partial[blk * (kThreads / 32) + (threadIdx.x >> 5)] = akel;
 }
 
-// TCX cells per CTA (a row segment), MINB: CTAs per SM the register
-// allocation must allow (the autotuner's two knobs)
-template <int TCX, int MINB, bool INPLACE>
+// TCX cells per CTA (a row segment), G lanes per cell (the particles a CTA
+// has in flight: TCX*G), MINB: CTAs per SM the register allocation must
+// allow -- the autotuner's knobs besides the sort interval
+template <int TCX, int G, int MINB, bool INPLACE>
 __global__ void __launch_bounds__(TCX * G, MINB) k_push_cells_f32(Args32 a) {
   __shared__ float2 win[3][WY][TCX + 5];
   __shared__ DepQ dq[TCX * G / 32];
-  push_segment<TCX, INPLACE>(a, (int)blockIdx.x * TCX, (int)blockIdx.y,
+  push_segment<TCX, G, INPLACE>(a, (int)blockIdx.x * TCX, (int)blockIdx.y,
                              (int64_t)blockIdx.y * gridDim.x + blockIdx.x, win, dq);
 }
 
@@ -550,8 +555,9 @@ __global__ void __launch_bounds__(TCX * G, MINB) k_push_cells_f32(Args32 a) {
 // (tile0[p] .. tile0[p+1]-1 for pair p, row-major within the pair); each
 // CTA takes the next unclaimed segment from a counter until none is left,
 // so runs of unequal size and density share the SMs without a tail per run.
-template <int TCX, int MINB>
-__global__ void __launch_bounds__(TCX * G, MINB) k_ens_push_f32(const __grid_constant__ EnsPush32 e) {
+template <int TCX, int G, int MINB>
+__global__ void __launch_bounds__(TCX * G, MINB)
+    k_ens_push_f32(const __grid_constant__ EnsPush32 e) {
   __shared__ float2 win[3][WY][TCX + 5];
   __shared__ DepQ dq[TCX * G / 32];
   __shared__ int s_tile;
@@ -568,23 +574,24 @@ __global__ void __launch_bounds__(TCX * G, MINB) k_ens_push_f32(const __grid_con
     const int lt = t - e.tile0[lo];
     const int segs = e.segs[lo];
     const int row = lt / segs;
-    push_segment<TCX, false>(e.pair[lo], (lt - row * segs) * TCX, row, lt, win, dq);
+    push_segment<TCX, G, false>(e.pair[lo], (lt - row * segs) * TCX, row, lt, win, dq);
   }
 }
 
 struct Variant32 {
   const char *name;
-  int tcx;
+  int tcx, g;
   void (*kernel)(Args32);
   void (*kernel_inplace)(Args32);
   void (*ens_kernel)(const EnsPush32);
 };
-#define EM2G_VARIANT32(T, M)                                                          \
-  {"f32 tcx" #T " minb" #M, T, k_push_cells_f32<T, M, false>, k_push_cells_f32<T, M, true>, \
-   k_ens_push_f32<T, M>}
+#define EM2G_VARIANT32(T, GG, M)                                                         \
+  {"f32 tcx" #T " g" #GG " minb" #M, T, GG, k_push_cells_f32<T, GG, M, false>,          \
+   k_push_cells_f32<T, GG, M, true>, k_ens_push_f32<T, GG, M>}
 const Variant32 kVariants32[] = {
-    EM2G_VARIANT32(32, 4), EM2G_VARIANT32(32, 5), EM2G_VARIANT32(32, 6),
-    EM2G_VARIANT32(64, 2), EM2G_VARIANT32(64, 3),
+    EM2G_VARIANT32(32, 4, 4), EM2G_VARIANT32(32, 4, 5), EM2G_VARIANT32(32, 4, 6),
+    EM2G_VARIANT32(64, 4, 2), EM2G_VARIANT32(64, 4, 3), EM2G_VARIANT32(32, 8, 2),
+    EM2G_VARIANT32(32, 2, 8), EM2G_VARIANT32(64, 2, 4),
 };
 #undef EM2G_VARIANT32
 
@@ -658,11 +665,11 @@ __global__ void k_scatter_to_f32(const double *__restrict__ st, int64_t n, int n
 __global__ void k_gather_from_f32(const float *__restrict__ P, const int32_t *__restrict__ slot,
                                   const int32_t *__restrict__ off, int64_t cap, int nx, int ny,
                                   double *st, int64_t n) {
-  const int64_t cell = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / G;
-  const int gl = threadIdx.x & (G - 1);
+  const int64_t cell = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kCopyLanes;
+  const int gl = threadIdx.x & (kCopyLanes - 1);
   if (cell >= (int64_t)nx * ny) return;
   const int kx = (int)(cell % nx), ky = (int)(cell / nx);
-  for (int32_t i = off[cell] + gl; i < off[cell + 1]; i += G) {
+  for (int32_t i = off[cell] + gl; i < off[cell + 1]; i += kCopyLanes) {
     double x = kx + (double)P[i], y = ky + (double)P[cap + i];
     if (x < 0.0) x += nx;
     if (x >= nx) x -= nx;
@@ -726,7 +733,7 @@ int launch_push_cells_f32(em2g_ctx *c, int isp) {
   a.c = (float)c->P.c;
   a.ake_partial = c->red;
   const Variant32 &V = kVariants32[c->variant < num_variants_f32() ? c->variant : 0];
-  const int threads = V.tcx * G;
+  const int threads = V.tcx * V.g;
   const dim3 grid((unsigned)((c->g.nx + V.tcx - 1) / V.tcx), (unsigned)c->g.ny);
   const int64_t nparts = (int64_t)grid.x * grid.y * (threads / 32);
   if (nparts > c->red_blocks) return fail(EM2G_ERR_RANGE, "grid exceeds reduction scratch");
@@ -786,7 +793,7 @@ int upload_f32(em2g_ctx *c, int isp, const double *staging, int64_t n) {
 int download_f32(em2g_ctx *c, int isp, double *staging) {
   Species &S = c->sp[isp];
   if (S.n == 0) return EM2G_OK;
-  const int64_t nb = (c->ncell * G + 255) / 256;
+  const int64_t nb = (c->ncell * kCopyLanes + 255) / 256;
   k_gather_from_f32<<<(unsigned)nb, 256, 0, c->stream>>>(S.p32, S.slot, S.off, S.cap, c->g.nx,
                                                          c->g.ny, staging, S.n);
   c->launches += 1;
@@ -805,7 +812,7 @@ int ens_push(em2g_ens *e, int parity) {
   int32_t *offA = parity ? e->off_alt : e->off, *offB = parity ? e->off : e->off_alt;
   int32_t *cntA = parity ? e->cnt_alt : e->cnt, *cntB = parity ? e->cnt : e->cnt_alt;
   const Variant32 &V = kVariants32[e->variant < num_variants_f32() ? e->variant : 0];
-  const int threads = V.tcx * G;
+  const int threads = V.tcx * V.g;
   cudaStream_t st = e->stream;
   int rc = scan_counts(cntA, offB, e->ncell, 0, e->scan_tmp, st);
   if (rc) return rc;
@@ -901,7 +908,7 @@ int ens_download_pair(em2g_ens *e, int r, int s, double *staging) {
   const float *P = e->parity ? e->p32_alt : e->p32;
   const int32_t *slot = e->parity ? e->slot_alt : e->slot;
   const int32_t *off = e->parity ? e->off_alt : e->off;
-  const int64_t nb = ((int64_t)R.g.nx * R.g.ny * G + 255) / 256;
+  const int64_t nb = ((int64_t)R.g.nx * R.g.ny * kCopyLanes + 255) / 256;
   k_gather_from_f32<<<(unsigned)nb, 256, 0, e->stream>>>(P, slot, off + R.cell0[s], e->cap, R.g.nx,
                                                           R.g.ny, staging, n);
   EM2G_CUDA(cudaGetLastError());
