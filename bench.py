@@ -490,9 +490,11 @@ def run_ensemble(args, local):
     as one ensemble: one graph launch per step."""
     import torch
     from maccpic_b200.ensemble import harris_ensemble, load_harris
+    from maccpic_b200.autotune import autotune_ensemble
     cfgs = harris_ensemble(64, seed=0)
     ens = load_harris(cfgs, device=f"cuda:{local}")
     try:
+        tuned = autotune_ensemble(ens)  # the project's autotuner, on this batch
         ens.step(args.warmup)
         start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
@@ -508,7 +510,8 @@ def run_ensemble(args, local):
                 "value": n * args.steps / (ms / 1e3), "unit": METRIC,
                 "ms_per_step": ms / args.steps, "graph": True,
                 "kernels_per_step": cnt["kernels_per_step"],
-                "cg_iters_max": int(out["cg_iters"].max())}
+                "cg_iters_max": int(out["cg_iters"].max()),
+                "push_variant": tuned["variant"], "variant_step_ms": tuned["times_ms"]}
     finally:
         ens.close()
         torch.cuda.empty_cache()

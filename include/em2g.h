@@ -288,7 +288,8 @@ int em2g_ens_num_runs(em2g_ens *ens, int *nruns);
 int em2g_ens_set_stream(em2g_ens *ens, void *cuda_stream);
 /* 1 (default): replay a captured graph per step; 0: launch the kernels */
 int em2g_ens_set_graph(em2g_ens *ens, int on);
-/* one of the em2g_num_variants FP32 push variants */
+/* the FP32 push variants (as em2g_num_variants of an FP32 context) */
+int em2g_ens_num_variants(em2g_ens *ens, int *n);
 int em2g_ens_set_variant(em2g_ens *ens, int variant);
 /* one run's 13 arrays, as em2g_set_fields / em2g_get_fields */
 int em2g_ens_set_fields(em2g_ens *ens, int run, const double *host13);

@@ -90,3 +90,24 @@ def autotune(run, particles: int, steps: int = 2, warm: int = 1, cache: str | No
         except OSError:
             pass
     return {**result, "from_cache": False}
+
+
+def autotune_ensemble(ens, steps: int = 2, warm: int = 1) -> dict:
+    """Time every push variant on an ensemble (its current state, a few
+    graph-launched steps each; every step advances the runs) and keep the
+    fastest.  Returns {"variant", "name", "times_ms"}: mean wall time of a
+    step per variant."""
+    import time
+    import torch
+    times = []
+    for v in range(ens.num_variants()):
+        ens.set_variant(v)
+        ens.step(warm)
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        ens.step(steps)
+        torch.cuda.synchronize()
+        times.append((time.perf_counter() - t) * 1e3 / steps)
+    best = min(range(len(times)), key=lambda v: times[v])
+    ens.set_variant(best)
+    return {"variant": best, "times_ms": times}

@@ -254,6 +254,14 @@ int em2g_ens_set_graph(em2g_ens *e, int on) {
   return EM2G_OK;
 }
 
+int em2g_ens_num_variants(em2g_ens *e, int *n) {
+  int rc = check_ens(e);
+  if (rc) return rc;
+  if (!n) return fail(EM2G_ERR_INVALID, "null pointer");
+  *n = num_variants_f32();
+  return EM2G_OK;
+}
+
 int em2g_ens_set_variant(em2g_ens *e, int v) {
   int rc = check_ens(e);
   if (rc) return rc;

@@ -121,6 +121,11 @@ class Em2Ensemble:
     def set_graph(self, on: bool) -> None:
         check(self._L.em2g_ens_set_graph(self._h, 1 if on else 0))
 
+    def num_variants(self) -> int:
+        n = C.c_int()
+        check(self._L.em2g_ens_num_variants(self._h, C.byref(n)))
+        return n.value
+
     def set_variant(self, v: int) -> None:
         check(self._L.em2g_ens_set_variant(self._h, int(v)))
 
