@@ -20,19 +20,24 @@
 //                                      s- = (1/2-h)^2/2
 // and the relativistic Boris rotation on u.
 //
-// Work layout.  A CTA of 128 threads owns a row segment of 32 cells; 4 lanes
-// own one cell and walk its particles 4 at a time.  The scaled fields the
-// segment's particles can touch (x nodes x0-1 .. x0+35, y nodes y0-1 ..
+// Work layout.  A CTA owns a row segment of TCX cells (32 or 64); G lanes
+// (2, 4 or 8) own one cell and walk its particles G at a time, the next
+// particle's state loaded while the current one runs.  The scaled fields the
+// segment's particles can touch (x nodes x0-1 .. x0+TCX+3, y nodes y0-1 ..
 // y0+4) are staged once in shared memory as (E, B) pairs of the three
 // staggerings, so a gather is 27 shared float2 loads.  A particle still in
 // the lane's cell adds its rho and J into a 49-value register block (Jx 4x3,
-// Jy 3x4, Jz 3x3, rho 4x4); one that left it deposits with atomics.  At the
-// end of the cell the four blocks are summed with two shuffle levels and added
-// to the arrays once.  Each particle is written to the other buffer grouped
-// by the cell it started the step in, its position relative to that cell
-// (front slots by a running count for the common in-cell case, back slots by
-// an atomic for the rest), and the cells of the new positions are counted
-// for the next step's offsets: the counting sort rides along with the push.
+// Jy 3x4, Jz 3x3, rho 4x4); the deposits of one outside it go onto its
+// warp's stack in shared memory and are done with atomics 32 at a time, one
+// per lane.  At the end of the cell the G blocks are summed with shuffles and
+// added to the arrays once.  The gathers, the block updates, the weights and
+// the move use sm_100a's packed FP32 pairs (f32x2).  Each particle is written
+// to the other buffer grouped by the cell it started the step in, its
+// position relative to that cell (front slots by a running count for the
+// common in-cell case, back slots by an atomic for the rest), and the cells
+// of the new positions are counted for the next step's offsets: the counting
+// sort rides along with the push.  Between regroupings (the sort interval)
+// the push updates particles in place instead.
 #include <algorithm>
 #include <memory>
 
