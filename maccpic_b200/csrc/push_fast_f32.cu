@@ -281,6 +281,111 @@ __device__ __forceinline__ void drain_entry(const Args32 &a, const DepQ &Q, int 
   }
 }
 
+// What one particle's push leaves for the write-back and the warp's stack.
+struct PartOut {
+  float mx, my, ux, uy, uz;  // new position relative to the start cell, new u
+  int ox, oy;                // start cell - group cell (-1, 0 or 1 each)
+  int key_cur;               // start cell's key
+  bool in_cell_old;          // the start cell is the group cell
+  bool need_old, need_new;   // deposits for the warp's stack
+  int cx, cy, ncx, ncy;
+  float fx, fy, nfx, nfy, qx, qy, qz;
+};
+
+// Gather, Boris, move and the in-cell deposits of one particle at (xr, yr)
+// relative to the group cell (kx, ky) with momentum u; `act` false makes it
+// a dry run on harmless input (no deposits, no energy).  cinv = 1/c.
+template <int TCX>
+__device__ __forceinline__ void push_one(const Args32 &a, float2 (*win)[WY][TCX + 5], int x0,
+                                         int y0, int kx, int ky, bool act, float xr, float yr,
+                                         float ux, float uy, float uz, float cinv, Block32 &b,
+                                         double &akel, int &stay_new, PartOut &o) {
+  constexpr int WX = TCX + 5;
+  const int nx = a.nx, ny = a.ny, nxg = a.nxg;
+  // the cell the particle is in now (it may have left cell k last step)
+  const int ox = floor_small(xr), oy = floor_small(yr);
+  const int cxu = kx + ox, cyu = ky + oy;  // unwrapped
+  const int cx = wrap(cxu, nx), cy = wrap(cyu, ny);
+  const float fx = xr - (float)ox, fy = yr - (float)oy;
+  o.ox = ox;
+  o.oy = oy;
+  o.key_cur = cy * nx + cx;
+  o.in_cell_old = (ox == 0) && (oy == 0);
+  Wts hx, hy, nxw, nyw;
+  weights2(cx, cy, make_float2(fx, fy), hx, hy, nxw, nyw);
+  // gather from the shared window when the stencil is inside it (always,
+  // unless the particle wrapped around the box); else from global memory
+  float2 ebx, ebz, eby;
+  if (cxu == cx && cyu == cy && cx >= x0 - 1 && cx <= x0 + TCX && cy >= y0 - 1 &&
+      cy <= y0 + 1) {
+    const int c0 = cx - x0 + 1, r0 = cy - y0 + 1;  // window index of node (cx, cy)
+    ebx = gather_pair(&win[0][r0 + nyw.i - cy - 1][c0 + hx.i - cx - 1], WX, hx, nyw);
+    ebz = gather_pair(&win[1][r0 + hy.i - cy - 1][c0 + hx.i - cx - 1], WX, hx, hy);
+    eby = gather_pair(&win[2][r0 + hy.i - cy - 1][c0 + nxw.i - cx - 1], WX, nxw, hy);
+  } else {
+    ebx = gather_pair(a.ebx + (int64_t)(nyw.i - 1) * nxg + hx.i - 1, nxg, hx, nyw);
+    ebz = gather_pair(a.ebz + (int64_t)(hy.i - 1) * nxg + hx.i - 1, nxg, hx, hy);
+    eby = gather_pair(a.eby + (int64_t)(hy.i - 1) * nxg + nxw.i - 1, nxg, nxw, hy);
+  }
+  // relativistic Boris on u (pic/move.f90:176-203).  The reciprocal square
+  // roots and divisions are the hardware approximations (rsqrtf, a few ulp),
+  // well inside this path's FP32 error; gamma - 1 is taken as
+  // g^2 (1/gamma) / (1 + 1/gamma), free of the cancellation of gamma - 1.
+  const float gx = ux + ebx.x, gy = uy + eby.x, gz = uz + ebz.x;
+  const float g2 = gx * gx + gy * gy + gz * gz;
+  const float rg = rsqrtf(1.0f + g2);  // 1 / gamma
+  if (act) akel += (double)__fdividef(g2 * rg, 1.0f + rg);
+  const float dcg = rg * cinv;
+  float tx = dcg * ebx.y, ty = dcg * eby.y, tz = dcg * ebz.y;
+  const float vvx = gx + gy * tz - gz * ty;
+  const float vvy = gy + gz * tx - gx * tz;
+  const float vvz = gz + gx * ty - gy * tx;
+  const float f2 = __fdividef(2.0f, 1.0f + tx * tx + ty * ty + tz * tz);
+  tx *= f2;
+  ty *= f2;
+  tz *= f2;
+  ux = gx + vvy * tz - vvz * ty + ebx.x;
+  uy = gy + vvz * tx - vvx * tz + eby.x;
+  uz = gz + vvx * ty - vvy * tx + ebz.x;
+  const float ginv = rsqrtf(1.0f + ux * ux + uy * uy + uz * uz);
+  const float vx = ux * ginv, vy = uy * ginv, vz = uz * ginv;
+  const float qx = a.qd * vx, qy = a.qd * vy, qz = a.qd * vz;
+  o.qx = qx;
+  o.qy = qy;
+  o.qz = qz;
+  o.ux = ux;
+  o.uy = uy;
+  o.uz = uz;
+  // jm at the old position (pic/curnt.f90:53-132)
+  o.need_old = act && !o.in_cell_old;
+  o.cx = cx;
+  o.cy = cy;
+  o.fx = fx;
+  o.fy = fy;
+  if (act && o.in_cell_old) block_add_j(b, cx, cy, hx, hy, nxw, nyw, qx, qy, qz);
+  // move (pic/curnt.f90:181-194), relative to the start cell
+  const float2 mv = fma2(make_float2(vx, vy), make_float2(a.dtdx, a.dtdy), make_float2(fx, fy));
+  o.mx = mv.x;
+  o.my = mv.y;
+  const int nox = floor_small(mv.x), noy = floor_small(mv.y);
+  const int ncx = wrap(cx + nox, nx), ncy = wrap(cy + noy, ny);
+  const float nfx = mv.x - (float)nox, nfy = mv.y - (float)noy;
+  // rho and jp at the new position (pic/curnt.f90:197-303)
+  const bool stays = ncx == kx && ncy == ky;
+  o.need_new = act && !stays;
+  o.ncx = ncx;
+  o.ncy = ncy;
+  o.nfx = nfx;
+  o.nfy = nfy;
+  if (act && stays) {
+    Wts nhx, nhy, nnx, nny;
+    weights2(ncx, ncy, make_float2(nfx, nfy), nhx, nhy, nnx, nny);
+    block_add_rho(b, ncx, ncy, nnx, nny, a.qd);
+    block_add_j(b, ncx, ncy, nhx, nhy, nnx, nny, qx, qy, qz);
+    ++stay_new;
+  }
+}
+
 // One row segment: cells x0 .. x0+TCX-1 of row y0, by a CTA of TCX*G
 // threads; `blk` numbers the segment for the kinetic-energy partials.
 // INPLACE: a step between regroupings -- every particle keeps its slot in
@@ -309,6 +414,7 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
   const int lane = threadIdx.x & 31, gl = lane & (G - 1);
   const int kx = x0 + (int)(threadIdx.x / G), ky = y0;
   const bool valid = kx < nx;
+  const int kxs = valid ? kx : nx - 1;  // the cell lanes past the grid's edge work on
   const int64_t cell = (int64_t)ky * nx + kx;
   const int32_t beg = valid ? a.offA[cell] : 0;
   const int32_t end = valid ? a.offA[cell + 1] : 0;
@@ -326,7 +432,8 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
       b.jz2[r] = 0.0f;
     }
   }
-  double akel = 0.0;
+  double akel = 0.0;  // this lane's sum of gamma - 1
+  const float cinv = 1.0f / a.c;
   int stay_new = 0;  // particles of this lane whose new position is in cell k
   int home_count = 0;  // particles of this group written to the front of cell k
   DepQ &Q = dq[threadIdx.x >> 5];
@@ -334,161 +441,83 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
   const unsigned lt = (1u << lane) - 1u;
 
   // software pipeline: the next particle's state is loaded while this one runs
-  int32_t i = beg + gl;
   float pxr = 0.f, pyr = 0.f, pux = 0.f, puy = 0.f, puz = 0.f;
   int32_t pslot = 0;
-  if (i < end) {
-    pxr = a.A[i];
-    pyr = a.A[cap + i];
-    pux = a.A[2 * cap + i];
-    puy = a.A[3 * cap + i];
-    puz = a.A[4 * cap + i];
-    pslot = a.slotA[i];
+  if (beg + gl < end) {
+    const int32_t j = beg + gl;
+    pxr = a.A[j];
+    pyr = a.A[cap + j];
+    pux = a.A[2 * cap + j];
+    puy = a.A[3 * cap + j];
+    puz = a.A[4 * cap + j];
+    pslot = a.slotA[j];
   }
-  for (;; i += G) {
-    const bool active = i < end;
-    const unsigned am = __ballot_sync(0xffffffffu, active);
-    if (am == 0u) break;
-    const float xr = pxr, yr = pyr;
-    float ux = pux, uy = puy, uz = puz;
-    const int32_t slot = pslot;
-    const int32_t inext = i + G;
-    if (inext < end) {
-      pxr = a.A[inext];
-      pyr = a.A[cap + inext];
-      pux = a.A[2 * cap + inext];
-      puy = a.A[3 * cap + inext];
-      puz = a.A[4 * cap + inext];
-      pslot = a.slotA[inext];
+  for (int32_t i = beg + gl;; i += G) {
+    const bool act = i < end;
+    if (__ballot_sync(0xffffffffu, act) == 0u) break;
+    const float cxr = pxr, cyr = pyr, cux = pux, cuy = puy, cuz = puz;
+    const int32_t cslot = pslot;
+    const int32_t j = i + G;
+    if (j < end) {
+      pxr = a.A[j];
+      pyr = a.A[cap + j];
+      pux = a.A[2 * cap + j];
+      puy = a.A[3 * cap + j];
+      puz = a.A[4 * cap + j];
+      pslot = a.slotA[j];
     }
-    bool in_cell_old = false;
-    int key_cur = 0;
-    bool need_old = false, need_new = false;  // deposits for the warp's stack
-    int q_cx = 0, q_cy = 0, q_ncx = 0, q_ncy = 0;
-    float q_fx = 0.f, q_fy = 0.f, q_nfx = 0.f, q_nfy = 0.f, q_x = 0.f, q_y = 0.f, q_z = 0.f;
-    if (active) {
-      // the cell the particle is in now (it may have left cell k last step)
-      const int ox = floor_small(xr), oy = floor_small(yr);
-      const int cxu = kx + ox, cyu = ky + oy;  // unwrapped
-      const int cx = wrap(cxu, nx), cy = wrap(cyu, ny);
-      const float fx = xr - (float)ox, fy = yr - (float)oy;
-      key_cur = cy * nx + cx;
-      in_cell_old = (ox == 0) && (oy == 0);
-      Wts hx, hy, nxw, nyw;
-      weights2(cx, cy, make_float2(fx, fy), hx, hy, nxw, nyw);
-      // gather from the shared window when the stencil is inside it (always,
-      // unless the particle wrapped around the box); else from global memory
-      float2 ebx, ebz, eby;
-      if (cxu == cx && cyu == cy && cx >= x0 - 1 && cx <= x0 + TCX && cy >= y0 - 1 &&
-          cy <= y0 + 1) {
-        const int c0 = cx - x0 + 1, r0 = cy - y0 + 1;  // window index of node (cx, cy)
-        ebx = gather_pair(&win[0][r0 + nyw.i - cy - 1][c0 + hx.i - cx - 1], WX, hx, nyw);
-        ebz = gather_pair(&win[1][r0 + hy.i - cy - 1][c0 + hx.i - cx - 1], WX, hx, hy);
-        eby = gather_pair(&win[2][r0 + hy.i - cy - 1][c0 + nxw.i - cx - 1], WX, nxw, hy);
-      } else {
-        ebx = gather_pair(a.ebx + (int64_t)(nyw.i - 1) * nxg + hx.i - 1, nxg, hx, nyw);
-        ebz = gather_pair(a.ebz + (int64_t)(hy.i - 1) * nxg + hx.i - 1, nxg, hx, hy);
-        eby = gather_pair(a.eby + (int64_t)(hy.i - 1) * nxg + nxw.i - 1, nxg, nxw, hy);
+    // a lane without a particle runs on a dummy inside a real cell
+    PartOut o;
+    push_one<TCX>(a, win, x0, y0, kxs, ky, act, act ? cxr : 0.25f, act ? cyr : 0.25f, cux, cuy,
+                  cuz, cinv, b, akel, stay_new, o);
+    if (INPLACE) {
+      if (act) {
+        a.B[i] = o.mx + (float)o.ox;
+        a.B[cap + i] = o.my + (float)o.oy;
+        a.B[2 * cap + i] = o.ux;
+        a.B[3 * cap + i] = o.uy;
+        a.B[4 * cap + i] = o.uz;
       }
-      // relativistic Boris on u (pic/move.f90:176-203)
-      const float gx = ux + ebx.x, gy = uy + eby.x, gz = uz + ebz.x;
-      const float gm = sqrtf(1.0f + gx * gx + gy * gy + gz * gz);
-      akel += (double)gm - 1.0;
-      const float dcg = 1.0f / (a.c * gm);
-      float tx = dcg * ebx.y, ty = dcg * eby.y, tz = dcg * ebz.y;
-      const float vvx = gx + gy * tz - gz * ty;
-      const float vvy = gy + gz * tx - gx * tz;
-      const float vvz = gz + gx * ty - gy * tx;
-      const float f2 = 2.0f / (1.0f + tx * tx + ty * ty + tz * tz);
-      tx *= f2;
-      ty *= f2;
-      tz *= f2;
-      ux = gx + vvy * tz - vvz * ty + ebx.x;
-      uy = gy + vvz * tx - vvx * tz + eby.x;
-      uz = gz + vvx * ty - vvy * tx + ebz.x;
-      const float ginv = 1.0f / sqrtf(1.0f + ux * ux + uy * uy + uz * uz);
-      const float vx = ux * ginv, vy = uy * ginv, vz = uz * ginv;
-      const float qx = a.qd * vx, qy = a.qd * vy, qz = a.qd * vz;
-      // jm at the old position (pic/curnt.f90:53-132)
-      q_x = qx;
-      q_y = qy;
-      q_z = qz;
-      if (in_cell_old) {
-        block_add_j(b, cx, cy, hx, hy, nxw, nyw, qx, qy, qz);
-      } else {
-        need_old = true;
-        q_cx = cx;
-        q_cy = cy;
-        q_fx = fx;
-        q_fy = fy;
-      }
-      // move (pic/curnt.f90:181-194), relative to the start cell
-      const float2 mv = fma2(make_float2(vx, vy), make_float2(a.dtdx, a.dtdy),
-                             make_float2(fx, fy));
-      const float mx = mv.x, my = mv.y;
-      const int nox = floor_small(mx), noy = floor_small(my);
-      const int ncx = wrap(cx + nox, nx), ncy = wrap(cy + noy, ny);
-      const float nfx = mx - (float)nox, nfy = my - (float)noy;
-      Wts nhx, nhy, nnx, nny;
-      weights2(ncx, ncy, make_float2(nfx, nfy), nhx, nhy, nnx, nny);
-      // rho and jp at the new position (pic/curnt.f90:197-303)
-      if (ncx == kx && ncy == ky) {
-        block_add_rho(b, ncx, ncy, nnx, nny, a.qd);
-        block_add_j(b, ncx, ncy, nhx, nhy, nnx, nny, qx, qy, qz);
-        ++stay_new;
-      } else {
-        need_new = true;
-        q_ncx = ncx;
-        q_ncy = ncy;
-        q_nfx = nfx;
-        q_nfy = nfy;
-      }
-      if (INPLACE) {
-        a.B[i] = mx + (float)ox;
-        a.B[cap + i] = my + (float)oy;
-        a.B[2 * cap + i] = ux;
-        a.B[3 * cap + i] = uy;
-        a.B[4 * cap + i] = uz;
-      } else {
-        // write back grouped by the cell of the start of this step: particles
-        // that started it in cell k take the next slots from the front of k's
-        // segment in processing order (a running count per group, no
-        // atomics); the few that came from another cell's range fill it from
-        // the back
-        const unsigned inm = __ballot_sync(am, in_cell_old) & gmask;
+    } else {
+      // write back grouped by the cell of the start of this step: particles
+      // that started it in cell k take the next slots from the front of k's
+      // segment in processing order (a running count per group, no atomics);
+      // the few that came from another cell's range fill it from the back
+      const unsigned inm = __ballot_sync(0xffffffffu, act && o.in_cell_old) & gmask;
+      if (act) {
         int64_t pos;
-        if (in_cell_old)
-          pos = (int64_t)a.offB[key_cur] + home_count + __popc(inm & lt);
+        if (o.in_cell_old)
+          pos = (int64_t)a.offB[o.key_cur] + home_count + __popc(inm & lt);
         else
-          pos = (int64_t)a.offB[key_cur + 1] - 1 - atomicAdd(a.cursor + key_cur, 1);
-        home_count += __popc(inm);
-        a.B[pos] = mx;
-        a.B[cap + pos] = my;
-        a.B[2 * cap + pos] = ux;
-        a.B[3 * cap + pos] = uy;
-        a.B[4 * cap + pos] = uz;
-        a.slotB[pos] = slot;
+          pos = (int64_t)a.offB[o.key_cur + 1] - 1 - atomicAdd(a.cursor + o.key_cur, 1);
+        a.B[pos] = o.mx;
+        a.B[cap + pos] = o.my;
+        a.B[2 * cap + pos] = o.ux;
+        a.B[3 * cap + pos] = o.uy;
+        a.B[4 * cap + pos] = o.uz;
+        a.slotB[pos] = cslot;
       }
+      home_count += __popc(inm);
     }
-    // this iteration's out-of-cell deposits onto the warp's stack; whole
-    // warps of them done at once
-    const unsigned m_old = __ballot_sync(0xffffffffu, need_old);
-    const unsigned m_new = __ballot_sync(0xffffffffu, need_new);
+    // the out-of-cell deposits onto the warp's stack; whole warps of them
+    // done at once
+    const unsigned m_old = __ballot_sync(0xffffffffu, o.need_old);
+    const unsigned m_new = __ballot_sync(0xffffffffu, o.need_new);
     if (m_old | m_new) {
-      if (need_old) {
-        const int p = qn + __popc(m_old & lt);
-        Q.cx[p] = q_cx;
-        Q.cy[p] = q_cy;
-        Q.f[p] = make_float2(q_fx, q_fy);
-        Q.q[p] = make_float4(q_x, q_y, q_z, 0.0f);
+      if (o.need_old) {
+        const int q = qn + __popc(m_old & lt);
+        Q.cx[q] = o.cx;
+        Q.cy[q] = o.cy;
+        Q.f[q] = make_float2(o.fx, o.fy);
+        Q.q[q] = make_float4(o.qx, o.qy, o.qz, 0.0f);
       }
       const int qn1 = qn + __popc(m_old);
-      if (need_new) {
-        const int p = qn1 + __popc(m_new & lt);
-        Q.cx[p] = q_ncx;
-        Q.cy[p] = q_ncy;
-        Q.f[p] = make_float2(q_nfx, q_nfy);
-        Q.q[p] = make_float4(q_x, q_y, q_z, 1.0f);
+      if (o.need_new) {
+        const int q = qn1 + __popc(m_new & lt);
+        Q.cx[q] = o.ncx;
+        Q.cy[q] = o.ncy;
+        Q.f[q] = make_float2(o.nfx, o.nfy);
+        Q.q[q] = make_float4(o.qx, o.qy, o.qz, 1.0f);
       }
       qn = qn1 + __popc(m_new);
       __syncwarp();
