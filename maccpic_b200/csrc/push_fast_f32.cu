@@ -82,36 +82,14 @@ struct Wts {
   float m, s, p;  // weights of nodes i-1, i, i+1
 };
 
-// Packed FP32 pairs (sm_100a's f32x2 arithmetic): one instruction for the
-// two lanes of a pair, each rounded as its scalar FMA / multiply would be.
-__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
-  float2 r;
-  asm("{ .reg .b64 pa, pb, pc, pd;\n\t"
-      "mov.b64 pa, {%2, %3};\n\tmov.b64 pb, {%4, %5};\n\tmov.b64 pc, {%6, %7};\n\t"
-      "fma.rn.f32x2 pd, pa, pb, pc;\n\tmov.b64 {%0, %1}, pd; }"
-      : "=f"(r.x), "=f"(r.y)
-      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
-  return r;
-}
-__device__ __forceinline__ float2 mul2(float2 a, float2 b) {
-  float2 r;
-  asm("{ .reg .b64 pa, pb, pd;\n\t"
-      "mov.b64 pa, {%2, %3};\n\tmov.b64 pb, {%4, %5};\n\t"
-      "mul.rn.f32x2 pd, pa, pb;\n\tmov.b64 {%0, %1}, pd; }"
-      : "=f"(r.x), "=f"(r.y)
-      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
-  return r;
-}
+// Packed FP32 pairs (sm_100a's f32x2 arithmetic) through the compiler's
+// builtins, so that it allocates the register pairs itself: one instruction
+// for the two lanes of a pair, each rounded as its scalar FMA / multiply /
+// add would be.
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
 __device__ __forceinline__ float2 bc2(float v) { return make_float2(v, v); }
-__device__ __forceinline__ float2 add2(float2 a, float2 b) {
-  float2 r;
-  asm("{ .reg .b64 pa, pb, pd;\n\t"
-      "mov.b64 pa, {%2, %3};\n\tmov.b64 pb, {%4, %5};\n\t"
-      "add.rn.f32x2 pd, pa, pb;\n\tmov.b64 {%0, %1}, pd; }"
-      : "=f"(r.x), "=f"(r.y)
-      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
-  return r;
-}
 
 // The quadratic weights of both axes at once for offsets f = (fx, fy) in
 // cell (cx, cy) (the forms of the file header): cell-centred nodes, middle
@@ -244,11 +222,43 @@ __device__ __forceinline__ float group_sum(float v) {
   return v;
 }
 
-// element e of a group's block goes to the array from lane e mod G
+// Sum of a group's G values of one block element, read from the warp's
+// scratch row of that element at the group's first lane g0.
 template <int G>
-__device__ __forceinline__ void flush_one(float *A, int nxg, int ix, int iy, float v, int e,
-                                          int gl) {
-  if ((e & (G - 1)) == gl && v != 0.0f) atomicAdd(A + (int64_t)iy * nxg + ix, v);
+__device__ __forceinline__ float group_row_sum(const float *row, int g0) {
+  if constexpr (G == 2) {
+    const float2 v = *reinterpret_cast<const float2 *>(row + g0);
+    return v.x + v.y;
+  } else if constexpr (G == 4) {
+    const float4 v = *reinterpret_cast<const float4 *>(row + g0);
+    return (v.x + v.y) + (v.z + v.w);
+  } else {
+    static_assert(G == 8, "2, 4 or 8 lanes per cell");
+    const float4 v = *reinterpret_cast<const float4 *>(row + g0);
+    const float4 w = *reinterpret_cast<const float4 *>(row + g0 + 4);
+    return ((v.x + v.y) + (v.z + v.w)) + ((w.x + w.y) + (w.z + w.w));
+  }
+}
+
+// Add an array's block rows (R rows of C values, elements e0.. of the
+// scratch) of a group's cell (kx, ky) to the array: lane gl of the group
+// takes rows gl, gl+G, ..
+template <int G, int R, int C>
+__device__ __forceinline__ void flush_rows(float *A, int nxg, int kx, int ky, const float *red,
+                                           int e0, int gl, int g0) {
+#pragma unroll
+  for (int rr = 0; rr < (R + G - 1) / G; ++rr) {
+    const int r = gl + rr * G;
+    if (r < R) {
+      float *dst = A + (int64_t)(ky + r) * nxg + kx;
+      const float *src = red + (e0 + r * C) * 32;
+#pragma unroll
+      for (int k = 0; k < C; ++k) {
+        const float v = group_row_sum<G>(src + k * 32, g0);
+        if (v != 0.0f) atomicAdd(dst + k, v);
+      }
+    }
+  }
 }
 
 __device__ __forceinline__ int floor_small(float f) { return f < 0.0f ? -1 : (f >= 1.0f ? 1 : 0); }
@@ -268,6 +278,15 @@ struct DepQ {
   float2 f[kQCap];
   float4 q[kQCap];  // q*vx, q*vy, q*vz, kind
 };
+// A warp's shared scratch: its deposit stack while it pushes, then up to 24
+// block values of each of its lanes (value e of lane l at red[e*32 + l])
+// for the sums over each cell's lanes.
+constexpr int kRedVals = 24;
+union WarpScratch {
+  DepQ q;
+  float red[kRedVals * 32];
+};
+static_assert(sizeof(DepQ) == sizeof(float) * kRedVals * 32, "the stack holds 24 rows");
 
 __device__ __forceinline__ void drain_entry(const Args32 &a, const DepQ &Q, int e) {
   const int cx = Q.cx[e], cy = Q.cy[e];
@@ -313,11 +332,12 @@ __device__ __forceinline__ void push_one(const Args32 &a, float2 (*win)[WY][TCX 
   o.in_cell_old = (ox == 0) && (oy == 0);
   Wts hx, hy, nxw, nyw;
   weights2(cx, cy, make_float2(fx, fy), hx, hy, nxw, nyw);
-  // gather from the shared window when the stencil is inside it (always,
-  // unless the particle wrapped around the box); else from global memory
+  // gather from the shared window unless the particle wrapped around the
+  // box: unwrapped, its cell is within one of the group cell (kx in
+  // x0 .. x0+TCX-1, ky = y0), whose stencils the window holds; else from
+  // global memory
   float2 ebx, ebz, eby;
-  if (cxu == cx && cyu == cy && cx >= x0 - 1 && cx <= x0 + TCX && cy >= y0 - 1 &&
-      cy <= y0 + 1) {
+  if (cxu == cx && cyu == cy) {
     const int c0 = cx - x0 + 1, r0 = cy - y0 + 1;  // window index of node (cx, cy)
     ebx = gather_pair(&win[0][r0 + nyw.i - cy - 1][c0 + hx.i - cx - 1], WX, hx, nyw);
     ebz = gather_pair(&win[1][r0 + hy.i - cy - 1][c0 + hx.i - cx - 1], WX, hx, hy);
@@ -362,7 +382,11 @@ __device__ __forceinline__ void push_one(const Args32 &a, float2 (*win)[WY][TCX 
   o.cy = cy;
   o.fx = fx;
   o.fy = fy;
-  if (act && o.in_cell_old) block_add_j(b, cx, cy, hx, hy, nxw, nyw, qx, qy, qz);
+  // the in-cell deposits run in every lane, with zero charge where the
+  // particle is outside the lane's cell or there is none (the weights are
+  // finite, so the block is unchanged): no branch around them
+  const float mo = (act && o.in_cell_old) ? 1.0f : 0.0f;
+  block_add_j(b, kx, ky, hx, hy, nxw, nyw, qx * mo, qy * mo, qz * mo);
   // move (pic/curnt.f90:181-194), relative to the start cell
   const float2 mv = fma2(make_float2(vx, vy), make_float2(a.dtdx, a.dtdy), make_float2(fx, fy));
   o.mx = mv.x;
@@ -377,12 +401,13 @@ __device__ __forceinline__ void push_one(const Args32 &a, float2 (*win)[WY][TCX 
   o.ncy = ncy;
   o.nfx = nfx;
   o.nfy = nfy;
-  if (act && stays) {
+  {
+    const float ms = (act && stays) ? 1.0f : 0.0f;
     Wts nhx, nhy, nnx, nny;
-    weights2(ncx, ncy, make_float2(nfx, nfy), nhx, nhy, nnx, nny);
-    block_add_rho(b, ncx, ncy, nnx, nny, a.qd);
-    block_add_j(b, ncx, ncy, nhx, nhy, nnx, nny, qx, qy, qz);
-    ++stay_new;
+    weights2(kx, ky, make_float2(nfx, nfy), nhx, nhy, nnx, nny);
+    block_add_rho(b, kx, ky, nnx, nny, a.qd * ms);
+    block_add_j(b, kx, ky, nhx, nhy, nnx, nny, qx * ms, qy * ms, qz * ms);
+    stay_new += (act && stays) ? 1 : 0;
   }
 }
 
@@ -394,7 +419,7 @@ __device__ __forceinline__ void push_one(const Args32 &a, float2 (*win)[WY][TCX 
 // that they stay in (-1, 2)); the counts of the new cells are still taken.
 template <int TCX, int G, bool INPLACE>
 __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, int64_t blk,
-                                             float2 (*win)[WY][TCX + 5], DepQ *dq) {
+                                             float2 (*win)[WY][TCX + 5], WarpScratch *ws) {
   constexpr int kThreads = TCX * G;
   constexpr int WX = TCX + 5;  // window columns: x0-1 .. x0+TCX+3
   const int nx = a.nx, ny = a.ny, nxg = a.nxg;
@@ -417,6 +442,7 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
   const int kxs = valid ? kx : nx - 1;  // the cell lanes past the grid's edge work on
   const int64_t cell = (int64_t)ky * nx + kx;
   const int32_t beg = valid ? a.offA[cell] : 0;
+  const int32_t front = (!INPLACE && valid) ? a.offB[cell] : 0;  // cell k's first slot in B
   const int32_t end = valid ? a.offA[cell + 1] : 0;
   const int64_t cap = a.cap;
   const unsigned gmask = ((1u << G) - 1u) << (lane & ~(G - 1));  // this lane's group
@@ -436,7 +462,7 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
   const float cinv = 1.0f / a.c;
   int stay_new = 0;  // particles of this lane whose new position is in cell k
   int home_count = 0;  // particles of this group written to the front of cell k
-  DepQ &Q = dq[threadIdx.x >> 5];
+  DepQ &Q = ws[threadIdx.x >> 5].q;
   int qn = 0;  // entries on this warp's stack (the same in every lane)
   const unsigned lt = (1u << lane) - 1u;
 
@@ -487,7 +513,7 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
       if (act) {
         int64_t pos;
         if (o.in_cell_old)
-          pos = (int64_t)a.offB[o.key_cur] + home_count + __popc(inm & lt);
+          pos = (int64_t)front + home_count + __popc(inm & lt);  // key_cur == cell
         else
           pos = (int64_t)a.offB[o.key_cur + 1] - 1 - atomicAdd(a.cursor + o.key_cur, 1);
         a.B[pos] = o.mx;
@@ -534,39 +560,38 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
   const int stay = group_sum<G>((float)stay_new) + 0.5f;
   if (valid && gl == 0 && stay > 0) atomicAdd(a.cnt_next + cell, stay);
   if (__any_sync(0xffffffffu, valid && end > beg)) {
-    int e = 0;
+    // the G blocks of each cell summed through the warp's scratch (the
+    // stack is empty now), in three passes: rho, Jx and Jy, Jz
+    float *red = ws[threadIdx.x >> 5].red;
+    const int g0 = lane & ~(G - 1);
+    __syncwarp();
 #pragma unroll
     for (int r = 0; r < 4; ++r)
 #pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const float v = group_sum<G>(pick4(b.rho01[r], b.rho23[r], k));
-        if (valid) flush_one<G>(a.rho, nxg, kx + k, ky + r, v, e, gl);
-        ++e;
-      }
+      for (int k = 0; k < 4; ++k) red[(r * 4 + k) * 32 + lane] = pick4(b.rho01[r], b.rho23[r], k);
+    __syncwarp();
+    if (valid) flush_rows<G, 4, 4>(a.rho, nxg, kx, ky, red, 0, gl, g0);
+    __syncwarp();
 #pragma unroll
     for (int r = 0; r < 4; ++r)
 #pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        const float v = group_sum<G>(pick3(b.jx01[r], b.jx2[r], k));
-        if (valid) flush_one<G>(a.jx, nxg, kx + k, ky + r, v, e, gl);
-        ++e;
-      }
+      for (int k = 0; k < 3; ++k) red[(r * 3 + k) * 32 + lane] = pick3(b.jx01[r], b.jx2[r], k);
 #pragma unroll
     for (int r = 0; r < 3; ++r)
 #pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const float v = group_sum<G>(pick4(b.jy01[r], b.jy23[r], k));
-        if (valid) flush_one<G>(a.jy, nxg, kx + k, ky + r, v, e, gl);
-        ++e;
-      }
+      for (int k = 0; k < 4; ++k) red[(12 + r * 4 + k) * 32 + lane] = pick4(b.jy01[r], b.jy23[r], k);
+    __syncwarp();
+    if (valid) {
+      flush_rows<G, 4, 3>(a.jx, nxg, kx, ky, red, 0, gl, g0);
+      flush_rows<G, 3, 4>(a.jy, nxg, kx, ky, red, 12, gl, g0);
+    }
+    __syncwarp();
 #pragma unroll
     for (int r = 0; r < 3; ++r)
 #pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        const float v = group_sum<G>(pick3(b.jz01[r], b.jz2[r], k));
-        if (valid) flush_one<G>(a.jz, nxg, kx + k, ky + r, v, e, gl);
-        ++e;
-      }
+      for (int k = 0; k < 3; ++k) red[(r * 3 + k) * 32 + lane] = pick3(b.jz01[r], b.jz2[r], k);
+    __syncwarp();
+    if (valid) flush_rows<G, 3, 3>(a.jz, nxg, kx, ky, red, 0, gl, g0);
   }
   // per-warp partial of sum(gamma - 1); no block barrier at the end
   for (int o = 16; o > 0; o >>= 1) akel += __shfl_down_sync(0xffffffffu, akel, o);
@@ -579,9 +604,9 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
 template <int TCX, int G, int MINB, bool INPLACE>
 __global__ void __launch_bounds__(TCX * G, MINB) k_push_cells_f32(Args32 a) {
   __shared__ float2 win[3][WY][TCX + 5];
-  __shared__ DepQ dq[TCX * G / 32];
+  __shared__ WarpScratch ws[TCX * G / 32];
   push_segment<TCX, G, INPLACE>(a, (int)blockIdx.x * TCX, (int)blockIdx.y,
-                             (int64_t)blockIdx.y * gridDim.x + blockIdx.x, win, dq);
+                                (int64_t)blockIdx.y * gridDim.x + blockIdx.x, win, ws);
 }
 
 // Ensemble: every (run, species) pair of an ensemble in one persistent
@@ -593,7 +618,7 @@ template <int TCX, int G, int MINB>
 __global__ void __launch_bounds__(TCX * G, MINB)
     k_ens_push_f32(const __grid_constant__ EnsPush32 e) {
   __shared__ float2 win[3][WY][TCX + 5];
-  __shared__ DepQ dq[TCX * G / 32];
+  __shared__ WarpScratch ws[TCX * G / 32];
   __shared__ int s_tile;
   for (;;) {
     if (threadIdx.x == 0) s_tile = atomicAdd(e.counter, 1);
@@ -608,7 +633,7 @@ __global__ void __launch_bounds__(TCX * G, MINB)
     const int lt = t - e.tile0[lo];
     const int segs = e.segs[lo];
     const int row = lt / segs;
-    push_segment<TCX, G, false>(e.pair[lo], (lt - row * segs) * TCX, row, lt, win, dq);
+    push_segment<TCX, G, false>(e.pair[lo], (lt - row * segs) * TCX, row, lt, win, ws);
   }
 }
 
