@@ -143,19 +143,21 @@ __device__ __forceinline__ void scatter9(float *A, int nxg, const Wts &wx, const
   atomicAdd(rp + 1, wx.p * qp);
 }
 
-// The 49-value register block, kept as pairs where rows allow so that packed
-// FMAs update two values at once: Jx rows 4 x (2 + 1), Jy rows 3 x (2 + 2),
-// Jz rows 3 x (2 + 1), rho rows 4 x (2 + 2).
+// The 49-value register block, kept as pairs so that packed FMAs update two
+// values at once.  Jx (4 rows x 3) and Jz (3 x 3) pair rows -- per column k,
+// rows (0,1) and (2,3) of Jx, rows (0,1) and the single row 2 of Jz -- so
+// that both take the x weight of column k as the broadcast operand; Jy (3 x
+// 4) and rho (4 x 4) pair columns (0,1) and (2,3) of each row.
 struct Block32 {
-  float2 jx01[4], jy01[3], jy23[3], jz01[3], rho01[4], rho23[4];
-  float jx2[4], jz2[3];
+  float2 jxr01[3], jxr23[3], jzr01[3], jy01[3], jy23[3], rho01[4], rho23[4];
+  float jzr2[3];
 };
-// element (r, k) of each array of the block (r, k compile-time constants)
-__device__ __forceinline__ float pick4(const float2 &lo, const float2 &hi, int k) {
-  return k == 0 ? lo.x : k == 1 ? lo.y : k == 2 ? hi.x : hi.y;
+// element i of a row or column kept as pairs (i a compile-time constant)
+__device__ __forceinline__ float pick4(const float2 &lo, const float2 &hi, int i) {
+  return i == 0 ? lo.x : i == 1 ? lo.y : i == 2 ? hi.x : hi.y;
 }
-__device__ __forceinline__ float pick3(const float2 &lo, float last, int k) {
-  return k == 0 ? lo.x : k == 1 ? lo.y : last;
+__device__ __forceinline__ float pick3(const float2 &lo, float last, int i) {
+  return i == 0 ? lo.x : i == 1 ? lo.y : last;
 }
 
 __device__ __forceinline__ void spread4(const Wts &w, int c, float o[4]) {
@@ -174,21 +176,26 @@ __device__ __forceinline__ void block_add_j(Block32 &b, int cx, int cy, const Wt
   spread4(nxw, cx, wxn);
   spread4(nyw, cy, wyn);
   const float wxh[3] = {hx.m, hx.s, hx.p}, wyh[3] = {hy.m, hy.s, hy.p};
-  const float2 h01 = make_float2(wxh[0], wxh[1]);
   const float2 n01 = make_float2(wxn[0], wxn[1]), n23 = make_float2(wxn[2], wxn[3]);
+  // Jx(r, k) += (wyn[r] qx) wxh[k], Jz(r, k) += (wyh[r] qz) wxh[k]
+  const float2 ax01 = mul2(make_float2(wyn[0], wyn[1]), bc2(qx));
+  const float2 ax23 = mul2(make_float2(wyn[2], wyn[3]), bc2(qx));
+  const float2 az01 = mul2(make_float2(wyh[0], wyh[1]), bc2(qz));
+  const float az2 = wyh[2] * qz;
 #pragma unroll
-  for (int r = 0; r < 4; ++r) {
-    const float t = wyn[r] * qx;
-    b.jx01[r] = fma2(h01, bc2(t), b.jx01[r]);
-    b.jx2[r] = fmaf(wxh[2], t, b.jx2[r]);
+  for (int k = 0; k < 3; ++k) {
+    const float2 w = bc2(wxh[k]);
+    b.jxr01[k] = fma2(ax01, w, b.jxr01[k]);
+    b.jxr23[k] = fma2(ax23, w, b.jxr23[k]);
+    b.jzr01[k] = fma2(az01, w, b.jzr01[k]);
+    b.jzr2[k] = fmaf(az2, wxh[k], b.jzr2[k]);
   }
+  // Jy(r, k) += (wyh[r] qy) wxn[k]
 #pragma unroll
   for (int r = 0; r < 3; ++r) {
-    const float ty = wyh[r] * qy, tz = wyh[r] * qz;
+    const float ty = wyh[r] * qy;
     b.jy01[r] = fma2(n01, bc2(ty), b.jy01[r]);
     b.jy23[r] = fma2(n23, bc2(ty), b.jy23[r]);
-    b.jz01[r] = fma2(h01, bc2(tz), b.jz01[r]);
-    b.jz2[r] = fmaf(wxh[2], tz, b.jz2[r]);
   }
 }
 
@@ -289,7 +296,7 @@ union WarpScratch {
 static_assert(sizeof(DepQ) == sizeof(float) * kRedVals * 32, "the stack holds 24 rows");
 
 __device__ __forceinline__ void drain_entry(const Args32 &a, const DepQ &Q, int e) {
-  const int cx = Q.cx[e], cy = Q.cy[e];
+  const int cx = wrap(Q.cx[e], a.nx), cy = wrap(Q.cy[e], a.ny);  // entries are unwrapped
   const float4 qq = Q.q[e];
   Wts hx, hy, nxw, nyw;
   weights2(cx, cy, Q.f[e], hx, hy, nxw, nyw);
@@ -301,13 +308,14 @@ __device__ __forceinline__ void drain_entry(const Args32 &a, const DepQ &Q, int 
 }
 
 // What one particle's push leaves for the write-back and the warp's stack.
+// Cells are unwrapped (group cell + offsets, possibly -1 or n..n+1 across
+// the periodic boundary); whoever indexes the arrays with them wraps them.
 struct PartOut {
   float mx, my, ux, uy, uz;  // new position relative to the start cell, new u
   int ox, oy;                // start cell - group cell (-1, 0 or 1 each)
-  int key_cur;               // start cell's key
   bool in_cell_old;          // the start cell is the group cell
   bool need_old, need_new;   // deposits for the warp's stack
-  int cx, cy, ncx, ncy;
+  int cx, cy, ncx, ncy;      // start and end cells, unwrapped
   float fx, fy, nfx, nfy, qx, qy, qz;
 };
 
@@ -323,29 +331,28 @@ __device__ __forceinline__ void push_one(const Args32 &a, float2 (*win)[WY][TCX 
   const int nx = a.nx, ny = a.ny, nxg = a.nxg;
   // the cell the particle is in now (it may have left cell k last step)
   const int ox = floor_small(xr), oy = floor_small(yr);
-  const int cxu = kx + ox, cyu = ky + oy;  // unwrapped
-  const int cx = wrap(cxu, nx), cy = wrap(cyu, ny);
+  const int cx = kx + ox, cy = ky + oy;  // unwrapped
   const float fx = xr - (float)ox, fy = yr - (float)oy;
   o.ox = ox;
   o.oy = oy;
-  o.key_cur = cy * nx + cx;
   o.in_cell_old = (ox == 0) && (oy == 0);
-  Wts hx, hy, nxw, nyw;
+  Wts hx, hy, nxw, nyw;  // array indices of the unwrapped cell
   weights2(cx, cy, make_float2(fx, fy), hx, hy, nxw, nyw);
-  // gather from the shared window unless the particle wrapped around the
-  // box: unwrapped, its cell is within one of the group cell (kx in
-  // x0 .. x0+TCX-1, ky = y0), whose stencils the window holds; else from
-  // global memory
+  // gather from the shared window unless the particle is across the
+  // periodic boundary: then its cell is within one of the group cell (kx in
+  // x0 .. x0+TCX-1, ky = y0), whose stencils the window holds (window index
+  // = array index - (x0-1, y0-1), the stencil starting one node before i);
+  // else from global memory at the wrapped cell
   float2 ebx, ebz, eby;
-  if (cxu == cx && cyu == cy) {
-    const int c0 = cx - x0 + 1, r0 = cy - y0 + 1;  // window index of node (cx, cy)
-    ebx = gather_pair(&win[0][r0 + nyw.i - cy - 1][c0 + hx.i - cx - 1], WX, hx, nyw);
-    ebz = gather_pair(&win[1][r0 + hy.i - cy - 1][c0 + hx.i - cx - 1], WX, hx, hy);
-    eby = gather_pair(&win[2][r0 + hy.i - cy - 1][c0 + nxw.i - cx - 1], WX, nxw, hy);
+  if ((unsigned)cx < (unsigned)nx && (unsigned)cy < (unsigned)ny) {
+    ebx = gather_pair(&win[0][nyw.i - y0][hx.i - x0], WX, hx, nyw);
+    ebz = gather_pair(&win[1][hy.i - y0][hx.i - x0], WX, hx, hy);
+    eby = gather_pair(&win[2][hy.i - y0][nxw.i - x0], WX, nxw, hy);
   } else {
-    ebx = gather_pair(a.ebx + (int64_t)(nyw.i - 1) * nxg + hx.i - 1, nxg, hx, nyw);
-    ebz = gather_pair(a.ebz + (int64_t)(hy.i - 1) * nxg + hx.i - 1, nxg, hx, hy);
-    eby = gather_pair(a.eby + (int64_t)(hy.i - 1) * nxg + nxw.i - 1, nxg, nxw, hy);
+    const int sx = wrap(cx, nx) - cx, sy = wrap(cy, ny) - cy;
+    ebx = gather_pair(a.ebx + (int64_t)(nyw.i + sy - 1) * nxg + hx.i + sx - 1, nxg, hx, nyw);
+    ebz = gather_pair(a.ebz + (int64_t)(hy.i + sy - 1) * nxg + hx.i + sx - 1, nxg, hx, hy);
+    eby = gather_pair(a.eby + (int64_t)(hy.i + sy - 1) * nxg + nxw.i + sx - 1, nxg, nxw, hy);
   }
   // relativistic Boris on u (pic/move.f90:176-203).  The reciprocal square
   // roots and divisions are the hardware approximations (rsqrtf, a few ulp),
@@ -392,13 +399,14 @@ __device__ __forceinline__ void push_one(const Args32 &a, float2 (*win)[WY][TCX 
   o.mx = mv.x;
   o.my = mv.y;
   const int nox = floor_small(mv.x), noy = floor_small(mv.y);
-  const int ncx = wrap(cx + nox, nx), ncy = wrap(cy + noy, ny);
   const float nfx = mv.x - (float)nox, nfy = mv.y - (float)noy;
-  // rho and jp at the new position (pic/curnt.f90:197-303)
-  const bool stays = ncx == kx && ncy == ky;
+  // rho and jp at the new position (pic/curnt.f90:197-303); with at least 4
+  // cells a side, the new cell is the group cell exactly when the offsets
+  // cancel
+  const bool stays = ox + nox == 0 && oy + noy == 0;
   o.need_new = act && !stays;
-  o.ncx = ncx;
-  o.ncy = ncy;
+  o.ncx = cx + nox;
+  o.ncy = cy + noy;
   o.nfx = nfx;
   o.nfy = nfy;
   {
@@ -451,11 +459,10 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
   const float2 z2 = make_float2(0.0f, 0.0f);
 #pragma unroll
   for (int r = 0; r < 4; ++r) {
-    b.rho01[r] = b.rho23[r] = b.jx01[r] = z2;
-    b.jx2[r] = 0.0f;
+    b.rho01[r] = b.rho23[r] = z2;
     if (r < 3) {
-      b.jy01[r] = b.jy23[r] = b.jz01[r] = z2;
-      b.jz2[r] = 0.0f;
+      b.jxr01[r] = b.jxr23[r] = b.jzr01[r] = b.jy01[r] = b.jy23[r] = z2;
+      b.jzr2[r] = 0.0f;
     }
   }
   double akel = 0.0;  // this lane's sum of gamma - 1
@@ -513,9 +520,11 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
       if (act) {
         int64_t pos;
         if (o.in_cell_old)
-          pos = (int64_t)front + home_count + __popc(inm & lt);  // key_cur == cell
-        else
-          pos = (int64_t)a.offB[o.key_cur + 1] - 1 - atomicAdd(a.cursor + o.key_cur, 1);
+          pos = (int64_t)front + home_count + __popc(inm & lt);
+        else {
+          const int key = wrap(o.cy, ny) * nx + wrap(o.cx, nx);  // the start cell's key
+          pos = (int64_t)a.offB[key + 1] - 1 - atomicAdd(a.cursor + key, 1);
+        }
         a.B[pos] = o.mx;
         a.B[cap + pos] = o.my;
         a.B[2 * cap + pos] = o.ux;
@@ -575,7 +584,7 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
 #pragma unroll
     for (int r = 0; r < 4; ++r)
 #pragma unroll
-      for (int k = 0; k < 3; ++k) red[(r * 3 + k) * 32 + lane] = pick3(b.jx01[r], b.jx2[r], k);
+      for (int k = 0; k < 3; ++k) red[(r * 3 + k) * 32 + lane] = pick4(b.jxr01[k], b.jxr23[k], r);
 #pragma unroll
     for (int r = 0; r < 3; ++r)
 #pragma unroll
@@ -589,7 +598,7 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
 #pragma unroll
     for (int r = 0; r < 3; ++r)
 #pragma unroll
-      for (int k = 0; k < 3; ++k) red[(r * 3 + k) * 32 + lane] = pick3(b.jz01[r], b.jz2[r], k);
+      for (int k = 0; k < 3; ++k) red[(r * 3 + k) * 32 + lane] = pick3(b.jzr01[k], b.jzr2[k], r);
     __syncwarp();
     if (valid) flush_rows<G, 3, 3>(a.jz, nxg, kx, ky, red, 0, gl, g0);
   }
