@@ -101,8 +101,9 @@ bool is_fp32(const em2g_ctx *c) { return c->P.precision == EM2G_FP32; }
 
 // host FP64 arrays [first, first+count) of the field block -> device
 // The context's FP64 staging buffer on the device (particles: 6*n doubles
-// x, y, vx, vy, vz, gamma; fields: FP64 arrays), grown on demand and kept
-// until em2g_destroy so that repeated copies allocate nothing.
+// x, y, vx, vy, vz, gamma, and for FP32 contexts 32*n bytes of records
+// after them; fields: FP64 arrays), grown on demand and kept until
+// em2g_destroy so that repeated copies allocate nothing.
 int ensure_staging(em2g_ctx *c, int64_t ndoubles) {
   if (ndoubles <= c->staging_n) return EM2G_OK;
   EM2G_CUDA(cudaStreamSynchronize(c->stream));  // the old buffer may still be read
@@ -505,7 +506,7 @@ static int load_particles(em2g_ctx *c, int isp, int64_t n, const double *const *
   if (n == 0) {
     S.n = 0;
     S.sorted = false;
-    if (is_fp32(c)) return upload_f32(c, isp, nullptr, 0);
+    if (is_fp32(c)) return upload_f32(c, isp, nullptr, 0, nullptr);
     return EM2G_OK;
   }
   for (int k = 0; k < 6; ++k)
@@ -513,7 +514,8 @@ static int load_particles(em2g_ctx *c, int isp, int64_t n, const double *const *
   double *dst = S.part_alt;
   int64_t ld = S.cap;
   if (is_fp32(c)) {
-    const int rs = ensure_staging(c, 6 * n);
+    // 6*n FP64 values, then 32*n bytes of records for the regrouping
+    const int rs = ensure_staging(c, 10 * n);
     if (rs) return rs;
     dst = c->staging;
     ld = n;
@@ -529,7 +531,7 @@ static int load_particles(em2g_ctx *c, int isp, int64_t n, const double *const *
   if (hb[1]) return fail(EM2G_ERR_NONFINITE, std::to_string(hb[1]) + " particles with non-finite values");
   if (hb[0]) return fail(EM2G_ERR_RANGE, std::to_string(hb[0]) + " particles outside the grid");
   if (is_fp32(c)) {
-    if ((rc = upload_f32(c, isp, dst, n))) return rc;
+    if ((rc = upload_f32(c, isp, dst, n, dst + 6 * n))) return rc;
   } else {
     std::swap(S.part, S.part_alt);
     k_iota<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(S.slot, n);
@@ -572,8 +574,8 @@ int em2g_get_particles(em2g_ctx *c, int isp, int64_t *n, double *x, double *y, d
   if (!x && !y && !vx && !vy && !vz && !gamma) return EM2G_OK;  // count query
   if (!x || !y || !vx || !vy || !vz || !gamma) return fail(EM2G_ERR_INVALID, "null particle array");
   if (is_fp32(c)) {
-    if ((rc = ensure_staging(c, 6 * S.n))) return rc;
-    if ((rc = download_f32(c, isp, c->staging))) return rc;
+    if ((rc = ensure_staging(c, 10 * S.n))) return rc;  // values, then records
+    if ((rc = download_f32(c, isp, c->staging, c->staging + 6 * S.n))) return rc;
     double *dst[6] = {x, y, vx, vy, vz, gamma};
     for (int k = 0; k < 6; ++k)
       EM2G_CUDA(cudaMemcpyAsync(dst[k], c->staging + k * S.n, sizeof(double) * S.n,

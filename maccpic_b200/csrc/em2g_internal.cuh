@@ -140,8 +140,10 @@ const char *variant_name_f32(int v);
 // mixed-precision path (push_fast_f32.cu, fields_f32.cu)
 int launch_prescale_f32(em2g_ctx *c, int isp);
 int launch_push_cells_f32(em2g_ctx *c, int isp);
-int upload_f32(em2g_ctx *c, int isp, const double *staging, int64_t n);
-int download_f32(em2g_ctx *c, int isp, double *staging);
+// particle transfers of FP32 contexts: staging = 6*n FP64 values in slot
+// order; rec = 32*n bytes of scratch (16-byte aligned) for the regrouping
+int upload_f32(em2g_ctx *c, int isp, const double *staging, int64_t n, void *rec);
+int download_f32(em2g_ctx *c, int isp, double *staging, void *rec);
 int smooth2_f32(em2g_ctx *c, float *a);
 int cg_init_f32(em2g_ctx *c);
 int fields_f32(em2g_ctx *c, int it, bool want_energies);

@@ -729,6 +729,82 @@ __global__ void k_scatter_to_f32(const double *__restrict__ st, int64_t n, int n
   slot[pos] = (int32_t)j;
 }
 
+// Transfers between the caller's slot order and the cell-grouped layout of
+// a single context go through one 32-byte record per particle (a whole
+// sector, two 16-byte stores): moving a particle to a random position then
+// writes one full sector, where six separate arrays would write six partial
+// ones (each a read-modify-write in L2).  rec holds 2*n float4.
+//
+// FP64 slot-order staging -> records in cell-grouped order:
+// (xr, yr, ux, uy), (uz, slot, 0, 0)
+__global__ void k_scatter_rec(const double *__restrict__ st, int64_t n, int nx, int ny,
+                              const int32_t *__restrict__ off, int32_t *cursor, float4 *rec) {
+  const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool active = j < n;
+  const unsigned am = __ballot_sync(0xffffffffu, active);
+  if (!active) return;
+  const double x = st[j], y = st[n + j];
+  const int key = cell_key(x, y, nx, ny);
+  const int64_t pos = (int64_t)off[key] + agg_atomic_add(cursor, key, am);
+  const int cx = (int)x, cy = (int)y;
+  const double g = st[5 * n + j];
+  // offsets relative to the (unwrapped) cell holding x, y
+  rec[2 * pos] = make_float4((float)(x - cx), (float)(y - cy), (float)(st[2 * n + j] * g),
+                             (float)(st[3 * n + j] * g));
+  rec[2 * pos + 1] = make_float4((float)(st[4 * n + j] * g), __int_as_float((int32_t)j), 0.f, 0.f);
+}
+
+// records in cell-grouped order -> the FP32 arrays and slots
+__global__ void k_rec_to_soa(const float4 *__restrict__ rec, int64_t n, float *P, int32_t *slot,
+                             int64_t cap) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float4 a = rec[2 * i], b = rec[2 * i + 1];
+  P[i] = a.x;
+  P[cap + i] = a.y;
+  P[2 * cap + i] = a.z;
+  P[3 * cap + i] = a.w;
+  P[4 * cap + i] = b.x;
+  slot[i] = __float_as_int(b.y);
+}
+
+// cell-grouped FP32 -> records in slot order: (x, y) as doubles, wrapped
+// into the box, then (ux, uy, uz, 0)
+__global__ void k_grouped_to_rec(const float *__restrict__ P, const int32_t *__restrict__ slot,
+                                 const int32_t *__restrict__ off, int64_t cap, int nx, int ny,
+                                 float4 *rec) {
+  const int64_t cell = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kCopyLanes;
+  const int gl = threadIdx.x & (kCopyLanes - 1);
+  if (cell >= (int64_t)nx * ny) return;
+  const int kx = (int)(cell % nx), ky = (int)(cell / nx);
+  for (int32_t i = off[cell] + gl; i < off[cell + 1]; i += kCopyLanes) {
+    double x = kx + (double)P[i], y = ky + (double)P[cap + i];
+    if (x < 0.0) x += nx;
+    if (x >= nx) x -= nx;
+    if (y < 0.0) y += ny;
+    if (y >= ny) y -= ny;
+    const int64_t s = slot[i];
+    reinterpret_cast<double2 *>(rec)[2 * s] = make_double2(x, y);
+    rec[2 * s + 1] = make_float4(P[2 * cap + i], P[3 * cap + i], P[4 * cap + i], 0.f);
+  }
+}
+
+// records in slot order -> FP64 staging: x, y, vx, vy, vz, gamma
+__global__ void k_rec_to_fp64(const float4 *__restrict__ rec, int64_t n, double *st) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const double2 xy = reinterpret_cast<const double2 *>(rec)[2 * s];
+  const float4 u = rec[2 * s + 1];
+  const double ux = u.x, uy = u.y, uz = u.z;
+  const double g = sqrt(1.0 + ux * ux + uy * uy + uz * uz);
+  st[s] = xy.x;
+  st[n + s] = xy.y;
+  st[2 * n + s] = ux / g;
+  st[3 * n + s] = uy / g;
+  st[4 * n + s] = uz / g;
+  st[5 * n + s] = g;
+}
+
 // cell-grouped FP32 -> FP64 staging in slot order: x, y, vx, vy, vz, gamma
 __global__ void k_gather_from_f32(const float *__restrict__ P, const int32_t *__restrict__ slot,
                                   const int32_t *__restrict__ off, int64_t cap, int nx, int ny,
@@ -834,7 +910,7 @@ int launch_push_cells_f32(em2g_ctx *c, int isp) {
 }
 
 // staging (6*n doubles on the device, slot order) -> cell-grouped FP32
-int upload_f32(em2g_ctx *c, int isp, const double *staging, int64_t n) {
+int upload_f32(em2g_ctx *c, int isp, const double *staging, int64_t n, void *rec) {
   Species &S = c->sp[isp];
   EM2G_CUDA(cudaMemsetAsync(S.cnt, 0, sizeof(int32_t) * c->ncell, c->stream));
   EM2G_CUDA(cudaMemsetAsync(S.cursor, 0, sizeof(int32_t) * c->ncell, c->stream));
@@ -846,26 +922,32 @@ int upload_f32(em2g_ctx *c, int isp, const double *staging, int64_t n) {
   int rc = scan_cells(c, S.cnt, S.off);
   if (rc) return rc;
   if (n > 0) {
-    k_scatter_to_f32<<<nb, 256, 0, c->stream>>>(staging, n, c->g.nx, c->g.ny, S.off, S.cursor,
-                                                 S.p32, S.slot, S.cap);
+    float4 *r = static_cast<float4 *>(rec);
+    k_scatter_rec<<<nb, 256, 0, c->stream>>>(staging, n, c->g.nx, c->g.ny, S.off, S.cursor, r);
+    EM2G_CUDA(cudaGetLastError());
+    k_rec_to_soa<<<nb, 256, 0, c->stream>>>(r, n, S.p32, S.slot, S.cap);
     EM2G_CUDA(cudaGetLastError());
   }
-  c->launches += 2;
+  c->launches += 3;
   S.n = n;
   S.sorted = true;
   S.since_sort = 0;
   return EM2G_OK;
 }
 
-// cell-grouped FP32 -> staging (6*n doubles, slot order)
-int download_f32(em2g_ctx *c, int isp, double *staging) {
+// cell-grouped FP32 -> staging (6*n doubles, slot order) through the
+// records (32*n bytes at rec)
+int download_f32(em2g_ctx *c, int isp, double *staging, void *rec) {
   Species &S = c->sp[isp];
   if (S.n == 0) return EM2G_OK;
+  float4 *r = static_cast<float4 *>(rec);
   const int64_t nb = (c->ncell * kCopyLanes + 255) / 256;
-  k_gather_from_f32<<<(unsigned)nb, 256, 0, c->stream>>>(S.p32, S.slot, S.off, S.cap, c->g.nx,
-                                                         c->g.ny, staging, S.n);
-  c->launches += 1;
+  k_grouped_to_rec<<<(unsigned)nb, 256, 0, c->stream>>>(S.p32, S.slot, S.off, S.cap, c->g.nx,
+                                                        c->g.ny, r);
   EM2G_CUDA(cudaGetLastError());
+  k_rec_to_fp64<<<(unsigned)((S.n + 255) / 256), 256, 0, c->stream>>>(r, S.n, staging);
+  EM2G_CUDA(cudaGetLastError());
+  c->launches += 2;
   return EM2G_OK;
 }
 
