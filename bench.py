@@ -595,9 +595,9 @@ def run_e2e(args, cfg, rp, fields, parts_host, variant=0):
     for it in range(1, args.steps + 1):
         g.move_curnt()
         g.fields(it)
-    out_f[...] = g.get_fields()
+    g.get_fields(out=out_f)
     for s in range(2):
-        C_get_particles_into(g, s, out_p[s])
+        g.get_particles(s, out=out_p[s])
     el = time.perf_counter() - t
     g.close()
     n_total = sum(p.shape[1] for p in pnp)
@@ -608,15 +608,6 @@ def run_e2e(args, cfg, rp, fields, parts_host, variant=0):
             "d2h_bytes_per_step": (state + small * args.steps) / args.steps,
             "path": "em2g_set_fields/em2g_set_particles (pinned host, FP64 em2 layout), K x "
                     "(em2g_move_curnt, em2g_fields), em2g_get_fields/em2g_get_particles"}
-
-
-def C_get_particles_into(g, s, out):
-    import ctypes as C
-    from maccpic_b200._lib import check
-    n = C.c_int64()
-    ptrs = [out[k].ctypes.data_as(C.POINTER(C.c_double)) for k in range(6)]
-    check(g._L.em2g_get_particles(g._h, s, C.byref(n), *ptrs))
-    return n.value
 
 
 def main():

@@ -86,6 +86,14 @@ def _dp(a: np.ndarray):
     return a.ctypes.data_as(C.POINTER(C.c_double))
 
 
+def _check_out(out: np.ndarray, shape) -> None:
+    """A caller's output buffer must be C-contiguous float64 of `shape`."""
+    if (not isinstance(out, np.ndarray) or out.dtype != np.float64 or out.shape != tuple(shape)
+            or not out.flags.c_contiguous or not out.flags.writeable):
+        raise ValueError(f"out must be a writeable C-contiguous float64 array of shape "
+                         f"{tuple(shape)}")
+
+
 CUDA_STREAM_LEGACY = 1  # cudaStreamLegacy: the legacy default stream's handle
 
 
@@ -136,8 +144,14 @@ class Em2Gpu:
             raise ValueError(f"fields must have shape {(NFIELD,) + self.p.shape}")
         check(self._L.em2g_set_fields(self._h, _dp(a)))
 
-    def get_fields(self) -> np.ndarray:
-        out = np.empty((NFIELD,) + self.p.shape)
+    def get_fields(self, out: np.ndarray | None = None) -> np.ndarray:
+        """All 13 arrays, shape (13, ny+3, nx+3); into `out` (C-contiguous
+        float64 of that shape, e.g. pinned memory the caller keeps) if given."""
+        shape = (NFIELD,) + self.p.shape
+        if out is None:
+            out = np.empty(shape)
+        else:
+            _check_out(out, shape)
         check(self._L.em2g_get_fields(self._h, _dp(out)))
         return out
 
@@ -217,10 +231,15 @@ class Em2Gpu:
     def reset_counters(self) -> None:
         check(self._L.em2g_reset_counters(self._h))
 
-    def get_particles(self, isp: int) -> np.ndarray:
+    def get_particles(self, isp: int, out: np.ndarray | None = None) -> np.ndarray:
+        """(6, n) = x, y, vx, vy, vz, gamma in slot order; into `out`
+        (C-contiguous float64 of that shape) if given."""
         n = C.c_int64()
         check(self._L.em2g_get_particles(self._h, isp, C.byref(n), *([None] * 6)))
-        out = np.empty((6, n.value))
+        if out is None:
+            out = np.empty((6, n.value))
+        else:
+            _check_out(out, (6, n.value))
         if n.value:
             check(self._L.em2g_get_particles(self._h, isp, C.byref(n),
                                              *[_dp(out[k]) for k in range(6)]))

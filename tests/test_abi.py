@@ -175,3 +175,19 @@ def test_stream_handles_for_the_library():
     assert stream_handle(FakeStream(0)).value == CUDA_STREAM_LEGACY
     assert stream_handle(FakeStream(0x1234)).value == 0x1234
     assert stream_handle(0x5678).value == 0x5678
+
+
+def test_output_buffers_are_checked_without_gpu():
+    """A caller's output buffer for get_fields / get_particles must be a
+    writeable C-contiguous float64 array of the exact shape."""
+    import numpy as np
+    from maccpic_b200.em2 import _check_out
+
+    _check_out(np.empty((6, 10)), (6, 10))
+    bad = [np.empty((6, 9)), np.empty((6, 10), dtype=np.float32), np.empty((10, 6)).T,
+           np.empty((6, 20))[:, ::2]]
+    ro = np.empty((6, 10))
+    ro.flags.writeable = False
+    for b in bad + [ro, [[0.0] * 10] * 6]:
+        with pytest.raises(ValueError):
+            _check_out(b, (6, 10))

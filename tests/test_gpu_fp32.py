@@ -45,6 +45,29 @@ def test_fp32_fields_roundtrip(gpu):
         np.testing.assert_allclose(g.get_fields(), fld.astype(np.float32).astype(np.float64))
 
 
+def test_outputs_into_caller_buffers(gpu):
+    """get_fields / get_particles fill a caller's buffer (pinned memory here)
+    with what they would return; a buffer of the wrong shape is refused."""
+    import torch
+    from maccpic_b200.em2 import Em2Gpu
+    op, rp, fld, parts = harris(nx=64, ny=32, ppc=8)
+    with Em2Gpu(rp) as g:
+        g.set_fields(fld)
+        for s, p in enumerate(parts):
+            g.set_particles(s, p)
+        out_f = torch.empty(fld.shape, dtype=torch.float64).pin_memory().numpy()
+        assert g.get_fields(out=out_f) is out_f
+        np.testing.assert_array_equal(out_f, g.get_fields())
+        for s, p in enumerate(parts):
+            out_p = torch.empty(p.shape, dtype=torch.float64).pin_memory().numpy()
+            g.get_particles(s, out=out_p)
+            np.testing.assert_array_equal(out_p, g.get_particles(s))
+        with pytest.raises(ValueError):
+            g.get_particles(0, out=np.empty((6, parts[0].shape[1] - 1)))
+        with pytest.raises(ValueError):
+            g.get_fields(out=np.empty(fld.shape, dtype=np.float32))
+
+
 def test_fp32_step_against_fp64_oracle(gpu, oracle_lib):
     from maccpic_b200.em2 import Em2Gpu
     op, rp, fld, parts = harris()
