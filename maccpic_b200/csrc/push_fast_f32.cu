@@ -431,29 +431,52 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
   constexpr int kThreads = TCX * G;
   constexpr int WX = TCX + 5;  // window columns: x0-1 .. x0+TCX+3
   const int nx = a.nx, ny = a.ny, nxg = a.nxg;
-  // stage the segment's (E, B) window: array indices x0-1.., y0-1..
-  for (int t = threadIdx.x; t < 3 * WY * WX; t += kThreads) {
-    const int comp = t / (WY * WX), r = (t / WX) % WY, col = t % WX;
-    const int gx = x0 - 1 + col, gy = y0 - 1 + r;
-    float2 v = make_float2(0.f, 0.f);
-    if (gx >= 0 && gx <= nx + 2 && gy >= 0 && gy <= ny + 2) {
-      const float2 *src = comp == 0 ? a.ebx : (comp == 1 ? a.ebz : a.eby);
-      v = src[(int64_t)gy * nxg + gx];
-    }
-    win[comp][r][col] = v;
-  }
-  __syncthreads();
-
   const int lane = threadIdx.x & 31, gl = lane & (G - 1);
   const int kx = x0 + (int)(threadIdx.x / G), ky = y0;
   const bool valid = kx < nx;
   const int kxs = valid ? kx : nx - 1;  // the cell lanes past the grid's edge work on
   const int64_t cell = (int64_t)ky * nx + kx;
+  const int64_t cap = a.cap;
+  const unsigned gmask = ((1u << G) - 1u) << (lane & ~(G - 1));  // this lane's group
+  // The segment's start has three independent global loads -- the cell's
+  // range, the (E, B) window and the first particle -- issued together
+  // before the first wait: the range, then the window into registers, then
+  // the particle (once the range is in), then the window into shared memory.
   const int32_t beg = valid ? a.offA[cell] : 0;
   const int32_t front = (!INPLACE && valid) ? a.offB[cell] : 0;  // cell k's first slot in B
   const int32_t end = valid ? a.offA[cell + 1] : 0;
-  const int64_t cap = a.cap;
-  const unsigned gmask = ((1u << G) - 1u) << (lane & ~(G - 1));  // this lane's group
+  // the window: array indices x0-1.., y0-1..
+  constexpr int kWin = 3 * WY * WX, kWinPer = (kWin + kThreads - 1) / kThreads;
+  float2 wv[kWinPer];
+#pragma unroll
+  for (int u = 0; u < kWinPer; ++u) {
+    const int t = threadIdx.x + u * kThreads;
+    const int comp = t / (WY * WX), r = (t / WX) % WY, col = t % WX;
+    const int gx = x0 - 1 + col, gy = y0 - 1 + r;
+    wv[u] = make_float2(0.f, 0.f);
+    if (t < kWin && gx >= 0 && gx <= nx + 2 && gy >= 0 && gy <= ny + 2) {
+      const float2 *src = comp == 0 ? a.ebx : (comp == 1 ? a.ebz : a.eby);
+      wv[u] = src[(int64_t)gy * nxg + gx];
+    }
+  }
+  // software pipeline: the next particle's state is loaded while this one runs
+  float pxr = 0.f, pyr = 0.f, pux = 0.f, puy = 0.f, puz = 0.f;
+  int32_t pslot = 0;
+  if (beg + gl < end) {
+    const int32_t j = beg + gl;
+    pxr = a.A[j];
+    pyr = a.A[cap + j];
+    pux = a.A[2 * cap + j];
+    puy = a.A[3 * cap + j];
+    puz = a.A[4 * cap + j];
+    pslot = a.slotA[j];
+  }
+#pragma unroll
+  for (int u = 0; u < kWinPer; ++u) {
+    const int t = threadIdx.x + u * kThreads;
+    if (t < kWin) win[t / (WY * WX)][(t / WX) % WY][t % WX] = wv[u];
+  }
+  __syncthreads();
 
   Block32 b;
   const float2 z2 = make_float2(0.0f, 0.0f);
@@ -473,18 +496,6 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
   int qn = 0;  // entries on this warp's stack (the same in every lane)
   const unsigned lt = (1u << lane) - 1u;
 
-  // software pipeline: the next particle's state is loaded while this one runs
-  float pxr = 0.f, pyr = 0.f, pux = 0.f, puy = 0.f, puz = 0.f;
-  int32_t pslot = 0;
-  if (beg + gl < end) {
-    const int32_t j = beg + gl;
-    pxr = a.A[j];
-    pyr = a.A[cap + j];
-    pux = a.A[2 * cap + j];
-    puy = a.A[3 * cap + j];
-    puz = a.A[4 * cap + j];
-    pslot = a.slotA[j];
-  }
   for (int32_t i = beg + gl;; i += G) {
     const bool act = i < end;
     if (__ballot_sync(0xffffffffu, act) == 0u) break;
