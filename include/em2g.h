@@ -273,7 +273,8 @@ int em2g_adj_get_initial_particles_device(em2g_adj *adj, int isp, double *x, dou
  * tolerance).  The whole step is captured once into a CUDA graph and
  * replayed; nothing in it waits on the host.
  *
- * Every run is FP32 (precision EM2G_FP32) with energy_mode 0, on one device;
+ * Every run is FP32 (precision EM2G_FP32) with energy_mode 0, on one device,
+ * and all runs share one sort_interval (params.sort_interval, 0 or 1 = 1);
  * at most 160 (run, species) pairs, 2^31 - 1 particles and cells in all.
  * A run holds exactly np_max[s] particles of species s, set (once, or again
  * to replace them) by em2g_ens_set_particles* before the first step.
@@ -291,6 +292,10 @@ int em2g_ens_set_graph(em2g_ens *ens, int on);
 /* the FP32 push variants (as em2g_num_variants of an FP32 context) */
 int em2g_ens_num_variants(em2g_ens *ens, int *n);
 int em2g_ens_set_variant(em2g_ens *ens, int variant);
+/* regroup the particles by cell on every k-th step and update them in place
+ * in between, as em2g_set_sort_interval does for a context; k * c * dt must
+ * be < dx and dy in every run (0 or 1: every step) */
+int em2g_ens_set_sort_interval(em2g_ens *ens, int k);
 /* one run's 13 arrays, as em2g_set_fields / em2g_get_fields */
 int em2g_ens_set_fields(em2g_ens *ens, int run, const double *host13);
 int em2g_ens_get_fields(em2g_ens *ens, int run, double *host13);

@@ -36,7 +36,8 @@ EXPORTS = [
     "em2g_adj_backward", "em2g_adj_get_fields_device", "em2g_adj_get_particles_device",
     "em2g_adj_get_initial_particles_device",
     "em2g_ens_create", "em2g_ens_destroy", "em2g_ens_num_runs", "em2g_ens_set_stream",
-    "em2g_ens_set_graph", "em2g_ens_num_variants", "em2g_ens_set_variant", "em2g_ens_set_fields", "em2g_ens_get_fields",
+    "em2g_ens_set_graph", "em2g_ens_num_variants", "em2g_ens_set_variant",
+    "em2g_ens_set_sort_interval", "em2g_ens_set_fields", "em2g_ens_get_fields",
     "em2g_ens_set_particles", "em2g_ens_set_particles_device", "em2g_ens_get_particles",
     "em2g_ens_step", "em2g_ens_get_step", "em2g_ens_diagnostics", "em2g_ens_get_counters",
 ]
@@ -131,6 +132,7 @@ def lib() -> C.CDLL:
         "em2g_ens_set_graph": (C.c_int, [ctx, C.c_int]),
         "em2g_ens_num_variants": (C.c_int, [ctx, ip]),
         "em2g_ens_set_variant": (C.c_int, [ctx, C.c_int]),
+        "em2g_ens_set_sort_interval": (C.c_int, [ctx, C.c_int]),
         "em2g_ens_set_fields": (C.c_int, [ctx, C.c_int, dp]),
         "em2g_ens_get_fields": (C.c_int, [ctx, C.c_int, dp]),
         "em2g_ens_set_particles": (C.c_int, [ctx, C.c_int, C.c_int, C.c_int64] + [dp] * 6),

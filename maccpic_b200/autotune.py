@@ -30,7 +30,10 @@ def _step_ms(run, k: int, cycles: int) -> float:
     """Mean wall time of a step at sort interval k over whole cycles."""
     import time
     run.set_sort_interval(k)
-    run.step(k)  # align to a regrouping
+    # untimed: two cycles, so that an ensemble has captured the graph of
+    # every kind of step (in place or regrouping, either buffer and count
+    # parity) before the timing
+    run.step(2 * k)
     n = k * cycles
     t = time.perf_counter()
     run.step(n)
@@ -92,13 +95,15 @@ def autotune(run, particles: int, steps: int = 2, warm: int = 1, cache: str | No
     return {**result, "from_cache": False}
 
 
-def autotune_ensemble(ens, steps: int = 2, warm: int = 1) -> dict:
+def autotune_ensemble(ens, steps: int = 2, warm: int = 1, intervals=None) -> dict:
     """Time every push variant on an ensemble (its current state, a few
-    graph-launched steps each; every step advances the runs) and keep the
-    fastest.  Returns {"variant", "name", "times_ms"}: mean wall time of a
-    step per variant."""
+    graph-launched steps each; every step advances the runs), keep the
+    fastest, then time the sort intervals the drift bound allows with it.
+    Returns {"variant", "times_ms", "sort_interval", "interval_ms"}: mean
+    wall time of a step per variant and per interval."""
     import time
     import torch
+    ens.set_sort_interval(1)
     times = []
     for v in range(ens.num_variants()):
         ens.set_variant(v)
@@ -110,4 +115,11 @@ def autotune_ensemble(ens, steps: int = 2, warm: int = 1) -> dict:
         times.append((time.perf_counter() - t) * 1e3 / steps)
     best = min(range(len(times)), key=lambda v: times[v])
     ens.set_variant(best)
-    return {"variant": best, "times_ms": times}
+    kmax = ens.max_sort_interval()
+    if intervals is None:
+        intervals = sorted({k for k in (1, 2, 3, 4, 6, kmax) if 1 <= k <= kmax})
+    interval_ms = {k: _step_ms(ens, k, cycles=max(1, 6 // k)) for k in intervals}
+    k_best = min(interval_ms, key=interval_ms.get)
+    ens.set_sort_interval(k_best)
+    return {"variant": best, "times_ms": times, "sort_interval": k_best,
+            "interval_ms": {str(k): v for k, v in interval_ms.items()}}

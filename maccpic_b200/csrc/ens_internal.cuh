@@ -57,23 +57,28 @@ struct em2g_ens {
   double *dev_out = nullptr;     // kEnsOut per run
   double *host_out = nullptr;    // pinned mirror of dev_out
   int *host_status = nullptr;    // pinned mirror of cg_status
-  // particles; parity 0: current = p32/slot/off/cnt, next = the _alt set
+  // particles; parity 0: current = p32/slot/off, next = the _alt set;
+  // cparity 0: current cell counts = cnt.  A regrouping push flips both,
+  // an in-place push (between regroupings, sort_interval > 1) only cparity.
   float *p32 = nullptr, *p32_alt = nullptr;
   int32_t *slot = nullptr, *slot_alt = nullptr;
   int32_t *off = nullptr, *off_alt = nullptr, *cnt = nullptr, *cnt_alt = nullptr;
   int32_t *cursor = nullptr, *scan_tmp = nullptr;
   int64_t cap = 0, ncell = 0;
-  int parity = 0;
+  int parity = 0, cparity = 0;
+  int sort_interval = 1;  // regroup on every sort_interval-th push
+  int since_sort = 0;     // in-place pushes since the last regrouping
   double *staging = nullptr;  // 6 * staging_n doubles (uploads, downloads)
   int64_t staging_n = 0;
   int *counter = nullptr;     // the persistent push's segment counter
   int *d_it = nullptr;        // the step counter as the field kernels read it
   int it = 0;
   int variant = 0;
-  // one captured graph per buffer parity; invalid after a change of
-  // variant or stream
+  // one captured graph per (in place, parity, cparity); invalid after a
+  // change of variant, sort interval or stream
   bool use_graph = true;
-  cudaGraphExec_t exec[2] = {nullptr, nullptr};
+  cudaGraphExec_t exec[8] = {};
+  int64_t graph_kernels[8] = {};
   int64_t kernels_per_step = 0;
   int64_t launches = 0, graph_launches = 0;
 };
@@ -81,10 +86,10 @@ struct em2g_ens {
 namespace em2g {
 
 // push_fast_f32.cu
-int ens_push(em2g_ens *e, int parity);
+int ens_push(em2g_ens *e, int bp, int cp, bool inplace);
 int ens_upload_pair(em2g_ens *e, int r, int s, const double *staging);
 int ens_download_pair(em2g_ens *e, int r, int s, double *staging);
-int ens_push_kernels_per_step(const em2g_ens *e);
+int ens_push_kernels_per_step(const em2g_ens *e, bool inplace);
 // fields_ens.cu
 int ens_cg_setup(em2g_ens *e);
 int ens_prescale(em2g_ens *e);

@@ -7,8 +7,11 @@
 // segments from a counter, fed by one scan over all pairs' cell counts),
 // the kinetic energies (one launch), then em2's fields for every run, one
 // launch per stage and one cooperative launch for every run's CG
-// (fields_ens.cu).  The step is captured once per buffer parity into a
-// CUDA graph and replayed; nothing in it waits on the host.
+// (fields_ens.cu).  With a sort interval k > 1 the push regroups the
+// particles by cell on every k-th step only and updates them in place in
+// between, as single runs do.  Each kind of step (in place or regrouping,
+// and which buffers and counts are current) is captured once into a CUDA
+// graph and replayed; nothing in it waits on the host.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -44,18 +47,28 @@ void drop_graphs(em2g_ens *e) {
     }
 }
 
-int enqueue_step(em2g_ens *e, int parity) {
+// the next step's kind: in place between regroupings
+bool next_inplace(const em2g_ens *e) {
+  return e->sort_interval > 1 && e->since_sort + 1 < e->sort_interval;
+}
+
+int graph_key(const em2g_ens *e, bool inplace) {
+  return (inplace ? 4 : 0) + 2 * e->parity + e->cparity;
+}
+
+int enqueue_step(em2g_ens *e, bool inplace) {
   int rc;
   if ((rc = ens_prescale(e))) return rc;
-  if ((rc = ens_push(e, parity))) return rc;
+  if ((rc = ens_push(e, e->parity, e->cparity, inplace))) return rc;
   if ((rc = ens_tick(e))) return rc;
   return ens_fields(e);
 }
 
-int capture_step(em2g_ens *e, int parity) {
+int capture_step(em2g_ens *e, bool inplace) {
+  const int key = graph_key(e, inplace);
   cudaGraph_t g = nullptr;
   EM2G_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
-  const int rc = enqueue_step(e, parity);
+  const int rc = enqueue_step(e, inplace);
   const cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
   if (rc) {
     if (g) cudaGraphDestroy(g);
@@ -72,10 +85,10 @@ int capture_step(em2g_ens *e, int parity) {
     ge = cudaGraphNodeGetType(nodes[k], &t);
     if (t == cudaGraphNodeTypeKernel) ++kernels;
   }
-  if (ge == cudaSuccess) ge = cudaGraphInstantiate(&e->exec[parity], g, 0);
+  if (ge == cudaSuccess) ge = cudaGraphInstantiate(&e->exec[key], g, 0);
   cudaGraphDestroy(g);
   if (ge != cudaSuccess) return cuda_fail(ge, "step graph");
-  e->kernels_per_step = kernels;
+  e->graph_kernels[key] = kernels;
   return EM2G_OK;
 }
 
@@ -108,8 +121,8 @@ int em2g_ens_create(const em2g_params *runs, int nruns, em2g_ens **out) {
     if (rc) return rc;
     if (P.precision != EM2G_FP32) return fail(EM2G_ERR_INVALID, "ensemble runs are FP32");
     if (P.energy_mode != 0) return fail(EM2G_ERR_INVALID, "ensemble runs use energy_mode 0");
-    if (P.sort_interval > 1)
-      return fail(EM2G_ERR_INVALID, "ensemble runs regroup every step (sort_interval 0 or 1)");
+    if (std::max(P.sort_interval, 1) != std::max(runs[0].sort_interval, 1))
+      return fail(EM2G_ERR_INVALID, "ensemble runs share one sort_interval");
     if (P.device != runs[0].device) return fail(EM2G_ERR_INVALID, "runs on different devices");
     for (int s = 0; s < P.nsp; ++s) {
       if (P.np_max[s] < 1) return fail(EM2G_ERR_INVALID, "np_max must be the particle count");
@@ -128,6 +141,7 @@ int em2g_ens_create(const em2g_params *runs, int nruns, em2g_ens **out) {
     return code;
   };
   e->device = runs[0].device;
+  e->sort_interval = std::max(runs[0].sort_interval, 1);
   e->npairs = npairs;
   e->cap = cap;
   e->ncell = ncell;
@@ -274,6 +288,24 @@ int em2g_ens_set_variant(em2g_ens *e, int v) {
   return EM2G_OK;
 }
 
+int em2g_ens_set_sort_interval(em2g_ens *e, int k) {
+  int rc = check_ens(e);
+  if (rc) return rc;
+  for (const EnsRun &R : e->runs) {
+    em2g_params p = R.P;
+    p.sort_interval = k;
+    if ((rc = validate_params(&p))) return rc;  // k * c * dt < dx, dy for every run
+  }
+  k = std::max(k, 1);
+  if (k != e->sort_interval) {
+    EM2G_CUDA(cudaStreamSynchronize(e->stream));
+    drop_graphs(e);
+    e->sort_interval = k;
+    for (EnsRun &R : e->runs) R.P.sort_interval = k;
+  }
+  return EM2G_OK;
+}
+
 int em2g_ens_set_fields(em2g_ens *e, int run, const double *host13) {
   int rc = check_pair(e, run, 0);
   if (rc) return rc;
@@ -379,17 +411,26 @@ int em2g_ens_step(em2g_ens *e, int nsteps, double *ake_out, double *energies_out
   const int nr = (int)e->runs.size();
   EM2G_CUDA(cudaMemsetAsync(e->cg_status, 0, sizeof(int) * 2 * nr, e->stream));
   for (int k = 0; k < nsteps; ++k) {
+    const bool inplace = next_inplace(e);
     if (e->use_graph) {
-      if (!e->exec[e->parity] && (rc = capture_step(e, e->parity))) return rc;
-      EM2G_CUDA(cudaGraphLaunch(e->exec[e->parity], e->stream));
+      const int key = graph_key(e, inplace);
+      if (!e->exec[key] && (rc = capture_step(e, inplace))) return rc;
+      EM2G_CUDA(cudaGraphLaunch(e->exec[key], e->stream));
       e->graph_launches += 1;
+      e->kernels_per_step = e->graph_kernels[key];
     } else {
-      if ((rc = enqueue_step(e, e->parity))) return rc;
+      if ((rc = enqueue_step(e, inplace))) return rc;
       // prescale, tick, the push's and the fields' kernels
-      e->kernels_per_step = 2 + ens_push_kernels_per_step(e) + ens_fields_kernels(e);
+      e->kernels_per_step = 2 + ens_push_kernels_per_step(e, inplace) + ens_fields_kernels(e);
     }
     e->launches += e->kernels_per_step;
-    e->parity ^= 1;
+    if (inplace) {
+      ++e->since_sort;
+    } else {
+      e->since_sort = 0;
+      e->parity ^= 1;
+    }
+    e->cparity ^= 1;
     e->it += 1;
   }
   EM2G_CUDA(cudaMemcpyAsync(e->host_out, e->dev_out, sizeof(double) * kEnsOut * nr,

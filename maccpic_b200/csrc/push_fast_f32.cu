@@ -634,7 +634,8 @@ __global__ void __launch_bounds__(TCX * G, MINB) k_push_cells_f32(Args32 a) {
 // (tile0[p] .. tile0[p+1]-1 for pair p, row-major within the pair); each
 // CTA takes the next unclaimed segment from a counter until none is left,
 // so runs of unequal size and density share the SMs without a tail per run.
-template <int TCX, int G, int MINB>
+// INPLACE as for single runs (the ensemble's sort interval).
+template <int TCX, int G, int MINB, bool INPLACE>
 __global__ void __launch_bounds__(TCX * G, MINB)
     k_ens_push_f32(const __grid_constant__ EnsPush32 e) {
   __shared__ float2 win[3][WY][TCX + 5];
@@ -653,7 +654,7 @@ __global__ void __launch_bounds__(TCX * G, MINB)
     const int lt = t - e.tile0[lo];
     const int segs = e.segs[lo];
     const int row = lt / segs;
-    push_segment<TCX, G, false>(e.pair[lo], (lt - row * segs) * TCX, row, lt, win, ws);
+    push_segment<TCX, G, INPLACE>(e.pair[lo], (lt - row * segs) * TCX, row, lt, win, ws);
   }
 }
 
@@ -663,10 +664,12 @@ struct Variant32 {
   void (*kernel)(Args32);
   void (*kernel_inplace)(Args32);
   void (*ens_kernel)(const EnsPush32);
+  void (*ens_kernel_inplace)(const EnsPush32);
 };
 #define EM2G_VARIANT32(T, GG, M)                                                         \
   {"f32 tcx" #T " g" #GG " minb" #M, T, GG, k_push_cells_f32<T, GG, M, false>,          \
-   k_push_cells_f32<T, GG, M, true>, k_ens_push_f32<T, GG, M>}
+   k_push_cells_f32<T, GG, M, true>, k_ens_push_f32<T, GG, M, false>,                   \
+   k_ens_push_f32<T, GG, M, true>}
 const Variant32 kVariants32[] = {
     EM2G_VARIANT32(32, 4, 4), EM2G_VARIANT32(32, 4, 5), EM2G_VARIANT32(32, 4, 6),
     EM2G_VARIANT32(64, 4, 2), EM2G_VARIANT32(64, 4, 3), EM2G_VARIANT32(32, 8, 2),
@@ -964,20 +967,30 @@ int download_f32(em2g_ctx *c, int isp, double *staging, void *rec) {
 
 // ---- ensembles (ensemble_api.cu) ---------------------------------------
 
-// One push of every pair: offsets of the next grouping from the current
-// counts (one scan over all pairs), the persistent push, the kinetic
-// energies.  parity selects which buffer set is current.
-int ens_push(em2g_ens *e, int parity) {
-  float *A = parity ? e->p32_alt : e->p32, *B = parity ? e->p32 : e->p32_alt;
-  int32_t *slotA = parity ? e->slot_alt : e->slot, *slotB = parity ? e->slot : e->slot_alt;
-  int32_t *offA = parity ? e->off_alt : e->off, *offB = parity ? e->off : e->off_alt;
-  int32_t *cntA = parity ? e->cnt_alt : e->cnt, *cntB = parity ? e->cnt : e->cnt_alt;
+// One push of every pair: for a regrouping push, offsets of the next
+// grouping from the current counts (one scan over all pairs); the
+// persistent push; the kinetic energies.  bp selects the current particle
+// buffers and offsets, cp the current cell counts (which change on every
+// push, where the buffers change only on regrouping pushes); an in-place
+// push updates the current buffers.
+int ens_push(em2g_ens *e, int bp, int cp, bool inplace) {
+  float *A = bp ? e->p32_alt : e->p32, *B = bp ? e->p32 : e->p32_alt;
+  int32_t *slotA = bp ? e->slot_alt : e->slot, *slotB = bp ? e->slot : e->slot_alt;
+  int32_t *offA = bp ? e->off_alt : e->off, *offB = bp ? e->off : e->off_alt;
+  int32_t *cntA = cp ? e->cnt_alt : e->cnt, *cntB = cp ? e->cnt : e->cnt_alt;
+  if (inplace) {
+    B = A;
+    slotB = slotA;
+    offB = offA;
+  }
   const Variant32 &V = kVariants32[e->variant < num_variants_f32() ? e->variant : 0];
   const int threads = V.tcx * V.g;
   cudaStream_t st = e->stream;
-  int rc = scan_counts(cntA, offB, e->ncell, 0, e->scan_tmp, st);
-  if (rc) return rc;
-  EM2G_CUDA(cudaMemsetAsync(e->cursor, 0, sizeof(int32_t) * e->ncell, st));
+  int rc;
+  if (!inplace) {
+    if ((rc = scan_counts(cntA, offB, e->ncell, 0, e->scan_tmp, st))) return rc;
+    EM2G_CUDA(cudaMemsetAsync(e->cursor, 0, sizeof(int32_t) * e->ncell, st));
+  }
   EM2G_CUDA(cudaMemsetAsync(cntB, 0, sizeof(int32_t) * e->ncell, st));
   EM2G_CUDA(cudaMemsetAsync(e->counter, 0, sizeof(int), st));
   std::unique_ptr<EnsPush32> P(new EnsPush32());
@@ -1029,10 +1042,11 @@ int ens_push(em2g_ens *e, int parity) {
   P->tile0[p] = t;
   P->counter = e->counter;
   int per_sm = 0;
-  EM2G_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, V.ens_kernel, threads, 0));
+  auto kernel = inplace ? V.ens_kernel_inplace : V.ens_kernel;
+  EM2G_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0));
   if (per_sm < 1) return fail(EM2G_ERR_CUDA, "ensemble push kernel cannot be resident");
   const int blocks = std::min(per_sm * e->num_sms, t);
-  V.ens_kernel<<<blocks, threads, 0, st>>>(*P);
+  kernel<<<blocks, threads, 0, st>>>(*P);
   k_ens_ake<<<p, 256, 0, st>>>(*K);
   EM2G_CUDA(cudaGetLastError());
   return EM2G_OK;
@@ -1046,7 +1060,7 @@ int ens_upload_pair(em2g_ens *e, int r, int s, const double *staging) {
   float *P = e->parity ? e->p32_alt : e->p32;
   int32_t *slot = e->parity ? e->slot_alt : e->slot;
   int32_t *off = e->parity ? e->off_alt : e->off;
-  int32_t *cnt = e->parity ? e->cnt_alt : e->cnt;
+  int32_t *cnt = e->cparity ? e->cnt_alt : e->cnt;
   cudaStream_t st = e->stream;
   EM2G_CUDA(cudaMemsetAsync(cnt + c0, 0, sizeof(int32_t) * nc, st));
   EM2G_CUDA(cudaMemsetAsync(e->cursor + c0, 0, sizeof(int32_t) * nc, st));
@@ -1076,7 +1090,8 @@ int ens_download_pair(em2g_ens *e, int r, int s, double *staging) {
   return EM2G_OK;
 }
 
-// kernels one ens_push enqueues: scan (3), push, kinetic energies
-int ens_push_kernels_per_step(const em2g_ens *) { return 5; }
+// kernels one ens_push enqueues: scan (3, regrouping pushes only), push,
+// kinetic energies
+int ens_push_kernels_per_step(const em2g_ens *, bool inplace) { return inplace ? 2 : 5; }
 
 }  // namespace em2g

@@ -129,6 +129,19 @@ class Em2Ensemble:
     def set_variant(self, v: int) -> None:
         check(self._L.em2g_ens_set_variant(self._h, int(v)))
 
+    def set_sort_interval(self, k: int) -> None:
+        """Regroup every run's particles by cell on every k-th step and update
+        them in place in between (k * c * dt < dx, dy in every run)."""
+        check(self._L.em2g_ens_set_sort_interval(self._h, int(k)))
+        for r in self.runs:
+            r.sort_interval = int(k)
+
+    def max_sort_interval(self) -> int:
+        """The largest interval the drift bound allows in every run."""
+        import math
+        k = min(math.ceil(min(r.dx, r.dy) / (r.c * r.dt)) - 1 for r in self.runs)
+        return max(1, k)
+
     def set_stream(self, stream) -> None:
         """As Em2Gpu.set_stream."""
         check(self._L.em2g_ens_set_stream(self._h, stream_handle(stream)))

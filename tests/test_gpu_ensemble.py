@@ -189,3 +189,74 @@ def test_errors(gpu):
         with pytest.raises(Em2gError) as ei:
             f.step(1)
         assert ei.value.status == _lib.ERR_INVALID
+
+
+def test_sort_interval_tracks_single_runs(gpu):
+    """With a sort interval the ensemble pushes in place between regroupings,
+    as single contexts do: after the first step (in place) the particles are
+    bitwise those of single runs at the same interval, and over 7 steps at
+    interval 3 (two regroupings) the runs track them."""
+    cfgs = _cfgs()
+    states = [_state(c) for c in cfgs]
+    singles = [_single(c, *states[r]) for r, c in enumerate(cfgs)]
+    try:
+        with _ensemble(cfgs, states) as e:
+            e.set_sort_interval(3)
+            for g in singles:
+                g.set_sort_interval(3)
+            e.step(1)
+            assert e.counters()["kernels_per_step"] == 18  # no scan in place
+            for r, g in enumerate(singles):
+                g.step(1)
+                for s in range(2):
+                    np.testing.assert_array_equal(e.get_particles(r, s), g.get_particles(s))
+            out = None
+            for _ in range(6):
+                out = e.step(1)
+            assert e.it == 7 and e.counters()["graph_launches"] == 7
+            for r, g in enumerate(singles):
+                r1 = None
+                for _ in range(6):
+                    r1 = g.step(1)
+                np.testing.assert_allclose(out["ake"][r, :2], r1["ake"], rtol=1e-4)
+                fe, fg = e.get_fields(r), g.get_fields()
+                for k in range(3, 6):
+                    assert rel(fe[k], fg[k]) < 1e-3, (r, k)
+                for s in range(2):
+                    pe, pg = e.get_particles(r, s), g.get_particles(s)
+                    assert np.abs(pe[:2] - pg[:2]).max() < 1e-3
+    finally:
+        for g in singles:
+            g.close()
+
+
+def test_sort_interval_rules(gpu):
+    """k * c * dt < dx, dy in every run; runs created together share one
+    interval."""
+    import dataclasses
+    from maccpic_b200 import _lib
+    from maccpic_b200._lib import Em2gError
+    from maccpic_b200.ensemble import Em2Ensemble
+    cfgs = _cfgs()[:2]
+    states = [_state(c) for c in cfgs]
+    with _ensemble(cfgs, states) as e:
+        kmax = e.max_sort_interval()
+        assert kmax > 1
+        with pytest.raises(Em2gError) as ei:
+            e.set_sort_interval(kmax + 1)
+        assert ei.value.status == _lib.ERR_INVALID
+        with pytest.raises(Em2gError):
+            e.set_sort_interval(-1)
+        e.set_sort_interval(kmax)
+        e.step(kmax + 1)
+        e.set_sort_interval(0)
+        e.step(1)
+    n = [s[1][0].shape[1] for s in states]
+    runs = [c.run_params(np_max=[k, k], precision=_lib.FP32) for c, k in zip(cfgs, n)]
+    runs[0] = dataclasses.replace(runs[0], sort_interval=2)
+    with pytest.raises(Em2gError) as ei:
+        Em2Ensemble(runs)
+    assert ei.value.status == _lib.ERR_INVALID
+    runs[1] = dataclasses.replace(runs[1], sort_interval=2)
+    with Em2Ensemble(runs) as f:
+        assert all(r.sort_interval == 2 for r in f.runs)
