@@ -233,6 +233,12 @@ int finish_outputs(em2g_ctx *c, double *ake_out, double *energies_out, int *cg_i
   int rc = timing_collect(c);
   if (rc) return rc;
   if (st[0] != 0) return fail(EM2G_ERR_TIMEOUT, "cg: a grid barrier wait timed out");
+  if (c->host_out[kDevLost] != 0.0) {
+    const double lost = c->host_out[kDevLost];
+    EM2G_CUDA(cudaMemsetAsync(c->dev_out + kDevLost, 0, sizeof(double), c->stream));
+    return fail(EM2G_ERR_RANGE, "regrouping push: " + std::to_string((long long)lost) +
+                                    " particles fell outside their cells' ranges");
+  }
   if (ake_out)
     for (int s = 0; s < c->P.nsp; ++s) ake_out[s] = c->host_out[s];
   if (energies_out && energies_valid)

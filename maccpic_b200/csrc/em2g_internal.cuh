@@ -19,6 +19,10 @@ constexpr int kEnsMaxPairs = 160;  // partial sums per field in the energy reduc
 // the current fields, [16,18) reconnected flux of the two sheets, [18,20)
 // mean r^2 of the last Poisson solve before and after the CG
 constexpr int kDevOut = 32;
+// dev_out[kDevLost]: particles a regrouping push found no place for (their
+// cell counts disagreed with where they were; the state is then corrupt and
+// the step fails -- a guard, never expected to count)
+constexpr int kDevLost = kDevOut - 1;
 
 // Sets the per-thread error message and returns the status (api.cu).
 int fail(int status, const std::string &msg);

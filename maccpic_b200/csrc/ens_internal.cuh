@@ -22,6 +22,7 @@ namespace em2g {
 // per run: [0,4) ake of the last step, [4,10) energies of the last isav
 // step, [10,12) mean r^2 before and after the last CG
 constexpr int kEnsOut = 16;
+constexpr int kEnsLost = kEnsOut - 1;  // per run, as kDevLost of a context
 
 struct EnsRun {
   em2g_params P;

@@ -443,6 +443,16 @@ int em2g_ens_step(em2g_ens *e, int nsteps, double *ake_out, double *energies_out
     if (e->host_status[2 * r])
       return fail(EM2G_ERR_TIMEOUT, "cg of run " + std::to_string(r) + ": a barrier wait timed out");
   for (int r = 0; r < nr; ++r) {
+    const double lost = e->host_out[(int64_t)r * kEnsOut + kEnsLost];
+    if (lost != 0.0) {
+      EM2G_CUDA(cudaMemsetAsync(e->dev_out + (int64_t)r * kEnsOut + kEnsLost, 0, sizeof(double),
+                                e->stream));
+      return fail(EM2G_ERR_RANGE, "regrouping push of run " + std::to_string(r) + ": " +
+                                      std::to_string((long long)lost) +
+                                      " particles fell outside their cells' ranges");
+    }
+  }
+  for (int r = 0; r < nr; ++r) {
     const EnsRun &R = e->runs[r];
     const double *o = e->host_out + (int64_t)r * kEnsOut;
     if (ake_out)

@@ -48,6 +48,7 @@ namespace em2g {
 namespace {
 
 constexpr int kCopyLanes = 4;  // lanes per cell of the download gather
+constexpr float kBelowOne = 0.99999994f;  // the largest float below 1
 constexpr int WY = 6;  // window rows: y0-1 .. y0+4
 
 struct Args32 {
@@ -66,6 +67,7 @@ struct Args32 {
   int nx, ny, nxg;
   float qd, dtdx, dtdy, c;
   double *ake_partial;
+  double *lost;  // count of particles a regrouping push could not place
 };
 
 // the pairs of one ensemble push (a __grid_constant__ kernel parameter)
@@ -76,6 +78,7 @@ struct EnsPush32 {
   int segs[kEnsMaxPairs];
   Args32 pair[kEnsMaxPairs];
 };
+static_assert(sizeof(EnsPush32) <= 32764, "kernel parameters are limited to 32764 bytes");
 
 struct Wts {
   int i;          // array index of the middle node
@@ -516,8 +519,16 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
                   cuz, cinv, b, akel, stay_new, o);
     if (INPLACE) {
       if (act) {
-        a.B[i] = o.mx + (float)o.ox;
-        a.B[cap + i] = o.my + (float)o.oy;
+        // the offset relative to the group cell, kept in the cell the push
+        // counted for the next grouping (group cell + o + no): when that is
+        // the group cell itself, 1 plus a tiny negative move can round to
+        // exactly 1, which would read as the next cell (every other case is
+        // exact or rounds within its cell)
+        float xn = o.mx + (float)o.ox, yn = o.my + (float)o.oy;
+        if (o.ox + (o.ncx - o.cx) == 0) xn = fminf(xn, kBelowOne);
+        if (o.oy + (o.ncy - o.cy) == 0) yn = fminf(yn, kBelowOne);
+        a.B[i] = xn;
+        a.B[cap + i] = yn;
         a.B[2 * cap + i] = o.ux;
         a.B[3 * cap + i] = o.uy;
         a.B[4 * cap + i] = o.uz;
@@ -528,14 +539,22 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
       // segment in processing order (a running count per group, no atomics);
       // the few that came from another cell's range fill it from the back
       const unsigned inm = __ballot_sync(0xffffffffu, act && o.in_cell_old) & gmask;
+      int64_t pos = -1;
       if (act) {
-        int64_t pos;
         if (o.in_cell_old)
           pos = (int64_t)front + home_count + __popc(inm & lt);
         else {
           const int key = wrap(o.cy, ny) * nx + wrap(o.cx, nx);  // the start cell's key
           pos = (int64_t)a.offB[key + 1] - 1 - atomicAdd(a.cursor + key, 1);
         }
+        // a guard: the counts of the last push place every particle inside
+        // the buffer; a position outside it is counted and not written
+        if (pos < 0 || pos >= cap) {
+          atomicAdd(a.lost, 1.0);
+          pos = -1;
+        }
+      }
+      if (pos >= 0) {
         a.B[pos] = o.mx;
         a.B[cap + pos] = o.my;
         a.B[2 * cap + pos] = o.ux;
@@ -711,6 +730,27 @@ __global__ void k_prescale_f32(const float *__restrict__ fld, float2 *__restrict
   s[2 * w + k] = make_float2(ae * fld[EM2G_EY * w + k], ae * fld[EM2G_BY * w + k] + ty);
 }
 
+// The cell and FP32 offset of an FP64 position x in [0, n + 1/2) of a
+// periodic axis of n cells, as the push will read them back: the offset
+// x - cell rounded to FP32 can come out as exactly 1, which the push takes
+// for the next cell, so such a position is given to the next cell at offset
+// 0 (a shift below 2^-25 cells).  The histogram and the scatter of an
+// upload both use this, so that the counts match where particles go.
+struct CellF32 {
+  int c;    // cell, wrapped into 0 .. n-1
+  float r;  // offset in [0, 1) relative to the unwrapped cell
+};
+__device__ __forceinline__ CellF32 cell_f32(double x, int n) {
+  int c = (int)x;
+  float r = (float)(x - c);
+  if (r >= 1.0f) {
+    c += 1;
+    r = 0.0f;
+  }
+  if (c >= n) c -= n;
+  return CellF32{c, r};
+}
+
 // FP64 (x, y, vx, vy, vz, gamma) staging -> histogram of cells
 __global__ void k_hist64(const double *__restrict__ st, int64_t n, int nx, int ny,
                          int32_t *cnt) {
@@ -718,7 +758,8 @@ __global__ void k_hist64(const double *__restrict__ st, int64_t n, int nx, int n
   const bool active = j < n;
   const unsigned am = __ballot_sync(0xffffffffu, active);
   if (!active) return;
-  agg_atomic_add(cnt, cell_key(st[j], st[n + j], nx, ny), am);
+  const CellF32 cx = cell_f32(st[j], nx), cy = cell_f32(st[n + j], ny);
+  agg_atomic_add(cnt, cy.c * nx + cx.c, am);
 }
 
 // FP64 staging -> cell-grouped FP32 layout (slot j keeps its slot number)
@@ -729,14 +770,12 @@ __global__ void k_scatter_to_f32(const double *__restrict__ st, int64_t n, int n
   const bool active = j < n;
   const unsigned am = __ballot_sync(0xffffffffu, active);
   if (!active) return;
-  const double x = st[j], y = st[n + j];
-  const int key = cell_key(x, y, nx, ny);
+  const CellF32 cx = cell_f32(st[j], nx), cy = cell_f32(st[n + j], ny);
+  const int key = cy.c * nx + cx.c;
   const int64_t pos = (int64_t)off[key] + agg_atomic_add(cursor, key, am);
-  int cx = (int)x, cy = (int)y;
   const double g = st[5 * n + j];
-  // offsets relative to the (unwrapped) cell holding x, y
-  P[pos] = (float)(x - cx);
-  P[cap + pos] = (float)(y - cy);
+  P[pos] = cx.r;
+  P[cap + pos] = cy.r;
   P[2 * cap + pos] = (float)(st[2 * n + j] * g);
   P[3 * cap + pos] = (float)(st[3 * n + j] * g);
   P[4 * cap + pos] = (float)(st[4 * n + j] * g);
@@ -757,14 +796,11 @@ __global__ void k_scatter_rec(const double *__restrict__ st, int64_t n, int nx, 
   const bool active = j < n;
   const unsigned am = __ballot_sync(0xffffffffu, active);
   if (!active) return;
-  const double x = st[j], y = st[n + j];
-  const int key = cell_key(x, y, nx, ny);
+  const CellF32 cx = cell_f32(st[j], nx), cy = cell_f32(st[n + j], ny);
+  const int key = cy.c * nx + cx.c;
   const int64_t pos = (int64_t)off[key] + agg_atomic_add(cursor, key, am);
-  const int cx = (int)x, cy = (int)y;
   const double g = st[5 * n + j];
-  // offsets relative to the (unwrapped) cell holding x, y
-  rec[2 * pos] = make_float4((float)(x - cx), (float)(y - cy), (float)(st[2 * n + j] * g),
-                             (float)(st[3 * n + j] * g));
+  rec[2 * pos] = make_float4(cx.r, cy.r, (float)(st[2 * n + j] * g), (float)(st[3 * n + j] * g));
   rec[2 * pos + 1] = make_float4((float)(st[4 * n + j] * g), __int_as_float((int32_t)j), 0.f, 0.f);
 }
 
@@ -890,6 +926,7 @@ int launch_push_cells_f32(em2g_ctx *c, int isp) {
   a.dtdy = (float)(c->P.dt / c->P.dy);
   a.c = (float)c->P.c;
   a.ake_partial = c->red;
+  a.lost = c->dev_out + kDevLost;
   const Variant32 &V = kVariants32[c->variant < num_variants_f32() ? c->variant : 0];
   const int threads = V.tcx * V.g;
   const dim3 grid((unsigned)((c->g.nx + V.tcx - 1) / V.tcx), (unsigned)c->g.ny);
@@ -1027,6 +1064,7 @@ int ens_push(em2g_ens *e, int bp, int cp, bool inplace) {
       a.dtdy = (float)(R.P.dt / R.P.dy);
       a.c = (float)R.P.c;
       a.ake_partial = e->red + R.red_off[s];
+      a.lost = e->dev_out + (int64_t)r * kEnsOut + kEnsLost;
       const int segs = (R.g.nx + V.tcx - 1) / V.tcx;
       P->tile0[p] = t;
       P->segs[p] = segs;

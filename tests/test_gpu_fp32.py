@@ -191,3 +191,52 @@ def test_sort_interval_rejected_beyond_the_drift_bound(gpu):
             g.set_sort_interval(10)
         assert ei.value.status == _lib.ERR_INVALID
         g.set_sort_interval(9)
+
+
+def test_offsets_that_round_up_to_the_next_cell(gpu, oracle_lib):
+    """Positions a hair below a cell edge, whose FP32 offset rounds to
+    exactly 1, belong to the next cell in the FP32 layout: the upload groups
+    them there, and in-place pushes keep each offset inside the cell they
+    counted for the next grouping.  Every particle is placed (a push that
+    found no place for one would fail the step), and the run tracks the
+    oracle to the mixed path's bounds."""
+    import oracle
+    from maccpic_b200 import _lib
+    from maccpic_b200.em2 import Em2Gpu, RunParams
+    nx, ny, n = 32, 16, 4000
+    kw = dict(nx=nx, ny=ny, dx=0.5, dy=0.5, dt=0.05, qm=[-1.0, 1 / 25.0], q=[-0.02, 0.02],
+              dn=[1.0, 1.0], am=[0.02, 0.5], isav=4)
+    rng = np.random.default_rng(5)
+    x, y = rng.random(n) * nx, rng.random(n) * ny
+    k = np.arange(600)
+    x[:600] = (k % nx) + 1 - 1e-12  # includes nx - 1e-12, which wraps to cell 0
+    y[300:900] = (k % ny) + 1 - 1e-12
+    parts = []
+    for s in range(2):  # both species on the same positions: no net charge
+        u = rng.normal(scale=0.2 if s == 0 else 0.04, size=(3, n))
+        g = np.sqrt(1 + (u * u).sum(0))
+        parts.append(np.vstack([x, y, u / g, g]))
+    fld = np.zeros((13, ny + 3, nx + 3))
+    st = oracle_lib.State(oracle.Params(**kw), fld, parts)
+    rp = RunParams(np_max=[n, n], precision=_lib.FP32, **kw)
+    with Em2Gpu(rp) as g:
+        g.set_fields(fld)
+        for s, p in enumerate(parts):
+            g.set_particles(s, p)
+        q0 = g.get_particles(0)
+        d = np.abs(q0[:2] - parts[0][:2])
+        d = np.minimum(d, np.array([[nx], [ny]]) - d)
+        assert d.max() < 1e-6
+        g.set_sort_interval(g.max_sort_interval())
+        for _ in range(12):
+            st.step()
+            g.step(1)
+        for s in range(2):
+            p = g.get_particles(s)
+            d = p[:2] - st.parts[s][:2]
+            d -= np.array([[nx], [ny]]) * np.round(d / np.array([[nx], [ny]]))
+            assert np.abs(d).max() < 1e-3
+        got = g.get_fields()
+        for f in range(6):
+            scale = max(np.abs(st.fld[f]).max(), 1e-30)
+            assert np.abs(got[f] - st.fld[f]).max() / scale < 1e-2, f

@@ -408,3 +408,46 @@ def test_invalid_fields_leave_the_state(gpu, precision):
         with pytest.raises(Em2gError):
             g.set_particles(1, bad)
         g.step(1)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("case", ["vacuum", "pair"])
+def test_empty_and_single_particle_species(gpu, oracle_lib, precision, case):
+    """Species holding no particle ("vacuum": the fields alone) or a single
+    one ("pair": one electron at x = nx - 1e-12, which FP32 rounds onto the
+    next cell's edge, and one ion, so that the periodic Poisson problem stays
+    solvable) step like the oracle on either path: the grouping, scans,
+    pushes and copies at their empty and one-element edges.  FP64 to the
+    file's tolerance, with the oracle's CG iteration counts; FP32 to the
+    mixed path's bounds (tests/test_gpu_fp32.py: its CG may stop a few
+    iterations apart, each solve meeting mean r^2 < 1e-9): 1e-3 of a field's
+    max |value|, 1e-3 relative on ake and velocities, 1e-4 cells."""
+    import dataclasses
+    from maccpic_b200 import _lib
+    op, rp, fld, parts = random_case(nx=40, ny=24, n=16)
+    k = 0 if case == "vacuum" else 1
+    parts = [parts[0][:, 3:3 + k].copy(), parts[1][:, 5:5 + k].copy()]
+    fp32 = precision == "fp32"
+    rp = dataclasses.replace(rp, np_max=[1, 1], precision=_lib.FP32 if fp32 else _lib.FP64)
+    st = oracle_lib.State(op, fld, parts)
+    with make_gpu(rp, fld, parts) as g:
+        for s in range(2):
+            assert g.get_particles(s).shape == (6, k)
+        for _ in range(5):
+            r_ref = st.step()
+            r = g.step(1)
+            assert r["cg_iters"] < 1000 and r_ref["cg_iters"] < 1000
+            if not fp32:
+                assert r["cg_iters"] == r_ref["cg_iters"]
+            np.testing.assert_allclose(r["ake"], r_ref["ake"], rtol=1e-3 if fp32 else 1e-12)
+        got = g.get_fields()
+        for f in range(6):
+            assert rel(got[f], st.fld[f]) < (1e-3 if fp32 else TOL), f
+        n = np.array([[op.nx], [op.ny]])
+        for s in range(2):
+            p = g.get_particles(s)
+            assert p.shape == (6, k)
+            d = p[:2] - st.parts[s][:2]
+            d -= n * np.round(d / n)
+            assert d.size == 0 or np.abs(d).max() < (1e-4 if fp32 else 1e-12)
+            np.testing.assert_allclose(p[2:], st.parts[s][2:], rtol=1e-3 if fp32 else 1e-12)
