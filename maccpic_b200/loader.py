@@ -94,7 +94,7 @@ class HarrisConfig:
         return RunParams(nx=self.nx, ny=self.ny, dx=self.dx, dy=self.dx, dt=self.dt,
                          qm=qm, q=q, dn=dn, am=am,
                          np_max=np_max or [n, n], isav=self.isav, **kw)
-
+# the benchmark and test workloads (synthetic, seeded)
 
 # BASELINE workloads (synthetic, seeded)
 PRESETS = {

@@ -5,7 +5,7 @@ bounds below are the ones the mixed path is held to:
     cells, velocities to < 1e-6 relative;
   * after 50 steps of the double-Harris workload the field energy differs
     from the FP64 oracle's by < 1e-4 relative and E, B by < 1e-2 of their
-    max |value| (the north-star target is 1e-3 on the field energy).
+    max |value| (the mixed path is meant to stay within 1e-3 on the field energy).
 """
 import numpy as np
 import pytest

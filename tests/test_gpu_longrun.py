@@ -1,4 +1,4 @@
-"""A whole run against the oracle, judged by the seed-to-seed spread.
+"""A whole run against the oracle, compared within the seed-to-seed spread.
 
 The double-Harris workload at 256x128 cells, 16 particles per cell per
 species, runs 300 steps on the GPU (FP64, em2's arithmetic) and on the oracle
