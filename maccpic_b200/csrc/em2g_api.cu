@@ -343,6 +343,7 @@ int em2g_create(const em2g_params *p, em2g_ctx **out) {
   c->red_blocks = (int)((maxn + 255) / 256);
   if (c->red_blocks < 6 * kEnergyBlocks) c->red_blocks = 6 * kEnergyBlocks;
   ALLOC(c->red, sizeof(double) * c->red_blocks);
+  ALLOC(c->ake_l1, sizeof(double) * kAkeBlocks);
   ALLOC(c->dev_out, sizeof(double) * kDevOut);
 #undef ALLOC
   e = cudaMallocHost((void **)&c->host_out, sizeof(double) * kDevOut);
@@ -401,6 +402,7 @@ int em2g_destroy(em2g_ctx *c) {
     cudaFree(S.slot_alt);
   }
   cudaFree(c->red);
+  cudaFree(c->ake_l1);
   cudaFree(c->spec);
   cudaFree(c->staging);
   cudaFree(c->dev_out);

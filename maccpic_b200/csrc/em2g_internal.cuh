@@ -97,6 +97,7 @@ struct em2g_ctx {
   // reductions: ake partials per species, energy partials
   double *red = nullptr;       // reduction scratch
   int red_blocks = 0;
+  double *ake_l1 = nullptr;    // kAkeBlocks first-level sums of the ake partials
   double *dev_out = nullptr;   // small device results (ake[4], e[6])
   double *host_out = nullptr;  // pinned mirror of dev_out
   int num_sms = 0;
@@ -125,6 +126,10 @@ namespace em2g {
 int launch_prescale(em2g_ctx *c, int isp);
 // mode bit 1: move (gather + Boris); bit 2: curnt (deposit, move, deposit)
 int launch_push_f64(em2g_ctx *c, int isp, int mode);
+// the kinetic energy of species isp from the push's nblocks_used partials
+// in c->red: summed in a fixed order (kAkeBlocks blocks over contiguous
+// chunks, then one block), so that it does not change from run to run
+constexpr int kAkeBlocks = 256;
 int launch_ake_finish(em2g_ctx *c, int isp, int nblocks_used);
 int fields_f64(em2g_ctx *c, int it, bool want_energies, int *cg_iters);
 int smooth2_f64(em2g_ctx *c, double *a);

@@ -86,6 +86,24 @@ __global__ void k_prescale(const double *__restrict__ fld, double *__restrict__ 
   s[5 * w + k] = ae * fld[EM2G_BZ * w + k];
 }
 
+// first level of the ake sum: block b adds the partials of its contiguous
+// chunk, in a fixed order, into l1[b]
+__global__ void k_ake_level1(const double *__restrict__ partial, int nb, double *l1) {
+  __shared__ double red[32];
+  const int chunk = (nb + (int)gridDim.x - 1) / (int)gridDim.x;
+  const int lo = (int)blockIdx.x * chunk, hi = min(nb, lo + chunk);
+  double v = 0.0;
+  for (int i = lo + (int)threadIdx.x; i < hi; i += blockDim.x) v += partial[i];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (threadIdx.x == 0) l1[blockIdx.x] = v;
+  }
+}
+
 // one block: sum the per-block partials in a fixed order, times am*dn
 __global__ void k_ake_finish(const double *__restrict__ partial, int nb, double amdn_am,
                              double amdn_dn, double *out) {
@@ -152,8 +170,17 @@ int launch_push_f64(em2g_ctx *c, int isp, int mode) {
 }
 
 int launch_ake_finish(em2g_ctx *c, int isp, int nblocks_used) {
-  k_ake_finish<<<1, 1024, 0, c->stream>>>(c->red, nblocks_used, c->P.am[isp], c->P.dn[isp],
-                                          c->dev_out + isp);
+  const double *src = c->red;
+  int n = nblocks_used;
+  // many partials (the fast pushes write one per warp of a row segment):
+  // first spread the reading over kAkeBlocks blocks
+  if (n > 16 * kAkeBlocks) {
+    k_ake_level1<<<kAkeBlocks, 256, 0, c->stream>>>(c->red, n, c->ake_l1);
+    c->launches += 1;
+    src = c->ake_l1;
+    n = kAkeBlocks;
+  }
+  k_ake_finish<<<1, 1024, 0, c->stream>>>(src, n, c->P.am[isp], c->P.dn[isp], c->dev_out + isp);
   c->launches += 1;
   EM2G_CUDA(cudaGetLastError());
   return EM2G_OK;
