@@ -69,7 +69,8 @@ struct em2g_ens {
   int parity = 0, cparity = 0;
   int sort_interval = 1;  // regroup on every sort_interval-th push
   int since_sort = 0;     // in-place pushes since the last regrouping
-  double *staging = nullptr;  // 6 * staging_n doubles (uploads, downloads)
+  double *staging = nullptr;  // 10 * staging_n doubles: 6 per particle of FP64 values,
+                              // then a 32-byte record each (uploads, downloads)
   int64_t staging_n = 0;
   int *counter = nullptr;     // the persistent push's segment counter
   int *d_it = nullptr;        // the step counter as the field kernels read it
@@ -88,7 +89,7 @@ namespace em2g {
 
 // push_fast_f32.cu
 int ens_push(em2g_ens *e, int bp, int cp, bool inplace);
-int ens_upload_pair(em2g_ens *e, int r, int s, const double *staging);
+int ens_upload_pair(em2g_ens *e, int r, int s, double *staging);
 int ens_download_pair(em2g_ens *e, int r, int s, double *staging);
 int ens_push_kernels_per_step(const em2g_ens *e, bool inplace);
 // fields_ens.cu

@@ -92,12 +92,14 @@ int capture_step(em2g_ens *e, bool inplace) {
   return EM2G_OK;
 }
 
+// staging for n particles: 6*n FP64 values, then 32*n bytes of records
 int ensure_staging(em2g_ens *e, int64_t n) {
   if (n <= e->staging_n) return EM2G_OK;
+  EM2G_CUDA(cudaStreamSynchronize(e->stream));  // the old buffer may still be read
   cudaFree(e->staging);
   e->staging = nullptr;
   e->staging_n = 0;
-  EM2G_CUDA(cudaMalloc(&e->staging, sizeof(double) * 6 * n));
+  EM2G_CUDA(cudaMalloc(&e->staging, sizeof(double) * 10 * n));
   e->staging_n = n;
   return EM2G_OK;
 }

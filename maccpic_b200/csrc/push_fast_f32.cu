@@ -762,43 +762,26 @@ __global__ void k_hist64(const double *__restrict__ st, int64_t n, int nx, int n
   agg_atomic_add(cnt, cy.c * nx + cx.c, am);
 }
 
-// FP64 staging -> cell-grouped FP32 layout (slot j keeps its slot number)
-__global__ void k_scatter_to_f32(const double *__restrict__ st, int64_t n, int nx, int ny,
-                                 const int32_t *__restrict__ off, int32_t *cursor, float *P,
-                                 int32_t *slot, int64_t cap) {
-  const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const bool active = j < n;
-  const unsigned am = __ballot_sync(0xffffffffu, active);
-  if (!active) return;
-  const CellF32 cx = cell_f32(st[j], nx), cy = cell_f32(st[n + j], ny);
-  const int key = cy.c * nx + cx.c;
-  const int64_t pos = (int64_t)off[key] + agg_atomic_add(cursor, key, am);
-  const double g = st[5 * n + j];
-  P[pos] = cx.r;
-  P[cap + pos] = cy.r;
-  P[2 * cap + pos] = (float)(st[2 * n + j] * g);
-  P[3 * cap + pos] = (float)(st[3 * n + j] * g);
-  P[4 * cap + pos] = (float)(st[4 * n + j] * g);
-  slot[pos] = (int32_t)j;
-}
-
-// Transfers between the caller's slot order and the cell-grouped layout of
-// a single context go through one 32-byte record per particle (a whole
+// Transfers between the caller's slot order and the cell-grouped layout
+// (of a context, or of one (run, species) pair of an ensemble) go through
+// one 32-byte record per particle (a whole
 // sector, two 16-byte stores): moving a particle to a random position then
 // writes one full sector, where six separate arrays would write six partial
 // ones (each a read-modify-write in L2).  rec holds 2*n float4.
 //
 // FP64 slot-order staging -> records in cell-grouped order:
-// (xr, yr, ux, uy), (uz, slot, 0, 0)
+// (xr, yr, ux, uy), (uz, slot, 0, 0); record pos - base for buffer position
+// pos (base: the pair's first position in an ensemble's buffers, else 0)
 __global__ void k_scatter_rec(const double *__restrict__ st, int64_t n, int nx, int ny,
-                              const int32_t *__restrict__ off, int32_t *cursor, float4 *rec) {
+                              const int32_t *__restrict__ off, int32_t *cursor, int64_t base,
+                              float4 *rec) {
   const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const bool active = j < n;
   const unsigned am = __ballot_sync(0xffffffffu, active);
   if (!active) return;
   const CellF32 cx = cell_f32(st[j], nx), cy = cell_f32(st[n + j], ny);
   const int key = cy.c * nx + cx.c;
-  const int64_t pos = (int64_t)off[key] + agg_atomic_add(cursor, key, am);
+  const int64_t pos = (int64_t)off[key] + agg_atomic_add(cursor, key, am) - base;
   const double g = st[5 * n + j];
   rec[2 * pos] = make_float4(cx.r, cy.r, (float)(st[2 * n + j] * g), (float)(st[3 * n + j] * g));
   rec[2 * pos + 1] = make_float4((float)(st[4 * n + j] * g), __int_as_float((int32_t)j), 0.f, 0.f);
@@ -853,32 +836,6 @@ __global__ void k_rec_to_fp64(const float4 *__restrict__ rec, int64_t n, double 
   st[3 * n + s] = uy / g;
   st[4 * n + s] = uz / g;
   st[5 * n + s] = g;
-}
-
-// cell-grouped FP32 -> FP64 staging in slot order: x, y, vx, vy, vz, gamma
-__global__ void k_gather_from_f32(const float *__restrict__ P, const int32_t *__restrict__ slot,
-                                  const int32_t *__restrict__ off, int64_t cap, int nx, int ny,
-                                  double *st, int64_t n) {
-  const int64_t cell = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kCopyLanes;
-  const int gl = threadIdx.x & (kCopyLanes - 1);
-  if (cell >= (int64_t)nx * ny) return;
-  const int kx = (int)(cell % nx), ky = (int)(cell / nx);
-  for (int32_t i = off[cell] + gl; i < off[cell + 1]; i += kCopyLanes) {
-    double x = kx + (double)P[i], y = ky + (double)P[cap + i];
-    if (x < 0.0) x += nx;
-    if (x >= nx) x -= nx;
-    if (y < 0.0) y += ny;
-    if (y >= ny) y -= ny;
-    const double ux = P[2 * cap + i], uy = P[3 * cap + i], uz = P[4 * cap + i];
-    const double g = sqrt(1.0 + ux * ux + uy * uy + uz * uz);
-    const int64_t s = slot[i];
-    st[s] = x;
-    st[n + s] = y;
-    st[2 * n + s] = ux / g;
-    st[3 * n + s] = uy / g;
-    st[4 * n + s] = uz / g;
-    st[5 * n + s] = g;
-  }
 }
 
 }  // namespace
@@ -974,7 +931,7 @@ int upload_f32(em2g_ctx *c, int isp, const double *staging, int64_t n, void *rec
   if (rc) return rc;
   if (n > 0) {
     float4 *r = static_cast<float4 *>(rec);
-    k_scatter_rec<<<nb, 256, 0, c->stream>>>(staging, n, c->g.nx, c->g.ny, S.off, S.cursor, r);
+    k_scatter_rec<<<nb, 256, 0, c->stream>>>(staging, n, c->g.nx, c->g.ny, S.off, S.cursor, 0, r);
     EM2G_CUDA(cudaGetLastError());
     k_rec_to_soa<<<nb, 256, 0, c->stream>>>(r, n, S.p32, S.slot, S.cap);
     EM2G_CUDA(cudaGetLastError());
@@ -1090,9 +1047,10 @@ int ens_push(em2g_ens *e, int bp, int cp, bool inplace) {
   return EM2G_OK;
 }
 
-// pair (r, s) from FP64 staging (6*n doubles, slot order) into the current
-// buffers: histogram, this pair's offsets from its first slot, scatter
-int ens_upload_pair(em2g_ens *e, int r, int s, const double *staging) {
+// pair (r, s) from FP64 staging (6*n doubles, slot order, then 32*n bytes
+// for the records) into the current buffers: histogram, this pair's
+// offsets from its first position, records in cell order, transpose
+int ens_upload_pair(em2g_ens *e, int r, int s, double *staging) {
   const EnsRun &R = e->runs[r];
   const int64_t n = R.n[s], nc = (int64_t)R.g.nx * R.g.ny, c0 = R.cell0[s];
   float *P = e->parity ? e->p32_alt : e->p32;
@@ -1106,14 +1064,19 @@ int ens_upload_pair(em2g_ens *e, int r, int s, const double *staging) {
   if (n > 0) k_hist64<<<nb, 256, 0, st>>>(staging, n, R.g.nx, R.g.ny, cnt + c0);
   int rc = scan_counts(cnt + c0, off + c0, nc, (int32_t)R.base[s], e->scan_tmp, st);
   if (rc) return rc;
-  if (n > 0)
-    k_scatter_to_f32<<<nb, 256, 0, st>>>(staging, n, R.g.nx, R.g.ny, off + c0, e->cursor + c0,
-                                         P, slot, e->cap);
+  if (n > 0) {
+    float4 *rec = reinterpret_cast<float4 *>(staging + 6 * n);
+    k_scatter_rec<<<nb, 256, 0, st>>>(staging, n, R.g.nx, R.g.ny, off + c0, e->cursor + c0,
+                                      R.base[s], rec);
+    EM2G_CUDA(cudaGetLastError());
+    k_rec_to_soa<<<nb, 256, 0, st>>>(rec, n, P + R.base[s], slot + R.base[s], e->cap);
+  }
   EM2G_CUDA(cudaGetLastError());
   return EM2G_OK;
 }
 
 // pair (r, s) from the current buffers to FP64 staging in slot order
+// (6*n doubles, then 32*n bytes for the records)
 int ens_download_pair(em2g_ens *e, int r, int s, double *staging) {
   const EnsRun &R = e->runs[r];
   const int64_t n = R.n[s];
@@ -1121,9 +1084,12 @@ int ens_download_pair(em2g_ens *e, int r, int s, double *staging) {
   const float *P = e->parity ? e->p32_alt : e->p32;
   const int32_t *slot = e->parity ? e->slot_alt : e->slot;
   const int32_t *off = e->parity ? e->off_alt : e->off;
+  float4 *rec = reinterpret_cast<float4 *>(staging + 6 * n);
   const int64_t nb = ((int64_t)R.g.nx * R.g.ny * kCopyLanes + 255) / 256;
-  k_gather_from_f32<<<(unsigned)nb, 256, 0, e->stream>>>(P, slot, off + R.cell0[s], e->cap, R.g.nx,
-                                                          R.g.ny, staging, n);
+  k_grouped_to_rec<<<(unsigned)nb, 256, 0, e->stream>>>(P, slot, off + R.cell0[s], e->cap, R.g.nx,
+                                                         R.g.ny, rec);
+  EM2G_CUDA(cudaGetLastError());
+  k_rec_to_fp64<<<(unsigned)((n + 255) / 256), 256, 0, e->stream>>>(rec, n, staging);
   EM2G_CUDA(cudaGetLastError());
   return EM2G_OK;
 }
