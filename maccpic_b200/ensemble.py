@@ -22,7 +22,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import NFIELD, check
-from .em2 import RunParams, _dp, stream_handle
+from .em2 import RunParams, _check_out, _dp, stream_handle
 
 
 class Em2Ensemble:
@@ -68,8 +68,14 @@ class Em2Ensemble:
             raise ValueError(f"fields must have shape {(NFIELD,) + self.runs[run].shape}")
         check(self._L.em2g_ens_set_fields(self._h, run, _dp(a)))
 
-    def get_fields(self, run: int) -> np.ndarray:
-        out = np.empty((NFIELD,) + self.runs[run].shape)
+    def get_fields(self, run: int, out: np.ndarray | None = None) -> np.ndarray:
+        """Run `run`'s 13 arrays; into `out` (C-contiguous float64 of shape
+        (13, ny+3, nx+3), e.g. pinned memory the caller keeps) if given."""
+        shape = (NFIELD,) + self.runs[run].shape
+        if out is None:
+            out = np.empty(shape)
+        else:
+            _check_out(out, shape)
         check(self._L.em2g_ens_get_fields(self._h, run, _dp(out)))
         return out
 
@@ -91,11 +97,16 @@ class Em2Ensemble:
         ptrs = [C.c_void_p(part[k].data_ptr()) for k in range(6)]
         check(self._L.em2g_ens_set_particles_device(self._h, run, isp, part.shape[1], *ptrs))
 
-    def get_particles(self, run: int, isp: int) -> np.ndarray:
+    def get_particles(self, run: int, isp: int, out: np.ndarray | None = None) -> np.ndarray:
+        """(6, n) = x, y, vx, vy, vz, gamma of run `run`, species `isp`, in
+        slot order; into `out` (C-contiguous float64 of that shape) if given."""
         n = C.c_int64()
         check(self._L.em2g_ens_get_particles(self._h, run, isp, C.byref(n),
                                              *([None] * 6)))
-        out = np.empty((6, n.value))
+        if out is None:
+            out = np.empty((6, n.value))
+        else:
+            _check_out(out, (6, n.value))
         check(self._L.em2g_ens_get_particles(self._h, run, isp, C.byref(n),
                                              *[_dp(out[k]) for k in range(6)]))
         return out

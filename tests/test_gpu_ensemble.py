@@ -260,3 +260,25 @@ def test_sort_interval_rules(gpu):
     runs[1] = dataclasses.replace(runs[1], sort_interval=2)
     with Em2Ensemble(runs) as f:
         assert all(r.sort_interval == 2 for r in f.runs)
+
+
+def test_outputs_into_caller_buffers(gpu):
+    """The ensemble's getters fill a caller's buffer (pinned memory here) with
+    what they would return, as a context's do."""
+    import torch
+    cfgs = _cfgs()[:2]
+    states = [_state(c) for c in cfgs]
+    with _ensemble(cfgs, states) as e:
+        e.step(2)
+        for r in range(2):
+            want = e.get_fields(r)
+            out = torch.empty(want.shape, dtype=torch.float64).pin_memory().numpy()
+            assert e.get_fields(r, out=out) is out
+            np.testing.assert_array_equal(out, want)
+            for s in range(2):
+                want = e.get_particles(r, s)
+                out = torch.empty(want.shape, dtype=torch.float64).pin_memory().numpy()
+                e.get_particles(r, s, out=out)
+                np.testing.assert_array_equal(out, want)
+        with pytest.raises(ValueError):
+            e.get_particles(0, 0, out=np.empty((5, 3)))
