@@ -27,17 +27,23 @@
 // y0+4) are staged once in shared memory as (E, B) pairs of the three
 // staggerings, so a gather is 27 shared float2 loads.  A particle still in
 // the lane's cell adds its rho and J into a 49-value register block (Jx 4x3,
-// Jy 3x4, Jz 3x3, rho 4x4); the deposits of one outside it go onto its
-// warp's stack in shared memory and are done with atomics 32 at a time, one
-// per lane.  At the end of the cell the G blocks are summed with shuffles and
-// added to the arrays once.  The gathers, the block updates, the weights and
-// the move use sm_100a's packed FP32 pairs (f32x2).  Each particle is written
-// to the other buffer grouped by the cell it started the step in, its
-// position relative to that cell (front slots by a running count for the
-// common in-cell case, back slots by an atomic for the rest), and the cells
-// of the new positions are counted for the next step's offsets: the counting
-// sort rides along with the push.  Between regroupings (the sort interval)
-// the push updates particles in place instead.
+// Jy 3x4, Jz 3x3, rho 4x4) -- every lane runs the update, with zero charge
+// where its particle is elsewhere or absent; the deposits of one outside it
+// go onto its warp's stack in shared memory and are done with atomics 32 at
+// a time, one per lane.  At the end of the cell the lanes write their blocks
+// into the warp's (drained) stack and each lane of the cell's group adds
+// whole rows over the group before adding them to the arrays once.  Cells
+// are handled unwrapped (group cell + offset) and wrapped only where an array
+// is indexed.  The gathers, the block updates, the weights and the move use
+// sm_100a's packed FP32 pairs (f32x2).  Each particle is written to the other
+// buffer grouped by the cell it started the step in, its position relative
+// to that cell (front slots by a running count for the common in-cell case,
+// back slots by an atomic for the rest), and the cells of the new positions
+// are counted for the next step's offsets: the counting sort rides along
+// with the push.  The cell a particle is counted in is always the one its
+// stored FP32 offset reads back as (uploads and in-place writes keep to
+// that), and a regrouping push writes nothing outside the buffer.  Between
+// regroupings (the sort interval) the push updates particles in place.
 #include <algorithm>
 #include <memory>
 
