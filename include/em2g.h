@@ -47,7 +47,9 @@ enum em2g_status {
   EM2G_ERR_INVALID = 1,     /* bad argument or parameter */
   EM2G_ERR_CUDA = 2,        /* a CUDA runtime call failed */
   EM2G_ERR_NOMEM = 3,       /* device allocation failed */
-  EM2G_ERR_RANGE = 4,       /* particle outside the grid, count > capacity */
+  EM2G_ERR_RANGE = 4,       /* particle outside the grid, count > capacity; from a
+                               step: a regrouping push found no place for a particle
+                               (the particle state is then inconsistent) */
   EM2G_ERR_TIMEOUT = 5,     /* a bounded device-side wait gave up */
   EM2G_ERR_NONFINITE = 6    /* NaN/Inf found in host-provided input */
 };
