@@ -331,12 +331,12 @@ struct PartOut {
 // Gather, Boris, move and the in-cell deposits of one particle at (xr, yr)
 // relative to the group cell (kx, ky) with momentum u; `act` false makes it
 // a dry run on harmless input (no deposits, no energy).  cinv = 1/c.
-template <int TCX>
-__device__ __forceinline__ void push_one(const Args32 &a, float2 (*win)[WY][TCX + 5], int x0,
+template <int WXW>
+__device__ __forceinline__ void push_one(const Args32 &a, float2 (*win)[WY][WXW], int x0,
                                          int y0, int kx, int ky, bool act, float xr, float yr,
                                          float ux, float uy, float uz, float cinv, Block32 &b,
                                          double &akel, int &stay_new, PartOut &o) {
-  constexpr int WX = TCX + 5;
+  constexpr int WX = WXW;
   const int nx = a.nx, ny = a.ny, nxg = a.nxg;
   // the cell the particle is in now (it may have left cell k last step)
   const int ox = floor_small(xr), oy = floor_small(yr);
@@ -428,32 +428,38 @@ __device__ __forceinline__ void push_one(const Args32 &a, float2 (*win)[WY][TCX 
   }
 }
 
-// One row segment: cells x0 .. x0+TCX-1 of row y0, by a CTA of TCX*G
-// threads; `blk` numbers the segment for the kinetic-energy partials.
+// One row segment: cells x0 .. x0+NC*TCX-1 of row y0, by a CTA of TCX*G
+// threads; `blk` numbers the segment for the kinetic-energy partials.  Each
+// group of G lanes takes NC cells one after the other (x0 + g, then
+// x0 + TCX + g, ..): a warp runs as long as its groups' largest total, and
+// totals over several cells vary relatively less than single cells' counts,
+// so fewer lanes wait.
 // INPLACE: a step between regroupings -- every particle keeps its slot in
 // A (B == A) and its position stays relative to its group cell, so the
 // offsets drift by at most c*dt/dx per step (the interval is bounded so
 // that they stay in (-1, 2)); the counts of the new cells are still taken.
-template <int TCX, int G, bool INPLACE>
+template <int TCX, int G, int NC, bool INPLACE>
 __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, int64_t blk,
-                                             float2 (*win)[WY][TCX + 5], WarpScratch *ws) {
+                                             float2 (*win)[WY][NC * TCX + 5], WarpScratch *ws) {
   constexpr int kThreads = TCX * G;
-  constexpr int WX = TCX + 5;  // window columns: x0-1 .. x0+TCX+3
+  constexpr int WX = NC * TCX + 5;  // window columns: x0-1 .. x0+NC*TCX+3
   const int nx = a.nx, ny = a.ny, nxg = a.nxg;
   const int lane = threadIdx.x & 31, gl = lane & (G - 1);
-  const int kx = x0 + (int)(threadIdx.x / G), ky = y0;
-  const bool valid = kx < nx;
-  const int kxs = valid ? kx : nx - 1;  // the cell lanes past the grid's edge work on
-  const int64_t cell = (int64_t)ky * nx + kx;
+  int kx = x0 + (int)(threadIdx.x / G);  // this group's cell in the current pass
+  const int ky = y0;
+  bool valid = kx < nx;
+  int kxs = valid ? kx : nx - 1;  // the cell lanes past the grid's edge work on
+  int64_t cell = (int64_t)ky * nx + kx;
   const int64_t cap = a.cap;
   const unsigned gmask = ((1u << G) - 1u) << (lane & ~(G - 1));  // this lane's group
-  // The segment's start has three independent global loads -- the cell's
-  // range, the (E, B) window and the first particle -- issued together
-  // before the first wait: the range, then the window into registers, then
-  // the particle (once the range is in), then the window into shared memory.
-  const int32_t beg = valid ? a.offA[cell] : 0;
-  const int32_t front = (!INPLACE && valid) ? a.offB[cell] : 0;  // cell k's first slot in B
-  const int32_t end = valid ? a.offA[cell + 1] : 0;
+  // The segment's start has three independent global loads -- the first
+  // cell's range, the (E, B) window and the first particle -- issued
+  // together before the first wait: the range, then the window into
+  // registers, then the particle (once the range is in), then the window
+  // into shared memory.
+  int32_t beg = valid ? a.offA[cell] : 0;
+  int32_t front = (!INPLACE && valid) ? a.offB[cell] : 0;  // cell k's first slot in B
+  int32_t end = valid ? a.offA[cell + 1] : 0;
   // the window: array indices x0-1.., y0-1..
   constexpr int kWin = 3 * WY * WX, kWinPer = (kWin + kThreads - 1) / kThreads;
   float2 wv[kWinPer];
@@ -487,6 +493,30 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
   }
   __syncthreads();
 
+  double akel = 0.0;  // this lane's sum of gamma - 1
+  const float cinv = 1.0f / a.c;
+  DepQ &Q = ws[threadIdx.x >> 5].q;
+  int qn = 0;  // entries on this warp's stack (the same in every lane)
+  const unsigned lt = (1u << lane) - 1u;
+  for (int pass = 0; pass < NC; ++pass) {
+  if (pass > 0) {  // the group's next cell: its range and first particle
+    kx += TCX;
+    valid = kx < nx;
+    kxs = valid ? kx : nx - 1;
+    cell = (int64_t)ky * nx + kx;
+    beg = valid ? a.offA[cell] : 0;
+    front = (!INPLACE && valid) ? a.offB[cell] : 0;
+    end = valid ? a.offA[cell + 1] : 0;
+    if (beg + gl < end) {
+      const int32_t j = beg + gl;
+      pxr = a.A[j];
+      pyr = a.A[cap + j];
+      pux = a.A[2 * cap + j];
+      puy = a.A[3 * cap + j];
+      puz = a.A[4 * cap + j];
+      pslot = a.slotA[j];
+    }
+  }
   Block32 b;
   const float2 z2 = make_float2(0.0f, 0.0f);
 #pragma unroll
@@ -497,13 +527,8 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
       b.jzr2[r] = 0.0f;
     }
   }
-  double akel = 0.0;  // this lane's sum of gamma - 1
-  const float cinv = 1.0f / a.c;
   int stay_new = 0;  // particles of this lane whose new position is in cell k
   int home_count = 0;  // particles of this group written to the front of cell k
-  DepQ &Q = ws[threadIdx.x >> 5].q;
-  int qn = 0;  // entries on this warp's stack (the same in every lane)
-  const unsigned lt = (1u << lane) - 1u;
 
   for (int32_t i = beg + gl;; i += G) {
     const bool act = i < end;
@@ -521,7 +546,7 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
     }
     // a lane without a particle runs on a dummy inside a real cell
     PartOut o;
-    push_one<TCX>(a, win, x0, y0, kxs, ky, act, act ? cxr : 0.25f, act ? cyr : 0.25f, cux, cuy,
+    push_one<WX>(a, win, x0, y0, kxs, ky, act, act ? cxr : 0.25f, act ? cyr : 0.25f, cux, cuy,
                   cuz, cinv, b, akel, stay_new, o);
     if (INPLACE) {
       if (act) {
@@ -601,6 +626,7 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
   }
 
   if (lane < qn) drain_entry(a, Q, lane);
+  qn = 0;
   // the group's new-position counts for cell k, and its register blocks
   const int stay = group_sum<G>((float)stay_new) + 0.5f;
   if (valid && gl == 0 && stay > 0) atomicAdd(a.cnt_next + cell, stay);
@@ -638,6 +664,8 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
     __syncwarp();
     if (valid) flush_rows<G, 3, 3>(a.jz, nxg, kx, ky, red, 0, gl, g0);
   }
+  __syncwarp();  // the next pass's stack reuses the scratch just read
+  }  // pass
   // per-warp partial of sum(gamma - 1); no block barrier at the end
   for (int o = 16; o > 0; o >>= 1) akel += __shfl_down_sync(0xffffffffu, akel, o);
   if (lane == 0) a.ake_partial[blk * (kThreads / 32) + (threadIdx.x >> 5)] = akel;
@@ -646,11 +674,11 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
 // TCX cells per CTA (a row segment), G lanes per cell (the particles a CTA
 // has in flight: TCX*G), MINB: CTAs per SM the register allocation must
 // allow -- the autotuner's knobs besides the sort interval
-template <int TCX, int G, int MINB, bool INPLACE>
+template <int TCX, int G, int NC, int MINB, bool INPLACE>
 __global__ void __launch_bounds__(TCX * G, MINB) k_push_cells_f32(Args32 a) {
-  __shared__ float2 win[3][WY][TCX + 5];
+  __shared__ float2 win[3][WY][NC * TCX + 5];
   __shared__ WarpScratch ws[TCX * G / 32];
-  push_segment<TCX, G, INPLACE>(a, (int)blockIdx.x * TCX, (int)blockIdx.y,
+  push_segment<TCX, G, NC, INPLACE>(a, (int)blockIdx.x * (NC * TCX), (int)blockIdx.y,
                                 (int64_t)blockIdx.y * gridDim.x + blockIdx.x, win, ws);
 }
 
@@ -660,10 +688,10 @@ __global__ void __launch_bounds__(TCX * G, MINB) k_push_cells_f32(Args32 a) {
 // CTA takes the next unclaimed segment from a counter until none is left,
 // so runs of unequal size and density share the SMs without a tail per run.
 // INPLACE as for single runs (the ensemble's sort interval).
-template <int TCX, int G, int MINB, bool INPLACE>
+template <int TCX, int G, int NC, int MINB, bool INPLACE>
 __global__ void __launch_bounds__(TCX * G, MINB)
     k_ens_push_f32(const __grid_constant__ EnsPush32 e) {
-  __shared__ float2 win[3][WY][TCX + 5];
+  __shared__ float2 win[3][WY][NC * TCX + 5];
   __shared__ WarpScratch ws[TCX * G / 32];
   __shared__ int s_tile;
   for (;;) {
@@ -679,28 +707,34 @@ __global__ void __launch_bounds__(TCX * G, MINB)
     const int lt = t - e.tile0[lo];
     const int segs = e.segs[lo];
     const int row = lt / segs;
-    push_segment<TCX, G, INPLACE>(e.pair[lo], (lt - row * segs) * TCX, row, lt, win, ws);
+    push_segment<TCX, G, NC, INPLACE>(e.pair[lo], (lt - row * segs) * (NC * TCX), row, lt, win,
+                                      ws);
   }
 }
 
 struct Variant32 {
   const char *name;
-  int tcx, g;
+  int tcx, g;  // lanes per CTA: tcx * g
+  int cells;   // cells per CTA (segment width): tcx * cells per group
   void (*kernel)(Args32);
   void (*kernel_inplace)(Args32);
   void (*ens_kernel)(const EnsPush32);
   void (*ens_kernel_inplace)(const EnsPush32);
 };
-#define EM2G_VARIANT32(T, GG, M)                                                         \
-  {"f32 tcx" #T " g" #GG " minb" #M, T, GG, k_push_cells_f32<T, GG, M, false>,          \
-   k_push_cells_f32<T, GG, M, true>, k_ens_push_f32<T, GG, M, false>,                   \
-   k_ens_push_f32<T, GG, M, true>}
+#define EM2G_VARIANT32N(T, GG, N, M, NAME)                                                 \
+  {NAME, T, GG, T * N, k_push_cells_f32<T, GG, N, M, false>,                                \
+   k_push_cells_f32<T, GG, N, M, true>, k_ens_push_f32<T, GG, N, M, false>,                 \
+   k_ens_push_f32<T, GG, N, M, true>}
+#define EM2G_VARIANT32(T, GG, M) EM2G_VARIANT32N(T, GG, 1, M, "f32 tcx" #T " g" #GG " minb" #M)
 const Variant32 kVariants32[] = {
     EM2G_VARIANT32(32, 4, 4), EM2G_VARIANT32(32, 4, 5), EM2G_VARIANT32(32, 4, 6),
     EM2G_VARIANT32(64, 4, 2), EM2G_VARIANT32(64, 4, 3), EM2G_VARIANT32(32, 8, 2),
     EM2G_VARIANT32(32, 2, 8), EM2G_VARIANT32(64, 2, 4),
+    // two cells per group, one after the other
+    EM2G_VARIANT32N(32, 4, 2, 4, "f32 tcx32x2 g4 minb4"),
 };
 #undef EM2G_VARIANT32
+#undef EM2G_VARIANT32N
 
 // kinetic energy of every pair of an ensemble: block p sums pair p's
 // partials in a fixed order (pic/move.f90:183, :208)
@@ -892,7 +926,7 @@ int launch_push_cells_f32(em2g_ctx *c, int isp) {
   a.lost = c->dev_out + kDevLost;
   const Variant32 &V = kVariants32[c->variant < num_variants_f32() ? c->variant : 0];
   const int threads = V.tcx * V.g;
-  const dim3 grid((unsigned)((c->g.nx + V.tcx - 1) / V.tcx), (unsigned)c->g.ny);
+  const dim3 grid((unsigned)((c->g.nx + V.cells - 1) / V.cells), (unsigned)c->g.ny);
   const int64_t nparts = (int64_t)grid.x * grid.y * (threads / 32);
   if (nparts > c->red_blocks) return fail(EM2G_ERR_RANGE, "grid exceeds reduction scratch");
   const int nb = (int)nparts;
@@ -1028,7 +1062,7 @@ int ens_push(em2g_ens *e, int bp, int cp, bool inplace) {
       a.c = (float)R.P.c;
       a.ake_partial = e->red + R.red_off[s];
       a.lost = e->dev_out + (int64_t)r * kEnsOut + kEnsLost;
-      const int segs = (R.g.nx + V.tcx - 1) / V.tcx;
+      const int segs = (R.g.nx + V.cells - 1) / V.cells;
       P->tile0[p] = t;
       P->segs[p] = segs;
       t += segs * R.g.ny;
