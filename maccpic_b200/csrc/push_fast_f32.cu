@@ -732,6 +732,7 @@ const Variant32 kVariants32[] = {
     EM2G_VARIANT32(32, 2, 8), EM2G_VARIANT32(64, 2, 4),
     // two cells per group, one after the other
     EM2G_VARIANT32N(32, 4, 2, 4, "f32 tcx32x2 g4 minb4"),
+    EM2G_VARIANT32N(32, 4, 3, 4, "f32 tcx32x3 g4 minb4"),
 };
 #undef EM2G_VARIANT32
 #undef EM2G_VARIANT32N
