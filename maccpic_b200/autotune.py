@@ -42,10 +42,11 @@ def _step_ms(run, k: int, cycles: int) -> float:
 
 def autotune(run, particles: int, steps: int = 2, warm: int = 1, cache: str | None = DEFAULT_CACHE,
              use_cache: bool = True, intervals=None) -> dict:
-    """Time every variant on `run` (an Em2Gpu with its state loaded), keep the
-    fastest, then time the sort intervals with it (FP32 only).  Returns
-    {"variant", "name", "times_ms", "sort_interval", "interval_ms",
-    "from_cache"}."""
+    """Time every variant's regrouping push on `run` (an Em2Gpu with its state
+    loaded), then time whole steps at every admissible sort interval for the
+    fastest few, and keep the best (variant, interval).  Returns {"variant",
+    "name", "times_ms", "sort_interval", "interval_ms" (of the kept variant),
+    "candidates", "from_cache"}."""
     key = _key(run, particles)
     table = {}
     if cache and os.path.exists(cache):
@@ -72,19 +73,26 @@ def autotune(run, particles: int, steps: int = 2, warm: int = 1, cache: str | No
         c = run.counters()
         run.set_timing(False)
         times.append(c["push_ms"] / max(1, c["push_launches_timed"]))
-    best = min(range(n), key=lambda v: times[v])
-    run.set_variant(best)
+    # the variants within 10 % of the fastest regrouping push (at most 3) are
+    # timed as whole steps at every admissible interval: between regroupings
+    # the pushes run in place, and the variants' order can differ there
+    order = sorted(range(n), key=lambda v: times[v])
+    cands = [v for v in order[:3] if times[v] <= 1.1 * times[order[0]]]
     kmax = run.max_sort_interval()
     if intervals is None:
         intervals = sorted({k for k in (1, 2, 3, 4, 6, kmax) if 1 <= k <= kmax})
-    interval_ms = {}
-    for k in intervals:
-        interval_ms[k] = _step_ms(run, k, cycles=max(1, 12 // k))
-    k_best = min(interval_ms, key=interval_ms.get)
+    sweep = {}
+    for v in cands:
+        run.set_variant(v)
+        sweep[v] = {k: _step_ms(run, k, cycles=max(1, 12 // k)) for k in intervals}
+    best, k_best = min(((v, k) for v in cands for k in intervals), key=lambda vk: sweep[vk[0]][vk[1]])
+    run.set_variant(best)
     run.set_sort_interval(k_best)
+    interval_ms = sweep[best]
     run.reset_counters()
     result = {"variant": best, "name": run.variant()[1], "times_ms": times,
-              "sort_interval": k_best, "interval_ms": {str(k): v for k, v in interval_ms.items()}}
+              "sort_interval": k_best, "interval_ms": {str(k): v for k, v in interval_ms.items()},
+              "candidates": {str(v): {str(k): t for k, t in sweep[v].items()} for v in cands}}
     if cache:
         table[key] = result
         try:

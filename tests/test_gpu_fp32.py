@@ -240,3 +240,25 @@ def test_offsets_that_round_up_to_the_next_cell(gpu, oracle_lib):
         for f in range(6):
             scale = max(np.abs(st.fld[f]).max(), 1e-30)
             assert np.abs(got[f] - st.fld[f]).max() / scale < 1e-2, f
+
+
+def test_autotuner_keeps_the_fastest_variant_and_interval(gpu):
+    """The autotuner times the fastest few variants at every admissible sort
+    interval and leaves the context on the best pair it timed."""
+    from maccpic_b200 import autotune
+    from maccpic_b200.em2 import Em2Gpu
+    op, rp, fld, parts = harris(nx=128, ny=64, ppc=16)
+    with Em2Gpu(rp) as g:
+        g.set_fields(fld)
+        for s, p in enumerate(parts):
+            g.set_particles(s, p)
+        r = autotune.autotune(g, particles=parts[0].shape[1], cache=None, use_cache=False)
+        assert len(r["times_ms"]) == g.num_variants()
+        assert str(r["variant"]) in r["candidates"]
+        kmax = g.max_sort_interval()
+        for v, ms in r["candidates"].items():
+            assert set(ms) == {str(k) for k in (1, 2, 3, 4, 6, kmax) if k <= kmax}
+        best = min(t for ms in r["candidates"].values() for t in ms.values())
+        assert r["candidates"][str(r["variant"])][str(r["sort_interval"])] == best
+        assert g.variant()[0] == r["variant"] and g.p.sort_interval == r["sort_interval"]
+        g.step(2)
