@@ -105,10 +105,11 @@ def autotune(run, particles: int, steps: int = 2, warm: int = 1, cache: str | No
 
 def autotune_ensemble(ens, steps: int = 2, warm: int = 1, intervals=None) -> dict:
     """Time every push variant on an ensemble (its current state, a few
-    graph-launched steps each; every step advances the runs), keep the
-    fastest, then time the sort intervals the drift bound allows with it.
-    Returns {"variant", "times_ms", "sort_interval", "interval_ms"}: mean
-    wall time of a step per variant and per interval."""
+    graph-launched steps each; every step advances the runs), then time the
+    fastest few at every sort interval the drift bound allows and keep the
+    best pair.  Returns {"variant", "times_ms", "sort_interval",
+    "interval_ms", "candidates"}: mean wall time of a step per variant and
+    per interval."""
     import time
     import torch
     ens.set_sort_interval(1)
@@ -121,13 +122,19 @@ def autotune_ensemble(ens, steps: int = 2, warm: int = 1, intervals=None) -> dic
         ens.step(steps)
         torch.cuda.synchronize()
         times.append((time.perf_counter() - t) * 1e3 / steps)
-    best = min(range(len(times)), key=lambda v: times[v])
-    ens.set_variant(best)
+    # as autotune: the fastest few (within 10 %, at most 3) at every interval
+    order = sorted(range(len(times)), key=lambda v: times[v])
+    cands = [v for v in order[:3] if times[v] <= 1.1 * times[order[0]]]
     kmax = ens.max_sort_interval()
     if intervals is None:
         intervals = sorted({k for k in (1, 2, 3, 4, 6, kmax) if 1 <= k <= kmax})
-    interval_ms = {k: _step_ms(ens, k, cycles=max(1, 6 // k)) for k in intervals}
-    k_best = min(interval_ms, key=interval_ms.get)
+    sweep = {}
+    for v in cands:
+        ens.set_variant(v)
+        sweep[v] = {k: _step_ms(ens, k, cycles=max(1, 6 // k)) for k in intervals}
+    best, k_best = min(((v, k) for v in cands for k in intervals), key=lambda vk: sweep[vk[0]][vk[1]])
+    ens.set_variant(best)
     ens.set_sort_interval(k_best)
     return {"variant": best, "times_ms": times, "sort_interval": k_best,
-            "interval_ms": {str(k): v for k, v in interval_ms.items()}}
+            "interval_ms": {str(k): v for k, v in sweep[best].items()},
+            "candidates": {str(v): {str(k): t for k, t in sweep[v].items()} for v in cands}}
