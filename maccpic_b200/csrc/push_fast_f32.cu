@@ -499,172 +499,173 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
   int qn = 0;  // entries on this warp's stack (the same in every lane)
   const unsigned lt = (1u << lane) - 1u;
   for (int pass = 0; pass < NC; ++pass) {
-  if (pass > 0) {  // the group's next cell: its range and first particle
-    kx += TCX;
-    valid = kx < nx;
-    kxs = valid ? kx : nx - 1;
-    cell = (int64_t)ky * nx + kx;
-    beg = valid ? a.offA[cell] : 0;
-    front = (!INPLACE && valid) ? a.offB[cell] : 0;
-    end = valid ? a.offA[cell + 1] : 0;
-    if (beg + gl < end) {
-      const int32_t j = beg + gl;
-      pxr = a.A[j];
-      pyr = a.A[cap + j];
-      pux = a.A[2 * cap + j];
-      puy = a.A[3 * cap + j];
-      puz = a.A[4 * cap + j];
-      pslot = a.slotA[j];
+    if (pass > 0) {  // the group's next cell: its range and first particle
+      kx += TCX;
+      valid = kx < nx;
+      kxs = valid ? kx : nx - 1;
+      cell = (int64_t)ky * nx + kx;
+      beg = valid ? a.offA[cell] : 0;
+      front = (!INPLACE && valid) ? a.offB[cell] : 0;
+      end = valid ? a.offA[cell + 1] : 0;
+      if (beg + gl < end) {
+        const int32_t j = beg + gl;
+        pxr = a.A[j];
+        pyr = a.A[cap + j];
+        pux = a.A[2 * cap + j];
+        puy = a.A[3 * cap + j];
+        puz = a.A[4 * cap + j];
+        pslot = a.slotA[j];
+      }
     }
-  }
-  Block32 b;
-  const float2 z2 = make_float2(0.0f, 0.0f);
+    Block32 b;
+    const float2 z2 = make_float2(0.0f, 0.0f);
 #pragma unroll
-  for (int r = 0; r < 4; ++r) {
-    b.rho01[r] = b.rho23[r] = z2;
-    if (r < 3) {
-      b.jxr01[r] = b.jxr23[r] = b.jzr01[r] = b.jy01[r] = b.jy23[r] = z2;
-      b.jzr2[r] = 0.0f;
+    for (int r = 0; r < 4; ++r) {
+      b.rho01[r] = b.rho23[r] = z2;
+      if (r < 3) {
+        b.jxr01[r] = b.jxr23[r] = b.jzr01[r] = b.jy01[r] = b.jy23[r] = z2;
+        b.jzr2[r] = 0.0f;
+      }
     }
-  }
-  int stay_new = 0;  // particles of this lane whose new position is in cell k
-  int home_count = 0;  // particles of this group written to the front of cell k
+    int stay_new = 0;  // particles of this lane whose new position is in cell k
+    int home_count = 0;  // particles of this group written to the front of cell k
 
-  for (int32_t i = beg + gl;; i += G) {
-    const bool act = i < end;
-    if (__ballot_sync(0xffffffffu, act) == 0u) break;
-    const float cxr = pxr, cyr = pyr, cux = pux, cuy = puy, cuz = puz;
-    const int32_t cslot = pslot;
-    const int32_t j = i + G;
-    if (j < end) {
-      pxr = a.A[j];
-      pyr = a.A[cap + j];
-      pux = a.A[2 * cap + j];
-      puy = a.A[3 * cap + j];
-      puz = a.A[4 * cap + j];
-      pslot = a.slotA[j];
-    }
-    // a lane without a particle runs on a dummy inside a real cell
-    PartOut o;
-    push_one<WX>(a, win, x0, y0, kxs, ky, act, act ? cxr : 0.25f, act ? cyr : 0.25f, cux, cuy,
-                  cuz, cinv, b, akel, stay_new, o);
-    if (INPLACE) {
-      if (act) {
-        // the offset relative to the group cell, kept in the cell the push
-        // counted for the next grouping (group cell + o + no): when that is
-        // the group cell itself, 1 plus a tiny negative move can round to
-        // exactly 1, which would read as the next cell (every other case is
-        // exact or rounds within its cell)
-        float xn = o.mx + (float)o.ox, yn = o.my + (float)o.oy;
-        if (o.ox + (o.ncx - o.cx) == 0) xn = fminf(xn, kBelowOne);
-        if (o.oy + (o.ncy - o.cy) == 0) yn = fminf(yn, kBelowOne);
-        a.B[i] = xn;
-        a.B[cap + i] = yn;
-        a.B[2 * cap + i] = o.ux;
-        a.B[3 * cap + i] = o.uy;
-        a.B[4 * cap + i] = o.uz;
+    for (int32_t i = beg + gl;; i += G) {
+      const bool act = i < end;
+      if (__ballot_sync(0xffffffffu, act) == 0u) break;
+      const float cxr = pxr, cyr = pyr, cux = pux, cuy = puy, cuz = puz;
+      const int32_t cslot = pslot;
+      const int32_t j = i + G;
+      if (j < end) {
+        pxr = a.A[j];
+        pyr = a.A[cap + j];
+        pux = a.A[2 * cap + j];
+        puy = a.A[3 * cap + j];
+        puz = a.A[4 * cap + j];
+        pslot = a.slotA[j];
       }
-    } else {
-      // write back grouped by the cell of the start of this step: particles
-      // that started it in cell k take the next slots from the front of k's
-      // segment in processing order (a running count per group, no atomics);
-      // the few that came from another cell's range fill it from the back
-      const unsigned inm = __ballot_sync(0xffffffffu, act && o.in_cell_old) & gmask;
-      int64_t pos = -1;
-      if (act) {
-        if (o.in_cell_old)
-          pos = (int64_t)front + home_count + __popc(inm & lt);
-        else {
-          const int key = wrap(o.cy, ny) * nx + wrap(o.cx, nx);  // the start cell's key
-          pos = (int64_t)a.offB[key + 1] - 1 - atomicAdd(a.cursor + key, 1);
+      // a lane without a particle runs on a dummy inside a real cell
+      PartOut o;
+      push_one<WX>(a, win, x0, y0, kxs, ky, act, act ? cxr : 0.25f, act ? cyr : 0.25f, cux, cuy,
+                    cuz, cinv, b, akel, stay_new, o);
+      if (INPLACE) {
+        if (act) {
+          // the offset relative to the group cell, kept in the cell the push
+          // counted for the next grouping (group cell + o + no): when that is
+          // the group cell itself, 1 plus a tiny negative move can round to
+          // exactly 1, which would read as the next cell (every other case is
+          // exact or rounds within its cell)
+          float xn = o.mx + (float)o.ox, yn = o.my + (float)o.oy;
+          if (o.ox + (o.ncx - o.cx) == 0) xn = fminf(xn, kBelowOne);
+          if (o.oy + (o.ncy - o.cy) == 0) yn = fminf(yn, kBelowOne);
+          a.B[i] = xn;
+          a.B[cap + i] = yn;
+          a.B[2 * cap + i] = o.ux;
+          a.B[3 * cap + i] = o.uy;
+          a.B[4 * cap + i] = o.uz;
         }
-        // a guard: the counts of the last push place every particle inside
-        // the buffer; a position outside it is counted and not written
-        if (pos < 0 || pos >= cap) {
-          atomicAdd(a.lost, 1.0);
-          pos = -1;
+      } else {
+        // write back grouped by the cell of the start of this step: particles
+        // that started it in cell k take the next slots from the front of k's
+        // segment in processing order (a running count per group, no atomics);
+        // the few that came from another cell's range fill it from the back
+        const unsigned inm = __ballot_sync(0xffffffffu, act && o.in_cell_old) & gmask;
+        int64_t pos = -1;
+        if (act) {
+          if (o.in_cell_old)
+            pos = (int64_t)front + home_count + __popc(inm & lt);
+          else {
+            const int key = wrap(o.cy, ny) * nx + wrap(o.cx, nx);  // the start cell's key
+            pos = (int64_t)a.offB[key + 1] - 1 - atomicAdd(a.cursor + key, 1);
+          }
+          // a guard: the counts of the last push place every particle inside
+          // the buffer; a position outside it is counted and not written
+          if (pos < 0 || pos >= cap) {
+            atomicAdd(a.lost, 1.0);
+            pos = -1;
+          }
         }
+        if (pos >= 0) {
+          a.B[pos] = o.mx;
+          a.B[cap + pos] = o.my;
+          a.B[2 * cap + pos] = o.ux;
+          a.B[3 * cap + pos] = o.uy;
+          a.B[4 * cap + pos] = o.uz;
+          a.slotB[pos] = cslot;
+        }
+        home_count += __popc(inm);
       }
-      if (pos >= 0) {
-        a.B[pos] = o.mx;
-        a.B[cap + pos] = o.my;
-        a.B[2 * cap + pos] = o.ux;
-        a.B[3 * cap + pos] = o.uy;
-        a.B[4 * cap + pos] = o.uz;
-        a.slotB[pos] = cslot;
-      }
-      home_count += __popc(inm);
-    }
-    // the out-of-cell deposits onto the warp's stack; whole warps of them
-    // done at once
-    const unsigned m_old = __ballot_sync(0xffffffffu, o.need_old);
-    const unsigned m_new = __ballot_sync(0xffffffffu, o.need_new);
-    if (m_old | m_new) {
-      if (o.need_old) {
-        const int q = qn + __popc(m_old & lt);
-        Q.cx[q] = o.cx;
-        Q.cy[q] = o.cy;
-        Q.f[q] = make_float2(o.fx, o.fy);
-        Q.q[q] = make_float4(o.qx, o.qy, o.qz, 0.0f);
-      }
-      const int qn1 = qn + __popc(m_old);
-      if (o.need_new) {
-        const int q = qn1 + __popc(m_new & lt);
-        Q.cx[q] = o.ncx;
-        Q.cy[q] = o.ncy;
-        Q.f[q] = make_float2(o.nfx, o.nfy);
-        Q.q[q] = make_float4(o.qx, o.qy, o.qz, 1.0f);
-      }
-      qn = qn1 + __popc(m_new);
-      __syncwarp();
-      while (qn >= 32) {
-        qn -= 32;
-        drain_entry(a, Q, qn + lane);
+      // the out-of-cell deposits onto the warp's stack; whole warps of them
+      // done at once
+      const unsigned m_old = __ballot_sync(0xffffffffu, o.need_old);
+      const unsigned m_new = __ballot_sync(0xffffffffu, o.need_new);
+      if (m_old | m_new) {
+        if (o.need_old) {
+          const int q = qn + __popc(m_old & lt);
+          Q.cx[q] = o.cx;
+          Q.cy[q] = o.cy;
+          Q.f[q] = make_float2(o.fx, o.fy);
+          Q.q[q] = make_float4(o.qx, o.qy, o.qz, 0.0f);
+        }
+        const int qn1 = qn + __popc(m_old);
+        if (o.need_new) {
+          const int q = qn1 + __popc(m_new & lt);
+          Q.cx[q] = o.ncx;
+          Q.cy[q] = o.ncy;
+          Q.f[q] = make_float2(o.nfx, o.nfy);
+          Q.q[q] = make_float4(o.qx, o.qy, o.qz, 1.0f);
+        }
+        qn = qn1 + __popc(m_new);
         __syncwarp();
+        while (qn >= 32) {
+          qn -= 32;
+          drain_entry(a, Q, qn + lane);
+          __syncwarp();
+        }
       }
     }
-  }
 
-  if (lane < qn) drain_entry(a, Q, lane);
-  qn = 0;
-  // the group's new-position counts for cell k, and its register blocks
-  const int stay = group_sum<G>((float)stay_new) + 0.5f;
-  if (valid && gl == 0 && stay > 0) atomicAdd(a.cnt_next + cell, stay);
-  if (__any_sync(0xffffffffu, valid && end > beg)) {
-    // the G blocks of each cell summed through the warp's scratch (the
-    // stack is empty now), in three passes: rho, Jx and Jy, Jz
-    float *red = ws[threadIdx.x >> 5].red;
-    const int g0 = lane & ~(G - 1);
-    __syncwarp();
+    if (lane < qn) drain_entry(a, Q, lane);
+    qn = 0;
+    // the group's new-position counts for cell k, and its register blocks
+    const int stay = group_sum<G>((float)stay_new) + 0.5f;
+    if (valid && gl == 0 && stay > 0) atomicAdd(a.cnt_next + cell, stay);
+    if (__any_sync(0xffffffffu, valid && end > beg)) {
+      // the G blocks of each cell summed through the warp's scratch (the
+      // stack is empty now), in three passes: rho, Jx and Jy, Jz
+      float *red = ws[threadIdx.x >> 5].red;
+      const int g0 = lane & ~(G - 1);
+      __syncwarp();
 #pragma unroll
-    for (int r = 0; r < 4; ++r)
+      for (int r = 0; r < 4; ++r)
 #pragma unroll
-      for (int k = 0; k < 4; ++k) red[(r * 4 + k) * 32 + lane] = pick4(b.rho01[r], b.rho23[r], k);
-    __syncwarp();
-    if (valid) flush_rows<G, 4, 4>(a.rho, nxg, kx, ky, red, 0, gl, g0);
-    __syncwarp();
+        for (int k = 0; k < 4; ++k) red[(r * 4 + k) * 32 + lane] = pick4(b.rho01[r], b.rho23[r], k);
+      __syncwarp();
+      if (valid) flush_rows<G, 4, 4>(a.rho, nxg, kx, ky, red, 0, gl, g0);
+      __syncwarp();
 #pragma unroll
-    for (int r = 0; r < 4; ++r)
+      for (int r = 0; r < 4; ++r)
 #pragma unroll
-      for (int k = 0; k < 3; ++k) red[(r * 3 + k) * 32 + lane] = pick4(b.jxr01[k], b.jxr23[k], r);
+        for (int k = 0; k < 3; ++k) red[(r * 3 + k) * 32 + lane] = pick4(b.jxr01[k], b.jxr23[k], r);
 #pragma unroll
-    for (int r = 0; r < 3; ++r)
+      for (int r = 0; r < 3; ++r)
 #pragma unroll
-      for (int k = 0; k < 4; ++k) red[(12 + r * 4 + k) * 32 + lane] = pick4(b.jy01[r], b.jy23[r], k);
-    __syncwarp();
-    if (valid) {
-      flush_rows<G, 4, 3>(a.jx, nxg, kx, ky, red, 0, gl, g0);
-      flush_rows<G, 3, 4>(a.jy, nxg, kx, ky, red, 12, gl, g0);
+        for (int k = 0; k < 4; ++k)
+          red[(12 + r * 4 + k) * 32 + lane] = pick4(b.jy01[r], b.jy23[r], k);
+      __syncwarp();
+      if (valid) {
+        flush_rows<G, 4, 3>(a.jx, nxg, kx, ky, red, 0, gl, g0);
+        flush_rows<G, 3, 4>(a.jy, nxg, kx, ky, red, 12, gl, g0);
+      }
+      __syncwarp();
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) red[(r * 3 + k) * 32 + lane] = pick3(b.jzr01[k], b.jzr2[k], r);
+      __syncwarp();
+      if (valid) flush_rows<G, 3, 3>(a.jz, nxg, kx, ky, red, 0, gl, g0);
     }
-    __syncwarp();
-#pragma unroll
-    for (int r = 0; r < 3; ++r)
-#pragma unroll
-      for (int k = 0; k < 3; ++k) red[(r * 3 + k) * 32 + lane] = pick3(b.jzr01[k], b.jzr2[k], r);
-    __syncwarp();
-    if (valid) flush_rows<G, 3, 3>(a.jz, nxg, kx, ky, red, 0, gl, g0);
-  }
-  __syncwarp();  // the next pass's stack reuses the scratch just read
+    __syncwarp();  // the next pass's stack reuses the scratch just read
   }  // pass
   // per-warp partial of sum(gamma - 1); no block barrier at the end
   for (int o = 16; o > 0; o >>= 1) akel += __shfl_down_sync(0xffffffffu, akel, o);
@@ -1037,7 +1038,8 @@ int ens_push(em2g_ens *e, int bp, int cp, bool inplace) {
     float *fld = e->fld + R.fld_off;
     for (int s = 0; s < R.P.nsp; ++s, ++p) {
       Args32 &a = P->pair[p];
-      const float2 *sc = reinterpret_cast<const float2 *>(e->scaled + R.sc_off + (int64_t)s * 6 * w);
+      const float2 *sc =
+          reinterpret_cast<const float2 *>(e->scaled + R.sc_off + (int64_t)s * 6 * w);
       a.ebx = sc;
       a.ebz = sc + w;
       a.eby = sc + 2 * w;
