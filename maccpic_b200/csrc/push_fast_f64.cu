@@ -143,6 +143,25 @@ __device__ __forceinline__ void flush_one(double *A, int nxg, int ix, int iy, do
   if ((e & (G - 1)) == gl && v != 0.0) atomicAdd(A + (int64_t)iy * nxg + ix, v);
 }
 
+// Asynchronous copies global -> shared (cp.async): a lane's next particle
+// is fetched into shared memory while the current one runs (the kernel has
+// no registers left to hold it), one commit group per particle.
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
 // TCX cells per CTA (a row segment), MINB: CTAs per SM the register
 // allocation must allow (the autotuner's two knobs)
 template <int TCX, int MINB>
@@ -150,6 +169,9 @@ __global__ void __launch_bounds__(TCX * G, MINB) k_push_cells_f64(FastArgs a) {
   constexpr int kThreads = TCX * G;
   constexpr int WX = TCX + 5;  // window columns: array x0-1 .. x0+TCX+3
   __shared__ double2 win[3][WY][WX];
+  // each lane's next particle (x, y, vx, vy, vz, gamma; slot), two buffers
+  __shared__ double pf[2][6][kThreads];
+  __shared__ int32_t pfs[2][kThreads];
   const int nx = a.nx, ny = a.ny, nxg = a.nxg;
   const int x0 = blockIdx.x * TCX, y0 = blockIdx.y;
   for (int t = threadIdx.x; t < 3 * WY * WX; t += kThreads) {
@@ -187,15 +209,27 @@ __global__ void __launch_bounds__(TCX * G, MINB) k_push_cells_f64(FastArgs a) {
   int stay_new = 0;
   int home_count = 0;  // particles of this group written to the front of cell k
 
+  const int tid = threadIdx.x;
+  auto fetch = [&](int buf, int32_t j) {
+#pragma unroll
+    for (int c = 0; c < 6; ++c) cp_async8(&pf[buf][c][tid], a.A + (int64_t)c * cap + j);
+    cp_async4(&pfs[buf][tid], a.slotA + j);
+  };
+  if (beg + gl < end) fetch(0, beg + gl);
+  cp_async_commit();
+  int buf = 0;
   for (int32_t i = beg + gl;; i += G) {
     const bool active = i < end;
     const unsigned am = __ballot_sync(0xffffffffu, active);
     if (am == 0u) break;
+    if (i + G < end) fetch(buf ^ 1, i + G);
+    cp_async_commit();
+    cp_async_wait<1>();  // this particle's group (all but the newest) has landed
     if (active) {
-      double x = a.A[i], y = a.A[cap + i];
-      double vx = a.A[2 * cap + i], vy = a.A[3 * cap + i], vz = a.A[4 * cap + i];
-      double g = a.A[5 * cap + i];
-      const int32_t slot = a.slotA[i];
+      double x = pf[buf][0][tid], y = pf[buf][1][tid];
+      double vx = pf[buf][2][tid], vy = pf[buf][3][tid], vz = pf[buf][4][tid];
+      double g = pf[buf][5][tid];
+      const int32_t slot = pfs[buf][tid];
       const int key_cur = cell_key(x, y, nx, ny);
       const int pcx = (int)x, pcy = (int)y;  // the particle's cell, unwrapped
       const bool in_old = (pcx == cx) && (pcy == cy);
@@ -284,7 +318,9 @@ __global__ void __launch_bounds__(TCX * G, MINB) k_push_cells_f64(FastArgs a) {
       a.B[5 * cap + pos] = g;
       a.slotB[pos] = slot;
     }
+    buf ^= 1;
   }
+  cp_async_wait<0>();
 
   // this cell's count of new positions, then the register blocks
   int stay = stay_new;
