@@ -95,8 +95,6 @@ class HarrisConfig:
                          qm=qm, q=q, dn=dn, am=am,
                          np_max=np_max or [n, n], isav=self.isav, **kw)
 # the benchmark and test workloads (synthetic, seeded)
-
-# BASELINE workloads (synthetic, seeded)
 PRESETS = {
     "harris_256x128_ppc16": HarrisConfig(),
     "harris_2048x1024_ppc64": HarrisConfig(nx=2048, ny=1024, ppc=64, steps=1000),
