@@ -222,15 +222,6 @@ int validate(const em2g_params *p) {
   return EM2G_OK;
 }
 
-// the status word's timeout bits: 1 the CG's grid barrier, 2 a stencil's
-// bulk-copy staging
-std::string timeout_message(int bits) {
-  std::string m;
-  if (bits & 1) m = "cg: a grid barrier wait timed out";
-  if (bits & 2) m += std::string(m.empty() ? "" : "; ") + "a stencil's bulk-copy wait timed out";
-  return m;
-}
-
 int finish_outputs(em2g_ctx *c, double *ake_out, double *energies_out, int *cg_iters_out,
                    bool energies_valid) {
   EM2G_CUDA(cudaMemcpyAsync(c->host_out, c->dev_out, sizeof(double) * kDevOut,
@@ -241,7 +232,7 @@ int finish_outputs(em2g_ctx *c, double *ake_out, double *energies_out, int *cg_i
   EM2G_CUDA(cudaGetLastError());
   int rc = timing_collect(c);
   if (rc) return rc;
-  if (st[0] != 0) return fail(EM2G_ERR_TIMEOUT, timeout_message(st[0]));
+  if (st[0] != 0) return fail(EM2G_ERR_TIMEOUT, "cg: a grid barrier wait timed out");
   if (c->host_out[kDevLost] != 0.0) {
     const double lost = c->host_out[kDevLost];
     EM2G_CUDA(cudaMemsetAsync(c->dev_out + kDevLost, 0, sizeof(double), c->stream));
@@ -326,13 +317,13 @@ int em2g_create(const em2g_params *p, em2g_ctx **out) {
   } while (0)
   const bool fp32 = p->precision == EM2G_FP32;
   if (fp32) {
-    ALLOC(c->fld32, sizeof(float) * EM2G_NFIELD * w + kStageTail);
+    ALLOC(c->fld32, sizeof(float) * EM2G_NFIELD * w);
     ALLOC(c->scaled32, sizeof(float) * 6 * w * p->nsp);
-    ALLOC(c->smooth_tmp32, sizeof(float) * w + kStageTail);
+    ALLOC(c->smooth_tmp32, sizeof(float) * w);
   } else {
-    ALLOC(c->fld, sizeof(double) * EM2G_NFIELD * w + kStageTail);
+    ALLOC(c->fld, sizeof(double) * EM2G_NFIELD * w);
     ALLOC(c->scaled, sizeof(double) * 6 * w * p->nsp);
-    ALLOC(c->smooth_tmp, sizeof(double) * w + kStageTail);
+    ALLOC(c->smooth_tmp, sizeof(double) * w);
   }
   int64_t maxn = 0;
   for (int s = 0; s < p->nsp; ++s) {
@@ -767,14 +758,10 @@ int em2g_smooth2(em2g_ctx *c, int id) {
   int rc = check_ctx(c);
   if (rc) return rc;
   if (id < 0 || id >= EM2G_NFIELD) return fail(EM2G_ERR_INVALID, "bad field id");
-  EM2G_CUDA(cudaMemsetAsync(c->cg.status, 0, sizeof(int) * 2, c->stream));
   rc = is_fp32(c) ? smooth2_f32(c, c->fld32 + id * c->g.w)
                   : smooth2_f64(c, c->fld + id * c->g.w);
   if (rc) return rc;
-  int st = 0;
-  EM2G_CUDA(cudaMemcpyAsync(&st, c->cg.status, sizeof(st), cudaMemcpyDeviceToHost, c->stream));
   EM2G_CUDA(cudaStreamSynchronize(c->stream));
-  if (st != 0) return fail(EM2G_ERR_TIMEOUT, timeout_message(st));
   return EM2G_OK;
 }
 

@@ -23,9 +23,6 @@ constexpr int kDevOut = 32;
 // cell counts disagreed with where they were; the state is then corrupt and
 // the step fails -- a guard, never expected to count)
 constexpr int kDevLost = kDevOut - 1;
-// tail bytes after every field-block and smoothing-scratch allocation: the
-// stencils' bulk copies widen the last row they read to a 16-byte boundary
-constexpr int kStageTail = 64;
 
 // Sets the per-thread error message and returns the status (api.cu).
 int fail(int status, const std::string &msg);

@@ -192,9 +192,9 @@ int em2g_ens_create(const em2g_params *runs, int nruns, em2g_ens **out) {
     ce = cudaMalloc((void **)&(ptr), (bytes));                            \
     if (ce != cudaSuccess) return bail(cuda_fail(ce, "cudaMalloc " #ptr)); \
   } while (0)
-  ALLOC(e->fld, sizeof(float) * e->fld_n + kStageTail);
+  ALLOC(e->fld, sizeof(float) * e->fld_n);
   ALLOC(e->scaled, sizeof(float) * e->scaled_n);
-  ALLOC(e->tmp, sizeof(float) * e->tmp_n + kStageTail);
+  ALLOC(e->tmp, sizeof(float) * e->tmp_n);
   ALLOC(e->cgv, sizeof(float) * e->cgv_n);
   ALLOC(e->red, sizeof(double) * e->red_n);
   ALLOC(e->dev_out, sizeof(double) * (kEnsOut * (int64_t)nruns + 16));
@@ -442,10 +442,8 @@ int em2g_ens_step(em2g_ens *e, int nsteps, double *ake_out, double *energies_out
   EM2G_CUDA(cudaStreamSynchronize(e->stream));
   EM2G_CUDA(cudaGetLastError());
   for (int r = 0; r < nr; ++r)
-    if (const int bits = e->host_status[2 * r])
-      return fail(EM2G_ERR_TIMEOUT,
-                  "run " + std::to_string(r) + ": " +
-                      ((bits & 1) ? "a CG barrier wait timed out" : "a stencil's bulk-copy wait timed out"));
+    if (e->host_status[2 * r])
+      return fail(EM2G_ERR_TIMEOUT, "cg of run " + std::to_string(r) + ": a barrier wait timed out");
   for (int r = 0; r < nr; ++r) {
     const double lost = e->host_out[(int64_t)r * kEnsOut + kEnsLost];
     if (lost != 0.0) {

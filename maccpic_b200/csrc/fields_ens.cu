@@ -33,7 +33,6 @@ struct EnsRunDev {
   int nsp, isav, smooth_current, tiles_x;
   double anorml1;
   double *out;
-  int *status;  // the run's CG status: [0] timeout bits (stencil staging: bit 1)
 };
 
 struct EnsGrid32 {
@@ -45,7 +44,6 @@ struct EnsGrid32 {
   int wblk0[kEnsMaxRuns + 1];   // blocks of 256 elements of one array
   EnsRunDev run[kEnsMaxRuns];
 };
-static_assert(sizeof(EnsGrid32) <= 32764, "kernel parameters are limited to 32764 bytes");
 
 struct EnsCg32 {
   int nruns;
@@ -122,23 +120,18 @@ __global__ void __launch_bounds__(TX *TY) k_ens_sten(const __grid_constant__ Ens
   const int lb = blockIdx.x - e.sten0[r];
   const int tby = lb / R.tiles_x, tbx = lb - tby * R.tiles_x;
   const int64_t N = (int64_t)R.g.nx * R.g.ny;
-  if (OP == OP_BHALF || OP == OP_EFULL) {
-    __shared__ grid::Stage<float, 3> s3;
-    if (OP == OP_BHALF)
-      grid::b_half_at(R.g, R.fld, R.ctxh, R.ctyh, tbx, tby, s3, R.status);
-    else
-      grid::e_full_at(R.g, R.fld, R.ctx, R.cty, R.tem, tbx, tby, s3, R.status);
+  if (OP == OP_BHALF) {
+    grid::b_half_at(R.g, R.fld, R.ctxh, R.ctyh, tbx, tby);
+  } else if (OP == OP_EFULL) {
+    grid::e_full_at(R.g, R.fld, R.ctx, R.cty, R.tem, tbx, tby);
   } else if (OP == OP_SMOOTH_B || OP == OP_SMOOTH_C) {
-    // the whole block takes the same branch (run, array and step are the
-    // block's), so the staging's barrier is reached by every thread or none
     int arr;
     if (!smooth_target(e, R, set, (int)blockIdx.y, &arr)) return;
-    __shared__ grid::Stage<float, 1> s1;
     float *a = R.fld + arr * R.g.w, *d = R.tmp + blockIdx.y * R.g.w;
     if (OP == OP_SMOOTH_B)
-      grid::smooth_binomial_at(R.g, a, d, tbx, tby, s1, R.status);
+      grid::smooth_binomial_at(R.g, a, d, tbx, tby);
     else
-      grid::smooth_compensate_at(R.g, d, a, tbx, tby, s1, R.status);
+      grid::smooth_compensate_at(R.g, d, a, tbx, tby);
   } else if (OP == OP_RHS) {
     grid::poisson_rhs_at(R.g, R.fld, R.dx, R.dy, R.cgu + N, R.cgu + 2 * N, tbx, tby);
   } else {
@@ -191,7 +184,6 @@ std::unique_ptr<EnsGrid32> make_grid_table(em2g_ens *e) {
     D.g = G{R.g.nx, R.g.ny, R.g.nxg, R.g.w};
     D.fld = e->fld + R.fld_off;
     D.tmp = e->tmp + R.tmp_off;
-    D.status = e->cg_status + 2 * r;
     D.cgu = e->cgv + R.cg_off;
     D.sc = e->scaled + R.sc_off;
     const double ctx = R.P.dt * R.P.c / R.P.dx, cty = R.P.dt * R.P.c / R.P.dy;

@@ -16,8 +16,8 @@ template <typename T>
 int smooth2_t(em2g_ctx *c, T *a, T *tmp) {
   const G g = geom(c);
   const dim3 grd = grid_for(g.nx + 1, g.ny + 1), blk(TX, TY);
-  k_smooth_binomial<T><<<grd, blk, 0, c->stream>>>(g, a, tmp, c->cg.status);
-  k_smooth_compensate<T><<<grd, blk, 0, c->stream>>>(g, tmp, a, c->cg.status);
+  k_smooth_binomial<T><<<grd, blk, 0, c->stream>>>(g, a, tmp);
+  k_smooth_compensate<T><<<grd, blk, 0, c->stream>>>(g, tmp, a);
   c->launches += 2;
   EM2G_CUDA(cudaGetLastError());
   return EM2G_OK;
@@ -131,9 +131,9 @@ int fields_t(em2g_ctx *c, T *fld, T *tmp, int it, bool want_energies) {
   const double ctx = c->P.dt * c->P.c / c->P.dx, cty = c->P.dt * c->P.c / c->P.dy;
   const double ctxh = ctx * 0.5, ctyh = cty * 0.5, tem = 0.5 * c->P.dt;
   const dim3 grd = grid_for(g.nx + 1, g.ny + 1);
-  k_b_half<T><<<grd, blk, 0, c->stream>>>(g, fld, (T)ctxh, (T)ctyh, c->cg.status);
-  k_e_full<T><<<grd, blk, 0, c->stream>>>(g, fld, (T)ctx, (T)cty, (T)tem, c->cg.status);
-  k_b_half<T><<<grd, blk, 0, c->stream>>>(g, fld, (T)ctxh, (T)ctyh, c->cg.status);
+  k_b_half<T><<<grd, blk, 0, c->stream>>>(g, fld, (T)ctxh, (T)ctyh);
+  k_e_full<T><<<grd, blk, 0, c->stream>>>(g, fld, (T)ctx, (T)cty, (T)tem);
+  k_b_half<T><<<grd, blk, 0, c->stream>>>(g, fld, (T)ctxh, (T)ctyh);
   c->launches += 3;
   EM2G_CUDA(cudaGetLastError());
   // filters (pic/fields.f90:252-260)

@@ -76,218 +76,88 @@ __global__ void k_fold_y(G g, T *fld) {
   fold_y_at(g, fld, (int)(blockIdx.x * blockDim.x + threadIdx.x), (int)blockIdx.y);
 }
 
-// ---- stencil tiles staged in shared memory by the bulk-copy (TMA) engine
-//
-// A tile of TX x TY cells with its one-cell halo -- rows y0-1 .. y0+TY and
-// columns x0-1 .. x0+TX of a field array, clipped to the array's
-// (0..nx+2, 0..ny+2) -- comes in with one cp.async.bulk per row, all rows of
-// all staged arrays completing on one mbarrier.  A row of a field array
-// starts at any multiple of sizeof(T) ((nx+3) elements per row, arrays back
-// to back), while a bulk copy needs 16-byte aligned addresses and sizes, so
-// each row's span is widened to 16-byte boundaries (less than 16 bytes on
-// either side) and its start shift kept per row.  Widening never leaves the
-// allocation: rounding down stays above the 256-byte aligned base of the
-// allocation, and every field allocation carries kStageTail bytes of tail.
-// Waits are bounded: a thread that gives up sets bit 1 of the status word
-// the host reads after the step (bit 0 is the CG barrier's), waits once
-// more, as long again, for the copies in flight, and skips its cell.
-static_assert(kStageTail >= 16, "the widened last row stays in the allocation");
-constexpr int kStageSpinLimit = 1 << 15;  // waits of up to ~1 us each: ~30 ms
-
-template <typename T, int K>
-struct Stage {
-  static constexpr int kChunk = 16 / (int)sizeof(T);  // elements per 16 bytes
-  // widest span: TX+2 elements, kChunk-1 more on either side
-  static constexpr int kPitch = (TX + 2 + 2 * kChunk + kChunk - 1) / kChunk * kChunk;
-  static_assert(TX + 2 + 2 * (kChunk - 1) <= kPitch, "a widened row fits the pitch");
-  static_assert(kPitch * sizeof(T) % 16 == 0, "rows start on 16-byte boundaries");
-  alignas(16) T v[K][TY + 2][kPitch];
-  int shift[K][TY + 2];
-  unsigned long long bar;
-};
-
-__device__ __forceinline__ unsigned smem_addr(const void *p) {
-  return (unsigned)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ bool stage_wait(unsigned bar) {
-  for (int tries = 0; tries < kStageSpinLimit; ++tries) {
-    unsigned done;
-    // suspends until the phase completes, or for about 1 us at most
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0, %2;\n"
-        " selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(done)
-        : "r"(bar), "r"(1000u)
-        : "memory");
-    if (done) return true;
-  }
-  return false;
-}
-
-// The byte span of row y (columns xl..xh) of array a, widened to 16 bytes.
+// ---- Yee half step of B (pic/fields.f90:184-200, :231-247)
 template <typename T>
-__device__ __forceinline__ void stage_span(const G &g, const T *a, int xl, int xh, int y,
-                                           uintptr_t *start, unsigned *bytes, int *shift) {
-  const uintptr_t p0 = (uintptr_t)(a + at(g, xl, y));
-  const uintptr_t p1 = (uintptr_t)(a + at(g, xh, y) + 1);
-  *start = p0 & ~(uintptr_t)15;
-  *bytes = (unsigned)(((p1 + 15) & ~(uintptr_t)15) - *start);
-  *shift = (int)((p0 - *start) / sizeof(T));
-}
-
-// Every thread of the (TX, TY) block calls this; false in a thread that
-// gave up waiting.  Thread t < K x rows copies row t % rows of array
-// t / rows: it registers its bytes with its own arrival (the barrier counts
-// K x rows arrivals), then issues the copy, so the rows go out in parallel.
-template <typename T, int K>
-__device__ bool stage_tiles(const G &g, const T *const (&src)[K], int x0, int y0,
-                            Stage<T, K> &s, int *status) {
-  const unsigned bar = smem_addr(&s.bar);
-  const int tid = threadIdx.y * TX + threadIdx.x;
-  const int yl = y0 - 1, rows = min(y0 + TY, g.ny + 2) - yl + 1;
-  if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(K * rows) : "memory");
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-  }
-  __syncthreads();
-  if (tid < K * rows) {
-    const int k = tid / rows, r = tid - k * rows;
-    uintptr_t b0;
-    unsigned n;
-    stage_span(g, src[k], x0 - 1, min(x0 + TX, g.nx + 2), yl + r, &b0, &n, &s.shift[k][r]);
-    unsigned long long state;
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 %0, [%1], %2;"
-                 : "=l"(state)
-                 : "r"(bar), "r"(n)
-                 : "memory");
-    (void)state;
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
-        "[%3];" ::"r"(smem_addr(&s.v[k][r][0])),
-        "l"(b0), "r"(n), "r"(bar)
-        : "memory");
-  }
-  if (stage_wait(bar)) return true;
-  atomicOr(status, 2);
-  stage_wait(bar);
-  return false;
-}
-
-// element (ix+dx, iy+dy) of staged array k, (ix, iy) in the tile at (x0, y0)
-template <typename T, int K>
-__device__ __forceinline__ T staged(const Stage<T, K> &s, int k, int x0, int y0, int ix, int iy,
-                                    int dx, int dy) {
-  const int r = iy + dy - (y0 - 1);
-  return s.v[k][r][ix + dx - (x0 - 1) + s.shift[k][r]];
-}
-
-// ---- Yee half step of B (pic/fields.f90:184-200, :231-247); E staged
-template <typename T>
-__device__ __forceinline__ void b_half_at(const G &g, T *fld, T ctxh, T ctyh, int tbx, int tby,
-                                          Stage<T, 3> &s, int *status) {
-  const int x0 = 1 + tbx * TX, y0 = 1 + tby * TY;
-  const T *const src[3] = {fld + EM2G_EX * g.w, fld + EM2G_EY * g.w, fld + EM2G_EZ * g.w};
-  if (!stage_tiles<T, 3>(g, src, x0, y0, s, status)) return;
-  const int ix = x0 + threadIdx.x;
-  const int iy = y0 + threadIdx.y;
+__device__ __forceinline__ void b_half_at(const G &g, T *fld, T ctxh, T ctyh, int tbx, int tby) {
+  const int ix = 1 + tbx * TX + threadIdx.x;
+  const int iy = 1 + tby * TY + threadIdx.y;
   if (ix > g.nx + 1 || iy > g.ny + 1) return;
+  const T *ex = fld + EM2G_EX * g.w, *ey = fld + EM2G_EY * g.w, *ez = fld + EM2G_EZ * g.w;
   T *bx = fld + EM2G_BX * g.w, *by = fld + EM2G_BY * g.w, *bz = fld + EM2G_BZ * g.w;
   const int64_t c = at(g, ix, iy);
-  const T ezc = staged(s, 2, x0, y0, ix, iy, 0, 0);
-  const T vbx = bx[c] - ctyh * (ezc - staged(s, 2, x0, y0, ix, iy, 0, -1));
-  const T vby = by[c] + ctxh * (ezc - staged(s, 2, x0, y0, ix, iy, -1, 0));
-  const T vbz = bz[c] -
-                ctxh * (staged(s, 1, x0, y0, ix, iy, 1, 0) - staged(s, 1, x0, y0, ix, iy, 0, 0)) +
-                ctyh * (staged(s, 0, x0, y0, ix, iy, 0, 1) - staged(s, 0, x0, y0, ix, iy, 0, 0));
+  const T ezc = ez[c];
+  const T vbx = bx[c] - ctyh * (ezc - ez[c - g.nxg]);
+  const T vby = by[c] + ctxh * (ezc - ez[c - 1]);
+  const T vbz = bz[c] - ctxh * (ey[c + 1] - ey[c]) + ctyh * (ex[c + g.nxg] - ex[c]);
   store_with_guards(g, bx, ix, iy, vbx);
   store_with_guards(g, by, ix, iy, vby);
   store_with_guards(g, bz, ix, iy, vbz);
 }
 template <typename T>
-__global__ void __launch_bounds__(TX *TY) k_b_half(G g, T *fld, T ctxh, T ctyh, int *status) {
-  __shared__ Stage<T, 3> s;
-  b_half_at(g, fld, ctxh, ctyh, (int)blockIdx.x, (int)blockIdx.y, s, status);
+__global__ void k_b_half(G g, T *fld, T ctxh, T ctyh) {
+  b_half_at(g, fld, ctxh, ctyh, (int)blockIdx.x, (int)blockIdx.y);
 }
 
-// ---- Yee full step of E (pic/fields.f90:207-224); B staged
+// ---- Yee full step of E (pic/fields.f90:207-224)
 template <typename T>
 __device__ __forceinline__ void e_full_at(const G &g, T *fld, T ctx, T cty, T tem, int tbx,
-                                          int tby, Stage<T, 3> &s, int *status) {
-  const int x0 = 1 + tbx * TX, y0 = 1 + tby * TY;
-  const T *const src[3] = {fld + EM2G_BX * g.w, fld + EM2G_BY * g.w, fld + EM2G_BZ * g.w};
-  if (!stage_tiles<T, 3>(g, src, x0, y0, s, status)) return;
-  const int ix = x0 + threadIdx.x;
-  const int iy = y0 + threadIdx.y;
+                                          int tby) {
+  const int ix = 1 + tbx * TX + threadIdx.x;
+  const int iy = 1 + tby * TY + threadIdx.y;
   if (ix > g.nx + 1 || iy > g.ny + 1) return;
   T *ex = fld + EM2G_EX * g.w, *ey = fld + EM2G_EY * g.w, *ez = fld + EM2G_EZ * g.w;
+  const T *bx = fld + EM2G_BX * g.w, *by = fld + EM2G_BY * g.w, *bz = fld + EM2G_BZ * g.w;
   const T *jxm = fld + EM2G_JXM * g.w, *jxp = fld + EM2G_JXP * g.w,
-          *jym = fld + EM2G_JYM * g.w, *jyp = fld + EM2G_JYP * g.w,
-          *jzm = fld + EM2G_JZM * g.w, *jzp = fld + EM2G_JZP * g.w;
+               *jym = fld + EM2G_JYM * g.w, *jyp = fld + EM2G_JYP * g.w,
+               *jzm = fld + EM2G_JZM * g.w, *jzp = fld + EM2G_JZP * g.w;
   const int64_t c = at(g, ix, iy);
-  const T bzc = staged(s, 2, x0, y0, ix, iy, 0, 0);
-  const T vex = ex[c] + cty * (bzc - staged(s, 2, x0, y0, ix, iy, 0, -1)) -
-                tem * (jxm[c] + jxp[c]);
-  const T vey = ey[c] - ctx * (bzc - staged(s, 2, x0, y0, ix, iy, -1, 0)) -
-                tem * (jym[c] + jyp[c]);
-  const T vez = ez[c] +
-                ctx * (staged(s, 1, x0, y0, ix, iy, 1, 0) - staged(s, 1, x0, y0, ix, iy, 0, 0)) -
-                cty * (staged(s, 0, x0, y0, ix, iy, 0, 1) - staged(s, 0, x0, y0, ix, iy, 0, 0)) -
-                tem * (jzm[c] + jzp[c]);
+  const T bzc = bz[c];
+  const T vex = ex[c] + cty * (bzc - bz[c - g.nxg]) - tem * (jxm[c] + jxp[c]);
+  const T vey = ey[c] - ctx * (bzc - bz[c - 1]) - tem * (jym[c] + jyp[c]);
+  const T vez = ez[c] + ctx * (by[c + 1] - by[c]) - cty * (bx[c + g.nxg] - bx[c]) -
+                     tem * (jzm[c] + jzp[c]);
   store_with_guards(g, ex, ix, iy, vex);
   store_with_guards(g, ey, ix, iy, vey);
   store_with_guards(g, ez, ix, iy, vez);
 }
 template <typename T>
-__global__ void __launch_bounds__(TX *TY) k_e_full(G g, T *fld, T ctx, T cty, T tem,
-                                                   int *status) {
-  __shared__ Stage<T, 3> s;
-  e_full_at(g, fld, ctx, cty, tem, (int)blockIdx.x, (int)blockIdx.y, s, status);
+__global__ void k_e_full(G g, T *fld, T ctx, T cty, T tem) {
+  e_full_at(g, fld, ctx, cty, tem, (int)blockIdx.x, (int)blockIdx.y);
 }
 
 // ---- smooth2 (pic/smooth.f90:143-177): binomial pass into `d`, then the
-// compensation pass back into `s`; the source of each pass staged
+// compensation pass back into `s`.
 template <typename T>
-__device__ __forceinline__ void smooth_binomial_at(const G &g, const T *s, T *d, int tbx,
-                                                   int tby, Stage<T, 1> &t, int *status) {
-  const int x0 = 1 + tbx * TX, y0 = 1 + tby * TY;
-  const T *const src[1] = {s};
-  if (!stage_tiles<T, 1>(g, src, x0, y0, t, status)) return;
-  const int ix = x0 + threadIdx.x;
-  const int iy = y0 + threadIdx.y;
+__device__ __forceinline__ void smooth_binomial_at(const G &g, const T *__restrict__ s, T *d,
+                                                   int tbx, int tby) {
+  const int ix = 1 + tbx * TX + threadIdx.x;
+  const int iy = 1 + tby * TY + threadIdx.y;
   if (ix > g.nx + 1 || iy > g.ny + 1) return;
-  auto S = [&](int dx, int dy) { return staged(t, 0, x0, y0, ix, iy, dx, dy); };
-  const T v = (4 * S(0, 0) + 2 * (S(-1, 0) + S(1, 0) + S(0, -1) + S(0, 1)) + S(-1, -1) +
-               S(-1, 1) + S(1, -1) + S(1, 1)) /
-              T(16.0);
+  const int64_t c = at(g, ix, iy), n = g.nxg;
+  const T v = (4 * s[c] + 2 * (s[c - 1] + s[c + 1] + s[c - n] + s[c + n]) +
+                    s[c - 1 - n] + s[c - 1 + n] + s[c + 1 - n] + s[c + 1 + n]) /
+                   T(16.0);
   store_with_guards(g, d, ix, iy, v);
 }
 template <typename T>
-__global__ void __launch_bounds__(TX *TY) k_smooth_binomial(G g, const T *s, T *d, int *status) {
-  __shared__ Stage<T, 1> t;
-  smooth_binomial_at(g, s, d, (int)blockIdx.x, (int)blockIdx.y, t, status);
+__global__ void k_smooth_binomial(G g, const T *__restrict__ s, T *d) {
+  smooth_binomial_at(g, s, d, (int)blockIdx.x, (int)blockIdx.y);
 }
 template <typename T>
-__device__ __forceinline__ void smooth_compensate_at(const G &g, const T *d, T *s, int tbx,
-                                                     int tby, Stage<T, 1> &t, int *status) {
-  const int x0 = 1 + tbx * TX, y0 = 1 + tby * TY;
-  const T *const src[1] = {d};
-  if (!stage_tiles<T, 1>(g, src, x0, y0, t, status)) return;
-  const int ix = x0 + threadIdx.x;
-  const int iy = y0 + threadIdx.y;
+__device__ __forceinline__ void smooth_compensate_at(const G &g, const T *__restrict__ d, T *s,
+                                                     int tbx, int tby) {
+  const int ix = 1 + tbx * TX + threadIdx.x;
+  const int iy = 1 + tby * TY + threadIdx.y;
   if (ix > g.nx + 1 || iy > g.ny + 1) return;
-  auto D = [&](int dx, int dy) { return staged(t, 0, x0, y0, ix, iy, dx, dy); };
-  const T v = (20 * D(0, 0) - D(-1, 0) - D(1, 0) - D(0, -1) - D(0, 1) - D(-1, -1) - D(-1, 1) -
-               D(1, -1) - D(1, 1)) /
-              T(12.0);
+  const int64_t c = at(g, ix, iy), n = g.nxg;
+  const T v = (20 * d[c] - d[c - 1] - d[c + 1] - d[c - n] - d[c + n] - d[c - 1 - n] -
+                    d[c - 1 + n] - d[c + 1 - n] - d[c + 1 + n]) /
+                   T(12.0);
   store_with_guards(g, s, ix, iy, v);
 }
 template <typename T>
-__global__ void __launch_bounds__(TX *TY) k_smooth_compensate(G g, const T *d, T *s,
-                                                              int *status) {
-  __shared__ Stage<T, 1> t;
-  smooth_compensate_at(g, d, s, (int)blockIdx.x, (int)blockIdx.y, t, status);
+__global__ void k_smooth_compensate(G g, const T *__restrict__ d, T *s) {
+  smooth_compensate_at(g, d, s, (int)blockIdx.x, (int)blockIdx.y);
 }
 
 // ---- Poisson right-hand side (pic/fields.f90:392-405): f = (div E - rho)
