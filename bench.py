@@ -26,6 +26,9 @@ N > 1 : one process per GPU in em2's particle decomposition: each rank holds
         the whole grid and a full workload of particles (weak scaling), and
         rho/J and the kinetic energies are summed over ranks with an NCCL
         allreduce every step (pic/curnt.f90:363-376); time = max over ranks.
+--only-adjoint, --only-ensemble : one leg alone, printed as its own JSON
+        object (for profiling); --only-ensemble with --variant V and
+        --sort-interval K skips the autotuner.
 """
 from __future__ import annotations
 
@@ -62,6 +65,9 @@ def parse():
                     help="sort interval to use with --variant")
     ap.add_argument("--only-adjoint", action="store_true",
                     help="run only the adjoint leg and print its JSON")
+    ap.add_argument("--only-ensemble", action="store_true",
+                    help="run only the ensemble leg and print its JSON (with --variant and "
+                         "--sort-interval: those, without the autotuner)")
     # the 512x256 workload's adjoint: 800 steps, checkpoints every 50
     ap.add_argument("--adjoint-steps", type=int, default=800)
     ap.add_argument("--adjoint-checkpoint", type=int, default=50)
@@ -544,7 +550,13 @@ def run_ensemble(args, local):
     cfgs = harris_ensemble(64, seed=0)
     ens = load_harris(cfgs, device=f"cuda:{local}")
     try:
-        tuned = autotune_ensemble(ens)  # the project's autotuner, on this batch
+        if args.only_ensemble and args.variant is not None:
+            ens.set_variant(args.variant)
+            ens.set_sort_interval(args.sort_interval)
+            tuned = {"variant": args.variant, "sort_interval": args.sort_interval,
+                     "times_ms": None, "interval_ms": None}
+        else:
+            tuned = autotune_ensemble(ens)  # the project's autotuner, on this batch
         # warm-up: at least two regrouping cycles, so that the graph of every
         # kind of step is captured before the timing
         ens.step(max(args.warmup, 2 * tuned["sort_interval"]))
@@ -620,6 +632,11 @@ def main():
         from maccpic_b200 import build
         build.build()
         print(json.dumps({"adjoint": run_adjoint(args, 0)}), flush=True)
+        return
+    if args.only_ensemble:
+        from maccpic_b200 import build
+        build.build()
+        print(json.dumps({"ensemble": run_ensemble(args, 0)}), flush=True)
         return
     if args.impl == "reference":
         run_reference(args)
