@@ -2,7 +2,7 @@
 """Throughput of em2's time step on B200: particle-steps/s.
 
 One step is em2's main-loop pass move -> curnt -> it+1 -> fields
-(pic/main.f90:286-303) over the whole synthetic double-Harris workload
+(pic/main.f90:154-169) over the whole synthetic double-Harris workload
 (default 2048x1024 cells, 64 particles per cell per species, 268M
 particles), run through libem2g.  Prints one JSON line (rank 0).
 

@@ -5,14 +5,14 @@
  *
  * em2's step is four parameterless Fortran subroutines that act on the
  * module `global` (pic/global.f90:31-45), called from the main loop
- * (pic/main.f90:286-303):
+ * (pic/main.f90:154-169):
  *     call move; call curnt; [output]; it = it + 1; call fields
  * plus `smooth2(sm)` (pic/smooth.f90:95) which fields calls.  This library
  * keeps the state that `global` holds -- E, B, rho, the six current arrays
  * and the particles -- resident on one GPU and exposes one entry point per
  * subroutine, plus host/device copies of that state, so that a thin
  * iso_c_binding shim can stand in for move.o, curnt.o, fields.o and
- * smooth.o (pic/Makefile:4) without touching main.f90 or output.f90.
+ * smooth.o (pic/Makefile:7) without touching main.f90 or output.f90.
  *
  * Conventions
  *  - Every function returns an int status: EM2G_OK (0) or an EM2G_ERR_*
@@ -59,16 +59,16 @@ enum em2g_precision {
   EM2G_FP32 = 1   /* mixed: FP32 push/deposit/Yee, FP64 reductions */
 };
 
-/* field ids, in the order of the reference's arrays (pic/global.f90:127-129) */
+/* field ids, in the order of the reference's arrays (pic/global.f90:41-43) */
 enum em2g_field {
   EM2G_EX = 0, EM2G_EY, EM2G_EZ, EM2G_BX, EM2G_BY, EM2G_BZ, EM2G_RHO,
   EM2G_JXM, EM2G_JXP, EM2G_JYM, EM2G_JYP, EM2G_JZM, EM2G_JZP, EM2G_NFIELD
 };
 
 /* Run constants.  They replace the compile-time parameters of
- * pic/input.f90:9-43 and the derived constants of pic/global.f90:101-114;
+ * pic/input.f90:9-43 and the derived constants of pic/global.f90:18-28;
  * per-species values are those of com_den (pic/input.f90:61-69) and init
- * (pic/init.f90:295-297).  Fill with em2g_params_init() first. */
+ * (pic/init.f90:116-119).  Fill with em2g_params_init() first. */
 typedef struct em2g_params {
   uint32_t struct_size;  /* = sizeof(em2g_params) */
   int32_t nx, ny;        /* cells (>= 4 each) */
@@ -139,7 +139,7 @@ int em2g_set_particles_device(em2g_ctx *ctx, int isp, int64_t n, const double *x
  * pointers NULL it only reports the count. */
 int em2g_get_particles(em2g_ctx *ctx, int isp, int64_t *n, double *x, double *y,
                        double *vx, double *vy, double *vz, double *gamma);
-/* the step counter `it` of pic/global.f90:117 (fields reads it) */
+/* the step counter `it` of pic/global.f90:31 (fields reads it) */
 int em2g_set_step(em2g_ctx *ctx, int it);
 int em2g_get_step(em2g_ctx *ctx, int *it);
 
@@ -170,7 +170,7 @@ int em2g_smooth2(em2g_ctx *ctx, int field_id);
  * em2g_move then em2g_curnt, but the current is kept as the sum jm+jp in
  * the jxm/jym/jzm arrays with jxp/jyp/jzp zero (fields reads only the sum,
  * pic/fields.f90:211-214).  A shim can map em2's `call move` to nothing and
- * `call curnt` to this (nothing reads v between them, pic/main.f90:287-288). */
+ * `call curnt` to this (nothing reads v between them, pic/main.f90:154-155). */
 int em2g_move_curnt(em2g_ctx *ctx, double *ake_out);
 
 /* ---- fused fast path -------------------------------------------------

@@ -205,7 +205,7 @@ std::unique_ptr<EnsGrid32> make_grid_table(em2g_ens *e) {
     D.tiles_x = (R.g.nx + 1 + TX - 1) / TX;
     const double alx = R.P.dx * R.g.nx, aly = R.P.dy * R.g.ny;
     const double q = R.P.qme / R.P.wpe / R.P.c;
-    D.anorml1 = 0.5 * R.P.dx * R.P.dy * (q * q / (alx * aly));  // pic/global.f90:112
+    D.anorml1 = 0.5 * R.P.dx * R.P.dy * (q * q / (alx * aly));  // pic/global.f90:26-27
     D.out = e->dev_out + (int64_t)r * kEnsOut;
     t->sten0[r] = s0;
     t->foldx0[r] = fx;

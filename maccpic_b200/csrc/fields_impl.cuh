@@ -96,7 +96,7 @@ int energies_t(em2g_ctx *c, const T *fld) {
   int lo = 1, hi = g.ny;
   const double alx = c->P.dx * g.nx, aly = c->P.dy * g.ny;
   const double t = c->P.qme / c->P.wpe / c->P.c;
-  const double rnmec2i = t * t / (alx * aly);  // pic/global.f90:112
+  const double rnmec2i = t * t / (alx * aly);  // pic/global.f90:26-27
   const double anorml1 = 0.5 * c->P.dx * c->P.dy * rnmec2i;
   if (c->P.energy_mode == 1) {
     lo = 88;

@@ -26,7 +26,7 @@ import numpy as np
 
 def rank_slice(n: int, rank: int, world: int) -> slice:
     """Contiguous share of n slots for `rank`, as em2 gives each rank
-    MYRANK*maxnp+1 .. MYRANK*maxnp+np (pic/init.f90:204)."""
+    MYRANK*maxnp+1 .. MYRANK*maxnp+np (pic/init.f90:25)."""
     lo = n * rank // world
     hi = n * (rank + 1) // world
     return slice(lo, hi)

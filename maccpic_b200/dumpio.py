@@ -11,7 +11,7 @@ before and after the data:
   (y, vx, vy, vz, g)  MYRANK*maxnp+1 .. (MYRANK+1)*maxnp
 
 The restart point is after ``curnt`` of the last step and before its
-``fields``; ``cont`` then calls ``fields`` once (pic/cont.f90:403-406) and the
+``fields``; ``cont`` then calls ``fields`` once (pic/cont.f90:97) and the
 main loop carries on.  :func:`save` / :func:`load` do the same for an
 :class:`~maccpic_b200.em2.Em2Gpu` (or any object with get/set_fields and
 get/set_particles), so runs can move between em2 and this library.
@@ -124,7 +124,7 @@ def save(run, directory: str, rank: int = 0) -> None:
 
 def load(run, directory: str, counts, rank: int = 0) -> None:
     """Read em2 restart files into an Em2Gpu; the caller then runs
-    fields(it0+1) as ``cont`` does (pic/cont.f90:403-406)."""
+    fields(it0+1) as ``cont`` does (pic/cont.f90:97)."""
     fld, parts = read_restart(directory, run.p.nx, run.p.ny, counts, rank)
     run.set_fields(fld)
     for s, p in enumerate(parts):

@@ -1,7 +1,7 @@
 """Host-side mirror of em2's step interface on the GPU.
 
 em2 (fanyumeng666/maccpic, pic/) advances its state with parameterless
-subroutines acting on the module ``global`` (pic/global.f90:117-131):
+subroutines acting on the module ``global`` (pic/global.f90:31-45):
 
     call move     ! pic/move.f90:2     -> Em2Gpu.move()   (returns ake)
     call curnt    ! pic/curnt.f90:2    -> Em2Gpu.curnt()
@@ -29,10 +29,10 @@ from ._lib import FIELD_ID, FIELD_NAMES, NFIELD, check
 
 @dataclass
 class RunParams:
-    """Run constants: pic/input.f90:9-43 and derived pic/global.f90:101-114.
+    """Run constants: pic/input.f90:9-43 and derived pic/global.f90:18-28.
 
     Per-species values follow com_den (pic/input.f90:61-69) and init
-    (pic/init.f90:295-297): ``qm`` charge/mass, ``q`` macro charge, ``dn``
+    (pic/init.f90:116-119): ``qm`` charge/mass, ``q`` macro charge, ``dn``
     relative density, ``am`` macro mass."""
     nx: int
     ny: int

@@ -6,12 +6,12 @@
  * 1.0, sheet-1 mean vz -0.0257 c / +0.1070 c, deposited jz 0.663 against
  * 0.669 from the discrete curl of B), which were produced by em2's own
  * loader.  Restated here, in the reference's evaluation order:
- *   init (fields and species constants)  pic/init.f90:225-298
+ *   init (fields and species constants)  pic/init.f90:2-130
  *   com_den                               pic/input.f90:61-69
- *   maxnp                                 pic/global.f90:101
+ *   maxnp                                 pic/global.f90:15
  *   creator                               pic/creator.f90:24-243
- *   smear                                 pic/smear.f90:247-292
- *   dran2 (ran2 of Numerical Recipes)     pic/dran2.f90:294-334
+ *   smear                                 pic/smear.f90:2-47
+ *   dran2 (ran2 of Numerical Recipes)     pic/dran2.f90:2-42
  *   setv (-dt/2 push, linear weights)     pic/setv.f90:30-133
  * Single-precision literals of the reference (0.1 in init.f90:251-252,
  * 0.001 in creator.f90:120) are kept as float constants.
@@ -30,7 +30,7 @@ typedef struct {
 
 static const double PI = 3.141592653589793;
 
-/* pic/global.f90:101 */
+/* pic/global.f90:15 */
 int64_t em2o_maxnp(const em2o_load_params *L) {
   const double gsum = (double)(L->ny / 2) +
                       2 * L->csw / L->dx * L->csden *
@@ -40,7 +40,7 @@ int64_t em2o_maxnp(const em2o_load_params *L) {
   return (int64_t)(tot / L->nproc);
 }
 
-/* pic/input.f90:61-69 and pic/init.f90:291-298 (nsp = 2) */
+/* pic/input.f90:61-69 and pic/init.f90:112-119 (nsp = 2) */
 void em2o_com_den(const em2o_load_params *L, double *q, double *qm,
                   double *dn, double *am) {
   const double wpe = 1.0, qme = -1.0, qmi = -qme / L->rmass;
@@ -53,7 +53,7 @@ void em2o_com_den(const em2o_load_params *L, double *q, double *qm,
   am[1] = q[1] / qmi;
 }
 
-/* pic/init.f90:228-271: zero fields, double-Harris Bx plus perturbation */
+/* pic/init.f90:46-92: zero fields, double-Harris Bx plus perturbation */
 void em2o_init_fields(const em2o_load_params *L, double *fld) {
   const int nx = L->nx, ny = L->ny, nx2 = nx + 2, ny2 = ny + 2;
   const int64_t nxg = nx + 3, w = (int64_t)(nx + 3) * (ny + 3);
@@ -88,7 +88,7 @@ void em2o_init_fields(const em2o_load_params *L, double *fld) {
 }
 
 /* ran2 with Bays-Durham shuffle, state kept as in the SAVE variables of
- * pic/dran2.f90:308-310 */
+ * pic/dran2.f90:16-18 */
 typedef struct {
   int32_t idum2, iy, iv[32];
 } ran2_state;
@@ -218,7 +218,7 @@ int em2o_creator(const em2o_load_params *L, int myrank, int64_t maxnp,
       Y(s, i) = Y(s, i - nph / 2) + yn * 0.5;
     }
   }
-  /* smear(10): pic/smear.f90:263-291 */
+  /* smear(10): pic/smear.f90:18-46 */
   ran2_state S;
   memset(&S, 0, sizeof S);
   S.idum2 = 123456789;

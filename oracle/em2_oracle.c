@@ -510,7 +510,7 @@ int em2o_poisson(const em2o_params *p, double *fld) {
 
 void em2o_energies(const em2o_params *p, const double *fld, double *e6) {
   /* pic/fields.f90:267-347.  rnmec2i = (qme/wpe/c)**2/(alx*aly),
-   * anorml1 = 0.5*dx*dy*rnmec2i (pic/global.f90:112-113). */
+   * anorml1 = 0.5*dx*dy*rnmec2i (pic/global.f90:26-27). */
   const int64_t nxg = NXG(p), w = W(p);
   const double alx = p->dx * p->nx, aly = p->dy * p->ny;
   const double t = p->qme / p->wpe / p->c;
