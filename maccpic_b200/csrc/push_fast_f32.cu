@@ -25,7 +25,9 @@
 // particle's state loaded while the current one runs.  The scaled fields the
 // segment's particles can touch (x nodes x0-1 .. x0+TCX+3, y nodes y0-1 ..
 // y0+4) are staged once in shared memory as (E, B) pairs of the three
-// staggerings, so a gather is 27 shared float2 loads.  A particle still in
+// staggerings, each window entry holding the pairs of two neighbouring x
+// nodes, so a gather is 9 shared float4 and 9 float2 loads (27 points).
+// A particle still in
 // the lane's cell adds its rho and J into a 49-value register block (Jx 4x3,
 // Jy 3x4, Jz 3x3, rho 4x4) -- every lane runs the update, with zero charge
 // where its particle is elsewhere or absent; the deposits of one outside it
@@ -131,6 +133,23 @@ __device__ __forceinline__ float2 gather_pair(const float2 *base, int pitch, con
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
     const float2 a = base[k * pitch], b = base[k * pitch + 1], c = base[k * pitch + 2];
+    r[k] = fma2(c, bc2(wx.p), fma2(b, bc2(wx.s), mul2(a, bc2(wx.m))));
+  }
+  return fma2(r[2], bc2(wy.p), fma2(r[1], bc2(wy.s), mul2(r[0], bc2(wy.m))));
+}
+
+// The same gather from the shared window, whose entry (row, col) holds the
+// pair of node col and the pair of node col+1: two loads per stencil row
+// (nodes i-1 and i together, then node i+1) instead of three, the same
+// arithmetic.
+__device__ __forceinline__ float2 gather_pair_win(const float4 *base, int pitch, const Wts &wx,
+                                                  const Wts &wy) {
+  float2 r[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const float4 ab = base[k * pitch];
+    const float2 c = *reinterpret_cast<const float2 *>(base + k * pitch + 2);
+    const float2 a = make_float2(ab.x, ab.y), b = make_float2(ab.z, ab.w);
     r[k] = fma2(c, bc2(wx.p), fma2(b, bc2(wx.s), mul2(a, bc2(wx.m))));
   }
   return fma2(r[2], bc2(wy.p), fma2(r[1], bc2(wy.s), mul2(r[0], bc2(wy.m))));
@@ -332,7 +351,7 @@ struct PartOut {
 // relative to the group cell (kx, ky) with momentum u; `act` false makes it
 // a dry run on harmless input (no deposits, no energy).  cinv = 1/c.
 template <int WXW>
-__device__ __forceinline__ void push_one(const Args32 &a, float2 (*win)[WY][WXW], int x0,
+__device__ __forceinline__ void push_one(const Args32 &a, float4 (*win)[WY][WXW], int x0,
                                          int y0, int kx, int ky, bool act, float xr, float yr,
                                          float ux, float uy, float uz, float cinv, Block32 &b,
                                          double &akel, int &stay_new, PartOut &o) {
@@ -354,9 +373,9 @@ __device__ __forceinline__ void push_one(const Args32 &a, float2 (*win)[WY][WXW]
   // else from global memory at the wrapped cell
   float2 ebx, ebz, eby;
   if ((unsigned)cx < (unsigned)nx && (unsigned)cy < (unsigned)ny) {
-    ebx = gather_pair(&win[0][nyw.i - y0][hx.i - x0], WX, hx, nyw);
-    ebz = gather_pair(&win[1][hy.i - y0][hx.i - x0], WX, hx, hy);
-    eby = gather_pair(&win[2][hy.i - y0][nxw.i - x0], WX, nxw, hy);
+    ebx = gather_pair_win(&win[0][nyw.i - y0][hx.i - x0], WX, hx, nyw);
+    ebz = gather_pair_win(&win[1][hy.i - y0][hx.i - x0], WX, hx, hy);
+    eby = gather_pair_win(&win[2][hy.i - y0][nxw.i - x0], WX, nxw, hy);
   } else {
     const int sx = wrap(cx, nx) - cx, sy = wrap(cy, ny) - cy;
     ebx = gather_pair(a.ebx + (int64_t)(nyw.i + sy - 1) * nxg + hx.i + sx - 1, nxg, hx, nyw);
@@ -440,7 +459,7 @@ __device__ __forceinline__ void push_one(const Args32 &a, float2 (*win)[WY][WXW]
 // that they stay in (-1, 2)); the counts of the new cells are still taken.
 template <int TCX, int G, int NC, bool INPLACE>
 __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, int64_t blk,
-                                             float2 (*win)[WY][NC * TCX + 5], WarpScratch *ws) {
+                                             float4 (*win)[WY][NC * TCX + 5], WarpScratch *ws) {
   constexpr int kThreads = TCX * G;
   constexpr int WX = NC * TCX + 5;  // window columns: x0-1 .. x0+NC*TCX+3
   const int nx = a.nx, ny = a.ny, nxg = a.nxg;
@@ -462,16 +481,18 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
   int32_t end = valid ? a.offA[cell + 1] : 0;
   // the window: array indices x0-1.., y0-1..
   constexpr int kWin = 3 * WY * WX, kWinPer = (kWin + kThreads - 1) / kThreads;
-  float2 wv[kWinPer];
+  float4 wv[kWinPer];  // (node col, node col+1)
 #pragma unroll
   for (int u = 0; u < kWinPer; ++u) {
     const int t = threadIdx.x + u * kThreads;
     const int comp = t / (WY * WX), r = (t / WX) % WY, col = t % WX;
     const int gx = x0 - 1 + col, gy = y0 - 1 + r;
-    wv[u] = make_float2(0.f, 0.f);
+    wv[u] = make_float4(0.f, 0.f, 0.f, 0.f);
     if (t < kWin && gx >= 0 && gx <= nx + 2 && gy >= 0 && gy <= ny + 2) {
       const float2 *src = comp == 0 ? a.ebx : (comp == 1 ? a.ebz : a.eby);
-      wv[u] = src[(int64_t)gy * nxg + gx];
+      const float2 v0 = src[(int64_t)gy * nxg + gx];
+      const float2 v1 = gx + 1 <= nx + 2 ? src[(int64_t)gy * nxg + gx + 1] : make_float2(0.f, 0.f);
+      wv[u] = make_float4(v0.x, v0.y, v1.x, v1.y);
     }
   }
   // software pipeline: the next particle's state is loaded while this one runs
@@ -677,7 +698,7 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
 // allow -- the autotuner's knobs besides the sort interval
 template <int TCX, int G, int NC, int MINB, bool INPLACE>
 __global__ void __launch_bounds__(TCX * G, MINB) k_push_cells_f32(Args32 a) {
-  __shared__ float2 win[3][WY][NC * TCX + 5];
+  __shared__ float4 win[3][WY][NC * TCX + 5];
   __shared__ WarpScratch ws[TCX * G / 32];
   push_segment<TCX, G, NC, INPLACE>(a, (int)blockIdx.x * (NC * TCX), (int)blockIdx.y,
                                 (int64_t)blockIdx.y * gridDim.x + blockIdx.x, win, ws);
@@ -692,7 +713,7 @@ __global__ void __launch_bounds__(TCX * G, MINB) k_push_cells_f32(Args32 a) {
 template <int TCX, int G, int NC, int MINB, bool INPLACE>
 __global__ void __launch_bounds__(TCX * G, MINB)
     k_ens_push_f32(const __grid_constant__ EnsPush32 e) {
-  __shared__ float2 win[3][WY][NC * TCX + 5];
+  __shared__ float4 win[3][WY][NC * TCX + 5];
   __shared__ WarpScratch ws[TCX * G / 32];
   __shared__ int s_tile;
   for (;;) {
