@@ -191,8 +191,11 @@ int em2g_step(em2g_ctx *ctx, int nsteps, double *ake_out, double *energies_out,
  * EM2G_SMOOTH2_STATIC_MAX_POINTS doubles (4 MiB, held by every GPU that loads
  * the library); larger grids are rejected with EM2G_ERR_RANGE.  The first
  * call on a device looks up that array's device address (make it before any
- * stream capture).  Calls share the scratch: calls that overlap on the GPU
- * race, so order them.  No memory is allocated or freed. */
+ * stream capture); calls outside a capture look it up again, calls during
+ * one use the address kept from the last.  Calls share the scratch: calls
+ * that overlap on the GPU race, so order them.  An error left pending by
+ * earlier CUDA work is reported (EM2G_ERR_CUDA) and left pending, not
+ * cleared.  No memory is allocated or freed. */
 #define EM2G_SMOOTH2_STATIC_MAX_POINTS (1 << 19)
 int em2g_smooth2_static(int nx, int ny, double *dev_array, void *cuda_stream);
 

@@ -17,9 +17,12 @@
 // previous call's leftovers never leak into a result.
 //
 // In host code `g_smooth2_scratch` names a host-side stand-in, not a device
-// address: the device address is fetched once per device with
-// cudaGetSymbolAddress, on the first call made with that device current.
-// That first call must therefore come before any stream capture begins.
+// address.  The device address comes from cudaGetSymbolAddress, looked up
+// again on every call made outside a stream capture (the module, and so the
+// array, can move when the caller makes another context current or resets
+// the device) and kept per device for calls made during a capture, where
+// only the kept address is used.  The first call on a device must therefore
+// come before any stream capture begins.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -90,18 +93,30 @@ extern "C" int em2g_smooth2_static(int nx, int ny, double *dev_array, void *cuda
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return em2g::cuda_fail(e, "cudaGetDevice");
   if (dev < 0 || dev >= kMaxDevices) return fail(EM2G_ERR_INVALID, "smooth2_static: device ordinal");
+  // an error left pending by earlier work of another component is not this
+  // call's: report it as such and leave it pending for its owner
+  e = cudaPeekAtLastError();
+  if (e != cudaSuccess)
+    return fail(EM2G_ERR_CUDA, std::string("smooth2_static: an earlier CUDA error is pending "
+                                           "(not from this call): ") + cudaGetErrorString(e));
+  cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  e = cudaStreamIsCapturing(st, &cap);
+  if (e != cudaSuccess) return em2g::cuda_fail(e, "cudaStreamIsCapturing");
   double *scratch = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_addr[dev]) {
+    if (cap == cudaStreamCaptureStatusNone) {
       void *p = nullptr;
       e = cudaGetSymbolAddress(&p, g_smooth2_scratch);
       if (e != cudaSuccess) return em2g::cuda_fail(e, "cudaGetSymbolAddress(g_smooth2_scratch)");
       g_scratch_addr[dev] = static_cast<double *>(p);
+    } else if (!g_scratch_addr[dev]) {
+      return fail(EM2G_ERR_INVALID,
+                  "smooth2_static: the first call on a device must come before a stream capture");
     }
     scratch = g_scratch_addr[dev];
   }
-  cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
   const dim3 blk(TX, TY), grd((nx + 1 + TX - 1) / TX, (ny + 1 + TY - 1) / TY);
   k_binomial_static<<<grd, blk, 0, st>>>(nx, ny, dev_array, scratch);
   k_compensate_static<<<grd, blk, 0, st>>>(nx, ny, scratch, dev_array);

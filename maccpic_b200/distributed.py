@@ -14,7 +14,8 @@ interface so that the same code drives the GPU library (:class:`GpuBackend`)
 and, in tests, the CPU oracle:
 
     backend.move_curnt() -> ake (nsp FP64 values of this rank's particles)
-    backend.deposits()   -> tensor view of this rank's rho/J block (7 arrays)
+    backend.deposits()   -> list of tensor views of this rank's rho/J arrays
+                            that hold deposits (each reduced in place)
     backend.fields(it)   -> (cg iterations, energies or None)
 """
 from __future__ import annotations
@@ -43,7 +44,13 @@ class _DeviceArray:
 class GpuBackend:
     """An :class:`~maccpic_b200.em2.Em2Gpu` context holding this rank's
     particles; the library runs on torch's current stream so that the
-    collectives are ordered after its kernels."""
+    collectives are ordered after its kernels.
+
+    The fused push (em2g_move_curnt) deposits the whole current, jm + jp,
+    into jxm, jym and jzm and leaves jxp, jyp and jzp zero (their only
+    consumer is the sum, pic/fields.f90:211-214), so the arrays to sum over
+    ranks are rho, jxm, jym and jzm: 4 of em2's 7 (pic/curnt.f90:363-369).
+    rho and jxm are adjacent in the field block, so they go as one view."""
 
     def __init__(self, gpu):
         import torch
@@ -53,15 +60,20 @@ class GpuBackend:
         ptr = C.c_void_p()
         _lib.check(gpu._L.em2g_field_device_ptr(gpu._h, _lib.FIELD_ID["rho"], C.byref(ptr)))
         w = (gpu.p.nx + 3) * (gpu.p.ny + 3)
-        typestr = "<f4" if gpu.p.precision == _lib.FP32 else "<f8"
-        # rho, jxm, jxp, jym, jyp, jzm, jzp are contiguous in the field block
-        self._view = torch.as_tensor(_DeviceArray(ptr.value, 7 * w, typestr), device="cuda")
+        fp32 = gpu.p.precision == _lib.FP32
+        typestr, word = ("<f4", 4) if fp32 else ("<f8", 8)
+        base = ptr.value  # rho; then jxm, jxp, jym, jyp, jzm, jzp, each w words
+
+        def view(first, count):
+            return torch.as_tensor(_DeviceArray(base + first * w * word, count * w, typestr),
+                                   device="cuda")
+        self._views = [view(0, 2), view(3, 1), view(5, 1)]  # rho+jxm, jym, jzm
 
     def move_curnt(self):
         return self.g.move_curnt()
 
     def deposits(self):
-        return self._view
+        return self._views
 
     def fields(self, it):
         return self.g.fields(it)
@@ -79,10 +91,11 @@ class ParticleDecomposition:
         import torch
         import torch.distributed as dist
         ake = np.asarray(self.b.move_curnt(), dtype=np.float64)
-        dep = self.b.deposits()
-        if dist.is_initialized() and dist.get_world_size(self.group) > 1:
-            dist.all_reduce(dep, op=dist.ReduceOp.SUM, group=self.group)
-            t = torch.tensor(ake, dtype=torch.float64, device=dep.device)
+        if dist.is_initialized():
+            deps = self.b.deposits()
+            for d in deps:
+                dist.all_reduce(d, op=dist.ReduceOp.SUM, group=self.group)
+            t = torch.tensor(ake, dtype=torch.float64, device=deps[0].device)
             dist.all_reduce(t, op=dist.ReduceOp.SUM, group=self.group)
             ake = t.cpu().numpy()
         n, e = self.b.fields(it)

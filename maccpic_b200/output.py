@@ -94,6 +94,26 @@ class Em2Output:
         if self._err is not None:
             raise RuntimeError("output writer failed") from self._err
 
+    # ---- em2's output call -----------------------------------------------------
+    def output(self, run, it: int, ake, isav: int = 20, iphs: int = 1000):
+        """What em2's ``output`` writes at step ``it`` (pic/output.f90:130-247),
+        from a GPU run (:class:`~maccpic_b200.em2.Em2Gpu`): the energy line at
+        it == 1 and every isav steps, with the field energies computed on the
+        GPU in FP64 for the current fields (``em2g_diagnostics``); the Bz frame
+        every 100 steps; the profiles every isav steps; the 2D snapshots every
+        iphs steps.  Arrays are copied from the device here, and formatted and
+        written on the worker thread."""
+        fields = None
+        if it == 1 or (it != 0 and it % isav == 0):
+            self.energies(it, run.diagnostics()["energies"], ake)
+            fields = run.get_fields()
+            # a new profile file every idata = 1024 records (pic/output.f90:204-215)
+            self.profiles(fields, iii=(it // isav) // 1024 + 1)
+        if it % 100 == 0:
+            self.bz_frame(it, run.get_field("bz"))
+        if it % iphs == 0:
+            self.snapshot(it, fields if fields is not None else run.get_fields())
+
     # ---- writers -----------------------------------------------------------
     def energies(self, it: int, e6, ake):
         """ene###.hst line (pic/output.f90:191-199); ake as move returns it."""

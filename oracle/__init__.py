@@ -99,6 +99,8 @@ def lib():
         L.em2o_init_fields.argtypes = [lp, dp]
         L.em2o_creator.restype = C.c_int
         L.em2o_creator.argtypes = [lp, C.c_int, C.c_int64, C.POINTER(dp)]
+        L.em2o_last_cg_residuals.restype = None
+        L.em2o_last_cg_residuals.argtypes = [dp]
         L.em2o_setv.restype = None
         L.em2o_setv.argtypes = [pp, dp, C.c_int, C.c_int64, dp]
         _lib = L
@@ -202,6 +204,14 @@ class State:
                             _dp(ake), _dp(e6))
         self.it += 1
         return {"cg_iters": n, "ake": ake[:nsp].copy(), "energies": e6}
+
+
+def last_cg_residuals() -> np.ndarray:
+    """Mean r^2 of the last cgm solve (any State or poisson call of this
+    process): before the first iteration and at exit."""
+    out = np.zeros(2)
+    lib().em2o_last_cg_residuals(_dp(out))
+    return out
 
 
 def smooth2(params: Params, a: np.ndarray) -> np.ndarray:

@@ -378,6 +378,13 @@ void em2o_smooth2(const em2o_params *p, double *sm) {
 /* cgm on (nx1, ny1) arrays stored 1-based in a (nx+2)*(ny+2) buffer;
  * pic/fields.f90:508-651 */
 #define CI(j, l) ((int64_t)(l) * (nx + 2) + (j))
+/* mean r^2 of the last cgm before its first iteration and at its exit (the
+ * quantities em2g_diagnostics reports; test bookkeeping, not part of em2) */
+static double g_last_res[2];
+void em2o_last_cg_residuals(double *out) {
+  out[0] = g_last_res[0];
+  out[1] = g_last_res[1];
+}
 static int cgm(const em2o_params *p, const double *f, double *u) {
   const int nx = p->nx, ny = p->ny, nx1 = nx + 1, ny1 = ny + 1;
   const size_t sz = (size_t)(nx + 2) * (size_t)(ny + 2);
@@ -402,6 +409,7 @@ static int cgm(const em2o_params *p, const double *f, double *u) {
     double rr = 0.0;
     for (int j = 1; j <= nx; ++j)
       for (int l = 1; l <= ny; ++l) rr = rr + sq(r[CI(j, l)]);
+    if (n == 1) g_last_res[0] = rr / nx / ny;
     for (int j = 1; j <= nx; ++j) {
       const int jm = (j == 1) ? nx : j - 1;
       for (int l = 1; l <= ny; ++l) {
@@ -429,6 +437,7 @@ static int cgm(const em2o_params *p, const double *f, double *u) {
     double r_norm = 0.0;
     for (int j = 1; j <= nx; ++j)
       for (int l = 1; l <= ny; ++l) r_norm = r_norm + sq(r1[CI(j, l)]);
+    g_last_res[1] = r_norm / nx / ny;
     if (r_norm / nx / ny < p->cg_eps) break;
     const double bk = r_norm / rr;
     for (int j = 1; j <= nx; ++j) {

@@ -76,6 +76,8 @@ void em2o_smooth2(const em2o_params *p, double *a);
  * Returns the CG iteration count n at exit (cg_maxits+1 if MAXITS was
  * exceeded, matching the loop variable after a completed DO loop). */
 int em2o_poisson(const em2o_params *p, double *fld);
+/* mean r^2 of the last cgm solve before its first iteration and at exit */
+void em2o_last_cg_residuals(double *out);
 
 /* field energies exe,eye,eze,bxe,bye,bze (pic/fields.f90:267-347) */
 void em2o_energies(const em2o_params *p, const double *fld, double *e6);

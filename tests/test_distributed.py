@@ -24,7 +24,8 @@ class OracleBackend:
         return ake
 
     def deposits(self):
-        return self._dep
+        # the oracle deposits jm and jp separately, as em2 does: all 7 arrays
+        return [self._dep]
 
     def fields(self, it):
         return self.st.fields(it)

@@ -4,7 +4,9 @@ their device memory themselves or are inside a stream capture) and so cannot
 create an em2g context.  Its scratch is a fixed static device array shared
 by all calls.  Checked against the context entry point em2g_smooth2 on two
 calls in a row (different grids, so the shared scratch is reused), with the
-tolerance of the FP64 stencil tests: bitwise equality.
+tolerance of the FP64 stencil tests: bitwise equality.  Each result is also
+checked bitwise against the oracle's smooth2, so the entry point is pinned
+to em2's filter independently of the context path.
 """
 import ctypes as C
 
@@ -34,14 +36,22 @@ def _static_smooth(nx, ny, t):
     torch.cuda.synchronize()
 
 
-def test_static_smooth2_matches_context_entry_point(gpu):
+def _oracle_smooth(oracle, nx, ny, a):
+    op = oracle.Params(nx=nx, ny=ny, dx=0.5, dy=0.5, dt=0.05, qm=[-1.0], q=[-1.0], dn=[1.0],
+                       am=[1.0], nsp=1)
+    return oracle.smooth2(op, a)
+
+
+def test_static_smooth2_matches_context_entry_point(gpu, oracle_lib):
     import torch
     rng = np.random.default_rng(21)
     for nx, ny in ((40, 24), (96, 70)):       # two calls in a row, two grids
         a = rng.normal(size=(ny + 3, nx + 3))
         t = torch.from_numpy(a.copy()).cuda()
         _static_smooth(nx, ny, t)
-        np.testing.assert_array_equal(t.cpu().numpy(), _reference_smooth(nx, ny, a))
+        got = t.cpu().numpy()
+        np.testing.assert_array_equal(got, _reference_smooth(nx, ny, a))
+        np.testing.assert_array_equal(got, _oracle_smooth(oracle_lib, nx, ny, a))
     # and twice on the same array
     nx, ny = 33, 17
     a = rng.normal(size=(ny + 3, nx + 3))
