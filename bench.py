@@ -306,7 +306,47 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def precision_compare(args, cfg, local, parts, fields, stream, tuned):
+class ParticleSource:
+    """The seeded particles of a workload on one GPU: drawn once and kept on
+    the device when both species' FP64 state (96 bytes per particle pair)
+    takes at most an eighth of the device's memory, otherwise drawn again
+    slice by slice for every upload (the 4096x2048, 100-per-cell workload:
+    80 GB of FP64 state beside a run of 80 GB FP32 or 175 GB FP64)."""
+
+    def __init__(self, cfg, local):
+        import torch
+        from maccpic_b200 import loader
+        self.cfg, self.device = cfg, f"cuda:{local}"
+        self.n = cfg.nx * cfg.ny * cfg.ppc
+        total = torch.cuda.get_device_properties(local).total_memory
+        self.parts = None
+        if 96 * self.n <= total // 8:
+            self.parts = loader.sample_particles_torch(cfg, device=self.device)
+            torch.cuda.synchronize()
+
+    def load(self, g):
+        import torch
+        from maccpic_b200 import loader
+        if self.parts is not None:
+            for s in range(2):
+                g.set_particles_device(s, self.parts[s])
+            return
+        for s in range(2):
+            g.set_particles_slices(s, self.n, (sl[s] for sl in loader.sample_particles_torch_slices(
+                self.cfg, device=self.device)))
+        torch.cuda.empty_cache()
+
+    def host(self):
+        """Both species in pinned host memory (whole mode only)."""
+        return [p.cpu().pin_memory() for p in self.parts]
+
+    def free(self):
+        import torch
+        self.parts = None
+        torch.cuda.empty_cache()
+
+
+def precision_compare(args, cfg, local, src, fields, stream, tuned):
     """The mixed FP32 path against the FP64 path from one initial state over
     the workload's own length (or --compare-steps), every `every` steps:
     the energy of each field component (Ex, Ey, Ez, By, Bz, and Bx - Bx(0),
@@ -317,23 +357,23 @@ def precision_compare(args, cfg, local, parts, fields, stream, tuned):
     import dataclasses
     import numpy as np
     import torch
-    from maccpic_b200 import _lib, loader
+    from maccpic_b200 import _lib
     from maccpic_b200.em2 import Em2Gpu
-    steps = args.compare_steps or cfg.steps
+    steps = args.compare_steps or cfg.check_steps or cfg.steps
     every = max(1, min(50, steps))
     nx, ny = cfg.nx, cfg.ny
     bx0 = fields[3, 1:ny + 1, 1:nx + 1]
     names = ["ex", "ey", "ez", "by", "bz", "bx_minus_bx0", "field_total", "flux_sheet1",
              "flux_sheet2", "kinetic"]
 
-    def series(precision, particles):
+    def series(precision, source):
+        torch.cuda.empty_cache()
         rp = cfg.run_params(device=local, precision=precision)
         g = Em2Gpu(rp)
         try:
             g.set_stream(stream)
             g.set_fields(fields)
-            for s in range(2):
-                g.set_particles_device(s, particles[s])
+            source.load(g)
             if precision == _lib.FP32:
                 g.set_variant(tuned["variant"])
                 g.set_sort_interval(tuned["sort_interval"])
@@ -357,13 +397,11 @@ def precision_compare(args, cfg, local, parts, fields, stream, tuned):
         finally:
             g.close()
 
-    q32, t32 = series(_lib.FP32, parts)
-    q64, t64 = series(_lib.FP64, parts)
-    other = loader.sample_particles_torch(dataclasses.replace(cfg, seed=cfg.seed + 1),
-                                          device=f"cuda:{local}")
+    q32, t32 = series(_lib.FP32, src)
+    q64, t64 = series(_lib.FP64, src)
+    other = ParticleSource(dataclasses.replace(cfg, seed=cfg.seed + 1), local)
     q64b, _ = series(_lib.FP64, other)
-    del other
-    torch.cuda.empty_cache()
+    other.free()
     rel = np.abs(q32 - q64) / np.abs(q64)
     spread = np.abs(q64b - q64) / np.abs(q64)
     return {"steps": steps, "every": every, "quantities": names,
@@ -375,7 +413,7 @@ def precision_compare(args, cfg, local, parts, fields, stream, tuned):
             "final_fp64": dict(zip(names, q64[-1].tolist()))}
 
 
-def measure(args, cfg, precision, local, parts, fields, stream, ws):
+def measure(args, cfg, precision, local, src, fields, stream, ws):
     """Device-resident run: warm-up, then K timed steps.  Returns timings,
     counters and the final fields and kinetic energies."""
     import torch
@@ -388,17 +426,17 @@ def measure(args, cfg, precision, local, parts, fields, stream, ws):
         # that the plasma is the same one, sampled N times more finely
         rp.q = [q / ws for q in rp.q]
         rp.am = [a / ws for a in rp.am]
+    torch.cuda.empty_cache()
     g = Em2Gpu(rp)
     g.set_stream(stream)
     g.set_fields(fields)
-    for s in range(2):
-        g.set_particles_device(s, parts[s])
+    src.load(g)
     torch.cuda.synchronize()
     # the project's autotuner picks the push variant and the sort interval on
     # this state (its steps are part of the warm-up), unless they are given
     from maccpic_b200 import autotune
     if args.variant is None:
-        tuned = autotune.autotune(g, particles=parts[0].shape[1], use_cache=False, cache=None)
+        tuned = autotune.autotune(g, particles=src.n, use_cache=False, cache=None)
     else:
         k = min(args.sort_interval, g.max_sort_interval())
         g.set_variant(args.variant)
@@ -407,8 +445,7 @@ def measure(args, cfg, precision, local, parts, fields, stream, ws):
                  "sort_interval": k, "interval_ms": None}
     # back to the initial state, so that every measured run starts from it
     g.set_fields(fields)
-    for s in range(2):
-        g.set_particles_device(s, parts[s])
+    src.load(g)
     g.it = 0
     if ws > 1:
         from maccpic_b200.distributed import GpuBackend, ParticleDecomposition
@@ -462,10 +499,9 @@ def run_ours(args):
     W = (cfg.nx + 3) * (cfg.ny + 3)
     import dataclasses
     rank_cfg = dataclasses.replace(cfg, seed=cfg.seed * 1000 + rank)
-    parts = loader.sample_particles_torch(rank_cfg, device=f"cuda:{local}")
-    torch.cuda.synchronize()
+    src = ParticleSource(rank_cfg, local)
 
-    main = measure(args, cfg, _lib.FP32 if fp32 else _lib.FP64, local, parts, fields, stream, ws)
+    main = measure(args, cfg, _lib.FP32 if fp32 else _lib.FP64, local, src, fields, stream, ws)
     ms = main["ms"]
     value = n_total * ws * args.steps / (ms / 1e3)
     # the FP64 path on the same initial state: its speed, timed as the main
@@ -473,18 +509,18 @@ def run_ours(args):
     # workload's whole length
     compare = None
     if fp32 and not args.no_fp64_compare:
-        ref = measure(args, cfg, _lib.FP64, local, parts, fields, stream, ws)
+        ref = measure(args, cfg, _lib.FP64, local, src, fields, stream, ws)
         compare = {"fp64_value": n_total * ws * args.steps / (ref["ms"] / 1e3),
                    "fp64_ms_per_step": ref["ms"] / args.steps,
                    "speedup_fp32_over_fp64": ref["ms"] / ms}
         if ws == 1:
-            compare.update(precision_compare(args, cfg, local, parts, fields, stream,
+            compare.update(precision_compare(args, cfg, local, src, fields, stream,
                                              main["tuned"]))
+    whole = src.parts is not None
     parts_host = None
-    if rank == 0 and (not args.no_e2e or not args.no_cpu_baseline):
-        parts_host = [p.cpu().pin_memory() for p in parts]
-    del parts
-    torch.cuda.empty_cache()
+    if rank == 0 and whole and (not args.no_e2e or not args.no_cpu_baseline):
+        parts_host = src.host()
+    src.free()
 
     cnt = main["counters"]
     # roofline of the dominant kernel (the fused push of one species):
@@ -501,7 +537,7 @@ def run_ours(args):
     traffic = profile_traffic(f"{kernel}_{args.config}")
 
     e2e = None
-    if rank == 0 and not args.no_e2e:
+    if rank == 0 and whole and not args.no_e2e:
         rp = cfg.run_params(precision=_lib.FP32 if fp32 else _lib.FP64,
                             sort_interval=main["tuned"]["sort_interval"])
         e2e = run_e2e(args, cfg, rp, fields, parts_host, main["tuned"]["variant"])
@@ -512,7 +548,7 @@ def run_ours(args):
     if rank == 0 and ws == 1 and not args.no_adjoint:
         adj = run_adjoint(args, local)
     cpu = None
-    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+    if rank == 0 and ws == 1 and whole and not args.no_cpu_baseline:
         cpu = cpu_baseline(cfg, fields, [p.numpy() for p in parts_host])
         del parts_host
     if rank == 0:
@@ -594,10 +630,19 @@ def run_adjoint(args, local):
         Bf = ws.final_B()
         t_rev, _ = timed(lambda: ws.backward([torch.zeros_like(b) for b in Bf],
                                              [torch.ones_like(b) * 1e-3 for b in Bf]))
+        # the gradient against central differences of the same forward
+        # (h = 1e-3, common random numbers) at growing horizons
+        fd = {}
+        for t in sorted({min(T, x) for x in (50, 100, 200, 400, T)}):
+            fd[t] = A.fd_check_cuda(cfg, theta, t, h=1e-3, checkpoint=K, draws=d, workspace=ws)
     finally:
         ws.close()
     torch.cuda.empty_cache()
-    return {"workload": "harris_512x256_ppc32", "particles": 2 * cfg.nx * cfg.ny * cfg.ppc,
+    n = 2 * cfg.nx * cfg.ny * cfg.ppc
+    w = (cfg.nx + 3) * (cfg.ny + 3)
+    mem = 8 * (-(-T // K) * (13 * w + 6 * n) + K * 6 * cfg.nx * cfg.ny)
+    agree = [t for t, r in fd.items() if max(r["rel_error"]) <= 0.01]
+    return {"workload": "harris_512x256_ppc32", "particles": n,
             "steps": T, "checkpoint": K, "flux": F, "dflux_dtheta": [float(x) for x in g],
             "forward_ms_per_step": t_fwd * 1e3 / T,
             "recording_forward_ms_per_step": t_rec * 1e3 / T,
@@ -605,6 +650,13 @@ def run_adjoint(args, local):
             "gradient_ms": t_grad * 1e3,
             "gradient_over_forward": t_grad / t_fwd,
             "workspace_setup_ms": t_setup * 1e3,
+            "workspace_bytes": mem,
+            "memory": "checkpoints every K steps (fields + particles) and K field slots; each "
+                      "segment recomputed from its checkpoint in the reverse sweep",
+            "fd_h": 1e-3,
+            "fd_rel_error": max(fd[T]["rel_error"]),
+            "fd": {str(t): r for t, r in fd.items()},
+            "fd_agree_1pct_max_steps": max(agree) if agree else 0,
             "forward": "em2g_step FP64, exact (spectral) Poisson solve"}
 
 

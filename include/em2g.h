@@ -97,7 +97,10 @@ typedef struct em2g_params {
   int32_t poisson;       /* 0: em2's CG (cgm, stops at mean r^2 < cg_eps);
                             1: exact solve by FFT (FP64; nx, ny powers of two
                             <= 8192), a smooth map for the adjoint */
-  int32_t reserved[14];
+  int32_t staging_mib;   /* device staging for host particle copies and the
+                            regrouping, in MiB; 0: 80 bytes x min(largest
+                            np_max, 2^24) (particles move through it in slices) */
+  int32_t reserved[13];
 } em2g_params;
 
 typedef struct em2g_ctx em2g_ctx;
@@ -125,8 +128,10 @@ int em2g_get_fields(em2g_ctx *ctx, double *host13);
 /* n particles of species isp (0-based), in slot order j = 0..n-1.  Input
  * is checked on the device (finite values, 0 <= x < nx+0.5, 0 <= y <
  * ny+0.5) before it replaces anything.  Host copies are staged through one
- * FP64 device buffer, kept until em2g_destroy: the field arrays copied and,
- * in FP32 contexts, 6 x the largest particle count copied, in doubles. */
+ * device buffer kept until em2g_destroy, as large as the field arrays
+ * copied and, for particles, params.staging_mib (by default at most
+ * 80 bytes x 2^24): particles go through it in slices, so it does not grow
+ * with their count. */
 int em2g_set_particles(em2g_ctx *ctx, int isp, int64_t n, const double *x,
                        const double *y, const double *vx, const double *vy,
                        const double *vz, const double *gamma);
@@ -139,6 +144,25 @@ int em2g_set_particles_device(em2g_ctx *ctx, int isp, int64_t n, const double *x
  * pointers NULL it only reports the count. */
 int em2g_get_particles(em2g_ctx *ctx, int isp, int64_t *n, double *x, double *y,
                        double *vx, double *vy, double *vz, double *gamma);
+/* The same in slices, for particle sets too large to hold twice on the
+ * host or the device (the caller produces and hands over one slice at a
+ * time): em2g_particles_begin announces n particles of species isp;
+ * em2g_particles_add copies slots first..first+count-1 -- slices in slot
+ * order, first = the number added so far -- from host memory (on_device 0)
+ * or device memory (1), checking them on the device; em2g_particles_end,
+ * once all n are in, makes them the species' particles, or returns
+ * EM2G_ERR_RANGE / EM2G_ERR_NONFINITE and keeps the old ones if any slot
+ * failed a check.  em2g_set_particles is one begin / add / end. */
+int em2g_particles_begin(em2g_ctx *ctx, int isp, int64_t n);
+int em2g_particles_add(em2g_ctx *ctx, int isp, int64_t first, int64_t count, const double *x,
+                       const double *y, const double *vx, const double *vy, const double *vz,
+                       const double *gamma, int on_device);
+int em2g_particles_end(em2g_ctx *ctx, int isp);
+/* slots first..first+count-1 of species isp into host (on_device 0) or
+ * device (1) arrays, in slot order (em2g_get_particles is all slots) */
+int em2g_get_particles_range(em2g_ctx *ctx, int isp, int64_t first, int64_t count, double *x,
+                             double *y, double *vx, double *vy, double *vz, double *gamma,
+                             int on_device);
 /* the step counter `it` of pic/global.f90:31 (fields reads it) */
 int em2g_set_step(em2g_ctx *ctx, int it);
 int em2g_get_step(em2g_ctx *ctx, int *it);
@@ -240,21 +264,30 @@ int em2g_reset_counters(em2g_ctx *ctx);
  * position (x, y) and u = gamma v (the quantity em2's Boris push advances,
  * pic/move.f90:176-203).
  *
- * em2g_adj_forward advances the context nsteps, keeping E and B of every
- * step and the particles every `checkpoint` steps.  After seeding the
- * adjoint of the final state, em2g_adj_backward sweeps back to the state
- * em2g_adj_forward started from: one kernel per step rebuilds the previous
+ * em2g_adj_forward advances the context nsteps, keeping a checkpoint of
+ * the whole state (fields and particles) every `checkpoint` steps.  After
+ * seeding the adjoint of the final state, em2g_adj_backward sweeps back to
+ * the state em2g_adj_forward started from, one segment of `checkpoint`
+ * steps at a time, last first: it restores the segment's checkpoint,
+ * recomputes the segment keeping E and B before each of its steps, then
+ * goes back through them -- one kernel per step rebuilds the previous
  * particle state by inverting the push (move, then the Boris rotation) and
- * applies the transposed step -- gathers of the current and charge adjoints
+ * applies the transposed step: gathers of the current and charge adjoints
  * at the particles, the Boris rotation reversed, scatters of the force
- * adjoint onto E and B -- and the kept checkpoints reset the rebuilt state
- * every `checkpoint` steps.  Field adjoints use the periodic (ny, nx) layout
+ * adjoint onto E and B; the checkpoint resets the rebuilt state at the
+ * segment's start.  Device memory: max_steps/checkpoint checkpoints of
+ * (13 (nx+3)(ny+3) + 6 x particles) doubles, plus `checkpoint` slots of
+ * 6 nx ny doubles.  At its end the context is back at the final state.
+ * em2g_adj_keep_all_fields(adj, 1) keeps E and B of every step in the
+ * forward sweep instead (max_steps slots) and skips the recomputation;
+ * 0 returns to the default.  Call it before em2g_adj_forward.  Field adjoints use the periodic (ny, nx) layout
  * (element [j][i] <-> em2 index (i+1, j+1)); particle adjoints are in slot
  * order. */
 typedef struct em2g_adj em2g_adj;
 int em2g_adj_create(em2g_ctx *ctx, int max_steps, int checkpoint, em2g_adj **out);
 int em2g_adj_destroy(em2g_adj *adj);
 int em2g_adj_forward(em2g_adj *adj, int nsteps);
+int em2g_adj_keep_all_fields(em2g_adj *adj, int on);
 /* adjoint of the final E, B: 6 arrays of ny*nx doubles (ex ey ez bx by bz),
  * device memory; particles' final adjoints are zero */
 int em2g_adj_seed_fields_device(em2g_adj *adj, const double *dev6);

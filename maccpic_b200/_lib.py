@@ -26,13 +26,15 @@ EXPORTS = [
     "em2g_abi_version", "em2g_last_error", "em2g_params_init", "em2g_create",
     "em2g_destroy", "em2g_set_stream", "em2g_synchronize", "em2g_set_field",
     "em2g_get_field", "em2g_set_fields", "em2g_get_fields", "em2g_set_particles",
-    "em2g_get_particles", "em2g_set_step", "em2g_get_step", "em2g_set_fields_device",
+    "em2g_get_particles", "em2g_particles_begin", "em2g_particles_add", "em2g_particles_end",
+    "em2g_get_particles_range", "em2g_set_step", "em2g_get_step", "em2g_set_fields_device",
     "em2g_get_fields_device", "em2g_field_device_ptr", "em2g_move", "em2g_curnt",
     "em2g_fields", "em2g_smooth2", "em2g_step", "em2g_set_particles_device",
     "em2g_move_curnt", "em2g_set_timing", "em2g_get_counters", "em2g_reset_counters",
     "em2g_smooth2_static", "em2g_diagnostics", "em2g_num_variants", "em2g_set_variant",
     "em2g_get_variant", "em2g_set_sort_interval",
-    "em2g_adj_create", "em2g_adj_destroy", "em2g_adj_forward", "em2g_adj_seed_fields_device",
+    "em2g_adj_create", "em2g_adj_destroy", "em2g_adj_forward", "em2g_adj_keep_all_fields",
+    "em2g_adj_seed_fields_device",
     "em2g_adj_backward", "em2g_adj_get_fields_device", "em2g_adj_get_particles_device",
     "em2g_adj_get_initial_particles_device",
     "em2g_ens_create", "em2g_ens_destroy", "em2g_ens_num_runs", "em2g_ens_set_stream",
@@ -57,7 +59,8 @@ class Em2gParams(C.Structure):
         ("cg_maxits", C.c_int32), ("energy_mode", C.c_int32),
         ("cg_eps", C.c_double), ("qme", C.c_double), ("wpe", C.c_double),
         ("device", C.c_int32), ("sort_interval", C.c_int32),
-        ("smooth_current", C.c_int32), ("poisson", C.c_int32), ("reserved", C.c_int32 * 14),
+        ("smooth_current", C.c_int32), ("poisson", C.c_int32), ("staging_mib", C.c_int32),
+        ("reserved", C.c_int32 * 13),
     ]
 
 
@@ -96,6 +99,12 @@ def lib() -> C.CDLL:
         "em2g_get_fields": (C.c_int, [ctx, dp]),
         "em2g_set_particles": (C.c_int, [ctx, C.c_int, C.c_int64] + [dp] * 6),
         "em2g_get_particles": (C.c_int, [ctx, C.c_int, i64p] + [dp] * 6),
+        "em2g_particles_begin": (C.c_int, [ctx, C.c_int, C.c_int64]),
+        "em2g_particles_add": (C.c_int, [ctx, C.c_int, C.c_int64, C.c_int64] + [vp] * 6
+                               + [C.c_int]),
+        "em2g_particles_end": (C.c_int, [ctx, C.c_int]),
+        "em2g_get_particles_range": (C.c_int, [ctx, C.c_int, C.c_int64, C.c_int64] + [vp] * 6
+                                     + [C.c_int]),
         "em2g_set_step": (C.c_int, [ctx, C.c_int]),
         "em2g_get_step": (C.c_int, [ctx, ip]),
         "em2g_set_fields_device": (C.c_int, [ctx, vp]),
@@ -120,6 +129,7 @@ def lib() -> C.CDLL:
         "em2g_adj_create": (C.c_int, [ctx, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
         "em2g_adj_destroy": (C.c_int, [ctx]),
         "em2g_adj_forward": (C.c_int, [ctx, C.c_int]),
+        "em2g_adj_keep_all_fields": (C.c_int, [ctx, C.c_int]),
         "em2g_adj_seed_fields_device": (C.c_int, [ctx, vp]),
         "em2g_adj_backward": (C.c_int, [ctx]),
         "em2g_adj_get_fields_device": (C.c_int, [ctx, vp]),

@@ -458,6 +458,12 @@ def _flatten(E, B, parts):
     return list(E) + list(B) + [t for p in parts for t in p]
 
 
+def flatten_state(E, B, parts):
+    """(E, B, particles) as the flat tensor list CudaRun takes and returns
+    adjoints for: Ex, Ey, Ez, Bx, By, Bz, then x, y, ux, uy, uz per species."""
+    return _flatten(E, B, parts)
+
+
 def _unflatten(ts, nsp):
     E, B = tuple(ts[0:3]), tuple(ts[3:6])
     parts = [tuple(ts[6 + 5 * s: 11 + 5 * s]) for s in range(nsp)]
@@ -692,7 +698,7 @@ class CudaAdjoint:
     particles) serves many gradients of runs of the same shape."""
 
     def __init__(self, k: StepConst, E, B, parts, max_steps: int, checkpoint: int,
-                 isav: int, smooth_current: int = 0, it0: int = 0):
+                 isav: int, smooth_current: int = 0, it0: int = 0, keep_all_fields=False):
         import ctypes as C
         from . import _lib
         from ._lib import check
@@ -716,6 +722,10 @@ class CudaAdjoint:
         h = C.c_void_p()
         check(self._L.em2g_adj_create(self.g._h, self.max_steps, self.checkpoint, C.byref(h)))
         self._h = h
+        # default: checkpoints every K steps and recomputation of each
+        # segment in the reverse sweep; keep_all_fields: E, B of every step
+        # kept instead (more memory, no second forward pass)
+        check(self._L.em2g_adj_keep_all_fields(self._h, int(bool(keep_all_fields))))
 
     def load(self, E, B, parts, it0: int = 0):
         """Replace the context's state (same grid and particle counts)."""
@@ -754,15 +764,20 @@ class CudaAdjoint:
         from ._lib import check
         check(self._L.em2g_adj_forward(self._h, int(steps)))
 
-    def final_B(self):
-        """Periodic B of the current state (device tensors)."""
+    def final_EB(self):
+        """Periodic E and B of the current state (device tensors)."""
         import ctypes as C
         from ._lib import check
         k = self.k
         out = torch.empty((13, k.ny + 3, k.nx + 3), dtype=torch.float64, device=self.dev)
         check(self._L.em2g_get_fields_device(self.g._h, C.c_void_p(out.data_ptr())))
         torch.cuda.synchronize(self.dev)
-        return tuple(out[3 + c, 1:k.ny + 1, 1:k.nx + 1].clone() for c in range(3))
+        f = [out[c, 1:k.ny + 1, 1:k.nx + 1].clone() for c in range(6)]
+        return tuple(f[:3]), tuple(f[3:])
+
+    def final_B(self):
+        """Periodic B of the current state (device tensors)."""
+        return self.final_EB()[1]
 
     def backward(self, lE, lB):
         """Adjoints of the initial state from those of the final E, B
@@ -784,39 +799,97 @@ class CudaAdjoint:
         return tuple(out[:3]), tuple(out[3:]), parts
 
 
+class CudaRun(torch.autograd.Function):
+    """T steps of the CUDA FP64 step (exact Poisson solve) as one autograd
+    node: forward maps the initial (E, B, particles) -- the flat tensors of
+    :func:`flatten_state`, particles as x, y, u = gamma v -- to the final E and B;
+    backward is the hand-written adjoint (em2g_adj_backward), which takes
+    the adjoints of the final E, B and returns those of the initial state.
+    The final particles are not outputs (their adjoints are zero).
+
+        Ef_Bf = CudaRun.apply(adj, steps, *flatten_state(E0, B0, P0))
+        flux(Ef_Bf[3:], k).backward()   # reaches what E0, B0, P0 came from
+    """
+
+    @staticmethod
+    def forward(ctx, adj, steps, *flat):
+        E, B, P = _unflatten([t.detach() for t in flat], adj.nsp)
+        adj.load(E, B, P)
+        adj.forward(int(steps))
+        Ef, Bf = adj.final_EB()
+        ctx.adj = adj
+        return (*Ef, *Bf)
+
+    @staticmethod
+    def backward(ctx, *g):
+        adj = ctx.adj
+        g = [t if t is not None else
+             torch.zeros((adj.k.ny, adj.k.nx), dtype=torch.float64, device=adj.dev) for t in g]
+        lE, lB, lP = adj.backward(g[:3], g[3:])
+        return (None, None, *_flatten(lE, lB, lP))
+
+
 def theta_gradient_cuda(cfg, theta, steps: int, checkpoint: int = 50, draws=None,
                         device="cuda", workspace: "CudaAdjoint | None" = None):
     """flux(T) and d flux(T) / d theta with the CUDA step and its adjoint
-    (exact Poisson solve); autograd only through the initial-state map.
-    `workspace`: a CudaAdjoint of this config's shape with max_steps >= steps
-    and this checkpoint interval, reused instead of allocating a new one."""
+    (exact Poisson solve), by autograd through :class:`CudaRun`: the
+    initial-state map theta -> state is differentiated by autograd, the T
+    steps by the hand-written adjoint.  `workspace`: a CudaAdjoint of this
+    config's shape with max_steps >= steps and this checkpoint interval,
+    reused instead of allocating a new one."""
     import contextlib
     draws = draws or make_draws(cfg, device=device)
     k = step_const(cfg)
     th = torch.tensor(theta, dtype=torch.float64, device=device, requires_grad=True)
-    with torch.enable_grad():
-        E0, B0, P0 = initial_state_torch(cfg, (th[0], th[1], th[2]), draws)
-        flat0 = _flatten(E0, B0, P0)
     if workspace is not None:
         if workspace.max_steps < steps or workspace.checkpoint != checkpoint:
             raise ValueError("workspace made for fewer steps or another checkpoint interval")
-        workspace.load(E0, B0, P0)
         ctx = contextlib.nullcontext(workspace)
     else:
+        with torch.no_grad():
+            E0, B0, P0 = initial_state_torch(cfg, tuple(theta), draws)
         ctx = CudaAdjoint(k, E0, B0, P0, steps, checkpoint, cfg.isav, cfg.smooth_current)
     with ctx as adj:
-        adj.forward(steps)
-        Bf = [b.requires_grad_(True) for b in adj.final_B()]
         with torch.enable_grad():
-            F = flux(Bf, k)
-            gB = torch.autograd.grad(F, Bf, allow_unused=True)
-        gB = [g if g is not None else torch.zeros_like(b) for g, b in zip(gB, Bf)]
-        lE, lB, lP = adj.backward([torch.zeros_like(b) for b in Bf], gB)
-    lam = _flatten(lE, lB, lP)
-    used = [(t, l) for t, l in zip(flat0, lam) if t.requires_grad]
-    g = torch.autograd.grad([t for t, _ in used], th, grad_outputs=[l for _, l in used],
-                            allow_unused=True)[0]
-    return float(F.detach()), g.detach().cpu().numpy()
+            E0, B0, P0 = initial_state_torch(cfg, (th[0], th[1], th[2]), draws)
+            out = CudaRun.apply(adj, steps, *_flatten(E0, B0, P0))
+            F = flux(out[3:], k)
+            F.backward()
+    return float(F.detach()), th.grad.detach().cpu().numpy()
+
+
+def fd_check_cuda(cfg, theta, steps: int, h: float = 1e-3, checkpoint: int = 50, draws=None,
+                  device="cuda", workspace: "CudaAdjoint | None" = None):
+    """The adjoint gradient of flux(T) against central finite differences of
+    the same CUDA forward, (flux(theta + h e_i) - flux(theta - h e_i)) / 2h,
+    with common random numbers (the same draws for every evaluation).
+    Returns {"flux", "adjoint", "fd", "rel_error"} (rel_error per component:
+    |adjoint - fd| / max(|fd|, 1e-3 max|fd|))."""
+    import numpy as np
+    draws = draws or make_draws(cfg, device=device)
+    F, g = theta_gradient_cuda(cfg, theta, steps, checkpoint, draws, device, workspace)
+    k = step_const(cfg)
+    fd = []
+    for i in range(3):
+        vals = []
+        for sgn in (1.0, -1.0):
+            th = list(theta)
+            th[i] += sgn * h
+            with torch.no_grad():
+                E0, B0, P0 = initial_state_torch(cfg, tuple(th), draws)
+            if workspace is not None:
+                workspace.load(E0, B0, P0)
+                workspace.g.step(steps)
+                vals.append(float(flux(workspace.final_B(), k)))
+            else:
+                with CudaAdjoint(k, E0, B0, P0, 1, 1, cfg.isav, cfg.smooth_current) as adj:
+                    adj.g.step(steps)
+                    vals.append(float(flux(adj.final_B(), k)))
+        fd.append((vals[0] - vals[1]) / (2 * h))
+    fd = np.array(fd)
+    floor = 1e-3 * np.abs(fd).max()
+    rel = np.abs(g - fd) / np.maximum(np.abs(fd), floor)
+    return {"flux": F, "adjoint": g.tolist(), "fd": fd.tolist(), "rel_error": rel.tolist()}
 
 
 def flux_of_theta_cuda(cfg, theta, steps: int, draws, device="cuda"):

@@ -14,9 +14,16 @@
 //   scatter of the force adjoint onto E and B, and the Boris rotation is
 //   reversed stage by stage.
 //
-// Memory.  The forward sweep keeps E and B before every step (6 periodic
-// arrays per step) and the particles every K steps.  The reverse sweep does
-// not recompute segments: the push is invertible, so one kernel per step
+// Memory.  The forward sweep keeps a checkpoint every K steps: the
+// context's field block and its particles (x, y, vx, vy, vz, gamma, slot
+// order).  The reverse sweep takes the segments last to first: it restores
+// the segment's checkpoint into the context, recomputes the segment's K
+// steps keeping E and B before each (K slots of 6 periodic arrays), and
+// sweeps back through them.  So the memory is O(T/K) checkpoints plus K
+// field slots, at the price of a second forward pass.  (A caller with
+// memory to spare can keep E and B of every step instead and skip the
+// recomputation: em2g_adj_keep_all_fields.)  The particles need no per-step
+// store in either mode: the push is invertible, so one kernel per step
 // rebuilds the previous particle state from the current one (x -= v dt/dx
 // with u's velocity, then the Boris rotation about the same t by the
 // opposite angle) and applies the transposed step to it.  Round-off of the
@@ -48,10 +55,14 @@ struct em2g_adj {
   double ae[EM2G_MAX_SPECIES] = {}, qd[EM2G_MAX_SPECIES] = {};
   int64_t n[EM2G_MAX_SPECIES] = {}, pb[EM2G_MAX_SPECIES] = {};  // particles, first index
   int64_t ptot = 0;
-  double *hist = nullptr;   // max_steps x 6 x N
-  double *ckpt = nullptr;   // nck x 5 x ptot (per species 5 x n, slot order)
+  double *hist = nullptr;   // nhist x 6 x N: E, B before each step of a segment
+  int nhist = 0;            // K (recomputation) or max_steps (every step kept)
+  bool keep_all = false;    // E, B of every step kept by the forward sweep
+  double *ckpt = nullptr;   // nck x 6 x ptot (per species 6 x n, slot order)
+  double *ckfld = nullptr;  // nck x 13 x w, the context's field block
   int nck = 0;
-  double *fin = nullptr;    // 5 x ptot, the state after the last recorded step
+  double *fin = nullptr;    // 6 x ptot, the particles after the last recorded step
+  double *finfld = nullptr; // 13 x w, the field block after it
   double *work = nullptr, *work_alt = nullptr;  // 10 x ptot (per species 10 x n)
   int32_t *slot = nullptr, *slot_alt = nullptr;
   int32_t *off = nullptr;   // per species ncell+1
@@ -603,23 +614,32 @@ __global__ void k_adj_record_fields(const double *fld, int nx, int ny, int64_t w
     out[k] = fld[c * w + (int64_t)(j + 1) * (nx + 3) + (i + 1)];
   }
 }
-// context particles (6 x cap, grouped, with slots) -> x, y, u (5 x n, slot order)
+// context particles (6 x cap, grouped, with slots) -> x, y, vx, vy, vz,
+// gamma (6 x n, slot order): a checkpoint the context can be reset to
 __global__ void k_adj_record_parts(const double *part, const int32_t *slot, int64_t n,
                                    int64_t cap, double *out) {
   PG_LOOP(n) {
     const int64_t s = slot[k];
-    const double g = part[5 * cap + k];
-    out[s] = part[k];
-    out[n + s] = part[cap + k];
-    out[2 * n + s] = part[2 * cap + k] * g;  // u = v gamma (pic/move.f90:176-178)
-    out[3 * n + s] = part[3 * cap + k] * g;
-    out[4 * n + s] = part[4 * cap + k] * g;
+    for (int c = 0; c < 6; ++c) out[c * n + s] = part[c * cap + k];
   }
 }
-// working set from a slot-order state: slot = index, adjoints zero
+// a checkpoint back into the context's particle arrays, slot order (the
+// next push sorts them by cell)
+__global__ void k_adj_reset_parts(const double *ck, int64_t n, int64_t cap, double *part,
+                                  int32_t *slot) {
+  PG_LOOP(n) {
+    for (int c = 0; c < 6; ++c) part[c * cap + k] = ck[c * n + k];
+    slot[k] = (int32_t)k;
+  }
+}
+// working set from a slot-order checkpoint: x, y, u = v gamma (the
+// quantity the Boris push advances, pic/move.f90:176-178), adjoints zero
 __global__ void k_adj_load(const double *st, int64_t n, double *P, int32_t *slot) {
   PG_LOOP(n) {
-    for (int c = 0; c < 5; ++c) P[c * n + k] = st[c * n + k];
+    const double g = st[5 * n + k];
+    P[k] = st[k];
+    P[n + k] = st[n + k];
+    for (int c = 2; c < 5; ++c) P[c * n + k] = st[c * n + k] * g;
     for (int c = 5; c < 10; ++c) P[c * n + k] = 0.0;
     slot[k] = (int32_t)k;
   }
@@ -628,7 +648,10 @@ __global__ void k_adj_load(const double *st, int64_t n, double *P, int32_t *slot
 __global__ void k_adj_restore(const double *st, int64_t n, double *P, const int32_t *slot) {
   PG_LOOP(n) {
     const int64_t s = slot[k];
-    for (int c = 0; c < 5; ++c) P[c * n + k] = st[c * n + s];
+    const double g = st[5 * n + s];
+    P[k] = st[s];
+    P[n + k] = st[n + s];
+    for (int c = 2; c < 5; ++c) P[c * n + k] = st[c * n + s] * g;
   }
 }
 __global__ void k_adj_hist(const double *P, int64_t n, int nx, int ny, int32_t *cnt) {
@@ -648,6 +671,18 @@ __global__ void k_adj_scatter(const double *P, const int32_t *slot, int64_t n, i
   const int64_t pos = (int64_t)off[key] + agg_atomic_add(cursor, key, am);
   for (int c = 0; c < 10; ++c) Q[c * n + pos] = P[c * n + k];
   qslot[pos] = slot[k];
+}
+// a checkpoint (x, y, v, gamma) as x, y, u = v gamma
+__global__ void k_adj_initial(const double *st, int64_t n, double *x, double *y, double *ux,
+                              double *uy, double *uz) {
+  PG_LOOP(n) {
+    const double g = st[5 * n + k];
+    x[k] = st[k];
+    y[k] = st[n + k];
+    ux[k] = st[2 * n + k] * g;
+    uy[k] = st[3 * n + k] * g;
+    uz[k] = st[4 * n + k] * g;
+  }
 }
 // adjoints (or the state) of the working set back to slot order
 __global__ void k_adj_unsort(const double *P, const int32_t *slot, int64_t n, int first,
@@ -801,9 +836,12 @@ int em2g_adj_create(em2g_ctx *ctx, int max_steps, int checkpoint, em2g_adj **out
     e = cudaMalloc((void **)&(ptr), (bytes));                              \
     if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc " #ptr));   \
   } while (0)
-  ALLOC(a->hist, sizeof(double) * 6 * N * max_steps);
-  ALLOC(a->ckpt, sizeof(double) * 5 * pt * a->nck);
-  ALLOC(a->fin, sizeof(double) * 5 * pt);
+  a->nhist = checkpoint < max_steps ? checkpoint : max_steps;
+  ALLOC(a->hist, sizeof(double) * 6 * N * a->nhist);
+  ALLOC(a->ckpt, sizeof(double) * 6 * pt * a->nck);
+  ALLOC(a->ckfld, sizeof(double) * EM2G_NFIELD * ctx->g.w * a->nck);
+  ALLOC(a->fin, sizeof(double) * 6 * pt);
+  ALLOC(a->finfld, sizeof(double) * EM2G_NFIELD * ctx->g.w);
   ALLOC(a->work, sizeof(double) * 10 * pt);
   ALLOC(a->work_alt, sizeof(double) * 10 * pt);
   ALLOC(a->slot, sizeof(int32_t) * pt);
@@ -827,8 +865,9 @@ int em2g_adj_create(em2g_ctx *ctx, int max_steps, int checkpoint, em2g_adj **out
 int em2g_adj_destroy(em2g_adj *a) {
   if (!a) return EM2G_OK;
   if (a->ctx) cudaSetDevice(a->ctx->device);
-  void *bufs[] = {a->hist, a->ckpt,  a->fin, a->work,     a->work_alt, a->slot, a->slot_alt,
-                  a->off,  a->cnt,   a->cursor, a->scan_tmp, a->g,    a->spec, a->scaled};
+  void *bufs[] = {a->hist, a->ckpt,     a->ckfld,    a->fin, a->finfld, a->work, a->work_alt,
+                  a->slot, a->slot_alt, a->off,      a->cnt, a->cursor, a->scan_tmp,
+                  a->g,    a->spec,     a->scaled};
   for (void *p : bufs) cudaFree(p);
   delete a;
   return EM2G_OK;
@@ -840,9 +879,58 @@ static int record_parts(em2g_adj *a, double *dst, cudaStream_t st) {
     if (S.n != a->n[s]) return fail(EM2G_ERR_INVALID, "particle count changed since em2g_adj_create");
     if (S.n > 0)
       k_adj_record_parts<<<blocks_for(S.n), 256, 0, st>>>(S.part, S.slot, S.n, S.cap,
-                                                          dst + 5 * a->pb[s]);
+                                                          dst + 6 * a->pb[s]);
   }
   EM2G_CUDA(cudaGetLastError());
+  return EM2G_OK;
+}
+
+// the context set to a kept state: field block fld, particles ck (6 x ptot,
+// slot order; sorted again by the next push), step counter it
+static int reset_context(em2g_adj *a, const double *fld, const double *ck, int it,
+                         cudaStream_t st) {
+  em2g_ctx *c = a->ctx;
+  EM2G_CUDA(cudaMemcpyAsync(c->fld, fld, sizeof(double) * EM2G_NFIELD * c->g.w,
+                            cudaMemcpyDeviceToDevice, st));
+  for (int s = 0; s < a->nsp; ++s) {
+    Species &S = c->sp[s];
+    if (S.n > 0)
+      k_adj_reset_parts<<<blocks_for(S.n), 256, 0, st>>>(ck + 6 * a->pb[s], S.n, S.cap, S.part,
+                                                         S.slot);
+    S.sorted = false;
+  }
+  EM2G_CUDA(cudaGetLastError());
+  c->jp_live = true;
+  c->it = it;
+  return EM2G_OK;
+}
+
+// checkpoint ck (the state before step ck*K): field block and particles
+static int record_checkpoint(em2g_adj *a, int ck, cudaStream_t st) {
+  em2g_ctx *c = a->ctx;
+  EM2G_CUDA(cudaMemcpyAsync(a->ckfld + (int64_t)EM2G_NFIELD * c->g.w * ck, c->fld,
+                            sizeof(double) * EM2G_NFIELD * c->g.w, cudaMemcpyDeviceToDevice,
+                            st));
+  return record_parts(a, a->ckpt + 6 * a->ptot * ck, st);
+}
+
+// the context reset to checkpoint ck
+static int reset_to_checkpoint(em2g_adj *a, int ck, cudaStream_t st) {
+  return reset_context(a, a->ckfld + (int64_t)EM2G_NFIELD * a->ctx->g.w * ck,
+                       a->ckpt + 6 * a->ptot * ck, a->it0 + ck * a->K, st);
+}
+
+// E and B before each of the steps k0..k1-1 into hist slots k - k0 (and
+// the context advanced to the state before step k1)
+static int record_segment(em2g_adj *a, int k0, int k1, cudaStream_t st) {
+  em2g_ctx *c = a->ctx;
+  for (int k = k0; k < k1; ++k) {
+    k_adj_record_fields<<<blocks_for(6 * a->N), 256, 0, st>>>(c->fld, a->nx, a->ny, c->g.w,
+                                                             a->hist + 6 * a->N * (k - k0));
+    EM2G_CUDA(cudaGetLastError());
+    int rc = step_enqueue(c);
+    if (rc) return rc;
+  }
   return EM2G_OK;
 }
 
@@ -856,17 +944,20 @@ int em2g_adj_forward(em2g_adj *a, int nsteps) {
   a->it0 = c->it;
   for (int k = 0; k < nsteps; ++k) {
     cudaStream_t st = c->stream;
-    k_adj_record_fields<<<blocks_for(6 * a->N), 256, 0, st>>>(c->fld, a->nx, a->ny, c->g.w,
-                                                             a->hist + 6 * a->N * k);
-    EM2G_CUDA(cudaGetLastError());
-    if (k % a->K == 0 && (rc = record_parts(a, a->ckpt + 5 * a->ptot * (k / a->K), st)))
-      return rc;
+    if (a->keep_all) {
+      k_adj_record_fields<<<blocks_for(6 * a->N), 256, 0, st>>>(c->fld, a->nx, a->ny, c->g.w,
+                                                               a->hist + 6 * a->N * k);
+      EM2G_CUDA(cudaGetLastError());
+    }
+    if (k % a->K == 0 && (rc = record_checkpoint(a, k / a->K, st))) return rc;
     // em2g_step's pass (the fast path: the stored particles are its own),
     // enqueued without waiting for it
     if ((rc = step_enqueue(c))) return rc;
     a->steps = k + 1;
   }
   if ((rc = record_parts(a, a->fin, c->stream))) return rc;
+  EM2G_CUDA(cudaMemcpyAsync(a->finfld, c->fld, sizeof(double) * EM2G_NFIELD * c->g.w,
+                            cudaMemcpyDeviceToDevice, c->stream));
   EM2G_CUDA(cudaStreamSynchronize(c->stream));
   EM2G_CUDA(cudaGetLastError());
   return EM2G_OK;
@@ -891,18 +982,25 @@ int em2g_adj_backward(em2g_adj *a) {
   cudaStream_t st = a->ctx->stream;
   for (int s = 0; s < a->nsp; ++s)
     if (a->n[s] > 0)
-      k_adj_load<<<blocks_for(a->n[s]), 256, 0, st>>>(a->fin + 5 * a->pb[s], a->n[s],
+      k_adj_load<<<blocks_for(a->n[s]), 256, 0, st>>>(a->fin + 6 * a->pb[s], a->n[s],
                                                       a->work + 10 * a->pb[s], a->slot + a->pb[s]);
   EM2G_CUDA(cudaGetLastError());
   if ((rc = regroup(a, st))) return rc;
   int since = 0;
+  int seg0 = a->steps;  // first step of the segment whose E, B are in hist
   for (int k = a->steps - 1; k >= 0; --k) {
+    if (!a->keep_all && k < seg0) {
+      // recompute the segment of step k from its checkpoint
+      seg0 = (k / a->K) * a->K;
+      if ((rc = reset_to_checkpoint(a, k / a->K, st))) return rc;
+      if ((rc = record_segment(a, seg0, k + 1, st))) return rc;
+    }
     if (since == kRegroup) {
       if ((rc = regroup(a, st))) return rc;
       since = 0;
     }
     if ((rc = fields_T(a, a->it0 + k + 1, st))) return rc;
-    const double *eb = a->hist + 6 * a->N * k;
+    const double *eb = a->hist + 6 * a->N * (a->keep_all ? k : k - seg0);
     for (int s = 0; s < a->nsp; ++s) {
       double2 *sc = a->scaled + 3 * a->N * s;
       k_adj_prescale<<<blocks_for(a->N), 256, 0, st>>>(eb, a->N, a->ae[s], sc);
@@ -934,15 +1032,37 @@ int em2g_adj_backward(em2g_adj *a) {
       }
       // at a checkpoint the kept exact state replaces the rebuilt one
       if (k % a->K == 0 && r.n > 0)
-        k_adj_restore<<<blocks_for(r.n), 256, 0, st>>>(a->ckpt + 5 * a->ptot * (k / a->K) +
-                                                           5 * a->pb[s],
+        k_adj_restore<<<blocks_for(r.n), 256, 0, st>>>(a->ckpt + 6 * a->ptot * (k / a->K) +
+                                                           6 * a->pb[s],
                                                        r.n, r.P, a->slot + a->pb[s]);
     }
     EM2G_CUDA(cudaGetLastError());
     ++since;
   }
+  // the recomputation moved the context: back to where the forward sweep
+  // left it
+  if (!a->keep_all && (rc = reset_context(a, a->finfld, a->fin, a->it0 + a->steps, st)))
+    return rc;
   EM2G_CUDA(cudaStreamSynchronize(st));
   a->swept = true;
+  return EM2G_OK;
+}
+
+int em2g_adj_keep_all_fields(em2g_adj *a, int on) {
+  int rc = check_adj(a);
+  if (rc) return rc;
+  const int n = on ? a->max_steps : std::min(a->K, a->max_steps);
+  if (n != a->nhist) {
+    EM2G_CUDA(cudaStreamSynchronize(a->ctx->stream));
+    cudaFree(a->hist);
+    a->hist = nullptr;
+    a->nhist = 0;
+    EM2G_CUDA(cudaMalloc((void **)&a->hist, sizeof(double) * 6 * a->N * n));
+    a->nhist = n;
+  }
+  a->keep_all = on != 0;
+  a->steps = 0;
+  a->seeded = a->swept = false;
   return EM2G_OK;
 }
 
@@ -986,11 +1106,10 @@ int em2g_adj_get_initial_particles_device(em2g_adj *a, int isp, double *x, doubl
   if (isp < 0 || isp >= a->nsp) return fail(EM2G_ERR_INVALID, "bad species index");
   if (!x || !y || !ux || !uy || !uz) return fail(EM2G_ERR_INVALID, "null pointer");
   const int64_t n = a->n[isp];
-  const double *src = a->ckpt + 5 * a->pb[isp];
-  double *dst[5] = {x, y, ux, uy, uz};
-  for (int k = 0; k < 5; ++k)
-    EM2G_CUDA(cudaMemcpyAsync(dst[k], src + k * n, sizeof(double) * n, cudaMemcpyDeviceToDevice,
-                              a->ctx->stream));
+  if (n > 0)
+    k_adj_initial<<<blocks_for(n), 256, 0, a->ctx->stream>>>(a->ckpt + 6 * a->pb[isp], n, x, y,
+                                                             ux, uy, uz);
+  EM2G_CUDA(cudaGetLastError());
   EM2G_CUDA(cudaStreamSynchronize(a->ctx->stream));
   return EM2G_OK;
 }

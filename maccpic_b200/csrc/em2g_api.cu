@@ -1,6 +1,7 @@
 // em2g_api.cu -- the C ABI of libem2g.so (declared in include/em2g.h):
 // context life cycle, state copies, and the move / curnt / fields /
 // smooth2 entry points that stand in for em2's subroutines.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -99,11 +100,9 @@ __global__ void k_f2d(const float *__restrict__ a, double *b, int64_t n) {
 
 bool is_fp32(const em2g_ctx *c) { return c->P.precision == EM2G_FP32; }
 
-// host FP64 arrays [first, first+count) of the field block -> device
-// The context's FP64 staging buffer on the device (particles: 6*n doubles
-// x, y, vx, vy, vz, gamma, and for FP32 contexts 32*n bytes of records
-// after them; fields: FP64 arrays), grown on demand and kept until
-// em2g_destroy so that repeated copies allocate nothing.
+// The context's FP64 staging buffer on the device (field arrays; slices of
+// particles in FP64; the records of a regrouping), grown on demand and kept
+// until em2g_destroy so that repeated copies allocate nothing.
 int ensure_staging(em2g_ctx *c, int64_t ndoubles) {
   if (ndoubles <= c->staging_n) return EM2G_OK;
   EM2G_CUDA(cudaStreamSynchronize(c->stream));  // the old buffer may still be read
@@ -201,6 +200,8 @@ int validate(const em2g_params *p) {
     return fail(EM2G_ERR_INVALID, "smooth_current must be 0 or 1");
   if (p->sort_interval < 0) return fail(EM2G_ERR_INVALID, "sort_interval must be >= 0");
   if (p->poisson != 0 && p->poisson != 1) return fail(EM2G_ERR_INVALID, "poisson must be 0 or 1");
+  if (p->staging_mib < 0 || p->staging_mib > (1 << 16))
+    return fail(EM2G_ERR_INVALID, "staging_mib must be 0..65536");
   if (p->poisson == 1 && (p->precision != EM2G_FP64 || !spectral_size_ok(p->nx, p->ny)))
     return fail(EM2G_ERR_INVALID,
                 "poisson 1 (spectral) needs FP64 and power-of-two nx, ny <= 8192");
@@ -252,12 +253,19 @@ int finish_outputs(em2g_ctx *c, double *ake_out, double *energies_out, int *cg_i
 int validate_params(const em2g_params *p) { return validate(p); }
 
 int check_particles_device(const double *part, int64_t n, int64_t ld, double xlim, double ylim,
-                           unsigned long long *bad, cudaStream_t st) {
-  EM2G_CUDA(cudaMemsetAsync(bad, 0, 2 * sizeof(unsigned long long), st));
+                           unsigned long long *bad, cudaStream_t st, bool reset) {
+  if (reset) EM2G_CUDA(cudaMemsetAsync(bad, 0, 2 * sizeof(unsigned long long), st));
   if (n > 0)
     k_check_particles<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(part, n, ld, xlim, ylim, bad);
   EM2G_CUDA(cudaGetLastError());
   return EM2G_OK;
+}
+
+int64_t staging_cap(const em2g_ctx *c) {
+  if (c->P.staging_mib > 0) return (int64_t)c->P.staging_mib << 20;
+  int64_t n = 1024;
+  for (int s = 0; s < c->P.nsp; ++s) n = std::max(n, c->sp[s].cap);
+  return 80 * std::min<int64_t>(n, (int64_t)1 << 24);
 }
 
 }  // namespace em2g
@@ -345,6 +353,7 @@ int em2g_create(const em2g_params *p, em2g_ctx **out) {
   ALLOC(c->red, sizeof(double) * c->red_blocks);
   ALLOC(c->ake_l1, sizeof(double) * kAkeBlocks);
   ALLOC(c->dev_out, sizeof(double) * kDevOut);
+  ALLOC(c->up_bad, sizeof(unsigned long long) * 2 * EM2G_MAX_SPECIES);
 #undef ALLOC
   e = cudaMallocHost((void **)&c->host_out, sizeof(double) * kDevOut);
   if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMallocHost"));
@@ -406,6 +415,7 @@ int em2g_destroy(em2g_ctx *c) {
   cudaFree(c->spec);
   cudaFree(c->staging);
   cudaFree(c->dev_out);
+  cudaFree(c->up_bad);
   if (c->host_out) cudaFreeHost(c->host_out);
   cg_free(c);
   sort_free(c);
@@ -502,50 +512,157 @@ int em2g_field_device_ptr(em2g_ctx *c, int id, void **dptr) {
   return EM2G_OK;
 }
 
-// n particles of species isp from six arrays (host or device memory, as
-// `kind` says): copied to a staging area on the device -- the FP64 reorder
-// target, or a temporary buffer for FP32 -- and checked there (positions in
-// [0, n+0.5), every value finite: em2 would read outside its arrays
-// otherwise); only input that passes replaces the species' particles.
-static int load_particles(em2g_ctx *c, int isp, int64_t n, const double *const *src,
-                          cudaMemcpyKind kind) {
+// ---- particle copies in slices -------------------------------------------
+//
+// An upload parks its slices in the species' alternate buffers (FP64: the
+// sort target; FP32: the regrouping target, with each particle's cell key)
+// and counts rejected values on the device; only the end of the upload,
+// once every slot is in and none was rejected, makes them the species'
+// particles.  Host slices go through the staging buffer, at most
+// staging_cap() bytes, so no buffer grows with the particle count.
+
+static int particles_begin(em2g_ctx *c, int isp, int64_t n) {
   Species &S = c->sp[isp];
   if (n < 0 || n > S.cap) return fail(EM2G_ERR_RANGE, "particle count exceeds np_max");
-  if (n == 0) {
-    S.n = 0;
-    S.sorted = false;
-    if (is_fp32(c)) return upload_f32(c, isp, nullptr, 0, nullptr);
-    return EM2G_OK;
-  }
+  EM2G_CUDA(cudaMemsetAsync(c->up_bad + 2 * isp, 0, 2 * sizeof(unsigned long long), c->stream));
+  if (is_fp32(c))
+    EM2G_CUDA(cudaMemsetAsync(S.cnt_alt, 0, sizeof(int32_t) * c->ncell, c->stream));
+  S.up_n = n;
+  S.up_added = 0;
+  return EM2G_OK;
+}
+
+// slots first..first+count from six arrays in host or device memory
+static int particles_add(em2g_ctx *c, int isp, int64_t first, int64_t count,
+                         const double *const *src, bool on_device) {
+  Species &S = c->sp[isp];
+  if (S.up_n < 0) return fail(EM2G_ERR_INVALID, "no particle upload open for this species");
+  if (first != S.up_added || count < 0 || first + count > S.up_n)
+    return fail(EM2G_ERR_INVALID, "particle slices must be added in slot order, within n");
+  if (count == 0) return EM2G_OK;
   for (int k = 0; k < 6; ++k)
     if (!src[k]) return fail(EM2G_ERR_INVALID, "null particle array");
-  double *dst = S.part_alt;
-  int64_t ld = S.cap;
-  if (is_fp32(c)) {
-    // 6*n FP64 values, then 32*n bytes of records for the regrouping
-    const int rs = ensure_staging(c, 10 * n);
-    if (rs) return rs;
-    dst = c->staging;
-    ld = n;
+  unsigned long long *bad = c->up_bad + 2 * isp;
+  const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  if (!is_fp32(c)) {
+    // parked at their slots in the sort target, checked there
+    for (int k = 0; k < 6; ++k)
+      EM2G_CUDA(cudaMemcpyAsync(S.part_alt + k * S.cap + first, src[k], sizeof(double) * count,
+                                kind, c->stream));
+    int rc = check_particles_device(S.part_alt + first, count, S.cap, c->P.nx + 0.5,
+                                    c->P.ny + 0.5, bad, c->stream, false);
+    if (rc) return rc;
+    S.up_added += count;
+    return EM2G_OK;
   }
-  for (int k = 0; k < 6; ++k)
-    EM2G_CUDA(cudaMemcpyAsync(dst + k * ld, src[k], sizeof(double) * n, kind, c->stream));
-  unsigned long long *bad = (unsigned long long *)c->red;  // 2 counters
-  int rc = check_particles_device(dst, n, ld, c->P.nx + 0.5, c->P.ny + 0.5, bad, c->stream);
+  if (on_device) {
+    int rc = stage_f32(c, isp, first, count, src, bad);
+    if (rc) return rc;
+    S.up_added += count;
+    return EM2G_OK;
+  }
+  // host slices through the staging buffer, 6 doubles per particle
+  const int64_t chunk = staging_cap(c) / 48;
+  int rc = ensure_staging(c, staging_cap(c) / 8);
   if (rc) return rc;
+  for (int64_t a = 0; a < count; a += chunk) {
+    const int64_t m = std::min(chunk, count - a);
+    const double *st[6];
+    for (int k = 0; k < 6; ++k) {
+      double *d = c->staging + k * m;
+      EM2G_CUDA(cudaMemcpyAsync(d, src[k] + a, sizeof(double) * m, cudaMemcpyHostToDevice,
+                                c->stream));
+      st[k] = d;
+    }
+    if ((rc = stage_f32(c, isp, first + a, m, st, bad))) return rc;
+  }
+  S.up_added += count;
+  return EM2G_OK;
+}
+
+static int particles_end(em2g_ctx *c, int isp) {
+  Species &S = c->sp[isp];
+  if (S.up_n < 0) return fail(EM2G_ERR_INVALID, "no particle upload open for this species");
+  if (S.up_added != S.up_n) {
+    S.up_n = -1;
+    return fail(EM2G_ERR_INVALID, "particle upload ended before every slot was added");
+  }
+  const int64_t n = S.up_n;
+  S.up_n = -1;
   unsigned long long hb[2] = {0, 0};
-  EM2G_CUDA(cudaMemcpyAsync(hb, bad, sizeof(hb), cudaMemcpyDeviceToHost, c->stream));
+  EM2G_CUDA(cudaMemcpyAsync(hb, c->up_bad + 2 * isp, sizeof(hb), cudaMemcpyDeviceToHost,
+                            c->stream));
   EM2G_CUDA(cudaStreamSynchronize(c->stream));
   if (hb[1]) return fail(EM2G_ERR_NONFINITE, std::to_string(hb[1]) + " particles with non-finite values");
   if (hb[0]) return fail(EM2G_ERR_RANGE, std::to_string(hb[0]) + " particles outside the grid");
+  int rc;
   if (is_fp32(c)) {
-    if ((rc = upload_f32(c, isp, dst, n, dst + 6 * n))) return rc;
+    if ((rc = ensure_staging(c, staging_cap(c) / 8))) return rc;
+    if ((rc = commit_f32(c, isp, n, c->staging, staging_cap(c) / 32))) return rc;
   } else {
     std::swap(S.part, S.part_alt);
-    k_iota<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(S.slot, n);
-    EM2G_CUDA(cudaGetLastError());
+    if (n > 0) {
+      k_iota<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(S.slot, n);
+      EM2G_CUDA(cudaGetLastError());
+    }
     S.n = n;
     S.sorted = false;
+  }
+  EM2G_CUDA(cudaStreamSynchronize(c->stream));
+  return EM2G_OK;
+}
+
+// n particles of species isp from six arrays (host or device memory): one
+// upload of a single slice
+static int load_particles(em2g_ctx *c, int isp, int64_t n, const double *const *src,
+                          bool on_device) {
+  int rc = particles_begin(c, isp, n);
+  if (rc) return rc;
+  if ((rc = particles_add(c, isp, 0, n, src, on_device))) {
+    c->sp[isp].up_n = -1;
+    return rc;
+  }
+  return particles_end(c, isp);
+}
+
+// slots first..first+count of species isp into six arrays in host or
+// device memory, in slot order
+static int particles_get(em2g_ctx *c, int isp, int64_t first, int64_t count,
+                         double *const *dst, bool on_device) {
+  Species &S = c->sp[isp];
+  if (first < 0 || count < 0 || first + count > S.n)
+    return fail(EM2G_ERR_RANGE, "slot range beyond the species' particles");
+  if (count == 0) return EM2G_OK;
+  for (int k = 0; k < 6; ++k)
+    if (!dst[k]) return fail(EM2G_ERR_INVALID, "null particle array");
+  const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  if (!is_fp32(c)) {
+    // restore slot order into the sort target, then copy the range
+    k_unsort<<<(unsigned)((S.n + 255) / 256), 256, 0, c->stream>>>(S.part, S.slot, S.part_alt,
+                                                                    S.n, S.cap);
+    EM2G_CUDA(cudaGetLastError());
+    for (int k = 0; k < 6; ++k)
+      EM2G_CUDA(cudaMemcpyAsync(dst[k], S.part_alt + k * S.cap + first, sizeof(double) * count,
+                                kind, c->stream));
+    EM2G_CUDA(cudaStreamSynchronize(c->stream));
+    return EM2G_OK;
+  }
+  // FP32: 32-byte records, then FP64 values (into the caller's device
+  // arrays directly, or into the staging buffer and across to the host)
+  const int64_t chunk = staging_cap(c) / (on_device ? 32 : 80);
+  int rc = ensure_staging(c, staging_cap(c) / 8);
+  if (rc) return rc;
+  for (int64_t a = 0; a < count; a += chunk) {
+    const int64_t m = std::min(chunk, count - a);
+    double *d[6];
+    void *rec = c->staging;
+    for (int k = 0; k < 6; ++k)
+      d[k] = on_device ? dst[k] + a : c->staging + 4 * m + k * m;
+    if ((rc = get_range_f32(c, isp, first + a, m, d, rec))) return rc;
+    if (!on_device) {
+      for (int k = 0; k < 6; ++k)
+        EM2G_CUDA(cudaMemcpyAsync(dst[k] + a, d[k], sizeof(double) * m, kind, c->stream));
+    }
   }
   EM2G_CUDA(cudaStreamSynchronize(c->stream));
   return EM2G_OK;
@@ -558,7 +675,7 @@ int em2g_set_particles(em2g_ctx *c, int isp, int64_t n, const double *x, const d
   if (rc) return rc;
   if (isp < 0 || isp >= c->P.nsp) return fail(EM2G_ERR_INVALID, "bad species index");
   const double *src[6] = {x, y, vx, vy, vz, gamma};
-  return load_particles(c, isp, n, src, cudaMemcpyHostToDevice);
+  return load_particles(c, isp, n, src, false);
 }
 
 int em2g_set_particles_device(em2g_ctx *c, int isp, int64_t n, const double *x,
@@ -568,7 +685,7 @@ int em2g_set_particles_device(em2g_ctx *c, int isp, int64_t n, const double *x,
   if (rc) return rc;
   if (isp < 0 || isp >= c->P.nsp) return fail(EM2G_ERR_INVALID, "bad species index");
   const double *src[6] = {x, y, vx, vy, vz, gamma};
-  return load_particles(c, isp, n, src, cudaMemcpyDeviceToDevice);
+  return load_particles(c, isp, n, src, true);
 }
 
 int em2g_get_particles(em2g_ctx *c, int isp, int64_t *n, double *x, double *y, double *vx,
@@ -580,26 +697,42 @@ int em2g_get_particles(em2g_ctx *c, int isp, int64_t *n, double *x, double *y, d
   if (n) *n = S.n;
   if (S.n == 0) return EM2G_OK;
   if (!x && !y && !vx && !vy && !vz && !gamma) return EM2G_OK;  // count query
-  if (!x || !y || !vx || !vy || !vz || !gamma) return fail(EM2G_ERR_INVALID, "null particle array");
-  if (is_fp32(c)) {
-    if ((rc = ensure_staging(c, 10 * S.n))) return rc;  // values, then records
-    if ((rc = download_f32(c, isp, c->staging, c->staging + 6 * S.n))) return rc;
-    double *dst[6] = {x, y, vx, vy, vz, gamma};
-    for (int k = 0; k < 6; ++k)
-      EM2G_CUDA(cudaMemcpyAsync(dst[k], c->staging + k * S.n, sizeof(double) * S.n,
-                                cudaMemcpyDeviceToHost, c->stream));
-    EM2G_CUDA(cudaStreamSynchronize(c->stream));
-    return EM2G_OK;
-  }
-  k_unsort<<<(unsigned)((S.n + 255) / 256), 256, 0, c->stream>>>(S.part, S.slot, S.part_alt,
-                                                                  S.n, S.cap);
-  EM2G_CUDA(cudaGetLastError());
   double *dst[6] = {x, y, vx, vy, vz, gamma};
-  for (int k = 0; k < 6; ++k)
-    EM2G_CUDA(cudaMemcpyAsync(dst[k], S.part_alt + k * S.cap, sizeof(double) * S.n,
-                              cudaMemcpyDeviceToHost, c->stream));
-  EM2G_CUDA(cudaStreamSynchronize(c->stream));
-  return EM2G_OK;
+  return particles_get(c, isp, 0, S.n, dst, false);
+}
+
+int em2g_particles_begin(em2g_ctx *c, int isp, int64_t n) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (isp < 0 || isp >= c->P.nsp) return fail(EM2G_ERR_INVALID, "bad species index");
+  return particles_begin(c, isp, n);
+}
+
+int em2g_particles_add(em2g_ctx *c, int isp, int64_t first, int64_t count, const double *x,
+                       const double *y, const double *vx, const double *vy, const double *vz,
+                       const double *gamma, int on_device) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (isp < 0 || isp >= c->P.nsp) return fail(EM2G_ERR_INVALID, "bad species index");
+  const double *src[6] = {x, y, vx, vy, vz, gamma};
+  return particles_add(c, isp, first, count, src, on_device != 0);
+}
+
+int em2g_particles_end(em2g_ctx *c, int isp) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (isp < 0 || isp >= c->P.nsp) return fail(EM2G_ERR_INVALID, "bad species index");
+  return particles_end(c, isp);
+}
+
+int em2g_get_particles_range(em2g_ctx *c, int isp, int64_t first, int64_t count, double *x,
+                             double *y, double *vx, double *vy, double *vz, double *gamma,
+                             int on_device) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (isp < 0 || isp >= c->P.nsp) return fail(EM2G_ERR_INVALID, "bad species index");
+  double *dst[6] = {x, y, vx, vy, vz, gamma};
+  return particles_get(c, isp, first, count, dst, on_device != 0);
 }
 
 int em2g_set_step(em2g_ctx *c, int it) {

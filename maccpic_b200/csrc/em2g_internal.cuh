@@ -64,6 +64,11 @@ struct Species {
   // ux, uy, uz; 5*cap floats, always grouped by cell (push_fast_f32.cu)
   float *p32 = nullptr, *p32_alt = nullptr;
   int since_sort = 0;  // FP32 pushes in place since the last regrouping
+  // an upload in slices (em2g_particles_begin / add / end): the announced
+  // count (-1: none open) and the slots added so far, in order.  The slices
+  // are parked in the alternate buffers; the species' particles change only
+  // at the end, once every slot passed the checks.
+  int64_t up_n = -1, up_added = 0;
 };
 
 // Device workspace of the Poisson/cgm solve (pic/fields.f90:370-651).
@@ -110,8 +115,12 @@ struct em2g_ctx {
   // the fast path deposits the whole current into jxm, jym, jzm)
   bool jp_live = true;
   double2 *spec = nullptr;  // nx*ny complex work of the spectral Poisson solve
-  double *staging = nullptr;  // FP64 staging of host copies (grown on demand)
+  // FP64 staging of host copies and the regrouping's records, grown on
+  // demand up to the field block or staging_cap(): particle copies go
+  // through it in slices, so it stays bounded on any particle count
+  double *staging = nullptr;
   int64_t staging_n = 0;
+  unsigned long long *up_bad = nullptr;  // per species: out of range, non-finite
   int64_t ncell = 0;
   int timing = 0;
   std::vector<cudaEvent_t> ev;  // start/stop pairs of the pending push launches
@@ -149,10 +158,22 @@ const char *variant_name_f32(int v);
 // mixed-precision path (push_fast_f32.cu, fields_f32.cu)
 int launch_prescale_f32(em2g_ctx *c, int isp);
 int launch_push_cells_f32(em2g_ctx *c, int isp);
-// particle transfers of FP32 contexts: staging = 6*n FP64 values in slot
-// order; rec = 32*n bytes of scratch (16-byte aligned) for the regrouping
-int upload_f32(em2g_ctx *c, int isp, const double *staging, int64_t n, void *rec);
-int download_f32(em2g_ctx *c, int isp, double *staging, void *rec);
+// particle transfers of FP32 contexts in slices (push_fast_f32.cu).
+// stage_f32: slots first..first+count from six device arrays (src[k][i] for
+// slot first+i), checked and parked unsorted in the alternate buffers, their
+// cells counted in cnt_alt, rejects counted in bad[0..2).  commit_f32: the
+// parked n particles regrouped by cell into the current buffers through
+// 32-byte records, rec_cap records at a time (rec: 16-byte aligned).
+// get_range_f32: slots first..first+count in FP64 into dst[k][i] (device
+// memory) through rec (32 bytes per slot of the range).
+int stage_f32(em2g_ctx *c, int isp, int64_t first, int64_t count, const double *const *src,
+              unsigned long long *bad);
+int commit_f32(em2g_ctx *c, int isp, int64_t n, void *rec, int64_t rec_cap);
+int get_range_f32(em2g_ctx *c, int isp, int64_t first, int64_t count, double *const *dst,
+                  void *rec);
+// bytes of the staging buffer particle copies go through: 80 bytes per
+// particle of the largest species, at most 80 * 2^24 (1.3 GB)
+int64_t staging_cap(const em2g_ctx *c);
 int smooth2_f32(em2g_ctx *c, float *a);
 int cg_init_f32(em2g_ctx *c);
 int fields_f32(em2g_ctx *c, int it, bool want_energies);
@@ -176,9 +197,10 @@ int step_enqueue(em2g_ctx *c);
 // the checks em2g_create applies to a parameter block (api.cu)
 int validate_params(const em2g_params *p);
 // counts particles of a 6 x ld FP64 block outside [0, xlim) x [0, ylim)
-// into bad[0] and those with non-finite values into bad[1] (api.cu)
+// into bad[0] and those with non-finite values into bad[1], after zeroing
+// both unless reset is false (api.cu)
 int check_particles_device(const double *part, int64_t n, int64_t ld, double xlim, double ylim,
-                           unsigned long long *bad, cudaStream_t st);
+                           unsigned long long *bad, cudaStream_t st, bool reset = true);
 // energies of the current fields and the reconnected flux of both sheets
 // of one FP32 field block into out[0..8); red: 6*kEnergyBlocks doubles
 // (diag.cu)

@@ -901,6 +901,121 @@ __global__ void k_rec_to_fp64(const float4 *__restrict__ rec, int64_t n, double 
   st[5 * n + s] = g;
 }
 
+// ---- a context's particle copies, in slices ------------------------------
+
+struct Src6 {
+  const double *a[6];  // x, y, vx, vy, vz, gamma; slot first+i at a[k][i]
+};
+struct Dst6 {
+  double *a[6];
+};
+
+// Slots first..first+count of an upload: checked (every value finite,
+// 0 <= x < xlim, 0 <= y < ylim), converted to the cell and FP32 offset the
+// push reads back (cell_f32) and to u = gamma v, and parked unsorted at
+// their slot in the alternate buffer P (offsets, u) with the cell's key in
+// key; the cells are counted in cnt.  A rejected particle is counted in
+// bad[0] (outside the grid) or bad[1] (non-finite) and parked with key -1.
+__global__ void k_stage_f32(Src6 src, int64_t count, int64_t first, int nx, int ny, double xlim,
+                            double ylim, float *P, int32_t *key, int64_t cap, int32_t *cnt,
+                            unsigned long long *bad) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool active = i < count;
+  const unsigned am = __ballot_sync(0xffffffffu, active);
+  if (!active) return;
+  double v[6];
+  bool finite = true;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    v[k] = src.a[k][i];
+    finite = finite && isfinite(v[k]);
+  }
+  const bool ok = finite && v[0] >= 0.0 && v[0] < xlim && v[1] >= 0.0 && v[1] < ylim;
+  if (!finite) atomicAdd(bad + 1, 1ull);
+  else if (!ok) atomicAdd(bad, 1ull);
+  int k = -1;
+  float xr = 0.f, yr = 0.f;
+  if (ok) {
+    const CellF32 cx = cell_f32(v[0], nx), cy = cell_f32(v[1], ny);
+    k = cy.c * nx + cx.c;
+    xr = cx.r;
+    yr = cy.r;
+  }
+  const unsigned om = __ballot_sync(am, ok);
+  if (ok) agg_atomic_add(cnt, k, om);
+  const int64_t j = first + i;
+  const double g = ok ? v[5] : 0.0;
+  P[j] = xr;
+  P[cap + j] = yr;
+  P[2 * cap + j] = (float)(v[2] * g);
+  P[3 * cap + j] = (float)(v[3] * g);
+  P[4 * cap + j] = (float)(v[4] * g);
+  key[j] = k;
+}
+
+// parked particle i takes the next position of its cell's range: its key
+// is replaced by that position
+__global__ void k_place(int32_t *key, int64_t n, const int32_t *__restrict__ off,
+                        int32_t *cursor) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool active = i < n;
+  const unsigned am = __ballot_sync(0xffffffffu, active);
+  if (!active) return;
+  const int k = key[i];
+  key[i] = off[k] + agg_atomic_add(cursor, k, am);
+}
+
+// the parked particles whose position lies in [p0, p0+len): one 32-byte
+// record each at rec[pos - p0], (xr, yr, ux, uy), (uz, slot, 0, 0)
+__global__ void k_window_rec(const float *__restrict__ P, const int32_t *__restrict__ pos,
+                             int64_t n, int64_t cap, int64_t p0, int64_t len, float4 *rec) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t q = (int64_t)pos[i] - p0;
+  if (q < 0 || q >= len) return;
+  rec[2 * q] = make_float4(P[i], P[cap + i], P[2 * cap + i], P[3 * cap + i]);
+  rec[2 * q + 1] = make_float4(P[4 * cap + i], __int_as_float((int32_t)i), 0.f, 0.f);
+}
+
+// cell-grouped FP32 -> records of the slots in [s0, s0+len), rec[slot - s0]:
+// (x, y) as doubles wrapped into the box, then (ux, uy, uz, 0)
+__global__ void k_grouped_to_rec_range(const float *__restrict__ P,
+                                       const int32_t *__restrict__ slot,
+                                       const int32_t *__restrict__ off, int64_t cap, int nx,
+                                       int ny, int64_t s0, int64_t len, float4 *rec) {
+  const int64_t cell = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kCopyLanes;
+  const int gl = threadIdx.x & (kCopyLanes - 1);
+  if (cell >= (int64_t)nx * ny) return;
+  const int kx = (int)(cell % nx), ky = (int)(cell / nx);
+  for (int32_t i = off[cell] + gl; i < off[cell + 1]; i += kCopyLanes) {
+    const int64_t q = (int64_t)slot[i] - s0;
+    if (q < 0 || q >= len) continue;
+    double x = kx + (double)P[i], y = ky + (double)P[cap + i];
+    if (x < 0.0) x += nx;
+    if (x >= nx) x -= nx;
+    if (y < 0.0) y += ny;
+    if (y >= ny) y -= ny;
+    reinterpret_cast<double2 *>(rec)[2 * q] = make_double2(x, y);
+    rec[2 * q + 1] = make_float4(P[2 * cap + i], P[3 * cap + i], P[4 * cap + i], 0.f);
+  }
+}
+
+// records in slot order -> six FP64 arrays: x, y, vx, vy, vz, gamma
+__global__ void k_rec_to_dst(const float4 *__restrict__ rec, int64_t len, Dst6 d) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= len) return;
+  const double2 xy = reinterpret_cast<const double2 *>(rec)[2 * s];
+  const float4 u = rec[2 * s + 1];
+  const double ux = u.x, uy = u.y, uz = u.z;
+  const double g = sqrt(1.0 + ux * ux + uy * uy + uz * uz);
+  d.a[0][s] = xy.x;
+  d.a[1][s] = xy.y;
+  d.a[2][s] = ux / g;
+  d.a[3][s] = uy / g;
+  d.a[4][s] = uz / g;
+  d.a[5][s] = g;
+}
+
 }  // namespace
 
 int num_variants_f32() { return (int)(sizeof(kVariants32) / sizeof(kVariants32[0])); }
@@ -980,43 +1095,63 @@ int launch_push_cells_f32(em2g_ctx *c, int isp) {
   return launch_ake_finish(c, isp, nb);
 }
 
-// staging (6*n doubles on the device, slot order) -> cell-grouped FP32
-int upload_f32(em2g_ctx *c, int isp, const double *staging, int64_t n, void *rec) {
+int stage_f32(em2g_ctx *c, int isp, int64_t first, int64_t count, const double *const *src,
+              unsigned long long *bad) {
   Species &S = c->sp[isp];
-  EM2G_CUDA(cudaMemsetAsync(S.cnt, 0, sizeof(int32_t) * c->ncell, c->stream));
-  EM2G_CUDA(cudaMemsetAsync(S.cursor, 0, sizeof(int32_t) * c->ncell, c->stream));
-  const unsigned nb = (unsigned)((n + 255) / 256);
-  if (n > 0) {
-    k_hist64<<<nb, 256, 0, c->stream>>>(staging, n, c->g.nx, c->g.ny, S.cnt);
-    EM2G_CUDA(cudaGetLastError());
-  }
+  if (count <= 0) return EM2G_OK;
+  Src6 a;
+  for (int k = 0; k < 6; ++k) a.a[k] = src[k];
+  k_stage_f32<<<(unsigned)((count + 255) / 256), 256, 0, c->stream>>>(
+      a, count, first, c->g.nx, c->g.ny, c->P.nx + 0.5, c->P.ny + 0.5, S.p32_alt, S.slot_alt,
+      S.cap, S.cnt_alt, bad);
+  c->launches += 1;
+  EM2G_CUDA(cudaGetLastError());
+  return EM2G_OK;
+}
+
+// The parked particles become the species' particles, grouped by cell:
+// offsets from the counts, a position for every particle, then the records
+// of one window of positions at a time, each window moved into the arrays
+// by a coalesced pass.
+int commit_f32(em2g_ctx *c, int isp, int64_t n, void *rec, int64_t rec_cap) {
+  Species &S = c->sp[isp];
+  std::swap(S.cnt, S.cnt_alt);  // the counts of the parked positions
   int rc = scan_cells(c, S.cnt, S.off);
   if (rc) return rc;
+  EM2G_CUDA(cudaMemsetAsync(S.cursor, 0, sizeof(int32_t) * c->ncell, c->stream));
   if (n > 0) {
+    const unsigned nb = (unsigned)((n + 255) / 256);
+    k_place<<<nb, 256, 0, c->stream>>>(S.slot_alt, n, S.off, S.cursor);
+    EM2G_CUDA(cudaGetLastError());
+    c->launches += 1;
     float4 *r = static_cast<float4 *>(rec);
-    k_scatter_rec<<<nb, 256, 0, c->stream>>>(staging, n, c->g.nx, c->g.ny, S.off, S.cursor, 0, r);
-    EM2G_CUDA(cudaGetLastError());
-    k_rec_to_soa<<<nb, 256, 0, c->stream>>>(r, n, S.p32, S.slot, S.cap);
-    EM2G_CUDA(cudaGetLastError());
+    for (int64_t p0 = 0; p0 < n; p0 += rec_cap) {
+      const int64_t len = std::min(rec_cap, n - p0);
+      k_window_rec<<<nb, 256, 0, c->stream>>>(S.p32_alt, S.slot_alt, n, S.cap, p0, len, r);
+      k_rec_to_soa<<<(unsigned)((len + 255) / 256), 256, 0, c->stream>>>(r, len, S.p32 + p0,
+                                                                          S.slot + p0, S.cap);
+      EM2G_CUDA(cudaGetLastError());
+      c->launches += 2;
+    }
   }
-  c->launches += 3;
   S.n = n;
   S.sorted = true;
   S.since_sort = 0;
   return EM2G_OK;
 }
 
-// cell-grouped FP32 -> staging (6*n doubles, slot order) through the
-// records (32*n bytes at rec)
-int download_f32(em2g_ctx *c, int isp, double *staging, void *rec) {
+int get_range_f32(em2g_ctx *c, int isp, int64_t first, int64_t count, double *const *dst,
+                  void *rec) {
   Species &S = c->sp[isp];
-  if (S.n == 0) return EM2G_OK;
+  if (count <= 0) return EM2G_OK;
   float4 *r = static_cast<float4 *>(rec);
   const int64_t nb = (c->ncell * kCopyLanes + 255) / 256;
-  k_grouped_to_rec<<<(unsigned)nb, 256, 0, c->stream>>>(S.p32, S.slot, S.off, S.cap, c->g.nx,
-                                                        c->g.ny, r);
+  k_grouped_to_rec_range<<<(unsigned)nb, 256, 0, c->stream>>>(S.p32, S.slot, S.off, S.cap,
+                                                               c->g.nx, c->g.ny, first, count, r);
   EM2G_CUDA(cudaGetLastError());
-  k_rec_to_fp64<<<(unsigned)((S.n + 255) / 256), 256, 0, c->stream>>>(r, S.n, staging);
+  Dst6 d;
+  for (int k = 0; k < 6; ++k) d.a[k] = dst[k];
+  k_rec_to_dst<<<(unsigned)((count + 255) / 256), 256, 0, c->stream>>>(r, count, d);
   EM2G_CUDA(cudaGetLastError());
   c->launches += 2;
   return EM2G_OK;

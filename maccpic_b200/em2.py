@@ -59,6 +59,7 @@ class RunParams:
     sort_interval: int = 0
     smooth_current: int = 0     # 1: smooth2 the current every step (not in em2)
     poisson: int = 0            # 0: em2's CG; 1: exact spectral solve (FP64, 2^k sides)
+    staging_mib: int = 0        # device staging for particle copies (0: the default)
 
     @property
     def shape(self):
@@ -69,7 +70,7 @@ class RunParams:
         check(_lib.lib().em2g_params_init(C.byref(P)))
         for name in ("nx", "ny", "nsp", "isav", "precision", "dx", "dy", "dt", "c",
                      "cg_maxits", "energy_mode", "cg_eps", "qme", "wpe", "device",
-                     "sort_interval", "smooth_current", "poisson"):
+                     "sort_interval", "smooth_current", "poisson", "staging_mib"):
             setattr(P, name, getattr(self, name))
         for name in ("qm", "q", "dn", "am", "tx", "ty"):
             arr = getattr(P, name)
@@ -185,6 +186,59 @@ class Em2Gpu:
         n = part.shape[1]
         ptrs = [C.c_void_p(part[k].data_ptr()) for k in range(6)]
         check(self._L.em2g_set_particles_device(self._h, isp, n, *ptrs))
+
+    def set_particles_slices(self, isp: int, n: int, slices) -> None:
+        """n particles of species isp handed over one slice at a time, for
+        sets too large to hold whole (em2g_particles_begin / add / end):
+        `slices` yields (6, m) float64 arrays -- numpy (host) or CUDA
+        tensors on this context's device -- in slot order, m summing to n.
+        The species keeps its old particles unless all n arrive and pass
+        the library's checks."""
+        L = self._L
+        check(L.em2g_particles_begin(self._h, isp, int(n)))
+        first = 0
+        try:
+            for a in slices:
+                if isinstance(a, np.ndarray):
+                    a = np.ascontiguousarray(a, dtype=np.float64)
+                    ptrs = [C.c_void_p(a[k].ctypes.data) for k in range(6)]
+                    dev = 0
+                else:
+                    import torch
+                    if a.dtype != torch.float64 or not a.is_cuda:
+                        raise ValueError("device slices must be float64 CUDA tensors")
+                    a = a.contiguous()
+                    ptrs = [C.c_void_p(a[k].data_ptr()) for k in range(6)]
+                    dev = 1
+                if a.ndim != 2 or a.shape[0] != 6:
+                    raise ValueError("slices must have shape (6, m)")
+                m = int(a.shape[1])
+                check(L.em2g_particles_add(self._h, isp, first, m, *ptrs, dev))
+                # the slice is read on the library's stream: wait for it before
+                # the caller may free or reuse its memory
+                check(L.em2g_synchronize(self._h))
+                first += m
+        finally:
+            rc = L.em2g_particles_end(self._h, isp)
+        check(rc)
+
+    def get_particles_range(self, isp: int, first: int, count: int, out=None):
+        """Slots first..first+count-1 of species isp as (6, count) x, y, vx,
+        vy, vz, gamma: into `out` (a C-contiguous float64 numpy array, or a
+        float64 CUDA tensor for a device-side copy) or a new numpy array."""
+        if out is None:
+            out = np.empty((6, count))
+        if isinstance(out, np.ndarray):
+            _check_out(out, (6, count))
+            ptrs = [C.c_void_p(out[k].ctypes.data) for k in range(6)]
+            dev = 0
+        else:
+            if tuple(out.shape) != (6, count) or not out.is_contiguous() or not out.is_cuda:
+                raise ValueError("out must be a contiguous (6, count) float64 CUDA tensor")
+            ptrs = [C.c_void_p(out[k].data_ptr()) for k in range(6)]
+            dev = 1
+        check(self._L.em2g_get_particles_range(self._h, isp, int(first), int(count), *ptrs, dev))
+        return out
 
     def set_stream(self, stream) -> None:
         """Enqueue further work on this cudaStream_t (int handle, or a torch

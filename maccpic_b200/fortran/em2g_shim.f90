@@ -31,8 +31,8 @@ module em2g_c
     integer(c_int64_t) :: np_max(4)
     integer(c_int32_t) :: cg_maxits, energy_mode
     real(c_double)     :: cg_eps, qme, wpe
-    integer(c_int32_t) :: device, sort_interval, smooth_current, poisson
-    integer(c_int32_t) :: reserved(14)
+    integer(c_int32_t) :: device, sort_interval, smooth_current, poisson, staging_mib
+    integer(c_int32_t) :: reserved(13)
   end type em2g_params
 
   interface

@@ -51,6 +51,7 @@ class HarrisConfig:
     steps: int = 2000
     seed: int = 0
     smooth_current: int = 0     # binomial current filter every step (not in em2)
+    check_steps: int | None = None  # length of the FP32-vs-FP64 check (None: steps)
 
     @property
     def b0(self):
@@ -102,7 +103,8 @@ PRESETS = {
     # profiling size: particle buffers (0.4-0.8 GB) well above the 126 MB L2
     "harris_1024x512_ppc32": HarrisConfig(nx=1024, ny=512, ppc=32, steps=100),
     "harris_4096x2048_ppc100": HarrisConfig(nx=4096, ny=2048, ppc=100, mass_ratio=100.0,
-                                            dt=0.04, steps=2000, smooth_current=1),
+                                            dt=0.04, steps=2000, smooth_current=1,
+                                            check_steps=200),
 }
 
 
@@ -239,3 +241,20 @@ def sample_particles_torch(cfg: HarrisConfig, device="cuda", n: int | None = Non
         out.append(torch.stack([x, y, vx2, vy2, vz2, gam]).to(dtype))
         del vx2, vy2, vz2, gam
     return out
+
+
+def sample_particles_torch_slices(cfg: HarrisConfig, device="cuda", slice_size: int = 1 << 24):
+    """The double-Harris distribution of :func:`sample_particles_torch`,
+    drawn slice by slice on the GPU for workloads whose whole FP64 state
+    (48 bytes per particle and species) would not fit beside the run: yields
+    (electrons, ions), two (6, m) float64 tensors per slice, m = slice_size
+    except for the last, NX*NY*ppc particles in all per species.  Slice k
+    has its own Philox stream (seed, k), so any slice can be drawn again
+    alone; each slice splits its particles between background and sheets in
+    the proportion of the whole."""
+    import dataclasses
+    n = cfg.nx * cfg.ny * cfg.ppc
+    for k, first in enumerate(range(0, n, slice_size)):
+        m = min(slice_size, n - first)
+        sub = dataclasses.replace(cfg, seed=cfg.seed * 1000003 + 7 * k + 1)
+        yield sample_particles_torch(sub, device=device, n=m)

@@ -127,3 +127,48 @@ def test_reused_workspace_gives_the_same_gradient(gpu):
         np.testing.assert_allclose(g, g0, rtol=1e-9, atol=1e-13)
         with pytest.raises(ValueError):
             A.theta_gradient_cuda(cfg, THETA, 12, checkpoint=4, draws=d, workspace=ws)
+
+
+def test_recomputed_segments_match_kept_fields(gpu):
+    """The reverse sweep's default -- checkpoints every K steps, each
+    segment's E and B recomputed from its checkpoint -- gives the gradient
+    that keeping E and B of every step gives, and leaves the context at the
+    final state the forward sweep reached."""
+    cfg = _cfg()
+    d = A.make_draws(cfg, device="cuda")
+    k = A.step_const(cfg)
+    steps, K = 12, 5                      # segments of 5, 5 and 2 steps
+    E0, B0, P0 = A.initial_state_torch(cfg, THETA, d)
+    grads = []
+    for keep in (False, True):
+        with A.CudaAdjoint(k, E0, B0, P0, steps, K, cfg.isav, keep_all_fields=keep) as adj:
+            adj.forward(steps)
+            Ef, Bf = adj.final_EB()
+            seed = [torch.ones_like(b) * 1e-3 for b in Bf]
+            lE, lB, lP = adj.backward([torch.zeros_like(e) for e in Ef], seed)
+            Ef2, Bf2 = adj.final_EB()
+            for a, b in zip(Ef + Bf, Ef2 + Bf2):
+                assert torch.equal(a, b)
+            assert adj.g.it == steps
+            grads.append([t.clone() for t in list(lE) + list(lB) + [x for p in lP for x in p]])
+    for a, b in zip(*grads):
+        assert rel(a, b) < 1e-9
+
+
+def test_autograd_function_reaches_theta(gpu):
+    """flux.backward() through CudaRun reaches the initial-state parameters,
+    and a second backward through a fresh graph gives the same gradient."""
+    cfg = _cfg()
+    d = A.make_draws(cfg, device="cuda")
+    k = A.step_const(cfg)
+    with A.CudaAdjoint(k, *A.initial_state_torch(cfg, THETA, d), 8, 4, cfg.isav) as adj:
+        gs = []
+        for _ in range(2):
+            th = torch.tensor(THETA, dtype=torch.float64, device="cuda", requires_grad=True)
+            E0, B0, P0 = A.initial_state_torch(cfg, (th[0], th[1], th[2]), d)
+            out = A.CudaRun.apply(adj, 8, *A.flatten_state(E0, B0, P0))
+            A.flux(out[3:], k).backward()
+            assert th.grad is not None and torch.isfinite(th.grad).all()
+            gs.append(th.grad.clone())
+    assert torch.allclose(gs[0], gs[1], rtol=1e-12, atol=0)
+    assert gs[0].abs().max() > 0

@@ -282,3 +282,50 @@ def test_outputs_into_caller_buffers(gpu):
                 np.testing.assert_array_equal(out, want)
         with pytest.raises(ValueError):
             e.get_particles(0, 0, out=np.empty((5, 3)))
+
+
+def test_runs_against_the_oracle(gpu, oracle_lib):
+    """Every run of an ensemble -- mass ratios 25, 49 and 100, uneven grids --
+    against the FP64 oracle stepping the same state, at the mixed path's
+    tolerances (those of test_gpu_fp32): kinetic energies to 1e-5 relative
+    every step, total field energy to 1e-4 at the isav steps, E and B to
+    1e-2 of their largest value and positions to 1e-3 cells after 40
+    steps; the FP64 reconnected flux and energies the ensemble reports for a
+    run equal a host computation from its downloaded fields."""
+    cfgs = _cfgs()
+    states = [_state(c) for c in cfgs]
+    oracles = []
+    for c, (fld, parts) in zip(cfgs, states):
+        rp = c.run_params()
+        op = oracle_lib.Params(nx=c.nx, ny=c.ny, dx=rp.dx, dy=rp.dy, dt=rp.dt, qm=rp.qm, q=rp.q,
+                               dn=rp.dn, am=rp.am, isav=rp.isav)
+        oracles.append(oracle_lib.State(op, fld, parts))
+    with _ensemble(cfgs, states) as e:
+        for k in range(1, 41):
+            r = e.step(1)
+            for i, (c, st) in enumerate(zip(cfgs, oracles)):
+                ref = st.step()
+                np.testing.assert_allclose(r["ake"][i, :2], ref["ake"], rtol=1e-5)
+                assert r["cg_iters"][i] >= 1
+                if k % c.isav == 0:
+                    tot, tot_ref = r["energies"][i].sum(), ref["energies"].sum()
+                    assert abs(tot - tot_ref) / tot_ref < 1e-4, (i, k, tot, tot_ref)
+        for i, (c, st) in enumerate(zip(cfgs, oracles)):
+            got = e.get_fields(i)
+            for f in range(6):
+                scale = np.abs(st.fld[f]).max()
+                assert np.abs(got[f] - st.fld[f]).max() / scale < 1e-2, (i, f)
+            for s in range(2):
+                q = e.get_particles(i, s)
+                for ax, n in ((0, c.nx), (1, c.ny)):
+                    d = np.abs(q[ax] - st.parts[s][ax])
+                    assert np.minimum(d, n - d).max() < 1e-3, (i, s, ax)
+            d = e.diagnostics(i)
+            a = got[:6, 1:c.ny + 1, 1:c.nx + 1]
+            e6 = 0.5 * (a * a).sum(axis=(1, 2)) / (c.nx * c.ny)
+            np.testing.assert_allclose(d["energies"], e6, rtol=1e-12)
+            by = got[4]
+            for sheet, row in enumerate((c.ny // 4, c.ny // 4 + c.ny // 2)):
+                b = 0.5 * (by[row, 1:c.nx + 1] + by[row + 1, 1:c.nx + 1])
+                psi = -np.cumsum(b) * c.dx
+                np.testing.assert_allclose(d["flux"][sheet], psi.max() - psi.min(), rtol=1e-11)
