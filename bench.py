@@ -677,23 +677,37 @@ def run_ensemble(args, local):
                      "times_ms": None, "interval_ms": None}
         else:
             tuned = autotune_ensemble(ens)  # the project's autotuner, on this batch
-        # warm-up: at least two regrouping cycles, so that the graph of every
-        # kind of step is captured before the timing
-        ens.step(max(args.warmup, 2 * tuned["sort_interval"]))
-        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        start.record()
-        out = ens.step(args.steps)
-        stop.record()
-        torch.cuda.synchronize()
-        ms = start.elapsed_time(stop)
-        cnt = ens.counters()
+        def timed_steps():
+            # warm-up: at least two regrouping cycles, so that the graph of
+            # every kind of step is captured before the timing
+            ens.step(max(args.warmup, 2 * tuned["sort_interval"]))
+            start = torch.cuda.Event(enable_timing=True)
+            stop = torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            start.record()
+            out = ens.step(args.steps)
+            stop.record()
+            torch.cuda.synchronize()
+            return start.elapsed_time(stop), out, ens.counters()["kernels_per_step"]
+
+        # one graph launch per step of the stage-by-stage kernels, then of the
+        # single persistent launch that runs every stage
+        ms_staged, out, k_staged = timed_steps()
+        ens.set_fused(True)
+        ms_fused, out_f, k_fused = timed_steps()
+        fused = ms_fused <= ms_staged
+        ms = ms_fused if fused else ms_staged
+        out = out_f if fused else out
         n = ens.particles
         return {"workload": "harris_ensemble_64runs", "runs": len(cfgs), "particles": n,
                 "grids": [min(c.nx for c in cfgs), max(c.nx for c in cfgs)],
                 "value": n * args.steps / (ms / 1e3), "unit": METRIC,
                 "ms_per_step": ms / args.steps, "graph": True,
-                "kernels_per_step": cnt["kernels_per_step"],
+                "step": "one persistent launch" if fused else "one launch per stage",
+                "kernels_per_step": k_fused if fused else k_staged,
+                "fused_ms_per_step": ms_fused / args.steps,
+                "staged_ms_per_step": ms_staged / args.steps,
+                "staged_kernels_per_step": k_staged,
                 "cg_iters_max": int(out["cg_iters"].max()),
                 "push_variant": tuned["variant"], "variant_step_ms": tuned["times_ms"],
                 "sort_interval": tuned["sort_interval"],

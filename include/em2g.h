@@ -327,6 +327,11 @@ int em2g_ens_num_runs(em2g_ens *ens, int *nruns);
 int em2g_ens_set_stream(em2g_ens *ens, void *cuda_stream);
 /* 1 (default): replay a captured graph per step; 0: launch the kernels */
 int em2g_ens_set_graph(em2g_ens *ens, int on);
+/* 1: each step is one persistent, cooperative kernel launch whose blocks
+ * run every stage above in turn, meeting at bounded grid barriers (a wait
+ * that gives up fails the step with EM2G_ERR_TIMEOUT); 0: one launch per
+ * stage.  The results are the same up to the order of FP32 sums. */
+int em2g_ens_set_fused(em2g_ens *ens, int on);
 /* the FP32 push variants (as em2g_num_variants of an FP32 context) */
 int em2g_ens_num_variants(em2g_ens *ens, int *n);
 int em2g_ens_set_variant(em2g_ens *ens, int variant);

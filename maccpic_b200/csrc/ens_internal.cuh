@@ -79,6 +79,15 @@ struct em2g_ens {
   // one captured graph per (in place, parity, cparity); invalid after a
   // change of variant, sort interval or stream
   bool use_graph = true;
+  // 1: each step is one persistent, cooperative launch (ens_step.cu);
+  // 0: one launch per stage (push_fast_f32.cu, fields_ens.cu)
+  bool fused = false;
+  void *fused_tab = nullptr;       // 8 step tables, one per kind of step
+  unsigned *step_sync = nullptr;   // [0, 2) the step's grid barrier, [2] its timeout flag
+  double *fused_partial = nullptr; // the CG's partial sums, 2 per block of the launch
+  int32_t *fused_sums = nullptr;   // the scan's chunk totals
+  int fused_blocks = 0;
+  bool fused_ready[8] = {};        // step tables written for the current variant
   cudaGraphExec_t exec[8] = {};
   int64_t graph_kernels[8] = {};
   int64_t kernels_per_step = 0;
@@ -98,5 +107,9 @@ int ens_prescale(em2g_ens *e);
 int ens_tick(em2g_ens *e);
 int ens_fields(em2g_ens *e);
 int ens_fields_kernels(const em2g_ens *e);
+// ens_step.cu: the table of step kind `key` written to the device (before
+// the launch or its capture), and the step as one cooperative launch
+int ens_fused_prepare(em2g_ens *e, int key, bool inplace);
+int ens_fused_launch(em2g_ens *e, int key, bool inplace);
 
 }  // namespace em2g

@@ -45,6 +45,7 @@ void drop_graphs(em2g_ens *e) {
       cudaGraphExecDestroy(x);
       x = nullptr;
     }
+  for (bool &r : e->fused_ready) r = false;  // the fused step's tables follow the variant
 }
 
 // the next step's kind: in place between regroupings
@@ -58,6 +59,7 @@ int graph_key(const em2g_ens *e, bool inplace) {
 
 int enqueue_step(em2g_ens *e, bool inplace) {
   int rc;
+  if (e->fused) return ens_fused_launch(e, graph_key(e, inplace), inplace);
   if ((rc = ens_prescale(e))) return rc;
   if ((rc = ens_push(e, e->parity, e->cparity, inplace))) return rc;
   if ((rc = ens_tick(e))) return rc;
@@ -67,6 +69,8 @@ int enqueue_step(em2g_ens *e, bool inplace) {
 int capture_step(em2g_ens *e, bool inplace) {
   const int key = graph_key(e, inplace);
   cudaGraph_t g = nullptr;
+  int prc;
+  if (e->fused && (prc = ens_fused_prepare(e, key, inplace))) return prc;
   EM2G_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
   const int rc = enqueue_step(e, inplace);
   const cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
@@ -235,7 +239,8 @@ int em2g_ens_destroy(em2g_ens *e) {
   void *bufs[] = {e->fld,   e->scaled,  e->tmp,      e->cgv,        e->red,     e->dev_out,
                   e->p32,   e->p32_alt, e->slot,     e->slot_alt,   e->off,     e->off_alt,
                   e->cnt,   e->cnt_alt, e->cursor,   e->scan_tmp,   e->counter, e->d_it,
-                  e->staging, e->cg_partial, e->cg_bar, e->cg_status};
+                  e->staging, e->cg_partial, e->cg_bar, e->cg_status, e->fused_tab,
+                  e->step_sync, e->fused_partial, e->fused_sums};
   for (void *p : bufs) cudaFree(p);
   if (e->host_out) cudaFreeHost(e->host_out);
   if (e->host_status) cudaFreeHost(e->host_status);
@@ -259,6 +264,17 @@ int em2g_ens_set_stream(em2g_ens *e, void *stream) {
   if (s != e->stream) {
     EM2G_CUDA(cudaStreamSynchronize(e->stream));
     e->stream = s;
+  }
+  return EM2G_OK;
+}
+
+int em2g_ens_set_fused(em2g_ens *e, int on) {
+  int rc = check_ens(e);
+  if (rc) return rc;
+  if ((on != 0) != e->fused) {
+    EM2G_CUDA(cudaStreamSynchronize(e->stream));
+    drop_graphs(e);
+    e->fused = on != 0;
   }
   return EM2G_OK;
 }
@@ -412,6 +428,8 @@ int em2g_ens_step(em2g_ens *e, int nsteps, double *ake_out, double *energies_out
       if (!R.loaded[s]) return fail(EM2G_ERR_INVALID, "set every run's particles before stepping");
   const int nr = (int)e->runs.size();
   EM2G_CUDA(cudaMemsetAsync(e->cg_status, 0, sizeof(int) * 2 * nr, e->stream));
+  if (e->step_sync)
+    EM2G_CUDA(cudaMemsetAsync(e->step_sync + 2, 0, sizeof(unsigned), e->stream));
   for (int k = 0; k < nsteps; ++k) {
     const bool inplace = next_inplace(e);
     if (e->use_graph) {
@@ -420,6 +438,11 @@ int em2g_ens_step(em2g_ens *e, int nsteps, double *ake_out, double *energies_out
       EM2G_CUDA(cudaGraphLaunch(e->exec[key], e->stream));
       e->graph_launches += 1;
       e->kernels_per_step = e->graph_kernels[key];
+    } else if (e->fused) {
+      const int key = graph_key(e, inplace);
+      if ((rc = ens_fused_prepare(e, key, inplace))) return rc;
+      if ((rc = enqueue_step(e, inplace))) return rc;
+      e->kernels_per_step = 1;
     } else {
       if ((rc = enqueue_step(e, inplace))) return rc;
       // prescale, tick, the push's and the fields' kernels
@@ -439,8 +462,18 @@ int em2g_ens_step(em2g_ens *e, int nsteps, double *ake_out, double *energies_out
                             cudaMemcpyDeviceToHost, e->stream));
   EM2G_CUDA(cudaMemcpyAsync(e->host_status, e->cg_status, sizeof(int) * 2 * nr,
                             cudaMemcpyDeviceToHost, e->stream));
+  unsigned step_timeout = 0;
+  if (e->step_sync)
+    EM2G_CUDA(cudaMemcpyAsync(&step_timeout, e->step_sync + 2, sizeof(unsigned),
+                              cudaMemcpyDeviceToHost, e->stream));
   EM2G_CUDA(cudaStreamSynchronize(e->stream));
   EM2G_CUDA(cudaGetLastError());
+  if (step_timeout) {
+    // the barrier's count is left undefined by a wait that gave up
+    EM2G_CUDA(cudaMemsetAsync(e->step_sync, 0, sizeof(unsigned) * 3, e->stream));
+    EM2G_CUDA(cudaStreamSynchronize(e->stream));
+    return fail(EM2G_ERR_TIMEOUT, "fused ensemble step: a grid barrier wait timed out");
+  }
   for (int r = 0; r < nr; ++r)
     if (e->host_status[2 * r])
       return fail(EM2G_ERR_TIMEOUT, "cg of run " + std::to_string(r) + ": a barrier wait timed out");

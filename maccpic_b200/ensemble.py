@@ -132,6 +132,11 @@ class Em2Ensemble:
     def set_graph(self, on: bool) -> None:
         check(self._L.em2g_ens_set_graph(self._h, 1 if on else 0))
 
+    def set_fused(self, on: bool) -> None:
+        """True: each step is one persistent, cooperative kernel launch
+        (em2g_ens_set_fused); False: one launch per stage."""
+        check(self._L.em2g_ens_set_fused(self._h, 1 if on else 0))
+
     def num_variants(self) -> int:
         n = C.c_int()
         check(self._L.em2g_ens_num_variants(self._h, C.byref(n)))

@@ -329,3 +329,42 @@ def test_runs_against_the_oracle(gpu, oracle_lib):
                 b = 0.5 * (by[row, 1:c.nx + 1] + by[row + 1, 1:c.nx + 1])
                 psi = -np.cumsum(b) * c.dx
                 np.testing.assert_allclose(d["flux"][sheet], psi.max() - psi.min(), rtol=1e-11)
+
+
+@pytest.mark.parametrize("graph,interval,smooth", [(True, 1, 0), (False, 1, 0), (True, 3, 0),
+                                                   (True, 1, 1)],
+                         ids=["graph", "direct", "in-place", "current-filter"])
+def test_fused_step_matches_staged_launches(gpu, graph, interval, smooth):
+    """The step as one persistent, cooperative launch (em2g_ens_set_fused)
+    against the stage-by-stage launches: after one step the particles are
+    bitwise equal (the same arithmetic on the same fields) and the kinetic
+    energies equal to their summation order; over the next steps, the FP32
+    deposit atomics adding in another order, fields, energies and kinetic
+    energies stay within FP32 round-off growth.  The runs' isav of 20, 20 and
+    5 exercise the E/B filter and the energies inside the launch."""
+    import dataclasses
+    cfgs = [dataclasses.replace(c, smooth_current=smooth) for c in _cfgs()]
+    states = [_state(c) for c in cfgs]
+    with _ensemble(cfgs, states) as a, _ensemble(cfgs, states) as b:
+        b.set_fused(True)
+        b.set_graph(graph)
+        a.set_sort_interval(interval)
+        b.set_sort_interval(interval)
+        ra, rb = a.step(1), b.step(1)
+        np.testing.assert_allclose(rb["ake"], ra["ake"], rtol=1e-12)
+        for r in range(len(cfgs)):
+            for s in range(2):
+                np.testing.assert_array_equal(b.get_particles(r, s), a.get_particles(r, s))
+        assert b.counters()["kernels_per_step"] == 1
+        for _ in range(9):
+            ra, rb = a.step(1), b.step(1)
+        np.testing.assert_allclose(rb["ake"], ra["ake"], rtol=1e-4)
+        assert (rb["cg_iters"] >= 1).all()
+        for r, c in enumerate(cfgs):
+            fa, fb = a.get_fields(r), b.get_fields(r)
+            for k in range(6):
+                assert rel(fb[k], fa[k]) < 1e-3, (r, k)
+            if 10 % c.isav == 0:
+                np.testing.assert_allclose(rb["energies"][r], ra["energies"][r], rtol=1e-4)
+        if graph:
+            assert b.counters()["graph_launches"] == 10
