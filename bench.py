@@ -630,6 +630,14 @@ def run_adjoint(args, local):
         Bf = ws.final_B()
         t_rev, _ = timed(lambda: ws.backward([torch.zeros_like(b) for b in Bf],
                                              [torch.ones_like(b) * 1e-3 for b in Bf]))
+        # the same gradient with E and B of every step kept instead of
+        # recomputed (more memory, no second forward pass)
+        from maccpic_b200._lib import check
+        check(ws._L.em2g_adj_keep_all_fields(ws._h, 1))
+        A.theta_gradient_cuda(cfg, theta, min(T, 4), checkpoint=K, draws=d, workspace=ws)
+        t_grad_keep, (F2, g2) = timed(lambda: A.theta_gradient_cuda(
+            cfg, theta, T, checkpoint=K, draws=d, workspace=ws))
+        check(ws._L.em2g_adj_keep_all_fields(ws._h, 0))
         # the gradient against central differences of the same forward
         # (h = 1e-3, common random numbers) at growing horizons
         fd = {}
@@ -651,6 +659,10 @@ def run_adjoint(args, local):
             "gradient_over_forward": t_grad / t_fwd,
             "workspace_setup_ms": t_setup * 1e3,
             "workspace_bytes": mem,
+            "keep_all_fields": {"gradient_over_forward": t_grad_keep / t_fwd,
+                                "gradient_ms": t_grad_keep * 1e3,
+                                "workspace_bytes": mem + 8 * (T - K) * 6 * cfg.nx * cfg.ny,
+                                "dflux_dtheta": [float(x) for x in g2]},
             "memory": "checkpoints every K steps (fields + particles) and K field slots; each "
                       "segment recomputed from its checkpoint in the reverse sweep",
             "fd_h": 1e-3,
@@ -695,6 +707,7 @@ def run_ensemble(args, local):
         ms_staged, out, k_staged = timed_steps()
         ens.set_fused(True)
         ms_fused, out_f, k_fused = timed_steps()
+        phases = ens.phase_ms()
         fused = ms_fused <= ms_staged
         ms = ms_fused if fused else ms_staged
         out = out_f if fused else out
@@ -708,6 +721,7 @@ def run_ensemble(args, local):
                 "fused_ms_per_step": ms_fused / args.steps,
                 "staged_ms_per_step": ms_staged / args.steps,
                 "staged_kernels_per_step": k_staged,
+                "fused_phase_ms": [round(x, 4) for x in phases if x > 0],
                 "cg_iters_max": int(out["cg_iters"].max()),
                 "push_variant": tuned["variant"], "variant_step_ms": tuned["times_ms"],
                 "sort_interval": tuned["sort_interval"],

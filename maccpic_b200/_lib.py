@@ -38,7 +38,8 @@ EXPORTS = [
     "em2g_adj_backward", "em2g_adj_get_fields_device", "em2g_adj_get_particles_device",
     "em2g_adj_get_initial_particles_device",
     "em2g_ens_create", "em2g_ens_destroy", "em2g_ens_num_runs", "em2g_ens_set_stream",
-    "em2g_ens_set_graph", "em2g_ens_set_fused", "em2g_ens_num_variants", "em2g_ens_set_variant",
+    "em2g_ens_set_graph", "em2g_ens_set_fused", "em2g_ens_get_phase_ns",
+    "em2g_ens_num_variants", "em2g_ens_set_variant",
     "em2g_ens_set_sort_interval", "em2g_ens_set_fields", "em2g_ens_get_fields",
     "em2g_ens_set_particles", "em2g_ens_set_particles_device", "em2g_ens_get_particles",
     "em2g_ens_step", "em2g_ens_get_step", "em2g_ens_diagnostics", "em2g_ens_get_counters",
@@ -141,6 +142,7 @@ def lib() -> C.CDLL:
         "em2g_ens_set_stream": (C.c_int, [ctx, vp]),
         "em2g_ens_set_graph": (C.c_int, [ctx, C.c_int]),
         "em2g_ens_set_fused": (C.c_int, [ctx, C.c_int]),
+        "em2g_ens_get_phase_ns": (C.c_int, [ctx, i64p, C.c_int]),
         "em2g_ens_num_variants": (C.c_int, [ctx, ip]),
         "em2g_ens_set_variant": (C.c_int, [ctx, C.c_int]),
         "em2g_ens_set_sort_interval": (C.c_int, [ctx, C.c_int]),

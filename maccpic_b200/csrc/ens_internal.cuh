@@ -86,6 +86,7 @@ struct em2g_ens {
   unsigned *step_sync = nullptr;   // [0, 2) the step's grid barrier, [2] its timeout flag
   double *fused_partial = nullptr; // the CG's partial sums, 2 per block of the launch
   int32_t *fused_sums = nullptr;   // the scan's chunk totals
+  unsigned long long *fused_marks = nullptr;  // global timer at the fused step's barriers
   int fused_blocks = 0;
   bool fused_ready[8] = {};        // step tables written for the current variant
   cudaGraphExec_t exec[8] = {};
@@ -111,5 +112,6 @@ int ens_fields_kernels(const em2g_ens *e);
 // the launch or its capture), and the step as one cooperative launch
 int ens_fused_prepare(em2g_ens *e, int key, bool inplace);
 int ens_fused_launch(em2g_ens *e, int key, bool inplace);
+int ens_fused_phase_ns(em2g_ens *e, int64_t *out, int n);
 
 }  // namespace em2g

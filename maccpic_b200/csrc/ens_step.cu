@@ -32,7 +32,7 @@ __device__ __forceinline__ T ld(const T *p) {
 }
 
 // exclusive scan of all pairs' cell counts (regrouping steps), in chunks
-constexpr int kScanChunk = 1024;
+constexpr int kScanChunk = 4096;
 
 struct EnsScanArgs {
   const int32_t *in;  // counts of the current positions, all pairs
@@ -55,7 +55,16 @@ struct EnsStepTab {
   int any_smooth_current;
   unsigned *bar;      // the step's grid barrier: arrival count, generation
   int *status;        // 1 when a barrier wait gave up
+  unsigned long long *marks;  // the global timer at the start and after each barrier
 };
+
+constexpr int kMaxMarks = 32;
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 // ---- the per-cell stages, with loads through L2 --------------------------
 
@@ -204,9 +213,16 @@ __global__ void __launch_bounds__(TCX * G, MINB) k_ens_step(const EnsStepTab *tp
   const int nr = eg.nruns;
   const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t gstride = (int64_t)gridDim.x * blockDim.x;
+  // block 0's thread 0 notes the time at the start and after each barrier:
+  // the phases' durations, for the design notes (em2g_ens_get_phase_ns)
+  int nmark = 0;
+  if (gtid == 0) t.marks[nmark] = global_ns();
+  ++nmark;
 #define EM2G_SYNC_ALL()                                                 \
   do {                                                                  \
     if (!grid::grid_barrier(t.bar, gridDim.x, t.status)) return;        \
+    if (gtid == 0 && nmark < kMaxMarks) t.marks[nmark] = global_ns();   \
+    ++nmark;                                                            \
   } while (0)
 
   // ---- (E, B) pairs of every species, counters to zero, the first pass
@@ -273,16 +289,37 @@ __global__ void __launch_bounds__(TCX * G, MINB) k_ens_step(const EnsStepTab *tp
   }
   EM2G_SYNC_ALL();
   if (!INPLACE) {
-    // the chunk totals scanned by one thread, then added to every chunk
+    // the chunk totals scanned by block 0, then added to every chunk
     const EnsScanArgs &sc = t.scan;
-    if (gtid == 0) {
-      int32_t run = 0;
-      for (int c = 0; c < sc.nchunks; ++c) {
-        const int32_t x = ld(sc.sums + c);
-        sc.sums[c] = run;
-        run += x;
+    if (blockIdx.x == 0) {
+      int32_t *wt = reinterpret_cast<int32_t *>(sh);
+      const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+      int32_t carry = 0;
+      for (int base = 0; base < sc.nchunks; base += blockDim.x) {
+        const int c = base + threadIdx.x;
+        const int32_t v = c < sc.nchunks ? ld(sc.sums + c) : 0;
+        int32_t incl = v;
+        for (int o = 1; o < 32; o <<= 1) {
+          const int32_t u = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += u;
+        }
+        if (lane == 31) wt[wid] = incl;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+          int32_t run = 0;
+          for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
+            const int32_t x = wt[k];
+            wt[k] = run;
+            run += x;
+          }
+          wt[32] = run;
+        }
+        __syncthreads();
+        if (c < sc.nchunks) sc.sums[c] = carry + wt[wid] + incl - v;
+        carry += wt[32];
+        __syncthreads();
       }
-      sc.out[sc.n] = run;
+      if (threadIdx.x == 0) sc.out[sc.n] = carry;
     }
     EM2G_SYNC_ALL();
     for (int c = blockIdx.x; c < sc.nchunks; c += gridDim.x) {
@@ -490,6 +527,8 @@ static int fused_alloc(em2g_ens *e) {
   EM2G_CUDA(cudaMalloc((void **)&e->fused_partial, sizeof(double) * 2 * max_blocks));
   const int64_t nchunks = (e->ncell + kScanChunk - 1) / kScanChunk;
   EM2G_CUDA(cudaMalloc((void **)&e->fused_sums, sizeof(int32_t) * (nchunks + 1)));
+  EM2G_CUDA(cudaMalloc((void **)&e->fused_marks, sizeof(unsigned long long) * kMaxMarks));
+  EM2G_CUDA(cudaMemset(e->fused_marks, 0, sizeof(unsigned long long) * kMaxMarks));
   return EM2G_OK;
 }
 
@@ -569,6 +608,7 @@ int ens_fused_prepare(em2g_ens *e, int key, bool inplace) {
   T->any_smooth_current = e->any_smooth_current ? 1 : 0;
   T->bar = e->step_sync;
   T->status = reinterpret_cast<int *>(e->step_sync + 2);
+  T->marks = e->fused_marks;
   EM2G_CUDA(cudaMemcpyAsync(static_cast<EnsStepTab *>(e->fused_tab) + key, T.get(),
                             sizeof(EnsStepTab), cudaMemcpyHostToDevice, e->stream));
   EM2G_CUDA(cudaStreamSynchronize(e->stream));
@@ -586,6 +626,17 @@ int ens_fused_launch(em2g_ens *e, int key, bool inplace) {
   EM2G_CUDA(cudaLaunchCooperativeKernel(
       inplace ? (const void *)F.inplace : (const void *)F.regroup, dim3(e->fused_blocks),
       dim3(F.threads), args, 0, e->stream));
+  return EM2G_OK;
+}
+
+// the durations between the marks of the last fused step (ns)
+int ens_fused_phase_ns(em2g_ens *e, int64_t *out, int n) {
+  if (!e->fused_marks) return fail(EM2G_ERR_INVALID, "no fused step has run");
+  unsigned long long h[kMaxMarks];
+  EM2G_CUDA(cudaMemcpyAsync(h, e->fused_marks, sizeof(h), cudaMemcpyDeviceToHost, e->stream));
+  EM2G_CUDA(cudaStreamSynchronize(e->stream));
+  for (int k = 0; k < n; ++k)
+    out[k] = (k + 1 < kMaxMarks && h[k + 1] >= h[k] && h[k] != 0) ? (int64_t)(h[k + 1] - h[k]) : 0;
   return EM2G_OK;
 }
 

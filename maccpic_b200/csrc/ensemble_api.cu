@@ -240,7 +240,7 @@ int em2g_ens_destroy(em2g_ens *e) {
                   e->p32,   e->p32_alt, e->slot,     e->slot_alt,   e->off,     e->off_alt,
                   e->cnt,   e->cnt_alt, e->cursor,   e->scan_tmp,   e->counter, e->d_it,
                   e->staging, e->cg_partial, e->cg_bar, e->cg_status, e->fused_tab,
-                  e->step_sync, e->fused_partial, e->fused_sums};
+                  e->step_sync, e->fused_partial, e->fused_sums, e->fused_marks};
   for (void *p : bufs) cudaFree(p);
   if (e->host_out) cudaFreeHost(e->host_out);
   if (e->host_status) cudaFreeHost(e->host_status);
@@ -522,6 +522,13 @@ int em2g_ens_diagnostics(em2g_ens *e, int run, double *out, int nout) {
   EM2G_CUDA(cudaStreamSynchronize(e->stream));
   for (int k = 0; k < std::min(nout, EM2G_NDIAG); ++k) out[k] = h[k];
   return EM2G_OK;
+}
+
+int em2g_ens_get_phase_ns(em2g_ens *e, int64_t *ns, int n) {
+  int rc = check_ens(e);
+  if (rc) return rc;
+  if (!ns || n < 1 || n > 31) return fail(EM2G_ERR_INVALID, "ns must hold 1..31 values");
+  return ens_fused_phase_ns(e, ns, n);
 }
 
 int em2g_ens_get_counters(em2g_ens *e, int64_t *kernel_launches, int64_t *graph_launches,

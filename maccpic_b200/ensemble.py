@@ -132,6 +132,13 @@ class Em2Ensemble:
     def set_graph(self, on: bool) -> None:
         check(self._L.em2g_ens_set_graph(self._h, 1 if on else 0))
 
+    def phase_ms(self, n: int = 24):
+        """Durations (ms) of the last fused step's phases: from the launch's
+        start to its first grid barrier, then between barriers."""
+        out = (C.c_int64 * n)()
+        check(self._L.em2g_ens_get_phase_ns(self._h, out, n))
+        return [v / 1e6 for v in out]
+
     def set_fused(self, on: bool) -> None:
         """True: each step is one persistent, cooperative kernel launch
         (em2g_ens_set_fused); False: one launch per stage."""

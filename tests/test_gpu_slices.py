@@ -57,8 +57,9 @@ def test_slices_equal_one_piece(gpu, precision):
     for back, f, ake in got[1:]:
         for s in range(2):
             np.testing.assert_array_equal(back[s], got[0][0][s])
-        # the deposits' atomics may add in another order
-        tol = 1e-12 if precision == 0 else 1e-5
+        # the deposits' atomics may add in another order (FP32: that round-off,
+        # grown over three steps, is ~2e-5 of the largest value)
+        tol = 1e-12 if precision == 0 else 1e-4
         for k in range(6):
             scale = max(np.abs(got[0][1][k]).max(), 1e-300)
             assert np.abs(f[k] - got[0][1][k]).max() / scale < tol, k
