@@ -82,7 +82,8 @@ struct em2g_ens {
   // 1: each step is one persistent, cooperative launch (ens_step.cu);
   // 0: one launch per stage (push_fast_f32.cu, fields_ens.cu)
   bool fused = false;
-  void *fused_tab = nullptr;       // 8 step tables, one per kind of step
+  void *fused_tab = nullptr;       // 8 step tables, one per kind of step (device)
+  void *fused_push = nullptr;      // 8 push tables, the launch's parameter (host)
   unsigned *step_sync = nullptr;   // [0, 2) the step's grid barrier, [2] its timeout flag
   double *fused_partial = nullptr; // the CG's partial sums, 2 per block of the launch
   int32_t *fused_sums = nullptr;   // the scan's chunk totals

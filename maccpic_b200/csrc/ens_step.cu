@@ -42,9 +42,12 @@ struct EnsScanArgs {
   int nchunks;
 };
 
+// The step's tables besides the push's, which travel as a kernel parameter
+// (the constant bank, as for the stage-by-stage push: the segment loop
+// reads a pair's arguments without loads that stores could invalidate).
 struct EnsStepTab {
-  EnsPush32 push;
   EnsAke ake;
+  int npairs;
   EnsGrid32 grid;
   EnsCg32 cg;
   EnsScanArgs scan;
@@ -202,10 +205,10 @@ __device__ __forceinline__ void for_tiles(const EnsGrid32 &e, F f) {
 }
 
 template <int TCX, int G, int NC, int MINB, bool INPLACE>
-__global__ void __launch_bounds__(TCX * G, MINB) k_ens_step(const EnsStepTab *tp) {
+__global__ void __launch_bounds__(TCX * G, MINB)
+    k_ens_step(const __grid_constant__ EnsPush32 e, const EnsStepTab *tp) {
   __shared__ float4 win[3][WY][NC * TCX + 5];
   __shared__ WarpScratch ws[TCX * G / 32];
-  __shared__ Args32 s_pair;
   __shared__ int s_tile;
   __shared__ double sh[33];
   const EnsStepTab &t = *tp;
@@ -249,7 +252,7 @@ __global__ void __launch_bounds__(TCX * G, MINB) k_ens_step(const EnsStepTab *tp
       t.cnt_next[k] = 0;
       if (!INPLACE) t.cursor[k] = 0;
     }
-    if (gtid == 0) *t.push.counter = 0;
+    if (gtid == 0) *e.counter = 0;
     for (int r = (int)gtid; r < nr; r += (int)gstride) t.cg.a[r].bar[0] = 0u;
     if (!INPLACE) {
       // each chunk's exclusive scan, its total aside
@@ -332,7 +335,6 @@ __global__ void __launch_bounds__(TCX * G, MINB) k_ens_step(const EnsStepTab *tp
 
   // ---- the push of every pair, row segments claimed from a counter
   {
-    const EnsPush32 &e = t.push;
     for (;;) {
       if (threadIdx.x == 0) s_tile = atomicAdd(e.counter, 1);
       __syncthreads();  // also: every thread is done with the last segment
@@ -343,14 +345,11 @@ __global__ void __launch_bounds__(TCX * G, MINB) k_ens_step(const EnsStepTab *tp
         const int mid = (lo + hi + 1) >> 1;
         if (e.tile0[mid] <= tl) lo = mid; else hi = mid - 1;
       }
-      if (threadIdx.x == 0) s_pair = e.pair[lo];
-      __syncthreads();
       const int lt = tl - e.tile0[lo];
       const int segs = e.segs[lo];
       const int row = lt / segs;
-      push_segment<TCX, G, NC, INPLACE>(s_pair, (lt - row * segs) * (NC * TCX), row, lt, win,
-                                        ws);
-      __syncthreads();  // s_tile and s_pair are rewritten by the next claim
+      push_segment<TCX, G, NC, INPLACE>(e.pair[lo], (lt - row * segs) * (NC * TCX), row, lt,
+                                        win, ws);
     }
   }
   EM2G_SYNC_ALL();
@@ -358,7 +357,7 @@ __global__ void __launch_bounds__(TCX * G, MINB) k_ens_step(const EnsStepTab *tp
   // ---- kinetic energies, the step counter, the fold in x, then in y
   {
     const EnsAke &a = t.ake;
-    for (int p = blockIdx.x; p < t.push.npairs; p += gridDim.x) {
+    for (int p = blockIdx.x; p < t.npairs; p += gridDim.x) {
       double v = 0.0;
       for (int i = threadIdx.x; i < a.count[p]; i += blockDim.x) v += ld(a.partial[p] + i);
       v = grid::block_sum(v, sh);
@@ -486,8 +485,8 @@ __global__ void __launch_bounds__(TCX * G, MINB) k_ens_step(const EnsStepTab *tp
 }
 
 struct FusedVariant {
-  void (*regroup)(const EnsStepTab *);
-  void (*inplace)(const EnsStepTab *);
+  void (*regroup)(const EnsPush32, const EnsStepTab *);
+  void (*inplace)(const EnsPush32, const EnsStepTab *);
   int threads, cells;
 };
 #define EM2G_FUSED(T, GG, N, M) \
@@ -520,6 +519,7 @@ int fused_blocks(const em2g_ens *e, int *blocks) {
 // scan's chunk totals.
 static int fused_alloc(em2g_ens *e) {
   if (e->fused_tab) return EM2G_OK;
+  e->fused_push = ::operator new(sizeof(EnsPush32) * 8);
   EM2G_CUDA(cudaMalloc(&e->fused_tab, sizeof(EnsStepTab) * 8));
   EM2G_CUDA(cudaMalloc((void **)&e->step_sync, sizeof(unsigned) * 4));
   EM2G_CUDA(cudaMemset(e->step_sync, 0, sizeof(unsigned) * 4));
@@ -547,8 +547,10 @@ int ens_fused_prepare(em2g_ens *e, int key, bool inplace) {
   if (blocks < nr) return fail(EM2G_ERR_RANGE, "more runs than blocks of the fused step");
   std::unique_ptr<EnsStepTab> T(new EnsStepTab());
   const int bp = e->parity, cp = e->cparity;
-  ens_push_tables(e, bp, cp, inplace, F.cells, F.threads, &T->push, &T->ake);
-  T->push.counter = e->counter;
+  EnsPush32 *P = static_cast<EnsPush32 *>(e->fused_push) + key;
+  ens_push_tables(e, bp, cp, inplace, F.cells, F.threads, P, &T->ake);
+  P->counter = e->counter;
+  T->npairs = P->npairs;
   T->grid = *make_grid_table(e);
   // every run's CG: blocks in proportion to its cells (at least one, at
   // most one per blockDim cells), summing to at most the launch's blocks
@@ -622,7 +624,8 @@ int ens_fused_prepare(em2g_ens *e, int key, bool inplace) {
 int ens_fused_launch(em2g_ens *e, int key, bool inplace) {
   const FusedVariant &F = fused_variant(e);
   const EnsStepTab *tab = static_cast<const EnsStepTab *>(e->fused_tab) + key;
-  void *args[] = {(void *)&tab};
+  EnsPush32 *push = static_cast<EnsPush32 *>(e->fused_push) + key;
+  void *args[] = {(void *)push, (void *)&tab};
   EM2G_CUDA(cudaLaunchCooperativeKernel(
       inplace ? (const void *)F.inplace : (const void *)F.regroup, dim3(e->fused_blocks),
       dim3(F.threads), args, 0, e->stream));

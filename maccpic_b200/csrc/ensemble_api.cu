@@ -242,6 +242,7 @@ int em2g_ens_destroy(em2g_ens *e) {
                   e->staging, e->cg_partial, e->cg_bar, e->cg_status, e->fused_tab,
                   e->step_sync, e->fused_partial, e->fused_sums, e->fused_marks};
   for (void *p : bufs) cudaFree(p);
+  ::operator delete(e->fused_push);
   if (e->host_out) cudaFreeHost(e->host_out);
   if (e->host_status) cudaFreeHost(e->host_status);
   if (e->own_stream) cudaStreamDestroy(e->own_stream);
