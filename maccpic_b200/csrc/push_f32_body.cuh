@@ -29,7 +29,9 @@ struct Args32 {
   const float2 *__restrict__ ebz;  // (a*Ez, a*Bz): x half, y half
   const float2 *__restrict__ eby;  // (a*Ey, a*By): x node, y half
   float *rho, *jx, *jy, *jz;
-  const float *__restrict__ A;  // xr, yr, ux, uy, uz
+  // particles: entry j of 4*cap floats holds (xr, yr, ux, uy) as one float4
+  // (one 128-bit load or store), then cap floats hold uz
+  const float *__restrict__ A;
   const int32_t *__restrict__ slotA;
   float *B;
   int32_t *slotB;
@@ -463,13 +465,18 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
   // software pipeline: the next particle's state is loaded while this one runs
   float pxr = 0.f, pyr = 0.f, pux = 0.f, puy = 0.f, puz = 0.f;
   int32_t pslot = 0;
+  const float4 *__restrict__ A4 = reinterpret_cast<const float4 *>(a.A);
+  const float *__restrict__ Auz = a.A + 4 * cap;
+  float4 *B4 = reinterpret_cast<float4 *>(a.B);
+  float *Buz = a.B + 4 * cap;
   if (beg + gl < end) {
     const int32_t j = beg + gl;
-    pxr = a.A[j];
-    pyr = a.A[cap + j];
-    pux = a.A[2 * cap + j];
-    puy = a.A[3 * cap + j];
-    puz = a.A[4 * cap + j];
+    const float4 q = A4[j];
+    pxr = q.x;
+    pyr = q.y;
+    pux = q.z;
+    puy = q.w;
+    puz = Auz[j];
     pslot = a.slotA[j];
   }
 #pragma unroll
@@ -495,11 +502,12 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
       end = valid ? a.offA[cell + 1] : 0;
       if (beg + gl < end) {
         const int32_t j = beg + gl;
-        pxr = a.A[j];
-        pyr = a.A[cap + j];
-        pux = a.A[2 * cap + j];
-        puy = a.A[3 * cap + j];
-        puz = a.A[4 * cap + j];
+        const float4 q = A4[j];
+        pxr = q.x;
+        pyr = q.y;
+        pux = q.z;
+        puy = q.w;
+        puz = Auz[j];
         pslot = a.slotA[j];
       }
     }
@@ -523,11 +531,12 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
       const int32_t cslot = pslot;
       const int32_t j = i + G;
       if (j < end) {
-        pxr = a.A[j];
-        pyr = a.A[cap + j];
-        pux = a.A[2 * cap + j];
-        puy = a.A[3 * cap + j];
-        puz = a.A[4 * cap + j];
+        const float4 q = A4[j];
+        pxr = q.x;
+        pyr = q.y;
+        pux = q.z;
+        puy = q.w;
+        puz = Auz[j];
         pslot = a.slotA[j];
       }
       // a lane without a particle runs on a dummy inside a real cell
@@ -544,11 +553,8 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
           float xn = o.mx + (float)o.ox, yn = o.my + (float)o.oy;
           if (o.ox + (o.ncx - o.cx) == 0) xn = fminf(xn, kBelowOne);
           if (o.oy + (o.ncy - o.cy) == 0) yn = fminf(yn, kBelowOne);
-          a.B[i] = xn;
-          a.B[cap + i] = yn;
-          a.B[2 * cap + i] = o.ux;
-          a.B[3 * cap + i] = o.uy;
-          a.B[4 * cap + i] = o.uz;
+          B4[i] = make_float4(xn, yn, o.ux, o.uy);
+          Buz[i] = o.uz;
         }
       } else {
         // write back grouped by the cell of the start of this step: particles
@@ -572,11 +578,8 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
           }
         }
         if (pos >= 0) {
-          a.B[pos] = o.mx;
-          a.B[cap + pos] = o.my;
-          a.B[2 * cap + pos] = o.ux;
-          a.B[3 * cap + pos] = o.uy;
-          a.B[4 * cap + pos] = o.uz;
+          B4[pos] = make_float4(o.mx, o.my, o.ux, o.uy);
+          Buz[pos] = o.uz;
           a.slotB[pos] = cslot;
         }
         home_count += __popc(inm);

@@ -196,18 +196,16 @@ __global__ void k_scatter_rec(const double *__restrict__ st, int64_t n, int nx, 
   rec[2 * pos + 1] = make_float4((float)(st[4 * n + j] * g), __int_as_float((int32_t)j), 0.f, 0.f);
 }
 
-// records in cell-grouped order -> the FP32 arrays and slots
+// records in cell-grouped order -> entries first.. of the FP32 particle
+// arrays ((xr, yr, ux, uy) float4s, then uz) and slots
 __global__ void k_rec_to_soa(const float4 *__restrict__ rec, int64_t n, float *P, int32_t *slot,
-                             int64_t cap) {
+                             int64_t cap, int64_t first) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const float4 a = rec[2 * i], b = rec[2 * i + 1];
-  P[i] = a.x;
-  P[cap + i] = a.y;
-  P[2 * cap + i] = a.z;
-  P[3 * cap + i] = a.w;
-  P[4 * cap + i] = b.x;
-  slot[i] = __float_as_int(b.y);
+  reinterpret_cast<float4 *>(P)[first + i] = a;
+  P[4 * cap + first + i] = b.x;
+  slot[first + i] = __float_as_int(b.y);
 }
 
 // cell-grouped FP32 -> records in slot order: (x, y) as doubles, wrapped
@@ -220,14 +218,15 @@ __global__ void k_grouped_to_rec(const float *__restrict__ P, const int32_t *__r
   if (cell >= (int64_t)nx * ny) return;
   const int kx = (int)(cell % nx), ky = (int)(cell / nx);
   for (int32_t i = off[cell] + gl; i < off[cell + 1]; i += kCopyLanes) {
-    double x = kx + (double)P[i], y = ky + (double)P[cap + i];
+    const float4 q = reinterpret_cast<const float4 *>(P)[i];
+    double x = kx + (double)q.x, y = ky + (double)q.y;
     if (x < 0.0) x += nx;
     if (x >= nx) x -= nx;
     if (y < 0.0) y += ny;
     if (y >= ny) y -= ny;
     const int64_t s = slot[i];
     reinterpret_cast<double2 *>(rec)[2 * s] = make_double2(x, y);
-    rec[2 * s + 1] = make_float4(P[2 * cap + i], P[3 * cap + i], P[4 * cap + i], 0.f);
+    rec[2 * s + 1] = make_float4(q.z, q.w, P[4 * cap + i], 0.f);
   }
 }
 
@@ -291,10 +290,8 @@ __global__ void k_stage_f32(Src6 src, int64_t count, int64_t first, int nx, int 
   if (ok) agg_atomic_add(cnt, k, om);
   const int64_t j = first + i;
   const double g = ok ? v[5] : 0.0;
-  P[j] = xr;
-  P[cap + j] = yr;
-  P[2 * cap + j] = (float)(v[2] * g);
-  P[3 * cap + j] = (float)(v[3] * g);
+  reinterpret_cast<float4 *>(P)[j] =
+      make_float4(xr, yr, (float)(v[2] * g), (float)(v[3] * g));
   P[4 * cap + j] = (float)(v[4] * g);
   key[j] = k;
 }
@@ -319,7 +316,7 @@ __global__ void k_window_rec(const float *__restrict__ P, const int32_t *__restr
   if (i >= n) return;
   const int64_t q = (int64_t)pos[i] - p0;
   if (q < 0 || q >= len) return;
-  rec[2 * q] = make_float4(P[i], P[cap + i], P[2 * cap + i], P[3 * cap + i]);
+  rec[2 * q] = reinterpret_cast<const float4 *>(P)[i];
   rec[2 * q + 1] = make_float4(P[4 * cap + i], __int_as_float((int32_t)i), 0.f, 0.f);
 }
 
@@ -336,13 +333,14 @@ __global__ void k_grouped_to_rec_range(const float *__restrict__ P,
   for (int32_t i = off[cell] + gl; i < off[cell + 1]; i += kCopyLanes) {
     const int64_t q = (int64_t)slot[i] - s0;
     if (q < 0 || q >= len) continue;
-    double x = kx + (double)P[i], y = ky + (double)P[cap + i];
+    const float4 p = reinterpret_cast<const float4 *>(P)[i];
+    double x = kx + (double)p.x, y = ky + (double)p.y;
     if (x < 0.0) x += nx;
     if (x >= nx) x -= nx;
     if (y < 0.0) y += ny;
     if (y >= ny) y -= ny;
     reinterpret_cast<double2 *>(rec)[2 * q] = make_double2(x, y);
-    rec[2 * q + 1] = make_float4(P[2 * cap + i], P[3 * cap + i], P[4 * cap + i], 0.f);
+    rec[2 * q + 1] = make_float4(p.z, p.w, P[4 * cap + i], 0.f);
   }
 }
 
@@ -474,8 +472,8 @@ int commit_f32(em2g_ctx *c, int isp, int64_t n, void *rec, int64_t rec_cap) {
     for (int64_t p0 = 0; p0 < n; p0 += rec_cap) {
       const int64_t len = std::min(rec_cap, n - p0);
       k_window_rec<<<nb, 256, 0, c->stream>>>(S.p32_alt, S.slot_alt, n, S.cap, p0, len, r);
-      k_rec_to_soa<<<(unsigned)((len + 255) / 256), 256, 0, c->stream>>>(r, len, S.p32 + p0,
-                                                                          S.slot + p0, S.cap);
+      k_rec_to_soa<<<(unsigned)((len + 255) / 256), 256, 0, c->stream>>>(r, len, S.p32, S.slot,
+                                                                          S.cap, p0);
       EM2G_CUDA(cudaGetLastError());
       c->launches += 2;
     }
@@ -561,7 +559,7 @@ int ens_upload_pair(em2g_ens *e, int r, int s, double *staging) {
     k_scatter_rec<<<nb, 256, 0, st>>>(staging, n, R.g.nx, R.g.ny, off + c0, e->cursor + c0,
                                       R.base[s], rec);
     EM2G_CUDA(cudaGetLastError());
-    k_rec_to_soa<<<nb, 256, 0, st>>>(rec, n, P + R.base[s], slot + R.base[s], e->cap);
+    k_rec_to_soa<<<nb, 256, 0, st>>>(rec, n, P, slot, e->cap, R.base[s]);
   }
   EM2G_CUDA(cudaGetLastError());
   return EM2G_OK;
