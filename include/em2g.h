@@ -332,8 +332,8 @@ int em2g_ens_set_graph(em2g_ens *ens, int on);
  * that gives up fails the step with EM2G_ERR_TIMEOUT); 0: one launch per
  * stage.  The results are the same up to the order of FP32 sums. */
 int em2g_ens_set_fused(em2g_ens *ens, int on);
-/* the last fused step's phases: ns[k] = time from the k-th to the (k+1)-th
- * of its marks (the launch's start, then each grid barrier), 0 past the
+/* the last fused step's phases: ns[k] = time between consecutive marks
+ * (the launch's start, then each grid barrier the step passed), 0 past the
  * last; at most 31 values */
 int em2g_ens_get_phase_ns(em2g_ens *ens, int64_t *ns, int n);
 /* the FP32 push variants (as em2g_num_variants of an FP32 context) */

@@ -420,6 +420,14 @@ int em2g_destroy(em2g_ctx *c) {
   cg_free(c);
   sort_free(c);
   for (cudaEvent_t e : c->ev) cudaEventDestroy(e);
+  for (int h = 0; h < 2; ++h) {
+    if (c->half_copied[h]) cudaEventDestroy(c->half_copied[h]);
+    if (c->half_used[h]) cudaEventDestroy(c->half_used[h]);
+  }
+  if (c->copy_stream) {
+    cudaStreamSynchronize(c->copy_stream);
+    cudaStreamDestroy(c->copy_stream);
+  }
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
   return EM2G_OK;
@@ -521,6 +529,22 @@ int em2g_field_device_ptr(em2g_ctx *c, int id, void **dptr) {
 // particles.  Host slices go through the staging buffer, at most
 // staging_cap() bytes, so no buffer grows with the particle count.
 
+// the copy stream and the halves' events, made on first use; the copy
+// stream then waits for everything already enqueued on the context's stream
+// (earlier users of the staging buffer)
+static int copy_setup(em2g_ctx *c) {
+  if (!c->copy_stream) {
+    EM2G_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+    for (int h = 0; h < 2; ++h) {
+      EM2G_CUDA(cudaEventCreateWithFlags(&c->half_copied[h], cudaEventDisableTiming));
+      EM2G_CUDA(cudaEventCreateWithFlags(&c->half_used[h], cudaEventDisableTiming));
+    }
+  }
+  EM2G_CUDA(cudaEventRecord(c->half_used[0], c->stream));
+  EM2G_CUDA(cudaEventRecord(c->half_used[1], c->stream));
+  return EM2G_OK;
+}
+
 static int particles_begin(em2g_ctx *c, int isp, int64_t n) {
   Species &S = c->sp[isp];
   if (n < 0 || n > S.cap) return fail(EM2G_ERR_RANGE, "particle count exceeds np_max");
@@ -561,20 +585,34 @@ static int particles_add(em2g_ctx *c, int isp, int64_t first, int64_t count,
     S.up_added += count;
     return EM2G_OK;
   }
-  // host slices through the staging buffer, 6 doubles per particle
-  const int64_t chunk = staging_cap(c) / 48;
-  int rc = ensure_staging(c, staging_cap(c) / 8);
+  // host slices through the two halves of the staging buffer, 6 doubles per
+  // particle: the copy of one half (copy stream) overlaps the check and
+  // conversion of the other (the context's stream)
+  const int64_t half = staging_cap(c) / 16;  // doubles per half
+  const int64_t chunk = half / 6;
+  int rc = ensure_staging(c, 2 * half);
   if (rc) return rc;
-  for (int64_t a = 0; a < count; a += chunk) {
+  if ((rc = copy_setup(c))) return rc;
+  for (int64_t a = 0, i = 0; a < count; a += chunk, ++i) {
+    const int h = (int)(i & 1);
     const int64_t m = std::min(chunk, count - a);
+    EM2G_CUDA(cudaStreamWaitEvent(c->copy_stream, c->half_used[h], 0));
     const double *st[6];
     for (int k = 0; k < 6; ++k) {
-      double *d = c->staging + k * m;
+      double *d = c->staging + h * half + k * m;
       EM2G_CUDA(cudaMemcpyAsync(d, src[k] + a, sizeof(double) * m, cudaMemcpyHostToDevice,
-                                c->stream));
+                                c->copy_stream));
       st[k] = d;
     }
-    if ((rc = stage_f32(c, isp, first + a, m, st, bad))) return rc;
+    EM2G_CUDA(cudaEventRecord(c->half_copied[h], c->copy_stream));
+    EM2G_CUDA(cudaStreamWaitEvent(c->stream, c->half_copied[h], 0));
+    if ((rc = stage_f32(c, isp, first + a, m, st, bad))) {
+      // later users of the staging buffer (on the context's stream) wait for
+      // the copy this slice started
+      cudaStreamSynchronize(c->copy_stream);
+      return rc;
+    }
+    EM2G_CUDA(cudaEventRecord(c->half_used[h], c->stream));
   }
   S.up_added += count;
   return EM2G_OK;
@@ -649,21 +687,40 @@ static int particles_get(em2g_ctx *c, int isp, int64_t first, int64_t count,
   }
   // FP32: 32-byte records, then FP64 values (into the caller's device
   // arrays directly, or into the staging buffer and across to the host)
-  const int64_t chunk = staging_cap(c) / (on_device ? 32 : 80);
   int rc = ensure_staging(c, staging_cap(c) / 8);
   if (rc) return rc;
-  for (int64_t a = 0; a < count; a += chunk) {
-    const int64_t m = std::min(chunk, count - a);
-    double *d[6];
-    void *rec = c->staging;
-    for (int k = 0; k < 6; ++k)
-      d[k] = on_device ? dst[k] + a : c->staging + 4 * m + k * m;
-    if ((rc = get_range_f32(c, isp, first + a, m, d, rec))) return rc;
-    if (!on_device) {
-      for (int k = 0; k < 6; ++k)
-        EM2G_CUDA(cudaMemcpyAsync(dst[k] + a, d[k], sizeof(double) * m, kind, c->stream));
+  if (on_device) {
+    const int64_t chunk = staging_cap(c) / 32;  // records only
+    for (int64_t a = 0; a < count; a += chunk) {
+      const int64_t m = std::min(chunk, count - a);
+      double *d[6];
+      for (int k = 0; k < 6; ++k) d[k] = dst[k] + a;
+      if ((rc = get_range_f32(c, isp, first + a, m, d, c->staging))) return rc;
     }
+    EM2G_CUDA(cudaStreamSynchronize(c->stream));
+    return EM2G_OK;
   }
+  // to the host through the two halves of the staging buffer: the copy of
+  // one half (copy stream) overlaps the gather into the other
+  const int64_t half = staging_cap(c) / 16;  // doubles per half
+  const int64_t chunk = half / 10;          // 32 B of record, 48 B of values each
+  if ((rc = copy_setup(c))) return rc;
+  for (int64_t a = 0, i = 0; a < count; a += chunk, ++i) {
+    const int h = (int)(i & 1);
+    const int64_t m = std::min(chunk, count - a);
+    double *base = c->staging + h * half;
+    double *d[6];
+    for (int k = 0; k < 6; ++k) d[k] = base + 4 * m + k * m;
+    // this half's previous contents have crossed to the host
+    EM2G_CUDA(cudaStreamWaitEvent(c->stream, c->half_copied[h], 0));
+    if ((rc = get_range_f32(c, isp, first + a, m, d, base))) return rc;
+    EM2G_CUDA(cudaEventRecord(c->half_used[h], c->stream));
+    EM2G_CUDA(cudaStreamWaitEvent(c->copy_stream, c->half_used[h], 0));
+    for (int k = 0; k < 6; ++k)
+      EM2G_CUDA(cudaMemcpyAsync(dst[k] + a, d[k], sizeof(double) * m, kind, c->copy_stream));
+    EM2G_CUDA(cudaEventRecord(c->half_copied[h], c->copy_stream));
+  }
+  EM2G_CUDA(cudaStreamSynchronize(c->copy_stream));
   EM2G_CUDA(cudaStreamSynchronize(c->stream));
   return EM2G_OK;
 }

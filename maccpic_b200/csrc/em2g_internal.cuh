@@ -121,6 +121,11 @@ struct em2g_ctx {
   double *staging = nullptr;
   int64_t staging_n = 0;
   unsigned long long *up_bad = nullptr;  // per species: out of range, non-finite
+  // host particle copies overlap their PCIe transfers with the device work on
+  // the other half of the staging buffer: a second stream for the copies and,
+  // per half, events marking its copy done and its device work done
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t half_copied[2] = {nullptr, nullptr}, half_used[2] = {nullptr, nullptr};
   int64_t ncell = 0;
   int timing = 0;
   std::vector<cudaEvent_t> ev;  // start/stop pairs of the pending push launches

@@ -213,19 +213,23 @@ __global__ void __launch_bounds__(TCX * G, MINB)
   __shared__ double sh[33];
   const EnsStepTab &t = *tp;
   const EnsGrid32 &eg = t.grid;
-  const int nr = eg.nruns;
-  const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int64_t gstride = (int64_t)gridDim.x * blockDim.x;
-  // block 0's thread 0 notes the time at the start and after each barrier:
-  // the phases' durations, for the design notes (em2g_ens_get_phase_ns)
-  int nmark = 0;
-  if (gtid == 0) t.marks[nmark] = global_ns();
-  ++nmark;
-#define EM2G_SYNC_ALL()                                                 \
+  // Nothing computed here stays live across the push phase, whose register
+  // budget is the push's own: the run count, the global thread index and
+  // stride are re-read or recomputed from the builtins where used.
+#define nr (eg.nruns)
+#define gtid ((int64_t)blockIdx.x * blockDim.x + threadIdx.x)
+#define gstride ((int64_t)gridDim.x * blockDim.x)
+  // block 0's thread 0 notes the time at the start and after each barrier
+  // (mark k after the k-th barrier): the phases' durations, for the design
+  // notes (em2g_ens_get_phase_ns)
+  if (gtid == 0) {
+    for (int k = 1; k < kMaxMarks; ++k) t.marks[k] = 0;  // a step in place skips two
+    t.marks[0] = global_ns();
+  }
+#define EM2G_SYNC_ALL(k)                                                \
   do {                                                                  \
     if (!grid::grid_barrier(t.bar, gridDim.x, t.status)) return;        \
-    if (gtid == 0 && nmark < kMaxMarks) t.marks[nmark] = global_ns();   \
-    ++nmark;                                                            \
+    if (gtid == 0) t.marks[k] = global_ns();                            \
   } while (0)
 
   // ---- (E, B) pairs of every species, counters to zero, the first pass
@@ -290,7 +294,7 @@ __global__ void __launch_bounds__(TCX * G, MINB)
       }
     }
   }
-  EM2G_SYNC_ALL();
+  EM2G_SYNC_ALL(1);
   if (!INPLACE) {
     // the chunk totals scanned by block 0, then added to every chunk
     const EnsScanArgs &sc = t.scan;
@@ -324,13 +328,13 @@ __global__ void __launch_bounds__(TCX * G, MINB)
       }
       if (threadIdx.x == 0) sc.out[sc.n] = carry;
     }
-    EM2G_SYNC_ALL();
+    EM2G_SYNC_ALL(2);
     for (int c = blockIdx.x; c < sc.nchunks; c += gridDim.x) {
       const int32_t add = ld(sc.sums + c);
       const int64_t lo = (int64_t)c * kScanChunk, hi = min(lo + kScanChunk, sc.n);
       for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) sc.out[i] = ld(sc.out + i) + add;
     }
-    EM2G_SYNC_ALL();
+    EM2G_SYNC_ALL(3);
   }
 
   // ---- the push of every pair, row segments claimed from a counter
@@ -352,7 +356,7 @@ __global__ void __launch_bounds__(TCX * G, MINB)
                                         win, ws);
     }
   }
-  EM2G_SYNC_ALL();
+  EM2G_SYNC_ALL(4);
 
   // ---- kinetic energies, the step counter, the fold in x, then in y
   {
@@ -371,7 +375,7 @@ __global__ void __launch_bounds__(TCX * G, MINB)
       f_fold_x(eg.run[r].g, eg.run[r].fld, (b - eg.foldx0[r]) * 128 + (rem % 128), k);
     }
   }
-  EM2G_SYNC_ALL();
+  EM2G_SYNC_ALL(5);
   {
     const int64_t nfy = (int64_t)eg.foldy0[nr] * 128;
     for (int64_t v = gtid; v < nfy * 7; v += gstride) {
@@ -380,7 +384,7 @@ __global__ void __launch_bounds__(TCX * G, MINB)
       f_fold_y(eg.run[r].g, eg.run[r].fld, (b - eg.foldy0[r]) * 128 + (rem % 128), k);
     }
   }
-  EM2G_SYNC_ALL();
+  EM2G_SYNC_ALL(6);
   const int it = ld(eg.it);
   // ---- the optional current filter after the fold (no em2 counterpart)
   if (t.any_smooth_current) {
@@ -391,7 +395,7 @@ __global__ void __launch_bounds__(TCX * G, MINB)
         f_smooth_b(R.g, R.fld + arr * R.g.w, R.tmp + y * R.g.w, ix, iy);
       }
     });
-    EM2G_SYNC_ALL();
+    EM2G_SYNC_ALL(7);
     for_tiles(eg, [&](const EnsRunDev &R, int ix, int iy) {
       if (!R.smooth_current) return;
       for (int y = 0; y < 3; ++y) {
@@ -399,60 +403,60 @@ __global__ void __launch_bounds__(TCX * G, MINB)
         f_smooth_c(R.g, R.tmp + y * R.g.w, R.fld + arr * R.g.w, ix, iy);
       }
     });
-    EM2G_SYNC_ALL();
+    EM2G_SYNC_ALL(8);
   }
   // ---- Yee: B/2, E, B/2 (pic/fields.f90:184-247)
   for_tiles(eg, [&](const EnsRunDev &R, int ix, int iy) {
     f_b_half(R.g, R.fld, R.ctxh, R.ctyh, ix, iy);
   });
-  EM2G_SYNC_ALL();
+  EM2G_SYNC_ALL(9);
   for_tiles(eg, [&](const EnsRunDev &R, int ix, int iy) {
     f_e_full(R.g, R.fld, R.ctx, R.cty, R.tem, ix, iy);
   });
-  EM2G_SYNC_ALL();
+  EM2G_SYNC_ALL(10);
   for_tiles(eg, [&](const EnsRunDev &R, int ix, int iy) {
     f_b_half(R.g, R.fld, R.ctxh, R.ctyh, ix, iy);
   });
-  EM2G_SYNC_ALL();
+  EM2G_SYNC_ALL(11);
   // ---- smooth2 of rho every step, of E and B every isav steps
   // (pic/fields.f90:252-260)
   for_tiles(eg, [&](const EnsRunDev &R, int ix, int iy) {
     f_smooth_b(R.g, R.fld + EM2G_RHO * R.g.w, R.tmp, ix, iy);
   });
-  EM2G_SYNC_ALL();
+  EM2G_SYNC_ALL(12);
   for_tiles(eg, [&](const EnsRunDev &R, int ix, int iy) {
     f_smooth_c(R.g, R.tmp, R.fld + EM2G_RHO * R.g.w, ix, iy);
   });
-  EM2G_SYNC_ALL();
+  EM2G_SYNC_ALL(13);
   for_tiles(eg, [&](const EnsRunDev &R, int ix, int iy) {
     if (it % R.isav != 0) return;
     for (int y = 0; y < 6; ++y)
       f_smooth_b(R.g, R.fld + (EM2G_EX + y) * R.g.w, R.tmp + y * R.g.w, ix, iy);
   });
-  EM2G_SYNC_ALL();
+  EM2G_SYNC_ALL(14);
   for_tiles(eg, [&](const EnsRunDev &R, int ix, int iy) {
     if (it % R.isav != 0) return;
     for (int y = 0; y < 6; ++y)
       f_smooth_c(R.g, R.tmp + y * R.g.w, R.fld + (EM2G_EX + y) * R.g.w, ix, iy);
   });
-  EM2G_SYNC_ALL();
+  EM2G_SYNC_ALL(15);
   // ---- Poisson: right-hand side, every run's CG on its own blocks, the
   // correction (pic/fields.f90:370-651)
   for_tiles(eg, [&](const EnsRunDev &R, int ix, int iy) {
     const int64_t N = (int64_t)R.g.nx * R.g.ny;
     f_rhs(R.g, R.fld, R.dx, R.dy, R.cgu + N, R.cgu + 2 * N, ix, iy);
   });
-  EM2G_SYNC_ALL();
+  EM2G_SYNC_ALL(16);
   if ((int)blockIdx.x < t.cg.blk0[nr]) {
     const int r = find_run(t.cg.blk0, nr, blockIdx.x);
     grid::cg_body(t.cg.a[r], (int)blockIdx.x - t.cg.blk0[r],
                   (unsigned)(t.cg.blk0[r + 1] - t.cg.blk0[r]), sh);
   }
-  EM2G_SYNC_ALL();
+  EM2G_SYNC_ALL(17);
   for_tiles(eg, [&](const EnsRunDev &R, int ix, int iy) {
     f_correct(R.g, R.fld, R.cgu, R.dx, R.dy, ix, iy);
   });
-  EM2G_SYNC_ALL();
+  EM2G_SYNC_ALL(18);
   // ---- energies on isav steps (pic/fields.f90:267-347, whole grid), rho
   // and J back to zero (pic/fields.f90:353-365)
   for (int vb = blockIdx.x; vb < nr * 6; vb += gridDim.x) {
@@ -482,6 +486,9 @@ __global__ void __launch_bounds__(TCX * G, MINB)
     }
   }
 #undef EM2G_SYNC_ALL
+#undef nr
+#undef gtid
+#undef gstride
 }
 
 struct FusedVariant {
@@ -638,8 +645,15 @@ int ens_fused_phase_ns(em2g_ens *e, int64_t *out, int n) {
   unsigned long long h[kMaxMarks];
   EM2G_CUDA(cudaMemcpyAsync(h, e->fused_marks, sizeof(h), cudaMemcpyDeviceToHost, e->stream));
   EM2G_CUDA(cudaStreamSynchronize(e->stream));
-  for (int k = 0; k < n; ++k)
-    out[k] = (k + 1 < kMaxMarks && h[k + 1] >= h[k] && h[k] != 0) ? (int64_t)(h[k + 1] - h[k]) : 0;
+  // marks left at zero belong to phases the step skipped
+  int m = 0;
+  unsigned long long last = h[0];
+  for (int k = 1; k < kMaxMarks && m < n; ++k) {
+    if (h[k] == 0) continue;
+    out[m++] = h[k] >= last ? (int64_t)(h[k] - last) : 0;
+    last = h[k];
+  }
+  for (; m < n; ++m) out[m] = 0;
   return EM2G_OK;
 }
 
