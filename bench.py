@@ -618,11 +618,13 @@ def run_adjoint(args, local):
         torch.cuda.synchronize()
         return time.perf_counter() - t, out
 
-    # one workspace (context, per-step E and B, checkpoints) for every
-    # gradient below, as a caller computing many gradients keeps it
+    # one workspace (context, per-step E and B slots, checkpoints) for every
+    # gradient below, as a caller computing many gradients keeps it; by
+    # default it holds as many steps' E and B as half the free memory takes
     t_setup, ws = timed(lambda: A.CudaAdjoint(k, *A.initial_state_torch(cfg, theta, d), T, K,
                                               cfg.isav))
     try:
+        slots = ws.field_slots()
         ws.g.step(2)
         ws.load(*A.initial_state_torch(cfg, theta, d))
         t_fwd, _ = timed(lambda: ws.g.step(T))
@@ -634,14 +636,18 @@ def run_adjoint(args, local):
         Bf = ws.final_B()
         t_rev, _ = timed(lambda: ws.backward([torch.zeros_like(b) for b in Bf],
                                              [torch.ones_like(b) * 1e-3 for b in Bf]))
-        # the same gradient with E and B of every step kept instead of
-        # recomputed (more memory, no second forward pass)
-        from maccpic_b200._lib import check
-        check(ws._L.em2g_adj_keep_all_fields(ws._h, 1))
+        # the same gradient in the least memory: K slots, every step before
+        # the last K recomputed from its checkpoint in the reverse sweep
+        ws.set_field_slots(K)
         A.theta_gradient_cuda(cfg, theta, min(T, 4), checkpoint=K, draws=d, workspace=ws)
-        t_grad_keep, (F2, g2) = timed(lambda: A.theta_gradient_cuda(
+        t_grad_min, (F2, g2) = timed(lambda: A.theta_gradient_cuda(
             cfg, theta, T, checkpoint=K, draws=d, workspace=ws))
-        check(ws._L.em2g_adj_keep_all_fields(ws._h, 0))
+        ws.load(*A.initial_state_torch(cfg, theta, d))
+        ws.forward(T)
+        Bf = ws.final_B()
+        t_rev_min, _ = timed(lambda: ws.backward([torch.zeros_like(b) for b in Bf],
+                                                 [torch.ones_like(b) * 1e-3 for b in Bf]))
+        ws.set_field_slots(slots)
         # the gradient against central differences of the same forward
         # (h = 1e-3, common random numbers) at growing horizons
         fd = {}
@@ -652,23 +658,28 @@ def run_adjoint(args, local):
     torch.cuda.empty_cache()
     n = 2 * cfg.nx * cfg.ny * cfg.ppc
     w = (cfg.nx + 3) * (cfg.ny + 3)
-    mem = 8 * (-(-T // K) * (13 * w + 6 * n) + K * 6 * cfg.nx * cfg.ny)
+    ck_bytes = 8 * -(-T // K) * (13 * w + 6 * n)
+    slot_bytes = 8 * 6 * cfg.nx * cfg.ny
     agree = [t for t, r in fd.items() if max(r["rel_error"]) <= 0.01]
     return {"workload": "harris_512x256_ppc32", "particles": n,
             "steps": T, "checkpoint": K, "flux": F, "dflux_dtheta": [float(x) for x in g],
+            "field_slots": slots, "recomputed_steps": max(0, T - slots),
             "forward_ms_per_step": t_fwd * 1e3 / T,
             "recording_forward_ms_per_step": t_rec * 1e3 / T,
             "reverse_ms_per_step": t_rev * 1e3 / T,
             "gradient_ms": t_grad * 1e3,
             "gradient_over_forward": t_grad / t_fwd,
             "workspace_setup_ms": t_setup * 1e3,
-            "workspace_bytes": mem,
-            "keep_all_fields": {"gradient_over_forward": t_grad_keep / t_fwd,
-                                "gradient_ms": t_grad_keep * 1e3,
-                                "workspace_bytes": mem + 8 * (T - K) * 6 * cfg.nx * cfg.ny,
-                                "dflux_dtheta": [float(x) for x in g2]},
-            "memory": "checkpoints every K steps (fields + particles) and K field slots; each "
-                      "segment recomputed from its checkpoint in the reverse sweep",
+            "workspace_bytes": ck_bytes + slots * slot_bytes,
+            "least_memory": {"field_slots": K, "recomputed_steps": max(0, T - K),
+                             "gradient_over_forward": t_grad_min / t_fwd,
+                             "gradient_ms": t_grad_min * 1e3,
+                             "reverse_ms_per_step": t_rev_min * 1e3 / T,
+                             "workspace_bytes": ck_bytes + K * slot_bytes,
+                             "dflux_dtheta": [float(x) for x in g2]},
+            "memory": "checkpoints every K steps (fields + particles); E and B of the last "
+                      "field_slots steps kept by the forward sweep, every step before them "
+                      "recomputed a segment at a time from its checkpoint in the reverse sweep",
             "fd_h": 1e-3,
             "fd_rel_error": max(fd[T]["rel_error"]),
             "fd": {str(t): r for t, r in fd.items()},

@@ -278,9 +278,13 @@ int em2g_reset_counters(em2g_ctx *ctx);
  * segment's start.  Device memory: max_steps/checkpoint checkpoints of
  * (13 (nx+3)(ny+3) + 6 x particles) doubles, plus `checkpoint` slots of
  * 6 nx ny doubles.  At its end the context is back at the final state.
- * em2g_adj_keep_all_fields(adj, 1) keeps E and B of every step in the
- * forward sweep instead (max_steps slots) and skips the recomputation;
- * 0 returns to the default.  Call it before em2g_adj_forward.  Field adjoints use the periodic (ny, nx) layout
+ * em2g_adj_field_slots(adj, n), checkpoint <= n <= max_steps, sets the
+ * number of slots: the forward sweep fills them with E and B of its last
+ * n steps, which the reverse sweep uses as they are, and only the steps
+ * before them are recomputed (in the slots already gone through); with n
+ * >= the steps run nothing is.  em2g_adj_keep_all_fields(adj, 1) is n =
+ * max_steps, 0 is n = checkpoint (the default).  Call either before
+ * em2g_adj_forward.  Field adjoints use the periodic (ny, nx) layout
  * (element [j][i] <-> em2 index (i+1, j+1)); particle adjoints are in slot
  * order. */
 typedef struct em2g_adj em2g_adj;
@@ -288,6 +292,8 @@ int em2g_adj_create(em2g_ctx *ctx, int max_steps, int checkpoint, em2g_adj **out
 int em2g_adj_destroy(em2g_adj *adj);
 int em2g_adj_forward(em2g_adj *adj, int nsteps);
 int em2g_adj_keep_all_fields(em2g_adj *adj, int on);
+int em2g_adj_field_slots(em2g_adj *adj, int nslots);
+int em2g_adj_get_field_slots(em2g_adj *adj, int *nslots);
 /* adjoint of the final E, B: 6 arrays of ny*nx doubles (ex ey ez bx by bz),
  * device memory; particles' final adjoints are zero */
 int em2g_adj_seed_fields_device(em2g_adj *adj, const double *dev6);

@@ -34,6 +34,7 @@ EXPORTS = [
     "em2g_smooth2_static", "em2g_diagnostics", "em2g_num_variants", "em2g_set_variant",
     "em2g_get_variant", "em2g_set_sort_interval",
     "em2g_adj_create", "em2g_adj_destroy", "em2g_adj_forward", "em2g_adj_keep_all_fields",
+    "em2g_adj_field_slots", "em2g_adj_get_field_slots",
     "em2g_adj_seed_fields_device",
     "em2g_adj_backward", "em2g_adj_get_fields_device", "em2g_adj_get_particles_device",
     "em2g_adj_get_initial_particles_device",
@@ -131,6 +132,8 @@ def lib() -> C.CDLL:
         "em2g_adj_destroy": (C.c_int, [ctx]),
         "em2g_adj_forward": (C.c_int, [ctx, C.c_int]),
         "em2g_adj_keep_all_fields": (C.c_int, [ctx, C.c_int]),
+        "em2g_adj_field_slots": (C.c_int, [ctx, C.c_int]),
+        "em2g_adj_get_field_slots": (C.c_int, [ctx, C.POINTER(C.c_int)]),
         "em2g_adj_seed_fields_device": (C.c_int, [ctx, vp]),
         "em2g_adj_backward": (C.c_int, [ctx]),
         "em2g_adj_get_fields_device": (C.c_int, [ctx, vp]),

@@ -698,7 +698,8 @@ class CudaAdjoint:
     particles) serves many gradients of runs of the same shape."""
 
     def __init__(self, k: StepConst, E, B, parts, max_steps: int, checkpoint: int,
-                 isav: int, smooth_current: int = 0, it0: int = 0, keep_all_fields=False):
+                 isav: int, smooth_current: int = 0, it0: int = 0, keep_all_fields=False,
+                 field_slots=None, memory_fraction: float = 0.5):
         import ctypes as C
         from . import _lib
         from ._lib import check
@@ -722,10 +723,42 @@ class CudaAdjoint:
         h = C.c_void_p()
         check(self._L.em2g_adj_create(self.g._h, self.max_steps, self.checkpoint, C.byref(h)))
         self._h = h
-        # default: checkpoints every K steps and recomputation of each
-        # segment in the reverse sweep; keep_all_fields: E, B of every step
-        # kept instead (more memory, no second forward pass)
-        check(self._L.em2g_adj_keep_all_fields(self._h, int(bool(keep_all_fields))))
+        # checkpoints every K steps; E and B of the last `field_slots` steps
+        # kept by the forward sweep and the steps before them recomputed a
+        # segment at a time in the reverse sweep.  field_slots=None takes as
+        # many steps as fit in `memory_fraction` of the device memory still
+        # free (at least K, at most max_steps); keep_all_fields takes one
+        # per step (no recomputation)
+        if keep_all_fields:
+            field_slots = self.max_steps
+        elif field_slots is None:
+            field_slots = self.slots_that_fit(memory_fraction)
+        self.set_field_slots(field_slots)
+
+    def slot_bytes(self) -> int:
+        """Device bytes of one step's E and B slot."""
+        return 6 * 8 * self.k.nx * self.k.ny
+
+    def slots_that_fit(self, memory_fraction: float = 0.5) -> int:
+        """Field slots that `memory_fraction` of the free device memory holds
+        beside the ones allocated now, clamped to checkpoint .. max_steps."""
+        free, _ = torch.cuda.mem_get_info(self.dev)
+        have = self.field_slots()
+        n = have + int(free * memory_fraction) // self.slot_bytes()
+        return max(min(self.checkpoint, self.max_steps), min(self.max_steps, n))
+
+    def set_field_slots(self, n: int):
+        """Steps whose E and B the forward sweep keeps (checkpoint ..
+        max_steps); the reverse sweep recomputes the steps before them."""
+        from ._lib import check
+        check(self._L.em2g_adj_field_slots(self._h, int(n)))
+
+    def field_slots(self) -> int:
+        import ctypes as C
+        from ._lib import check
+        n = C.c_int()
+        check(self._L.em2g_adj_get_field_slots(self._h, C.byref(n)))
+        return n.value
 
     def load(self, E, B, parts, it0: int = 0):
         """Replace the context's state (same grid and particle counts)."""

@@ -20,9 +20,11 @@
 // the segment's checkpoint into the context, recomputes the segment's K
 // steps keeping E and B before each (K slots of 6 periodic arrays), and
 // sweeps back through them.  So the memory is O(T/K) checkpoints plus K
-// field slots, at the price of a second forward pass.  (A caller with
-// memory to spare can keep E and B of every step instead and skip the
-// recomputation: em2g_adj_keep_all_fields.)  The particles need no per-step
+// field slots, at the price of a second forward pass.  With more slots
+// (em2g_adj_field_slots; em2g_adj_keep_all_fields for one per step) the
+// forward sweep fills them with E and B of its last steps, which the
+// reverse sweep then uses without recomputing; only the steps before them
+// are recomputed, a segment at a time, in the slots already gone through.  The particles need no per-step
 // store in either mode: the push is invertible, so one kernel per step
 // rebuilds the previous particle state from the current one (x -= v dt/dx
 // with u's velocity, then the Boris rotation about the same t by the
@@ -55,9 +57,9 @@ struct em2g_adj {
   double ae[EM2G_MAX_SPECIES] = {}, qd[EM2G_MAX_SPECIES] = {};
   int64_t n[EM2G_MAX_SPECIES] = {}, pb[EM2G_MAX_SPECIES] = {};  // particles, first index
   int64_t ptot = 0;
-  double *hist = nullptr;   // nhist x 6 x N: E, B before each step of a segment
-  int nhist = 0;            // K (recomputation) or max_steps (every step kept)
-  bool keep_all = false;    // E, B of every step kept by the forward sweep
+  double *hist = nullptr;   // nhist x 6 x N: E, B before each step
+  int nhist = 0;            // K .. max_steps slots
+  int keep_from = 0;        // the forward sweep kept E, B of steps keep_from..steps-1
   double *ckpt = nullptr;   // nck x 6 x ptot (per species 6 x n, slot order)
   double *ckfld = nullptr;  // nck x 13 x w, the context's field block
   int nck = 0;
@@ -942,11 +944,13 @@ int em2g_adj_forward(em2g_adj *a, int nsteps) {
   a->steps = 0;
   a->seeded = a->swept = false;
   a->it0 = c->it;
+  // the last nhist steps' E and B go into the slots as the sweep passes
+  a->keep_from = nsteps > a->nhist ? nsteps - a->nhist : 0;
   for (int k = 0; k < nsteps; ++k) {
     cudaStream_t st = c->stream;
-    if (a->keep_all) {
-      k_adj_record_fields<<<blocks_for(6 * a->N), 256, 0, st>>>(c->fld, a->nx, a->ny, c->g.w,
-                                                               a->hist + 6 * a->N * k);
+    if (k >= a->keep_from) {
+      k_adj_record_fields<<<blocks_for(6 * a->N), 256, 0, st>>>(
+          c->fld, a->nx, a->ny, c->g.w, a->hist + 6 * a->N * (k - a->keep_from));
       EM2G_CUDA(cudaGetLastError());
     }
     if (k % a->K == 0 && (rc = record_checkpoint(a, k / a->K, st))) return rc;
@@ -987,10 +991,12 @@ int em2g_adj_backward(em2g_adj *a) {
   EM2G_CUDA(cudaGetLastError());
   if ((rc = regroup(a, st))) return rc;
   int since = 0;
-  int seg0 = a->steps;  // first step of the segment whose E, B are in hist
+  const int keep_from = a->keep_from;
+  int seg0 = keep_from;  // first step of the recomputed segment whose E, B are in hist
   for (int k = a->steps - 1; k >= 0; --k) {
-    if (!a->keep_all && k < seg0) {
-      // recompute the segment of step k from its checkpoint
+    if (k < seg0) {
+      // recompute the segment of step k from its checkpoint, into the
+      // slots from 0 (the kept steps after it are done with)
       seg0 = (k / a->K) * a->K;
       if ((rc = reset_to_checkpoint(a, k / a->K, st))) return rc;
       if ((rc = record_segment(a, seg0, k + 1, st))) return rc;
@@ -1000,7 +1006,7 @@ int em2g_adj_backward(em2g_adj *a) {
       since = 0;
     }
     if ((rc = fields_T(a, a->it0 + k + 1, st))) return rc;
-    const double *eb = a->hist + 6 * a->N * (a->keep_all ? k : k - seg0);
+    const double *eb = a->hist + 6 * a->N * (k >= keep_from ? k - keep_from : k - seg0);
     for (int s = 0; s < a->nsp; ++s) {
       double2 *sc = a->scaled + 3 * a->N * s;
       k_adj_prescale<<<blocks_for(a->N), 256, 0, st>>>(eb, a->N, a->ae[s], sc);
@@ -1039,19 +1045,22 @@ int em2g_adj_backward(em2g_adj *a) {
     EM2G_CUDA(cudaGetLastError());
     ++since;
   }
-  // the recomputation moved the context: back to where the forward sweep
+  // a recomputation moved the context: back to where the forward sweep
   // left it
-  if (!a->keep_all && (rc = reset_context(a, a->finfld, a->fin, a->it0 + a->steps, st)))
+  if (keep_from > 0 && (rc = reset_context(a, a->finfld, a->fin, a->it0 + a->steps, st)))
     return rc;
   EM2G_CUDA(cudaStreamSynchronize(st));
   a->swept = true;
   return EM2G_OK;
 }
 
-int em2g_adj_keep_all_fields(em2g_adj *a, int on) {
+int em2g_adj_field_slots(em2g_adj *a, int nslots) {
   int rc = check_adj(a);
   if (rc) return rc;
-  const int n = on ? a->max_steps : std::min(a->K, a->max_steps);
+  const int lo = std::min(a->K, a->max_steps);
+  if (nslots < lo || nslots > a->max_steps)
+    return fail(EM2G_ERR_RANGE, "field slots outside checkpoint .. max_steps");
+  const int n = nslots;
   if (n != a->nhist) {
     EM2G_CUDA(cudaStreamSynchronize(a->ctx->stream));
     cudaFree(a->hist);
@@ -1060,9 +1069,22 @@ int em2g_adj_keep_all_fields(em2g_adj *a, int on) {
     EM2G_CUDA(cudaMalloc((void **)&a->hist, sizeof(double) * 6 * a->N * n));
     a->nhist = n;
   }
-  a->keep_all = on != 0;
   a->steps = 0;
   a->seeded = a->swept = false;
+  return EM2G_OK;
+}
+
+int em2g_adj_keep_all_fields(em2g_adj *a, int on) {
+  int rc = check_adj(a);
+  if (rc) return rc;
+  return em2g_adj_field_slots(a, on ? a->max_steps : std::min(a->K, a->max_steps));
+}
+
+int em2g_adj_get_field_slots(em2g_adj *a, int *nslots) {
+  int rc = check_adj(a);
+  if (rc) return rc;
+  if (!nslots) return fail(EM2G_ERR_INVALID, "null pointer");
+  *nslots = a->nhist;
   return EM2G_OK;
 }
 

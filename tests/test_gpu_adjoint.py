@@ -130,18 +130,22 @@ def test_reused_workspace_gives_the_same_gradient(gpu):
 
 
 def test_recomputed_segments_match_kept_fields(gpu):
-    """The reverse sweep's default -- checkpoints every K steps, each
-    segment's E and B recomputed from its checkpoint -- gives the gradient
-    that keeping E and B of every step gives, and leaves the context at the
-    final state the forward sweep reached."""
+    """Checkpoints every K steps with E and B of the last n steps kept and
+    the steps before them recomputed from their checkpoints give the
+    gradient that keeping E and B of every step gives, for n = K (the least
+    memory), an n that splits a segment, and every step; each leaves the
+    context at the final state the forward sweep reached."""
     cfg = _cfg()
     d = A.make_draws(cfg, device="cuda")
     k = A.step_const(cfg)
     steps, K = 12, 5                      # segments of 5, 5 and 2 steps
     E0, B0, P0 = A.initial_state_torch(cfg, THETA, d)
     grads = []
-    for keep in (False, True):
-        with A.CudaAdjoint(k, E0, B0, P0, steps, K, cfg.isav, keep_all_fields=keep) as adj:
+    # 12 slots: nothing recomputed; 8: steps 0-3 (part of the first segment);
+    # 5: steps 0-6 (a whole segment and part of the next)
+    for slots in (steps, 8, K):
+        with A.CudaAdjoint(k, E0, B0, P0, steps, K, cfg.isav, field_slots=slots) as adj:
+            assert adj.field_slots() == slots
             adj.forward(steps)
             Ef, Bf = adj.final_EB()
             seed = [torch.ones_like(b) * 1e-3 for b in Bf]
@@ -151,8 +155,30 @@ def test_recomputed_segments_match_kept_fields(gpu):
                 assert torch.equal(a, b)
             assert adj.g.it == steps
             grads.append([t.clone() for t in list(lE) + list(lB) + [x for p in lP for x in p]])
-    for a, b in zip(*grads):
-        assert rel(a, b) < 1e-9
+    for other in grads[1:]:
+        for a, b in zip(grads[0], other):
+            assert rel(a, b) < 1e-9
+
+
+def test_field_slots_bounds_and_default(gpu):
+    """Slots are bounded by the checkpoint interval and max_steps; the
+    default holds every step when they fit, and keep_all_fields is
+    max_steps."""
+    from maccpic_b200._lib import Em2gError
+    cfg = _cfg()
+    d = A.make_draws(cfg, device="cuda")
+    k = A.step_const(cfg)
+    E0, B0, P0 = A.initial_state_torch(cfg, THETA, d)
+    with A.CudaAdjoint(k, E0, B0, P0, 12, 5, cfg.isav) as adj:
+        assert adj.field_slots() == 12          # a few MB: every step fits
+        for bad in (4, 13):
+            with pytest.raises(Em2gError):
+                adj.set_field_slots(bad)
+        adj.set_field_slots(5)
+        assert adj.field_slots() == 5
+        assert adj.slots_that_fit(0.0) == 5
+    with A.CudaAdjoint(k, E0, B0, P0, 12, 5, cfg.isav, keep_all_fields=True) as adj:
+        assert adj.field_slots() == 12
 
 
 def test_autograd_function_reaches_theta(gpu):
