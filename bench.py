@@ -792,7 +792,7 @@ def run_e2e(args, cfg, rp, fields, parts_host, variant=0):
     return {"value": n_total * args.steps / el, "unit": METRIC,
             "h2d_bytes_per_step": state / args.steps,
             "d2h_bytes_per_step": (state * downloads + small * args.steps) / args.steps,
-            "downloads": downloads, "isav": rp.isav,
+            "downloads": downloads, "isav": rp.isav, "n_gpus": 1,
             "path": "em2g_set_fields/em2g_set_particles (pinned host, FP64 em2 layout) once, K x "
                     "(em2g_move_curnt, em2g_fields), em2g_get_fields/em2g_get_particles every "
                     "isav steps and at the end"}
