@@ -15,8 +15,8 @@
 // Phases read data that other blocks wrote in earlier phases of the same
 // launch, so those reads go through L2 (ld.global.cg): a line an SM cached
 // in L1 earlier in the launch may since have been rewritten by another SM.
-// The stencil arithmetic is that of grid_kernels.cuh, expression for
-// expression, with those loads; the push is push_f32_body.cuh's, reading
+// The stencils are grid_kernels.cuh's own, with its L2 load policy; the
+// push is push_f32_body.cuh's, reading
 // only data written by earlier launches or, for the (E, B) pairs, written in
 // the first phase before any read of them.  The block shape is the push
 // variant's (TCX*G threads); a 32x8 stencil tile takes 256/(TCX*G) passes.
@@ -69,121 +69,35 @@ __device__ __forceinline__ unsigned long long global_ns() {
   return t;
 }
 
-// ---- the per-cell stages, with loads through L2 --------------------------
+// ---- the per-cell stages: grid_kernels.cuh's, reading through L2 ---------
 
 __device__ __forceinline__ void f_fold_x(const G &g, float *fld, int iy, int k) {
-  if (iy > g.ny + 2) return;
-  float *a = fld + (EM2G_RHO + k) * g.w + (int64_t)iy * g.nxg;
-  const int nx = g.nx;
-  const float a1 = ld(a + 1) + ld(a + nx + 1);
-  const float a2 = ld(a + 2) + ld(a + nx + 2);
-  const float an = ld(a + nx) + ld(a);
-  a[1] = a1;
-  a[2] = a2;
-  a[nx] = an;
-  a[nx + 1] = a1;
-  a[nx + 2] = a2;
-  a[0] = an;
+  grid::fold_x_at<float, grid::LdL2>(g, fld, iy, k);
 }
-
 __device__ __forceinline__ void f_fold_y(const G &g, float *fld, int ix, int k) {
-  if (ix > g.nx + 2) return;
-  float *a = fld + (EM2G_RHO + k) * g.w + ix;
-  const int64_t s = g.nxg;
-  const int ny = g.ny;
-  const float a1 = ld(a + 1 * s) + ld(a + (ny + 1) * s);
-  const float a2 = ld(a + 2 * s) + ld(a + (ny + 2) * s);
-  const float an = ld(a + ny * s) + ld(a);
-  a[1 * s] = a1;
-  a[2 * s] = a2;
-  a[ny * s] = an;
-  a[(ny + 1) * s] = a1;
-  a[(ny + 2) * s] = a2;
-  a[0] = an;
+  grid::fold_y_at<float, grid::LdL2>(g, fld, ix, k);
 }
-
 __device__ __forceinline__ void f_b_half(const G &g, float *fld, float ctxh, float ctyh, int ix,
                                          int iy) {
-  if (ix > g.nx + 1 || iy > g.ny + 1) return;
-  const float *ex = fld + EM2G_EX * g.w, *ey = fld + EM2G_EY * g.w, *ez = fld + EM2G_EZ * g.w;
-  float *bx = fld + EM2G_BX * g.w, *by = fld + EM2G_BY * g.w, *bz = fld + EM2G_BZ * g.w;
-  const int64_t c = grid::at(g, ix, iy);
-  const float ezc = ld(ez + c);
-  const float vbx = ld(bx + c) - ctyh * (ezc - ld(ez + c - g.nxg));
-  const float vby = ld(by + c) + ctxh * (ezc - ld(ez + c - 1));
-  const float vbz = ld(bz + c) - ctxh * (ld(ey + c + 1) - ld(ey + c)) +
-                    ctyh * (ld(ex + c + g.nxg) - ld(ex + c));
-  grid::store_with_guards(g, bx, ix, iy, vbx);
-  grid::store_with_guards(g, by, ix, iy, vby);
-  grid::store_with_guards(g, bz, ix, iy, vbz);
+  grid::b_half_cell<float, grid::LdL2>(g, fld, ctxh, ctyh, ix, iy);
 }
-
 __device__ __forceinline__ void f_e_full(const G &g, float *fld, float ctx, float cty, float tem,
                                          int ix, int iy) {
-  if (ix > g.nx + 1 || iy > g.ny + 1) return;
-  float *ex = fld + EM2G_EX * g.w, *ey = fld + EM2G_EY * g.w, *ez = fld + EM2G_EZ * g.w;
-  const float *bx = fld + EM2G_BX * g.w, *by = fld + EM2G_BY * g.w, *bz = fld + EM2G_BZ * g.w;
-  const float *jxm = fld + EM2G_JXM * g.w, *jxp = fld + EM2G_JXP * g.w,
-              *jym = fld + EM2G_JYM * g.w, *jyp = fld + EM2G_JYP * g.w,
-              *jzm = fld + EM2G_JZM * g.w, *jzp = fld + EM2G_JZP * g.w;
-  const int64_t c = grid::at(g, ix, iy);
-  const float bzc = ld(bz + c);
-  const float vex =
-      ld(ex + c) + cty * (bzc - ld(bz + c - g.nxg)) - tem * (ld(jxm + c) + ld(jxp + c));
-  const float vey = ld(ey + c) - ctx * (bzc - ld(bz + c - 1)) - tem * (ld(jym + c) + ld(jyp + c));
-  const float vez = ld(ez + c) + ctx * (ld(by + c + 1) - ld(by + c)) -
-                    cty * (ld(bx + c + g.nxg) - ld(bx + c)) - tem * (ld(jzm + c) + ld(jzp + c));
-  grid::store_with_guards(g, ex, ix, iy, vex);
-  grid::store_with_guards(g, ey, ix, iy, vey);
-  grid::store_with_guards(g, ez, ix, iy, vez);
+  grid::e_full_cell<float, grid::LdL2>(g, fld, ctx, cty, tem, ix, iy);
 }
-
 __device__ __forceinline__ void f_smooth_b(const G &g, const float *s, float *d, int ix, int iy) {
-  if (ix > g.nx + 1 || iy > g.ny + 1) return;
-  const int64_t c = grid::at(g, ix, iy), n = g.nxg;
-  const float v =
-      (4 * ld(s + c) + 2 * (ld(s + c - 1) + ld(s + c + 1) + ld(s + c - n) + ld(s + c + n)) +
-       ld(s + c - 1 - n) + ld(s + c - 1 + n) + ld(s + c + 1 - n) + ld(s + c + 1 + n)) /
-      16.0f;
-  grid::store_with_guards(g, d, ix, iy, v);
+  grid::smooth_binomial_cell<float, grid::LdL2>(g, s, d, ix, iy);
 }
-
 __device__ __forceinline__ void f_smooth_c(const G &g, const float *d, float *s, int ix, int iy) {
-  if (ix > g.nx + 1 || iy > g.ny + 1) return;
-  const int64_t c = grid::at(g, ix, iy), n = g.nxg;
-  const float v = (20 * ld(d + c) - ld(d + c - 1) - ld(d + c + 1) - ld(d + c - n) -
-                   ld(d + c + n) - ld(d + c - 1 - n) - ld(d + c - 1 + n) - ld(d + c + 1 - n) -
-                   ld(d + c + 1 + n)) /
-                  12.0f;
-  grid::store_with_guards(g, s, ix, iy, v);
+  grid::smooth_compensate_cell<float, grid::LdL2>(g, d, s, ix, iy);
 }
-
 __device__ __forceinline__ void f_rhs(const G &g, const float *fld, float dx, float dy, float *r,
                                       float *p, int ix, int iy) {
-  if (ix > g.nx || iy > g.ny) return;
-  const float *ex = fld + EM2G_EX * g.w, *ey = fld + EM2G_EY * g.w, *rho = fld + EM2G_RHO * g.w;
-  const int ixm = (ix == 1) ? g.nx : ix - 1;
-  const float f = (ld(ex + grid::at(g, ix, iy)) - ld(ex + grid::at(g, ixm, iy))) / dx +
-                  (ld(ey + grid::at(g, ix, iy)) - ld(ey + grid::at(g, ix, iy - 1))) / dy -
-                  ld(rho + grid::at(g, ix, iy));
-  const float fs = f * dx * dx;
-  const int64_t k = (int64_t)(iy - 1) * g.nx + (ix - 1);
-  r[k] = fs;
-  p[k] = fs;
+  grid::poisson_rhs_cell<float, grid::LdL2>(g, fld, dx, dy, r, p, ix, iy);
 }
-
 __device__ __forceinline__ void f_correct(const G &g, float *fld, const float *u, float dx,
                                           float dy, int ix, int iy) {
-  if (ix > g.nx || iy > g.ny) return;
-  float *ex = fld + EM2G_EX * g.w, *ey = fld + EM2G_EY * g.w;
-  const int64_t k = (int64_t)(iy - 1) * g.nx + (ix - 1);
-  const int64_t kxp = (int64_t)(iy - 1) * g.nx + (ix == g.nx ? 0 : ix);
-  const int64_t kyp = (int64_t)(iy == g.ny ? 0 : iy) * g.nx + (ix - 1);
-  const float uc = ld(u + k);
-  const float vx = ld(ex + grid::at(g, ix, iy)) - (ld(u + kxp) - uc) / dx;
-  const float vy = ld(ey + grid::at(g, ix, iy)) - (ld(u + kyp) - uc) / dy;
-  grid::store_images(g, ex, ix, iy, vx);
-  grid::store_images(g, ey, ix, iy, vy);
+  grid::poisson_correct_cell<float, grid::LdL2>(g, fld, u, dx, dy, ix, iy);
 }
 
 // one stencil stage over every run: 32x8 tiles numbered run after run

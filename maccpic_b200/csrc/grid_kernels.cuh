@@ -28,6 +28,19 @@ __device__ __forceinline__ int64_t at(const G &g, int ix, int iy) {
   return (int64_t)iy * g.nxg + ix;
 }
 
+// How a stage reads the arrays: plainly in a launch of its own, through L2
+// (ld.global.cg) inside a persistent launch whose earlier phases other SMs
+// wrote -- an L1 line cached before such a write would be stale.  The
+// arithmetic is the same expression for expression either way.
+struct LdPlain {
+  template <typename T>
+  __device__ __forceinline__ static T ld(const T *p) { return *p; }
+};
+struct LdL2 {
+  template <typename T>
+  __device__ __forceinline__ static T ld(const T *p) { return __ldcg(p); }
+};
+
 // store v at (ix,iy), 1<=ix<=nx+1, 1<=iy<=ny+1, and at its guard copies
 template <typename T>
 __device__ __forceinline__ void store_with_guards(const G &g, T *a, int ix, int iy, T v) {
@@ -40,58 +53,71 @@ __device__ __forceinline__ void store_with_guards(const G &g, T *a, int ix, int 
 }
 
 // ---- guard fold of rho and the 6 current arrays (pic/fields.f90:44-137)
-// x pass: one thread per (row iy in 0..ny+2, array)
-template <typename T>
+// x pass: row iy in 0..ny+2 of array k (the six positions are distinct for
+// nx >= 3; the library asks nx, ny >= 4)
+template <typename T, typename L = LdPlain>
 __device__ __forceinline__ void fold_x_at(const G &g, T *fld, int iy, int k) {
   if (iy > g.ny + 2) return;
   T *a = fld + (EM2G_RHO + k) * g.w + (int64_t)iy * g.nxg;
   const int nx = g.nx;
-  a[1] = a[1] + a[nx + 1];
-  a[2] = a[2] + a[nx + 2];
-  a[nx] = a[nx] + a[0];
-  a[nx + 1] = a[1];
-  a[nx + 2] = a[2];
-  a[0] = a[nx];
+  const T a1 = L::ld(a + 1) + L::ld(a + nx + 1);
+  const T a2 = L::ld(a + 2) + L::ld(a + nx + 2);
+  const T an = L::ld(a + nx) + L::ld(a);
+  a[1] = a1;
+  a[2] = a2;
+  a[nx] = an;
+  a[nx + 1] = a1;
+  a[nx + 2] = a2;
+  a[0] = an;
 }
 template <typename T>
 __global__ void k_fold_x(G g, T *fld) {
   fold_x_at(g, fld, (int)(blockIdx.x * blockDim.x + threadIdx.x), (int)blockIdx.y);
 }
-// y pass: one thread per (column ix in 0..nx+2, array)
-template <typename T>
+// y pass: column ix in 0..nx+2 of array k
+template <typename T, typename L = LdPlain>
 __device__ __forceinline__ void fold_y_at(const G &g, T *fld, int ix, int k) {
   if (ix > g.nx + 2) return;
   T *a = fld + (EM2G_RHO + k) * g.w + ix;
   const int64_t s = g.nxg;
   const int ny = g.ny;
-  a[1 * s] = a[1 * s] + a[(ny + 1) * s];
-  a[2 * s] = a[2 * s] + a[(ny + 2) * s];
-  a[ny * s] = a[ny * s] + a[0];
-  a[(ny + 1) * s] = a[1 * s];
-  a[(ny + 2) * s] = a[2 * s];
-  a[0] = a[ny * s];
+  const T a1 = L::ld(a + 1 * s) + L::ld(a + (ny + 1) * s);
+  const T a2 = L::ld(a + 2 * s) + L::ld(a + (ny + 2) * s);
+  const T an = L::ld(a + ny * s) + L::ld(a);
+  a[1 * s] = a1;
+  a[2 * s] = a2;
+  a[ny * s] = an;
+  a[(ny + 1) * s] = a1;
+  a[(ny + 2) * s] = a2;
+  a[0] = an;
 }
 template <typename T>
 __global__ void k_fold_y(G g, T *fld) {
   fold_y_at(g, fld, (int)(blockIdx.x * blockDim.x + threadIdx.x), (int)blockIdx.y);
 }
 
+// The cell stages take the cell (ix, iy); the *_at forms take a 32x8 tile
+// (tbx, tby) whose cell is given by the thread index.
+
 // ---- Yee half step of B (pic/fields.f90:184-200, :231-247)
-template <typename T>
-__device__ __forceinline__ void b_half_at(const G &g, T *fld, T ctxh, T ctyh, int tbx, int tby) {
-  const int ix = 1 + tbx * TX + threadIdx.x;
-  const int iy = 1 + tby * TY + threadIdx.y;
+template <typename T, typename L = LdPlain>
+__device__ __forceinline__ void b_half_cell(const G &g, T *fld, T ctxh, T ctyh, int ix, int iy) {
   if (ix > g.nx + 1 || iy > g.ny + 1) return;
   const T *ex = fld + EM2G_EX * g.w, *ey = fld + EM2G_EY * g.w, *ez = fld + EM2G_EZ * g.w;
   T *bx = fld + EM2G_BX * g.w, *by = fld + EM2G_BY * g.w, *bz = fld + EM2G_BZ * g.w;
   const int64_t c = at(g, ix, iy);
-  const T ezc = ez[c];
-  const T vbx = bx[c] - ctyh * (ezc - ez[c - g.nxg]);
-  const T vby = by[c] + ctxh * (ezc - ez[c - 1]);
-  const T vbz = bz[c] - ctxh * (ey[c + 1] - ey[c]) + ctyh * (ex[c + g.nxg] - ex[c]);
+  const T ezc = L::ld(ez + c);
+  const T vbx = L::ld(bx + c) - ctyh * (ezc - L::ld(ez + c - g.nxg));
+  const T vby = L::ld(by + c) + ctxh * (ezc - L::ld(ez + c - 1));
+  const T vbz = L::ld(bz + c) - ctxh * (L::ld(ey + c + 1) - L::ld(ey + c)) +
+                ctyh * (L::ld(ex + c + g.nxg) - L::ld(ex + c));
   store_with_guards(g, bx, ix, iy, vbx);
   store_with_guards(g, by, ix, iy, vby);
   store_with_guards(g, bz, ix, iy, vbz);
+}
+template <typename T>
+__device__ __forceinline__ void b_half_at(const G &g, T *fld, T ctxh, T ctyh, int tbx, int tby) {
+  b_half_cell(g, fld, ctxh, ctyh, 1 + tbx * TX + (int)threadIdx.x, 1 + tby * TY + (int)threadIdx.y);
 }
 template <typename T>
 __global__ void k_b_half(G g, T *fld, T ctxh, T ctyh) {
@@ -99,26 +125,33 @@ __global__ void k_b_half(G g, T *fld, T ctxh, T ctyh) {
 }
 
 // ---- Yee full step of E (pic/fields.f90:207-224)
-template <typename T>
-__device__ __forceinline__ void e_full_at(const G &g, T *fld, T ctx, T cty, T tem, int tbx,
-                                          int tby) {
-  const int ix = 1 + tbx * TX + threadIdx.x;
-  const int iy = 1 + tby * TY + threadIdx.y;
+template <typename T, typename L = LdPlain>
+__device__ __forceinline__ void e_full_cell(const G &g, T *fld, T ctx, T cty, T tem, int ix,
+                                            int iy) {
   if (ix > g.nx + 1 || iy > g.ny + 1) return;
   T *ex = fld + EM2G_EX * g.w, *ey = fld + EM2G_EY * g.w, *ez = fld + EM2G_EZ * g.w;
   const T *bx = fld + EM2G_BX * g.w, *by = fld + EM2G_BY * g.w, *bz = fld + EM2G_BZ * g.w;
   const T *jxm = fld + EM2G_JXM * g.w, *jxp = fld + EM2G_JXP * g.w,
-               *jym = fld + EM2G_JYM * g.w, *jyp = fld + EM2G_JYP * g.w,
-               *jzm = fld + EM2G_JZM * g.w, *jzp = fld + EM2G_JZP * g.w;
+          *jym = fld + EM2G_JYM * g.w, *jyp = fld + EM2G_JYP * g.w,
+          *jzm = fld + EM2G_JZM * g.w, *jzp = fld + EM2G_JZP * g.w;
   const int64_t c = at(g, ix, iy);
-  const T bzc = bz[c];
-  const T vex = ex[c] + cty * (bzc - bz[c - g.nxg]) - tem * (jxm[c] + jxp[c]);
-  const T vey = ey[c] - ctx * (bzc - bz[c - 1]) - tem * (jym[c] + jyp[c]);
-  const T vez = ez[c] + ctx * (by[c + 1] - by[c]) - cty * (bx[c + g.nxg] - bx[c]) -
-                     tem * (jzm[c] + jzp[c]);
+  const T bzc = L::ld(bz + c);
+  const T vex = L::ld(ex + c) + cty * (bzc - L::ld(bz + c - g.nxg)) -
+                tem * (L::ld(jxm + c) + L::ld(jxp + c));
+  const T vey = L::ld(ey + c) - ctx * (bzc - L::ld(bz + c - 1)) -
+                tem * (L::ld(jym + c) + L::ld(jyp + c));
+  const T vez = L::ld(ez + c) + ctx * (L::ld(by + c + 1) - L::ld(by + c)) -
+                cty * (L::ld(bx + c + g.nxg) - L::ld(bx + c)) -
+                tem * (L::ld(jzm + c) + L::ld(jzp + c));
   store_with_guards(g, ex, ix, iy, vex);
   store_with_guards(g, ey, ix, iy, vey);
   store_with_guards(g, ez, ix, iy, vez);
+}
+template <typename T>
+__device__ __forceinline__ void e_full_at(const G &g, T *fld, T ctx, T cty, T tem, int tbx,
+                                          int tby) {
+  e_full_cell(g, fld, ctx, cty, tem, 1 + tbx * TX + (int)threadIdx.x,
+              1 + tby * TY + (int)threadIdx.y);
 }
 template <typename T>
 __global__ void k_e_full(G g, T *fld, T ctx, T cty, T tem) {
@@ -127,33 +160,43 @@ __global__ void k_e_full(G g, T *fld, T ctx, T cty, T tem) {
 
 // ---- smooth2 (pic/smooth.f90:143-177): binomial pass into `d`, then the
 // compensation pass back into `s`.
+template <typename T, typename L = LdPlain>
+__device__ __forceinline__ void smooth_binomial_cell(const G &g, const T *__restrict__ s, T *d,
+                                                     int ix, int iy) {
+  if (ix > g.nx + 1 || iy > g.ny + 1) return;
+  const int64_t c = at(g, ix, iy), n = g.nxg;
+  const T v = (4 * L::ld(s + c) +
+               2 * (L::ld(s + c - 1) + L::ld(s + c + 1) + L::ld(s + c - n) + L::ld(s + c + n)) +
+               L::ld(s + c - 1 - n) + L::ld(s + c - 1 + n) + L::ld(s + c + 1 - n) +
+               L::ld(s + c + 1 + n)) /
+              T(16.0);
+  store_with_guards(g, d, ix, iy, v);
+}
 template <typename T>
 __device__ __forceinline__ void smooth_binomial_at(const G &g, const T *__restrict__ s, T *d,
                                                    int tbx, int tby) {
-  const int ix = 1 + tbx * TX + threadIdx.x;
-  const int iy = 1 + tby * TY + threadIdx.y;
-  if (ix > g.nx + 1 || iy > g.ny + 1) return;
-  const int64_t c = at(g, ix, iy), n = g.nxg;
-  const T v = (4 * s[c] + 2 * (s[c - 1] + s[c + 1] + s[c - n] + s[c + n]) +
-                    s[c - 1 - n] + s[c - 1 + n] + s[c + 1 - n] + s[c + 1 + n]) /
-                   T(16.0);
-  store_with_guards(g, d, ix, iy, v);
+  smooth_binomial_cell(g, s, d, 1 + tbx * TX + (int)threadIdx.x, 1 + tby * TY + (int)threadIdx.y);
 }
 template <typename T>
 __global__ void k_smooth_binomial(G g, const T *__restrict__ s, T *d) {
   smooth_binomial_at(g, s, d, (int)blockIdx.x, (int)blockIdx.y);
 }
+template <typename T, typename L = LdPlain>
+__device__ __forceinline__ void smooth_compensate_cell(const G &g, const T *__restrict__ d, T *s,
+                                                       int ix, int iy) {
+  if (ix > g.nx + 1 || iy > g.ny + 1) return;
+  const int64_t c = at(g, ix, iy), n = g.nxg;
+  const T v = (20 * L::ld(d + c) - L::ld(d + c - 1) - L::ld(d + c + 1) - L::ld(d + c - n) -
+               L::ld(d + c + n) - L::ld(d + c - 1 - n) - L::ld(d + c - 1 + n) -
+               L::ld(d + c + 1 - n) - L::ld(d + c + 1 + n)) /
+              T(12.0);
+  store_with_guards(g, s, ix, iy, v);
+}
 template <typename T>
 __device__ __forceinline__ void smooth_compensate_at(const G &g, const T *__restrict__ d, T *s,
                                                      int tbx, int tby) {
-  const int ix = 1 + tbx * TX + threadIdx.x;
-  const int iy = 1 + tby * TY + threadIdx.y;
-  if (ix > g.nx + 1 || iy > g.ny + 1) return;
-  const int64_t c = at(g, ix, iy), n = g.nxg;
-  const T v = (20 * d[c] - d[c - 1] - d[c + 1] - d[c - n] - d[c + n] - d[c - 1 - n] -
-                    d[c - 1 + n] - d[c + 1 - n] - d[c + 1 + n]) /
-                   T(12.0);
-  store_with_guards(g, s, ix, iy, v);
+  smooth_compensate_cell(g, d, s, 1 + tbx * TX + (int)threadIdx.x,
+                         1 + tby * TY + (int)threadIdx.y);
 }
 template <typename T>
 __global__ void k_smooth_compensate(G g, const T *__restrict__ d, T *s) {
@@ -163,20 +206,25 @@ __global__ void k_smooth_compensate(G g, const T *__restrict__ d, T *s) {
 // ---- Poisson right-hand side (pic/fields.f90:392-405): f = (div E - rho)
 // * dx * dx on the nx*ny periodic grid; written straight into r (u = 0, so
 // cgm's first residual r = f - L u is f) and p = r.
-template <typename T>
-__device__ __forceinline__ void poisson_rhs_at(const G &g, const T *__restrict__ fld, T dx, T dy,
-                                               T *r, T *p, int tbx, int tby) {
-  const int ix = 1 + tbx * TX + threadIdx.x;
-  const int iy = 1 + tby * TY + threadIdx.y;
+template <typename T, typename L = LdPlain>
+__device__ __forceinline__ void poisson_rhs_cell(const G &g, const T *__restrict__ fld, T dx,
+                                                 T dy, T *r, T *p, int ix, int iy) {
   if (ix > g.nx || iy > g.ny) return;
   const T *ex = fld + EM2G_EX * g.w, *ey = fld + EM2G_EY * g.w, *rho = fld + EM2G_RHO * g.w;
   const int ixm = (ix == 1) ? g.nx : ix - 1;
-  const T f = (ex[at(g, ix, iy)] - ex[at(g, ixm, iy)]) / dx +
-                   (ey[at(g, ix, iy)] - ey[at(g, ix, iy - 1)]) / dy - rho[at(g, ix, iy)];
+  const T f = (L::ld(ex + at(g, ix, iy)) - L::ld(ex + at(g, ixm, iy))) / dx +
+              (L::ld(ey + at(g, ix, iy)) - L::ld(ey + at(g, ix, iy - 1))) / dy -
+              L::ld(rho + at(g, ix, iy));
   const T fs = f * dx * dx;
   const int64_t k = (int64_t)(iy - 1) * g.nx + (ix - 1);
   r[k] = fs;
   p[k] = fs;
+}
+template <typename T>
+__device__ __forceinline__ void poisson_rhs_at(const G &g, const T *__restrict__ fld, T dx, T dy,
+                                               T *r, T *p, int tbx, int tby) {
+  poisson_rhs_cell(g, fld, dx, dy, r, p, 1 + tbx * TX + (int)threadIdx.x,
+                   1 + tby * TY + (int)threadIdx.y);
 }
 template <typename T>
 __global__ void k_poisson_rhs(G g, const T *__restrict__ fld, T dx, T dy, T *r, T *p) {
@@ -199,21 +247,25 @@ __device__ __forceinline__ void store_images(const G &g, T *a, int ix, int iy, T
   for (int a1 = 0; a1 < nys; ++a1)
     for (int a0 = 0; a0 < nxs; ++a0) a[at(g, xs[a0], ys[a1])] = v;
 }
-template <typename T>
-__device__ __forceinline__ void poisson_correct_at(const G &g, T *fld, const T *__restrict__ u,
-                                                   T dx, T dy, int tbx, int tby) {
-  const int ix = 1 + tbx * TX + threadIdx.x;
-  const int iy = 1 + tby * TY + threadIdx.y;
+template <typename T, typename L = LdPlain>
+__device__ __forceinline__ void poisson_correct_cell(const G &g, T *fld, const T *__restrict__ u,
+                                                     T dx, T dy, int ix, int iy) {
   if (ix > g.nx || iy > g.ny) return;
   T *ex = fld + EM2G_EX * g.w, *ey = fld + EM2G_EY * g.w;
   const int64_t k = (int64_t)(iy - 1) * g.nx + (ix - 1);
   const int64_t kxp = (int64_t)(iy - 1) * g.nx + (ix == g.nx ? 0 : ix);
   const int64_t kyp = (int64_t)(iy == g.ny ? 0 : iy) * g.nx + (ix - 1);
-  const T uc = u[k];
-  const T vx = ex[at(g, ix, iy)] - (u[kxp] - uc) / dx;
-  const T vy = ey[at(g, ix, iy)] - (u[kyp] - uc) / dy;
+  const T uc = L::ld(u + k);
+  const T vx = L::ld(ex + at(g, ix, iy)) - (L::ld(u + kxp) - uc) / dx;
+  const T vy = L::ld(ey + at(g, ix, iy)) - (L::ld(u + kyp) - uc) / dy;
   store_images(g, ex, ix, iy, vx);
   store_images(g, ey, ix, iy, vy);
+}
+template <typename T>
+__device__ __forceinline__ void poisson_correct_at(const G &g, T *fld, const T *__restrict__ u,
+                                                   T dx, T dy, int tbx, int tby) {
+  poisson_correct_cell(g, fld, u, dx, dy, 1 + tbx * TX + (int)threadIdx.x,
+                       1 + tby * TY + (int)threadIdx.y);
 }
 template <typename T>
 __global__ void k_poisson_correct(G g, T *fld, const T *__restrict__ u, T dx, T dy) {

@@ -29,6 +29,7 @@
 #include <string>
 
 #include "em2g_internal.cuh"
+#include "grid_kernels.cuh"
 
 static __device__ __align__(256) double g_smooth2_scratch[EM2G_SMOOTH2_STATIC_MAX_POINTS];
 
@@ -38,42 +39,14 @@ constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
 double *g_scratch_addr[kMaxDevices] = {nullptr};
 
-constexpr int TX = 32, TY = 8;
-
-// store v at (ix,iy) and at the guard cells that copy it
-// (columns 0/nx+2 from nx/2, rows 0/ny+2 from ny/2; pic/smooth.f90:148-155)
-__device__ __forceinline__ void put(double *a, int nx, int ny, int64_t nxg, int ix, int iy,
-                                    double v) {
-  a[(int64_t)iy * nxg + ix] = v;
-  const int mx = (ix == nx) ? 0 : ((ix == 2) ? nx + 2 : -1);
-  const int my = (iy == ny) ? 0 : ((iy == 2) ? ny + 2 : -1);
-  if (mx >= 0) a[(int64_t)iy * nxg + mx] = v;
-  if (my >= 0) a[(int64_t)my * nxg + ix] = v;
-  if (mx >= 0 && my >= 0) a[(int64_t)my * nxg + mx] = v;
+// the two passes are the library's own stencils (grid_kernels.cuh), on the
+// guarded (nx+3) x (ny+3) array: binomial sm -> scratch, then compensation
+// scratch -> sm (pic/smooth.f90:143-146, :163-166)
+__global__ void k_binomial_static(em2g::grid::G g, const double *__restrict__ s, double *d) {
+  em2g::grid::smooth_binomial_at(g, s, d, (int)blockIdx.x, (int)blockIdx.y);
 }
-
-// 9-point binomial pass, sm -> scratch (pic/smooth.f90:143-146)
-__global__ void k_binomial_static(int nx, int ny, const double *__restrict__ s, double *d) {
-  const int ix = 1 + blockIdx.x * TX + threadIdx.x;
-  const int iy = 1 + blockIdx.y * TY + threadIdx.y;
-  if (ix > nx + 1 || iy > ny + 1) return;
-  const int64_t n = nx + 3, c = (int64_t)iy * n + ix;
-  const double v = (4 * s[c] + 2 * (s[c - 1] + s[c + 1] + s[c - n] + s[c + n]) +
-                    s[c - 1 - n] + s[c - 1 + n] + s[c + 1 - n] + s[c + 1 + n]) /
-                   16.0;
-  put(d, nx, ny, n, ix, iy, v);
-}
-
-// compensation pass, scratch -> sm (pic/smooth.f90:163-166)
-__global__ void k_compensate_static(int nx, int ny, const double *__restrict__ d, double *s) {
-  const int ix = 1 + blockIdx.x * TX + threadIdx.x;
-  const int iy = 1 + blockIdx.y * TY + threadIdx.y;
-  if (ix > nx + 1 || iy > ny + 1) return;
-  const int64_t n = nx + 3, c = (int64_t)iy * n + ix;
-  const double v = (20 * d[c] - d[c - 1] - d[c + 1] - d[c - n] - d[c + n] - d[c - 1 - n] -
-                    d[c - 1 + n] - d[c + 1 - n] - d[c + 1 + n]) /
-                   12.0;
-  put(s, nx, ny, n, ix, iy, v);
+__global__ void k_compensate_static(em2g::grid::G g, const double *__restrict__ d, double *s) {
+  em2g::grid::smooth_compensate_at(g, d, s, (int)blockIdx.x, (int)blockIdx.y);
 }
 
 }  // namespace
@@ -117,9 +90,12 @@ extern "C" int em2g_smooth2_static(int nx, int ny, double *dev_array, void *cuda
     }
     scratch = g_scratch_addr[dev];
   }
+  using em2g::grid::TX;
+  using em2g::grid::TY;
+  const em2g::grid::G g{nx, ny, nx + 3, (int64_t)(nx + 3) * (ny + 3)};
   const dim3 blk(TX, TY), grd((nx + 1 + TX - 1) / TX, (ny + 1 + TY - 1) / TY);
-  k_binomial_static<<<grd, blk, 0, st>>>(nx, ny, dev_array, scratch);
-  k_compensate_static<<<grd, blk, 0, st>>>(nx, ny, scratch, dev_array);
+  k_binomial_static<<<grd, blk, 0, st>>>(g, dev_array, scratch);
+  k_compensate_static<<<grd, blk, 0, st>>>(g, scratch, dev_array);
   e = cudaGetLastError();
   if (e != cudaSuccess) return em2g::cuda_fail(e, "smooth2_static launch");
   return EM2G_OK;
