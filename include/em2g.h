@@ -223,6 +223,20 @@ int em2g_step(em2g_ctx *ctx, int nsteps, double *ake_out, double *energies_out,
 #define EM2G_SMOOTH2_STATIC_MAX_POINTS (1 << 19)
 int em2g_smooth2_static(int nx, int ny, double *dev_array, void *cuda_stream);
 
+/* ---- em2's start-up velocity push (pic/setv.f90:36-128) -------------
+ * For loaders that draw v at t = 0: one Boris push of -dt/2 with the given
+ * E and B gathered with linear weights, as em2's fresh run does before its
+ * first step, applied in place to n particles of species isp in device
+ * memory (x, y, vx, vy, vz, gamma: 6 arrays of n doubles; v in, v and gamma
+ * at t = -dt/2 out; gamma is recomputed from v first).  dev_fields is the
+ * FP64 field block in em2's layout (13 arrays of (nx+3)*(ny+3), the order
+ * of em2g_field); p supplies nx, ny, dt, c and the species' qm, tx, ty.
+ * Each particle's result is bitwise em2's arithmetic.  Every particle must
+ * lie in [0,nx) x [0,ny) with |v| < 1, else nothing is changed
+ * (EM2G_ERR_RANGE).  No context is needed; the call waits for its check. */
+int em2g_setv_device(const em2g_params *p, int isp, const double *dev_fields, double *dev_parts,
+                     int64_t n, void *cuda_stream);
+
 /* ---- diagnostics (no counterpart subroutine; FP64 on the GPU) --------
  * out[0..6)  0.5 * mean over the interior of ex^2, ey^2, ez^2, bx^2, by^2,
  *            bz^2 of the current fields (em2's exe..bze over the whole grid,

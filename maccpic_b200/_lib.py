@@ -31,7 +31,7 @@ EXPORTS = [
     "em2g_get_fields_device", "em2g_field_device_ptr", "em2g_move", "em2g_curnt",
     "em2g_fields", "em2g_smooth2", "em2g_step", "em2g_set_particles_device",
     "em2g_move_curnt", "em2g_set_timing", "em2g_get_counters", "em2g_reset_counters",
-    "em2g_smooth2_static", "em2g_diagnostics", "em2g_num_variants", "em2g_set_variant",
+    "em2g_smooth2_static", "em2g_setv_device", "em2g_diagnostics", "em2g_num_variants", "em2g_set_variant",
     "em2g_get_variant", "em2g_set_sort_interval",
     "em2g_adj_create", "em2g_adj_destroy", "em2g_adj_forward", "em2g_adj_keep_all_fields",
     "em2g_adj_field_slots", "em2g_adj_get_field_slots",
@@ -123,6 +123,7 @@ def lib() -> C.CDLL:
         "em2g_get_counters": (C.c_int, [ctx, i64p, i64p, dp]),
         "em2g_reset_counters": (C.c_int, [ctx]),
         "em2g_smooth2_static": (C.c_int, [C.c_int, C.c_int, vp, vp]),
+        "em2g_setv_device": (C.c_int, [C.POINTER(Em2gParams), C.c_int, vp, vp, C.c_int64, vp]),
         "em2g_diagnostics": (C.c_int, [ctx, dp, C.c_int]),
         "em2g_num_variants": (C.c_int, [ctx, ip]),
         "em2g_set_variant": (C.c_int, [ctx, C.c_int]),

@@ -4,7 +4,8 @@
 under ``maccpic_b200/_build/`` and links ``maccpic_b200/libem2g.so``.
 Objects are rebuilt when their source or any header is newer.
 
-The FP64 drop-in kernels (``push_f64.cu``, ``fields_f64.cu``) are compiled
+The FP64 drop-in kernels (``push_f64.cu``, ``fields_f64.cu`` and the others in
+``NO_FMA``) are compiled
 with ``-fmad=false`` so that each product and sum is rounded separately, as
 em2's gfortran build does on x86-64; the FP32 kernels keep FMA contraction.
 """
@@ -25,7 +26,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
           "-I", os.path.join(ROOT, "include"), "--expt-relaxed-constexpr"]
-NO_FMA = {"push_f64.cu", "push_fast_f64.cu", "fields_f64.cu", "smooth2_static.cu"}
+NO_FMA = {"push_f64.cu", "push_fast_f64.cu", "fields_f64.cu", "smooth2_static.cu", "setv.cu"}
 
 
 def _headers():

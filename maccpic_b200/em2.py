@@ -353,3 +353,32 @@ class Em2Gpu:
         check(self._L.em2g_step(self._h, int(nsteps), _dp(ake), _dp(e6), C.byref(n)))
         return {"ake": ake[: self.p.nsp].copy(), "cg_iters": n.value,
                 "energies": e6 if self.it % self.p.isav == 0 else None}
+
+
+def setv_device(params: RunParams, isp: int, fields, parts, stream=None) -> None:
+    """em2's start-up push (pic/setv.f90:36-128) in place on the GPU: the
+    velocities of ``parts`` -- a (6, n) float64 CUDA tensor (x, y, vx, vy,
+    vz, gamma), v at t = 0 -- pushed back to t = -dt/2 with the E and B of
+    ``fields`` (a (13, ny+3, nx+3) float64 CUDA tensor, em2's layout)
+    gathered with linear weights, gamma recomputed.  Bitwise em2's
+    arithmetic; particles outside the box or not slower than c raise
+    :class:`~maccpic_b200._lib.Em2gError` and leave ``parts`` unchanged.
+    Runs on ``stream`` (default: torch's current stream) and returns once
+    the push is enqueued."""
+    import torch
+    shape = (NFIELD, params.ny + 3, params.nx + 3)
+    for name, t, want in (("fields", fields, shape), ("parts", parts, None)):
+        if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == torch.float64
+                and t.is_contiguous()):
+            raise ValueError(f"{name} must be a contiguous float64 CUDA tensor")
+        if want is not None and tuple(t.shape) != want:
+            raise ValueError(f"fields must have shape {want}")
+    if parts.dim() != 2 or parts.shape[0] != 6:
+        raise ValueError("parts must have shape (6, n)")
+    if stream is None:
+        stream = torch.cuda.current_stream(parts.device)
+    p = params.ctype()
+    with torch.cuda.device(parts.device):
+        check(_lib.lib().em2g_setv_device(C.byref(p), int(isp), C.c_void_p(fields.data_ptr()),
+                                          C.c_void_p(parts.data_ptr()), int(parts.shape[1]),
+                                          stream_handle(stream)))

@@ -243,6 +243,21 @@ def sample_particles_torch(cfg: HarrisConfig, device="cuda", n: int | None = Non
     return out
 
 
+def setv_torch(cfg: HarrisConfig, fields, parts, device="cuda") -> None:
+    """em2's start-up as its fresh run does it (pic/main.f90 -> setv): take
+    the drawn velocities as those at t = 0 and push them back to t = -dt/2
+    on the GPU with the initial E and B and linear weights
+    (pic/setv.f90:36-128, ``em2g_setv_device``), in place on each species'
+    (6, n) float64 CUDA tensor.  Without it the drawn velocities are taken
+    as the t = -dt/2 values directly."""
+    import torch
+    from .em2 import setv_device
+    fld = torch.as_tensor(np.ascontiguousarray(fields), dtype=torch.float64, device=device)
+    rp = cfg.run_params()
+    for s, p in enumerate(parts):
+        setv_device(rp, s, fld, p)
+
+
 def sample_particles_torch_slices(cfg: HarrisConfig, device="cuda", slice_size: int = 1 << 24):
     """The double-Harris distribution of :func:`sample_particles_torch`,
     drawn slice by slice on the GPU for workloads whose whole FP64 state

@@ -281,6 +281,15 @@ class Em2Setup:
         return P
 
 
+def setv(params: Params, fld: np.ndarray, isp: int, part: np.ndarray) -> np.ndarray:
+    """em2's start-up push (pic/setv.f90:36-128) on a copy of one species'
+    (6, n) block: v at t = 0 in, v and gamma at t = -dt/2 out."""
+    out = np.ascontiguousarray(part, dtype=np.float64).copy()
+    f = np.ascontiguousarray(fld, dtype=np.float64)
+    lib().em2o_setv(C.byref(params.ctype()), _dp(f), int(isp), out.shape[1], _dp(out))
+    return out
+
+
 def em2_startup(setup: Em2Setup):
     """Run em2's fresh-run start-up (init -> creator -> setv) for every rank
     and return (Params, State, maxnp).  Species blocks hold rank 0's slots,
