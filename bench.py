@@ -752,7 +752,10 @@ def run_e2e(args, cfg, rp, fields, parts_host, variant=0):
     then K steps of em2g_move_curnt (ake read back) and em2g_fields (CG count
     and energies read back), with every field array and every particle
     downloaded into the caller's pinned buffers whenever em2 would call
-    `output` (it % isav == 0, pic/main.f90:158-159) and after the last step."""
+    `output` (it % isav == 0, pic/main.f90:158-159) and after the last step.
+    K is the run's step count but at least one output interval (isav steps),
+    so that the one upload and the final download are spread over no fewer
+    steps than em2's own loop spreads each output over."""
     import torch
     from maccpic_b200.em2 import Em2Gpu
 
@@ -776,9 +779,10 @@ def run_e2e(args, cfg, rp, fields, parts_host, variant=0):
     for s in range(2):
         g.set_particles(s, pnp[s])
     g.it = 0
-    for it in range(1, args.steps + 1):
+    K = max(args.steps, rp.isav)
+    for it in range(1, K + 1):
         g.move_curnt()
-        if it % rp.isav == 0 or it == args.steps:
+        if it % rp.isav == 0 or it == K:
             g.get_fields(out=out_f)
             for s in range(2):
                 g.get_particles(s, out=out_p[s])
@@ -789,9 +793,9 @@ def run_e2e(args, cfg, rp, fields, parts_host, variant=0):
     n_total = sum(p.shape[1] for p in pnp)
     state = fnp.nbytes + sum(p.nbytes for p in pnp)
     small = 8 * (2 + 6) + 4
-    return {"value": n_total * args.steps / el, "unit": METRIC,
-            "h2d_bytes_per_step": state / args.steps,
-            "d2h_bytes_per_step": (state * downloads + small * args.steps) / args.steps,
+    return {"value": n_total * K / el, "unit": METRIC, "steps": K,
+            "h2d_bytes_per_step": state / K,
+            "d2h_bytes_per_step": (state * downloads + small * K) / K,
             "downloads": downloads, "isav": rp.isav, "n_gpus": 1,
             "path": "em2g_set_fields/em2g_set_particles (pinned host, FP64 em2 layout) once, K x "
                     "(em2g_move_curnt, em2g_fields), em2g_get_fields/em2g_get_particles every "
