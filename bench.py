@@ -653,6 +653,10 @@ def run_adjoint(args, local):
         fd = {}
         for t in sorted({min(T, x) for x in (50, 100, 200, 400, T)}):
             fd[t] = A.fd_check_cuda(cfg, theta, t, h=1e-3, checkpoint=K, draws=d, workspace=ws)
+        # at T, smaller steps: a difference over +-1e-3 is no longer linear
+        # after hundreds of steps of a kinetic plasma, one over +-1e-6 is
+        fd_h = {h: A.fd_check_cuda(cfg, theta, T, h=h, checkpoint=K, draws=d, workspace=ws)
+                for h in (1e-4, 1e-5, 1e-6)}
     finally:
         ws.close()
     torch.cuda.empty_cache()
@@ -684,6 +688,9 @@ def run_adjoint(args, local):
             "fd_rel_error": max(fd[T]["rel_error"]),
             "fd": {str(t): r for t, r in fd.items()},
             "fd_agree_1pct_max_steps": max(agree) if agree else 0,
+            "fd_at_T_by_h": {f"{h:g}": {"fd": r["fd"], "rel_error": r["rel_error"]}
+                             for h, r in fd_h.items()},
+            "fd_rel_error_at_T_smallest_h": max(fd_h[1e-6]["rel_error"]),
             "forward": "em2g_step FP64, exact (spectral) Poisson solve"}
 
 
