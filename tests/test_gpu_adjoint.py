@@ -7,7 +7,8 @@
 * the whole sweep (rebuilt states, checkpoints, regrouping) gives the
   PyTorch adjoint's d flux / d theta;
 * d flux / d theta agrees with central differences of the CUDA forward
-  (common random numbers, h = 1e-3) to within 1 %.
+  (common random numbers, h = 1e-3) to within 1 %, and over a longer
+  horizon with h = 1e-6 to 1e-3.
 """
 import numpy as np
 import pytest
@@ -113,6 +114,21 @@ def test_cuda_gradient_matches_central_differences(gpu):
         fd = (A.flux_of_theta_cuda(cfg, tp, steps, d)
               - A.flux_of_theta_cuda(cfg, tm, steps, d)) / (2 * h)
         assert abs(g[i] - fd) <= 0.01 * abs(fd) + 1e-9, (i, g[i], fd)
+
+
+def test_long_horizon_gradient_matches_small_step_differences(gpu):
+    """Over a horizon where the flux is no longer linear in theta across
+    +-1e-3, the adjoint is still the derivative: central differences with
+    h = 1e-6 (common random numbers, FP64 round-off ~1e-16 flux / h) agree
+    with it to 1e-3 relative, through a workspace that recomputes segments."""
+    cfg = _cfg(nx=64, ny=64, ppc=8, seed=11, isav=20)
+    d = A.make_draws(cfg, device="cuda")
+    k = A.step_const(cfg)
+    steps = 300
+    with A.CudaAdjoint(k, *A.initial_state_torch(cfg, THETA, d), steps, 50, cfg.isav,
+                       field_slots=50) as ws:
+        r = A.fd_check_cuda(cfg, THETA, steps, h=1e-6, checkpoint=50, draws=d, workspace=ws)
+    assert max(r["rel_error"]) < 1e-3, r
 
 
 def test_reused_workspace_gives_the_same_gradient(gpu):
