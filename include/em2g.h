@@ -261,6 +261,14 @@ int em2g_set_variant(em2g_ctx *ctx, int variant);
 int em2g_get_variant(em2g_ctx *ctx, int *variant, char *name, int name_len);
 /* em2g_params.sort_interval, changed between steps (same rules) */
 int em2g_set_sort_interval(em2g_ctx *ctx, int sort_interval);
+/* How the Yee updates and the smooth2 passes inside em2g_fields and
+ * em2g_smooth2 read their arrays (pic/fields.f90:184-247,
+ * pic/smooth.f90:143-177; no reference counterpart for the choice):
+ * 0 = direct loads per cell, 1 = tiles staged in shared memory by tensor
+ * copies (TMA) in a persistent kernel per stage.  Both round every cell as
+ * em2 does (FP64: bitwise the same); only their speed differs. */
+int em2g_set_stencils(em2g_ctx *ctx, int mode);
+int em2g_get_stencils(em2g_ctx *ctx, int *mode);
 
 /* ---- instrumentation ------------------------------------------------- */
 /* kernel launches since the last reset; with timing on, the number of

@@ -233,6 +233,8 @@ int finish_outputs(em2g_ctx *c, double *ake_out, double *energies_out, int *cg_i
   EM2G_CUDA(cudaGetLastError());
   int rc = timing_collect(c);
   if (rc) return rc;
+  if (st[0] & 2)
+    return fail(EM2G_ERR_TIMEOUT, "a TMA-staged stencil's wait for its tiles timed out");
   if (st[0] != 0) return fail(EM2G_ERR_TIMEOUT, "cg: a grid barrier wait timed out");
   if (c->host_out[kDevLost] != 0.0) {
     const double lost = c->host_out[kDevLost];
@@ -324,14 +326,18 @@ int em2g_create(const em2g_params *p, em2g_ctx **out) {
     if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc " #ptr)); \
   } while (0)
   const bool fp32 = p->precision == EM2G_FP32;
+  // the field block and the smooth2 scratch carry a tail of a few rows, so
+  // that the TMA-staged stages' tensor maps (whole lines of 16 bytes' worth
+  // of rows) lie inside the allocations; the tail is zero and never used
+  const int64_t tail = tma_tail_elems(c, fp32);
   if (fp32) {
-    ALLOC(c->fld32, sizeof(float) * EM2G_NFIELD * w);
+    ALLOC(c->fld32, sizeof(float) * (EM2G_NFIELD * w + tail));
     ALLOC(c->scaled32, sizeof(float) * 6 * w * p->nsp);
-    ALLOC(c->smooth_tmp32, sizeof(float) * w);
+    ALLOC(c->smooth_tmp32, sizeof(float) * (w + tail));
   } else {
-    ALLOC(c->fld, sizeof(double) * EM2G_NFIELD * w);
+    ALLOC(c->fld, sizeof(double) * (EM2G_NFIELD * w + tail));
     ALLOC(c->scaled, sizeof(double) * 6 * w * p->nsp);
-    ALLOC(c->smooth_tmp, sizeof(double) * w);
+    ALLOC(c->smooth_tmp, sizeof(double) * (w + tail));
   }
   int64_t maxn = 0;
   for (int s = 0; s < p->nsp; ++s) {
@@ -357,14 +363,19 @@ int em2g_create(const em2g_params *p, em2g_ctx **out) {
 #undef ALLOC
   e = cudaMallocHost((void **)&c->host_out, sizeof(double) * kDevOut);
   if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMallocHost"));
-  if (fp32)
-    e = cudaMemset(c->fld32, 0, sizeof(float) * EM2G_NFIELD * w);
-  else
-    e = cudaMemset(c->fld, 0, sizeof(double) * EM2G_NFIELD * w);
+  if (fp32) {
+    e = cudaMemset(c->fld32, 0, sizeof(float) * (EM2G_NFIELD * w + tail));
+    if (e == cudaSuccess) e = cudaMemset(c->smooth_tmp32, 0, sizeof(float) * (w + tail));
+  } else {
+    e = cudaMemset(c->fld, 0, sizeof(double) * (EM2G_NFIELD * w + tail));
+    if (e == cudaSuccess) e = cudaMemset(c->smooth_tmp, 0, sizeof(double) * (w + tail));
+  }
   if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMemset"));
   e = cudaMemset(c->dev_out, 0, sizeof(double) * kDevOut);
   if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMemset"));
   rc = fp32 ? cg_init_f32(c) : cg_init(c);
+  if (rc) return bail(rc);
+  rc = fp32 ? tma_init_f32(c) : tma_init_f64(c);
   if (rc) return bail(rc);
   if (p->poisson == 1) {
     e = cudaMalloc((void **)&c->spec, sizeof(double2) * (int64_t)p->nx * p->ny);
@@ -952,6 +963,31 @@ int em2g_smooth2(em2g_ctx *c, int id) {
                   : smooth2_f64(c, c->fld + id * c->g.w);
   if (rc) return rc;
   EM2G_CUDA(cudaStreamSynchronize(c->stream));
+  if (c->stencils == 1) {  // a TMA-staged pass that timed out marks cg.status
+    int st = 0;
+    EM2G_CUDA(cudaMemcpy(&st, c->cg.status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (st & 2) {
+      EM2G_CUDA(cudaMemsetAsync(c->cg.status, 0, sizeof(int), c->stream));
+      return fail(EM2G_ERR_TIMEOUT, "a TMA-staged stencil's wait for its tiles timed out");
+    }
+  }
+  return EM2G_OK;
+}
+
+int em2g_set_stencils(em2g_ctx *c, int mode) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (mode != 0 && mode != 1) return fail(EM2G_ERR_INVALID, "stencils: 0 (direct) or 1 (TMA)");
+  if (mode == 1 && !c->tma_ok) return fail(EM2G_ERR_INVALID, "TMA-staged stencils unavailable");
+  c->stencils = mode;
+  return EM2G_OK;
+}
+
+int em2g_get_stencils(em2g_ctx *c, int *mode) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!mode) return fail(EM2G_ERR_INVALID, "null output");
+  *mode = c->stencils;
   return EM2G_OK;
 }
 

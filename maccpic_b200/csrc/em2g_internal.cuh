@@ -1,6 +1,7 @@
 // em2g_internal.cuh -- context layout and kernel entry points shared by the
 // translation units of libem2g.so.  Not part of the public ABI.
 #pragma once
+#include <cuda.h>  // CUtensorMap (the map is encoded through the runtime's driver entry point)
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <string>
@@ -127,6 +128,14 @@ struct em2g_ctx {
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t half_copied[2] = {nullptr, nullptr}, half_used[2] = {nullptr, nullptr};
   int64_t ncell = 0;
+  // TMA-staged Yee and smooth2 stages (tma_stencil.cuh): tensor maps over the
+  // field block and over the smooth2 scratch, the persistent grid of each
+  // stage kernel, and which implementation the field solve runs (0: direct
+  // loads, 1: TMA-staged tiles; em2g_set_stencils)
+  CUtensorMap tmap_fld, tmap_tmp;
+  bool tma_ok = false;
+  int tma_grid[4] = {0, 0, 0, 0};
+  int stencils = 0;
   int timing = 0;
   std::vector<cudaEvent_t> ev;  // start/stop pairs of the pending push launches
   size_t ev_used = 0;
@@ -180,6 +189,14 @@ int get_range_f32(em2g_ctx *c, int isp, int64_t first, int64_t count, double *co
 // particle of the largest species, at most 80 * 2^24 (1.3 GB)
 int64_t staging_cap(const em2g_ctx *c);
 int smooth2_f32(em2g_ctx *c, float *a);
+// tensor maps and launch shapes of the TMA-staged stages (fields_f32.cu,
+// fields_f64.cu); the field block and the smooth2 scratch must carry
+// tma_tail_elems() elements of tail
+int tma_init_f32(em2g_ctx *c);
+int tma_init_f64(em2g_ctx *c);
+inline int64_t tma_tail_elems(const em2g_ctx *c, bool fp32) {
+  return (int64_t)(fp32 ? 4 : 2) * c->g.nxg;  // 16 bytes' worth of rows
+}
 int cg_init_f32(em2g_ctx *c);
 int fields_f32(em2g_ctx *c, int it, bool want_energies);
 // em2g_diagnostics into dev_out[10..20) (diag.cu)

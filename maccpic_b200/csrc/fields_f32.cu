@@ -9,6 +9,8 @@ int smooth2_f32(em2g_ctx *c, float *a) { return grid::smooth2_t<float>(c, a, c->
 
 int cg_init_f32(em2g_ctx *c) { return grid::cg_init_t<float>(c); }
 
+int tma_init_f32(em2g_ctx *c) { return grid::tma_init_t<float>(c, c->fld32, c->smooth_tmp32); }
+
 int fields_f32(em2g_ctx *c, int it, bool want_energies) {
   return grid::fields_t<float>(c, c->fld32, c->smooth_tmp32, it, want_energies);
 }

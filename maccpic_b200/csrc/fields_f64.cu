@@ -14,6 +14,8 @@ int smooth2_f64(em2g_ctx *c, double *a) {
 
 int cg_init(em2g_ctx *c) { return grid::cg_init_t<double>(c); }
 
+int tma_init_f64(em2g_ctx *c) { return grid::tma_init_t<double>(c, c->fld, c->smooth_tmp); }
+
 void cg_free(em2g_ctx *c) {
   cudaFree(c->cg.u);
   cudaFree(c->cg.partial);

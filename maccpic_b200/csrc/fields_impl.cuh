@@ -2,7 +2,10 @@
 // and the Poisson solve, templated on the storage type of the field block
 // (double: fields_f64.cu; float: fields_f32.cu).
 #pragma once
+#include <mutex>
+
 #include "grid_kernels.cuh"
+#include "tma_stencil.cuh"
 
 namespace em2g {
 namespace grid {
@@ -13,8 +16,127 @@ inline G geom(const em2g_ctx *c) { return G{c->g.nx, c->g.ny, c->g.nxg, c->g.w};
 inline dim3 grid_for(int nxc, int nyc) { return dim3((nxc + TX - 1) / TX, (nyc + TY - 1) / TY); }
 
 template <typename T>
+T *field_block(em2g_ctx *c);
+template <>
+inline float *field_block<float>(em2g_ctx *c) { return c->fld32; }
+template <>
+inline double *field_block<double>(em2g_ctx *c) { return c->fld; }
+
+// ---- TMA-staged stages (tma_stencil.cuh)
+
+// cuTensorMapEncodeTiled, looked up once through the runtime
+using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                   const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                   const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+inline int encode_tiled_fn(EncodeTiledFn *out) {
+  static std::mutex mu;
+  static EncodeTiledFn fn = nullptr;
+  std::lock_guard<std::mutex> lock(mu);
+  if (!fn) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    EM2G_CUDA(cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000,
+                                               cudaEnableDefault, &q));
+    if (q != cudaDriverEntryPointSuccess || !p)
+      return fail(EM2G_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+    fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  *out = fn;
+  return EM2G_OK;
+}
+
+// A map over `rows` field rows of nxg elements from `base` (16-byte
+// aligned), M rows to a line; the allocation must reach the last line's end.
+template <typename T>
+int encode_lines(CUtensorMap *m, T *base, int nxg, int64_t rows) {
+  using Gm = tma::Geo<T>;
+  EncodeTiledFn fn = nullptr;
+  int rc = encode_tiled_fn(&fn);
+  if (rc) return rc;
+  if (reinterpret_cast<uintptr_t>(base) % 16 != 0)
+    return fail(EM2G_ERR_CUDA, "tensor map base not 16-byte aligned");
+  const cuuint64_t dim[2] = {(cuuint64_t)Gm::M * nxg, (cuuint64_t)((rows + Gm::M - 1) / Gm::M)};
+  const cuuint64_t stride[1] = {(cuuint64_t)Gm::M * nxg * sizeof(T)};
+  const cuuint32_t box[2] = {(cuuint32_t)Gm::BW, (cuuint32_t)Gm::BH};
+  const cuuint32_t estride[2] = {1, 1};
+  const CUresult r =
+      fn(m, sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2,
+         base, dim, stride, box, estride, CU_TENSOR_MAP_INTERLEAVE_NONE,
+         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS)
+    return fail(EM2G_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+  return EM2G_OK;
+}
+
+template <typename T, int S>
+int tma_prepare_stage(em2g_ctx *c) {
+  constexpr int bytes = tma::smem_bytes<T, S>();
+  EM2G_CUDA(cudaFuncSetAttribute(tma::k_tma_stage<T, S>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  int per_sm = 0;
+  EM2G_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tma::k_tma_stage<T, S>,
+                                                          tma::Geo<T>::THREADS, bytes));
+  if (per_sm < 1) return fail(EM2G_ERR_CUDA, "TMA stage kernel cannot be resident");
+  c->tma_grid[S] = per_sm * c->num_sms;
+  return EM2G_OK;
+}
+
+// maps over the field block (13 arrays) and the smooth2 scratch (one), and
+// the stage kernels' persistent grids
+template <typename T>
+int tma_init_t(em2g_ctx *c, T *fld, T *tmp) {
+  const G g = geom(c);
+  int rc = encode_lines<T>(&c->tmap_fld, fld, g.nxg, (int64_t)EM2G_NFIELD * (g.ny + 3));
+  if (!rc) rc = encode_lines<T>(&c->tmap_tmp, tmp, g.nxg, (int64_t)(g.ny + 3));
+  if (!rc) rc = tma_prepare_stage<T, tma::kBHalf>(c);
+  if (!rc) rc = tma_prepare_stage<T, tma::kEFull>(c);
+  if (!rc) rc = tma_prepare_stage<T, tma::kBinomial>(c);
+  if (!rc) rc = tma_prepare_stage<T, tma::kCompensate>(c);
+  if (rc) return rc;
+  c->tma_ok = true;
+  return EM2G_OK;
+}
+
+template <typename T, int S>
+int tma_launch(em2g_ctx *c, const CUtensorMap &map, const int *row0, T *o0, T *o1, T *o2, T c0,
+               T c1, T c2) {
+  using Gm = tma::Geo<T>;
+  tma::Args<T> a;
+  a.g = geom(c);
+  a.ntx = (a.g.nx + 1 + Gm::TXO - 1) / Gm::TXO;
+  a.nty = (a.g.ny + 1 + Gm::TYO - 1) / Gm::TYO;
+  a.ntiles = a.ntx * a.nty;
+  for (int k = 0; k < tma::kMaxStaged; ++k) a.row0[k] = k < tma::Staged<S>::N ? row0[k] : 0;
+  a.out[0] = o0;
+  a.out[1] = o1;
+  a.out[2] = o2;
+  a.c0 = c0;
+  a.c1 = c1;
+  a.c2 = c2;
+  a.status = c->cg.status;
+  const int grid = a.ntiles < c->tma_grid[S] ? a.ntiles : c->tma_grid[S];
+  tma::k_tma_stage<T, S><<<grid, Gm::THREADS, tma::smem_bytes<T, S>(), c->stream>>>(map, a);
+  c->launches += 1;
+  EM2G_CUDA(cudaGetLastError());
+  return EM2G_OK;
+}
+
+template <typename T>
 int smooth2_t(em2g_ctx *c, T *a, T *tmp) {
   const G g = geom(c);
+  if (c->stencils == 1) {
+    // a is one of the field block's arrays: its row 0 in the block's map
+    const int64_t k = (a - field_block<T>(c)) / g.w;
+    const int src_row0 = (int)(k * (g.ny + 3)), tmp_row0 = 0;
+    int rc = tma_launch<T, tma::kBinomial>(c, c->tmap_fld, &src_row0, tmp, nullptr, nullptr, T(0),
+                                           T(0), T(0));
+    if (!rc)
+      rc = tma_launch<T, tma::kCompensate>(c, c->tmap_tmp, &tmp_row0, a, nullptr, nullptr, T(0),
+                                           T(0), T(0));
+    return rc;
+  }
   const dim3 grd = grid_for(g.nx + 1, g.ny + 1), blk(TX, TY);
   k_smooth_binomial<T><<<grd, blk, 0, c->stream>>>(g, a, tmp);
   k_smooth_compensate<T><<<grd, blk, 0, c->stream>>>(g, tmp, a);
@@ -130,12 +252,30 @@ int fields_t(em2g_ctx *c, T *fld, T *tmp, int it, bool want_energies) {
   // Yee (pic/fields.f90:184-247)
   const double ctx = c->P.dt * c->P.c / c->P.dx, cty = c->P.dt * c->P.c / c->P.dy;
   const double ctxh = ctx * 0.5, ctyh = cty * 0.5, tem = 0.5 * c->P.dt;
-  const dim3 grd = grid_for(g.nx + 1, g.ny + 1);
-  k_b_half<T><<<grd, blk, 0, c->stream>>>(g, fld, (T)ctxh, (T)ctyh);
-  k_e_full<T><<<grd, blk, 0, c->stream>>>(g, fld, (T)ctx, (T)cty, (T)tem);
-  k_b_half<T><<<grd, blk, 0, c->stream>>>(g, fld, (T)ctxh, (T)ctyh);
-  c->launches += 3;
-  EM2G_CUDA(cudaGetLastError());
+  if (c->stencils == 1) {
+    // staged arrays' rows in the block's map, in the stage kernels' order
+    const int rows = g.ny + 3;
+    const int bh[6] = {EM2G_EX * rows, EM2G_EY * rows, EM2G_EZ * rows,
+                       EM2G_BX * rows, EM2G_BY * rows, EM2G_BZ * rows};
+    const int ef[12] = {EM2G_BX * rows,  EM2G_BY * rows,  EM2G_BZ * rows,  EM2G_EX * rows,
+                        EM2G_EY * rows,  EM2G_EZ * rows,  EM2G_JXM * rows, EM2G_JXP * rows,
+                        EM2G_JYM * rows, EM2G_JYP * rows, EM2G_JZM * rows, EM2G_JZP * rows};
+    T *bx = fld + EM2G_BX * g.w, *by = fld + EM2G_BY * g.w, *bz = fld + EM2G_BZ * g.w;
+    T *ex = fld + EM2G_EX * g.w, *ey = fld + EM2G_EY * g.w, *ez = fld + EM2G_EZ * g.w;
+    int rc = tma_launch<T, tma::kBHalf>(c, c->tmap_fld, bh, bx, by, bz, (T)ctxh, (T)ctyh, T(0));
+    if (!rc)
+      rc = tma_launch<T, tma::kEFull>(c, c->tmap_fld, ef, ex, ey, ez, (T)ctx, (T)cty, (T)tem);
+    if (!rc)
+      rc = tma_launch<T, tma::kBHalf>(c, c->tmap_fld, bh, bx, by, bz, (T)ctxh, (T)ctyh, T(0));
+    if (rc) return rc;
+  } else {
+    const dim3 grd = grid_for(g.nx + 1, g.ny + 1);
+    k_b_half<T><<<grd, blk, 0, c->stream>>>(g, fld, (T)ctxh, (T)ctyh);
+    k_e_full<T><<<grd, blk, 0, c->stream>>>(g, fld, (T)ctx, (T)cty, (T)tem);
+    k_b_half<T><<<grd, blk, 0, c->stream>>>(g, fld, (T)ctxh, (T)ctyh);
+    c->launches += 3;
+    EM2G_CUDA(cudaGetLastError());
+  }
   // filters (pic/fields.f90:252-260)
   int rc = smooth2_t<T>(c, fld + EM2G_RHO * g.w, tmp);
   if (rc) return rc;

@@ -99,6 +99,41 @@ __global__ void k_fold_y(G g, T *fld) {
 // The cell stages take the cell (ix, iy); the *_at forms take a 32x8 tile
 // (tbx, tby) whose cell is given by the thread index.
 
+// ---- the stencils' arithmetic on loaded values.  Every implementation of
+// a stage (direct loads here, the TMA-staged tiles of tma_stencil.cuh, the
+// ensemble's kernels) calls these, so each rounds a cell as em2 does, in
+// the same order.  Suffixes name neighbours: _w (ix-1), _e (ix+1), _s
+// (iy-1), _n (iy+1).
+// pic/fields.f90:188-190
+template <typename T>
+__device__ __forceinline__ void b_half_vals(T bx, T by, T bz, T ezc, T ez_s, T ez_w, T ey_e,
+                                            T eyc, T ex_n, T exc, T ctxh, T ctyh, T &vbx,
+                                            T &vby, T &vbz) {
+  vbx = bx - ctyh * (ezc - ez_s);
+  vby = by + ctxh * (ezc - ez_w);
+  vbz = bz - ctxh * (ey_e - eyc) + ctyh * (ex_n - exc);
+}
+// pic/fields.f90:211-215
+template <typename T>
+__device__ __forceinline__ void e_full_vals(T ex, T ey, T ez, T bzc, T bz_s, T bz_w, T by_e,
+                                            T byc, T bx_n, T bxc, T jxm, T jxp, T jym, T jyp,
+                                            T jzm, T jzp, T ctx, T cty, T tem, T &vex, T &vey,
+                                            T &vez) {
+  vex = ex + cty * (bzc - bz_s) - tem * (jxm + jxp);
+  vey = ey - ctx * (bzc - bz_w) - tem * (jym + jyp);
+  vez = ez + ctx * (by_e - byc) - cty * (bx_n - bxc) - tem * (jzm + jzp);
+}
+// pic/smooth.f90:145-146 (c: the cell; then w, e, s, n; then sw, nw, se, ne)
+template <typename T>
+__device__ __forceinline__ T binomial_val(T c, T w, T e, T s, T n, T sw, T nw, T se, T ne) {
+  return (4 * c + 2 * (w + e + s + n) + sw + nw + se + ne) / T(16.0);
+}
+// pic/smooth.f90:163-164 (same order)
+template <typename T>
+__device__ __forceinline__ T compensate_val(T c, T w, T e, T s, T n, T sw, T nw, T se, T ne) {
+  return (20 * c - w - e - s - n - sw - nw - se - ne) / T(12.0);
+}
+
 // ---- Yee half step of B (pic/fields.f90:184-200, :231-247)
 template <typename T, typename L = LdPlain>
 __device__ __forceinline__ void b_half_cell(const G &g, T *fld, T ctxh, T ctyh, int ix, int iy) {
@@ -106,11 +141,10 @@ __device__ __forceinline__ void b_half_cell(const G &g, T *fld, T ctxh, T ctyh, 
   const T *ex = fld + EM2G_EX * g.w, *ey = fld + EM2G_EY * g.w, *ez = fld + EM2G_EZ * g.w;
   T *bx = fld + EM2G_BX * g.w, *by = fld + EM2G_BY * g.w, *bz = fld + EM2G_BZ * g.w;
   const int64_t c = at(g, ix, iy);
-  const T ezc = L::ld(ez + c);
-  const T vbx = L::ld(bx + c) - ctyh * (ezc - L::ld(ez + c - g.nxg));
-  const T vby = L::ld(by + c) + ctxh * (ezc - L::ld(ez + c - 1));
-  const T vbz = L::ld(bz + c) - ctxh * (L::ld(ey + c + 1) - L::ld(ey + c)) +
-                ctyh * (L::ld(ex + c + g.nxg) - L::ld(ex + c));
+  T vbx, vby, vbz;
+  b_half_vals(L::ld(bx + c), L::ld(by + c), L::ld(bz + c), L::ld(ez + c), L::ld(ez + c - g.nxg),
+              L::ld(ez + c - 1), L::ld(ey + c + 1), L::ld(ey + c), L::ld(ex + c + g.nxg),
+              L::ld(ex + c), ctxh, ctyh, vbx, vby, vbz);
   store_with_guards(g, bx, ix, iy, vbx);
   store_with_guards(g, by, ix, iy, vby);
   store_with_guards(g, bz, ix, iy, vbz);
@@ -135,14 +169,11 @@ __device__ __forceinline__ void e_full_cell(const G &g, T *fld, T ctx, T cty, T 
           *jym = fld + EM2G_JYM * g.w, *jyp = fld + EM2G_JYP * g.w,
           *jzm = fld + EM2G_JZM * g.w, *jzp = fld + EM2G_JZP * g.w;
   const int64_t c = at(g, ix, iy);
-  const T bzc = L::ld(bz + c);
-  const T vex = L::ld(ex + c) + cty * (bzc - L::ld(bz + c - g.nxg)) -
-                tem * (L::ld(jxm + c) + L::ld(jxp + c));
-  const T vey = L::ld(ey + c) - ctx * (bzc - L::ld(bz + c - 1)) -
-                tem * (L::ld(jym + c) + L::ld(jyp + c));
-  const T vez = L::ld(ez + c) + ctx * (L::ld(by + c + 1) - L::ld(by + c)) -
-                cty * (L::ld(bx + c + g.nxg) - L::ld(bx + c)) -
-                tem * (L::ld(jzm + c) + L::ld(jzp + c));
+  T vex, vey, vez;
+  e_full_vals(L::ld(ex + c), L::ld(ey + c), L::ld(ez + c), L::ld(bz + c), L::ld(bz + c - g.nxg),
+              L::ld(bz + c - 1), L::ld(by + c + 1), L::ld(by + c), L::ld(bx + c + g.nxg),
+              L::ld(bx + c), L::ld(jxm + c), L::ld(jxp + c), L::ld(jym + c), L::ld(jyp + c),
+              L::ld(jzm + c), L::ld(jzp + c), ctx, cty, tem, vex, vey, vez);
   store_with_guards(g, ex, ix, iy, vex);
   store_with_guards(g, ey, ix, iy, vey);
   store_with_guards(g, ez, ix, iy, vez);
@@ -165,11 +196,9 @@ __device__ __forceinline__ void smooth_binomial_cell(const G &g, const T *__rest
                                                      int ix, int iy) {
   if (ix > g.nx + 1 || iy > g.ny + 1) return;
   const int64_t c = at(g, ix, iy), n = g.nxg;
-  const T v = (4 * L::ld(s + c) +
-               2 * (L::ld(s + c - 1) + L::ld(s + c + 1) + L::ld(s + c - n) + L::ld(s + c + n)) +
-               L::ld(s + c - 1 - n) + L::ld(s + c - 1 + n) + L::ld(s + c + 1 - n) +
-               L::ld(s + c + 1 + n)) /
-              T(16.0);
+  const T v = binomial_val(L::ld(s + c), L::ld(s + c - 1), L::ld(s + c + 1), L::ld(s + c - n),
+                           L::ld(s + c + n), L::ld(s + c - 1 - n), L::ld(s + c - 1 + n),
+                           L::ld(s + c + 1 - n), L::ld(s + c + 1 + n));
   store_with_guards(g, d, ix, iy, v);
 }
 template <typename T>
@@ -186,10 +215,9 @@ __device__ __forceinline__ void smooth_compensate_cell(const G &g, const T *__re
                                                        int ix, int iy) {
   if (ix > g.nx + 1 || iy > g.ny + 1) return;
   const int64_t c = at(g, ix, iy), n = g.nxg;
-  const T v = (20 * L::ld(d + c) - L::ld(d + c - 1) - L::ld(d + c + 1) - L::ld(d + c - n) -
-               L::ld(d + c + n) - L::ld(d + c - 1 - n) - L::ld(d + c - 1 + n) -
-               L::ld(d + c + 1 - n) - L::ld(d + c + 1 + n)) /
-              T(12.0);
+  const T v = compensate_val(L::ld(d + c), L::ld(d + c - 1), L::ld(d + c + 1), L::ld(d + c - n),
+                             L::ld(d + c + n), L::ld(d + c - 1 - n), L::ld(d + c - 1 + n),
+                             L::ld(d + c + 1 - n), L::ld(d + c + 1 + n));
   store_with_guards(g, s, ix, iy, v);
 }
 template <typename T>

@@ -258,6 +258,17 @@ class Em2Gpu:
         check(self._L.em2g_set_sort_interval(self._h, int(k)))
         self.p.sort_interval = int(k)
 
+    def set_stencils(self, mode: int) -> None:
+        """How the Yee updates and smooth2 passes read their arrays: 0 direct
+        loads per cell, 1 tiles staged in shared memory by tensor copies.
+        The results are the same; only the speed differs."""
+        check(self._L.em2g_set_stencils(self._h, int(mode)))
+
+    def stencils(self) -> int:
+        m = C.c_int(0)
+        check(self._L.em2g_get_stencils(self._h, C.byref(m)))
+        return m.value
+
     def max_sort_interval(self) -> int:
         """The largest interval the drift bound allows (1 for FP64)."""
         if self.p.precision != _lib.FP32:
