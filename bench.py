@@ -72,6 +72,9 @@ def parse():
                     help="run only the ensemble leg and print its JSON (with --variant and "
                          "--sort-interval: those, without the autotuner)")
     # the 512x256 workload's adjoint: 800 steps, checkpoints every 50
+    ap.add_argument("--stencils", type=int, choices=[0, 1], default=0,
+                    help="Yee and smooth2 stages: 0 direct loads (the faster at every "
+                         "measured size, the default), 1 TMA-staged tiles")
     ap.add_argument("--adjoint-steps", type=int, default=800)
     ap.add_argument("--adjoint-checkpoint", type=int, default=50)
     return ap.parse_args()
@@ -429,6 +432,7 @@ def measure(args, cfg, precision, local, src, fields, stream, ws):
     torch.cuda.empty_cache()
     g = Em2Gpu(rp)
     g.set_stream(stream)
+    g.set_stencils(args.stencils)
     g.set_fields(fields)
     src.load(g)
     torch.cuda.synchronize()
@@ -567,6 +571,7 @@ def run_ours(args):
                        "precision": ("mixed: FP32 push/deposit/Yee, FP64 reductions"
                                      if fp32 else "FP64 (em2's arithmetic)"),
                        "path": "em2g_step (fused push, cell-sorted)",
+                       "stencils": "TMA-staged tiles" if args.stencils else "direct loads",
                        "l2": f"inputs larger than L2 (particle state "
                              f"{n_total * per_particle / 2 / 1e9:.1f} GB)",
                        "parallelism": (f"particle decomposition x{ws} (grid replicated, "

@@ -129,12 +129,10 @@ struct em2g_ctx {
   cudaEvent_t half_copied[2] = {nullptr, nullptr}, half_used[2] = {nullptr, nullptr};
   int64_t ncell = 0;
   // TMA-staged Yee and smooth2 stages (tma_stencil.cuh): tensor maps over the
-  // field block and over the smooth2 scratch, the persistent grid of each
-  // stage kernel, and which implementation the field solve runs (0: direct
-  // loads, 1: TMA-staged tiles; em2g_set_stencils)
+  // field block and over the smooth2 scratch, and which implementation the
+  // field solve runs (0: direct loads, 1: TMA-staged tiles; em2g_set_stencils)
   CUtensorMap tmap_fld, tmap_tmp;
   bool tma_ok = false;
-  int tma_grid[4] = {0, 0, 0, 0};
   int stencils = 0;
   int timing = 0;
   std::vector<cudaEvent_t> ev;  // start/stop pairs of the pending push launches

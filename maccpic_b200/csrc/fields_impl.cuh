@@ -79,12 +79,11 @@ int tma_prepare_stage(em2g_ctx *c) {
   EM2G_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tma::k_tma_stage<T, S>,
                                                           tma::Geo<T>::THREADS, bytes));
   if (per_sm < 1) return fail(EM2G_ERR_CUDA, "TMA stage kernel cannot be resident");
-  c->tma_grid[S] = per_sm * c->num_sms;
   return EM2G_OK;
 }
 
 // maps over the field block (13 arrays) and the smooth2 scratch (one), and
-// the stage kernels' persistent grids
+// the stage kernels' shared-memory sizes
 template <typename T>
 int tma_init_t(em2g_ctx *c, T *fld, T *tmp) {
   const G g = geom(c);
@@ -100,15 +99,16 @@ int tma_init_t(em2g_ctx *c, T *fld, T *tmp) {
 }
 
 template <typename T, int S>
-int tma_launch(em2g_ctx *c, const CUtensorMap &map, const int *row0, T *o0, T *o1, T *o2, T c0,
-               T c1, T c2) {
+int tma_launch(em2g_ctx *c, const CUtensorMap &map, const int *row0, const T *const *in, int nin,
+               T *o0, T *o1, T *o2, T c0, T c1, T c2) {
   using Gm = tma::Geo<T>;
   tma::Args<T> a;
   a.g = geom(c);
   a.ntx = (a.g.nx + 1 + Gm::TXO - 1) / Gm::TXO;
   a.nty = (a.g.ny + 1 + Gm::TYO - 1) / Gm::TYO;
   a.ntiles = a.ntx * a.nty;
-  for (int k = 0; k < tma::kMaxStaged; ++k) a.row0[k] = k < tma::Staged<S>::N ? row0[k] : 0;
+  for (int k = 0; k < tma::kStaged; ++k) a.row0[k] = k < tma::Staged<S>::N ? row0[k] : 0;
+  for (int k = 0; k < 9; ++k) a.in[k] = k < nin ? in[k] : nullptr;
   a.out[0] = o0;
   a.out[1] = o1;
   a.out[2] = o2;
@@ -116,8 +116,7 @@ int tma_launch(em2g_ctx *c, const CUtensorMap &map, const int *row0, T *o0, T *o
   a.c1 = c1;
   a.c2 = c2;
   a.status = c->cg.status;
-  const int grid = a.ntiles < c->tma_grid[S] ? a.ntiles : c->tma_grid[S];
-  tma::k_tma_stage<T, S><<<grid, Gm::THREADS, tma::smem_bytes<T, S>(), c->stream>>>(map, a);
+  tma::k_tma_stage<T, S><<<a.ntiles, Gm::THREADS, tma::smem_bytes<T, S>(), c->stream>>>(map, a);
   c->launches += 1;
   EM2G_CUDA(cudaGetLastError());
   return EM2G_OK;
@@ -130,11 +129,11 @@ int smooth2_t(em2g_ctx *c, T *a, T *tmp) {
     // a is one of the field block's arrays: its row 0 in the block's map
     const int64_t k = (a - field_block<T>(c)) / g.w;
     const int src_row0 = (int)(k * (g.ny + 3)), tmp_row0 = 0;
-    int rc = tma_launch<T, tma::kBinomial>(c, c->tmap_fld, &src_row0, tmp, nullptr, nullptr, T(0),
-                                           T(0), T(0));
+    int rc = tma_launch<T, tma::kBinomial>(c, c->tmap_fld, &src_row0, nullptr, 0, tmp, nullptr,
+                                           nullptr, T(0), T(0), T(0));
     if (!rc)
-      rc = tma_launch<T, tma::kCompensate>(c, c->tmap_tmp, &tmp_row0, a, nullptr, nullptr, T(0),
-                                           T(0), T(0));
+      rc = tma_launch<T, tma::kCompensate>(c, c->tmap_tmp, &tmp_row0, nullptr, 0, a, nullptr,
+                                           nullptr, T(0), T(0), T(0));
     return rc;
   }
   const dim3 grd = grid_for(g.nx + 1, g.ny + 1), blk(TX, TY);
@@ -253,20 +252,25 @@ int fields_t(em2g_ctx *c, T *fld, T *tmp, int it, bool want_energies) {
   const double ctx = c->P.dt * c->P.c / c->P.dx, cty = c->P.dt * c->P.c / c->P.dy;
   const double ctxh = ctx * 0.5, ctyh = cty * 0.5, tem = 0.5 * c->P.dt;
   if (c->stencils == 1) {
-    // staged arrays' rows in the block's map, in the stage kernels' order
+    // staged arrays' rows in the block's map (E for B/2, B for E), and the
+    // arrays read at the cell, in the stage kernels' order
     const int rows = g.ny + 3;
-    const int bh[6] = {EM2G_EX * rows, EM2G_EY * rows, EM2G_EZ * rows,
-                       EM2G_BX * rows, EM2G_BY * rows, EM2G_BZ * rows};
-    const int ef[12] = {EM2G_BX * rows,  EM2G_BY * rows,  EM2G_BZ * rows,  EM2G_EX * rows,
-                        EM2G_EY * rows,  EM2G_EZ * rows,  EM2G_JXM * rows, EM2G_JXP * rows,
-                        EM2G_JYM * rows, EM2G_JYP * rows, EM2G_JZM * rows, EM2G_JZP * rows};
+    const int e_rows[3] = {EM2G_EX * rows, EM2G_EY * rows, EM2G_EZ * rows};
+    const int b_rows[3] = {EM2G_BX * rows, EM2G_BY * rows, EM2G_BZ * rows};
     T *bx = fld + EM2G_BX * g.w, *by = fld + EM2G_BY * g.w, *bz = fld + EM2G_BZ * g.w;
     T *ex = fld + EM2G_EX * g.w, *ey = fld + EM2G_EY * g.w, *ez = fld + EM2G_EZ * g.w;
-    int rc = tma_launch<T, tma::kBHalf>(c, c->tmap_fld, bh, bx, by, bz, (T)ctxh, (T)ctyh, T(0));
+    const T *b_in[3] = {bx, by, bz};
+    const T *e_in[9] = {ex, ey, ez, fld + EM2G_JXM * g.w, fld + EM2G_JXP * g.w,
+                        fld + EM2G_JYM * g.w, fld + EM2G_JYP * g.w, fld + EM2G_JZM * g.w,
+                        fld + EM2G_JZP * g.w};
+    int rc = tma_launch<T, tma::kBHalf>(c, c->tmap_fld, e_rows, b_in, 3, bx, by, bz, (T)ctxh,
+                                        (T)ctyh, T(0));
     if (!rc)
-      rc = tma_launch<T, tma::kEFull>(c, c->tmap_fld, ef, ex, ey, ez, (T)ctx, (T)cty, (T)tem);
+      rc = tma_launch<T, tma::kEFull>(c, c->tmap_fld, b_rows, e_in, 9, ex, ey, ez, (T)ctx, (T)cty,
+                                      (T)tem);
     if (!rc)
-      rc = tma_launch<T, tma::kBHalf>(c, c->tmap_fld, bh, bx, by, bz, (T)ctxh, (T)ctyh, T(0));
+      rc = tma_launch<T, tma::kBHalf>(c, c->tmap_fld, e_rows, b_in, 3, bx, by, bz, (T)ctxh,
+                                      (T)ctyh, T(0));
     if (rc) return rc;
   } else {
     const dim3 grd = grid_for(g.nx + 1, g.ny + 1);

@@ -1,9 +1,9 @@
 // tma_stencil.cuh -- em2's Yee updates and smooth2 passes (pic/fields.f90:
-// 184-247, pic/smooth.f90:143-177) as TMA-staged tiles: a persistent CTA per
-// SM walks the grid's tiles, each tile's input arrays (with a one-cell halo)
-// brought into shared memory by tensor copies on an mbarrier while the CTA
-// computes the tile before it (two stages).  The arithmetic is grid_kernels'
-// value functions, so every cell rounds as the direct-load kernels round it.
+// 184-247, pic/smooth.f90:143-177) as TMA-staged tiles: a CTA per tile, the
+// arrays a stage reads at neighbouring cells brought into shared memory with
+// a one-cell halo by tensor copies on an mbarrier.  The arithmetic is
+// grid_kernels' value functions, so every cell rounds as the direct-load
+// kernels round it.
 //
 // The layout at the ABI is em2's: rows of (nx+3) elements, so a row starts on
 // any 4- or 8-byte boundary, and a tensor map's row stride must be a multiple
@@ -19,7 +19,7 @@
 // zero-filled by the copy and never read.
 //
 // The map covers the block rounded up to whole lines, so the allocations
-// behind it carry a tail of M rows (tail_elems).
+// behind it carry a tail of M rows (em2g_internal.cuh, tma_tail_elems).
 #pragma once
 #include <cuda.h>
 
@@ -29,6 +29,8 @@ namespace em2g {
 namespace tma {
 namespace {
 
+// Tiles of TXO x TYO cells, 256 threads (RT rows of TXO), each thread
+// ROWS cells of one column.
 template <typename T>
 struct Geo {
   static constexpr int M = 16 / (int)sizeof(T);  // field rows per line
@@ -36,6 +38,7 @@ struct Geo {
   static constexpr int TYO = 16;                         // output rows per tile
   static constexpr int THREADS = 256;
   static constexpr int RT = THREADS / TXO;  // rows of threads
+  static constexpr int ROWS = TYO / RT;      // cells per thread
   static constexpr int HR = TYO + 2;        // staged rows: iy0-1 .. iy0+TYO
   static constexpr int BH = (HR + M - 1) / M;  // box rows (lines)
   // box columns: ix0-1 .. ix0+TXO plus up to M-1 of alignment shift
@@ -49,27 +52,27 @@ struct Geo {
   static_assert(TYO % RT == 0, "rows of threads divide the tile");
 };
 
-// elements of tail an allocation needs behind a block of arrays for the map
-template <typename T>
-inline int64_t tail_elems(int nxg) { return (int64_t)Geo<T>::M * nxg; }
-
 enum Stage { kBHalf = 0, kEFull = 1, kBinomial = 2, kCompensate = 3 };
-constexpr int kMaxStaged = 12;
-// staged arrays per stage: B/2: ex ey ez (halo), bx by bz; E: bx by bz
-// (halo), ex ey ez, jxm jxp jym jyp jzm jzp; smooth2 passes: the source
+// Only the arrays a stage reads at neighbouring cells go through shared
+// memory: E for B/2 (pic/fields.f90:188-190), B for E (:211-215), the source
+// of a smooth2 pass.  The arrays read at the cell itself are loaded directly
+// (one coalesced load per cell, no reuse to stage).
+constexpr int kStaged = 3;
 template <int S>
 struct Staged {
-  static constexpr int N = S == kBHalf ? 6 : (S == kEFull ? 12 : 1);
+  static constexpr int N = (S == kBHalf || S == kEFull) ? 3 : 1;
+  static constexpr int NIN = S == kBHalf ? 3 : (S == kEFull ? 9 : 1);  // read at the cell
 };
 
 template <typename T>
 struct Args {
   grid::G g;
   int ntx, nty, ntiles;
-  int row0[kMaxStaged];  // each staged array's row 0 in the map's rows
-  T *out[3];             // arrays written (with em2's guard copies)
-  T c0, c1, c2;          // B/2: ctxh, ctyh; E: ctx, cty, tem
-  int *status;           // bit 1 set when a wait for a tile timed out
+  int row0[kStaged];  // each staged array's row 0 in the map's rows
+  const T *in[9];     // arrays read at the cell: B/2: bx by bz; E: ex ey ez jxm jxp jym jyp jzm jzp
+  T *out[3];          // arrays written (with em2's guard copies)
+  T c0, c1, c2;       // B/2: ctxh, ctyh; E: ctx, cty, tem
+  int *status;        // bit 1 set when a wait for a tile timed out
 };
 
 __device__ __forceinline__ unsigned smem_u32(const void *p) {
@@ -159,8 +162,30 @@ __device__ __forceinline__ const T *staged_row(const unsigned char *buf, int arr
   return reinterpret_cast<const T *>(buf + (arr * Gm::M + j) * Gm::SLOT) + tr * Gm::BW + sh;
 }
 
+// The arrays a stage reads at its cells, loaded before the tile's boxes
+// land: cell value q of this thread's column (row tyl + q RT of the tile).
 template <typename T, int S>
-__device__ __forceinline__ void compute_tile(const Args<T> &a, int t, const unsigned char *buf) {
+__device__ __forceinline__ void load_cells(const Args<T> &a, int t,
+                                           T (&cv)[Staged<S>::NIN][Geo<T>::ROWS]) {
+  using Gm = Geo<T>;
+  int ix0, iy0;
+  tile_origin(a, t, ix0, iy0);
+  const int txl = threadIdx.x % Gm::TXO, tyl = threadIdx.x / Gm::TXO;
+  const int ix = ix0 + txl;
+#pragma unroll
+  for (int q = 0; q < Gm::ROWS; ++q) {
+    const int iy = iy0 + tyl + q * Gm::RT;
+    const bool in = ix <= a.g.nx + 1 && iy <= a.g.ny + 1;
+    const int64_t c = grid::at(a.g, in ? ix : 1, in ? iy : 1);
+#pragma unroll
+    for (int k = 0; k < Staged<S>::NIN; ++k)
+      if constexpr (S == kBHalf || S == kEFull) cv[k][q] = a.in[k][c];
+  }
+}
+
+template <typename T, int S>
+__device__ __forceinline__ void compute_tile(const Args<T> &a, int t, const unsigned char *buf,
+                                             const T (&cv)[Staged<S>::NIN][Geo<T>::ROWS]) {
   using Gm = Geo<T>;
   constexpr int N = Staged<S>::N;
   int ix0, iy0;
@@ -173,40 +198,33 @@ __device__ __forceinline__ void compute_tile(const Args<T> &a, int t, const unsi
   const int ix = ix0 + txl, dx = txl + 1;
   if (ix > a.g.nx + 1) return;
 #pragma unroll
-  for (int q = 0; q < Gm::TYO / Gm::RT; ++q) {
+  for (int q = 0; q < Gm::ROWS; ++q) {
     const int oy = tyl + q * Gm::RT, iy = iy0 + oy, dy = oy + 1;
     if (iy > a.g.ny + 1) break;
     if constexpr (S == kBHalf) {
-      // staged: 0 ex, 1 ey, 2 ez, 3 bx, 4 by, 5 bz
+      // staged: 0 ex, 1 ey, 2 ez; at the cell: bx, by, bz
       const T *exc = staged_row<T>(buf, 0, dy, rb[0], nxg);
       const T *exn = staged_row<T>(buf, 0, dy + 1, rb[0], nxg);
       const T *eyc = staged_row<T>(buf, 1, dy, rb[1], nxg);
       const T *ezc = staged_row<T>(buf, 2, dy, rb[2], nxg);
       const T *ezs = staged_row<T>(buf, 2, dy - 1, rb[2], nxg);
-      const T *bxc = staged_row<T>(buf, 3, dy, rb[3], nxg);
-      const T *byc = staged_row<T>(buf, 4, dy, rb[4], nxg);
-      const T *bzc = staged_row<T>(buf, 5, dy, rb[5], nxg);
       T vbx, vby, vbz;
-      grid::b_half_vals(bxc[dx], byc[dx], bzc[dx], ezc[dx], ezs[dx], ezc[dx - 1], eyc[dx + 1],
+      grid::b_half_vals(cv[0][q], cv[1][q], cv[2][q], ezc[dx], ezs[dx], ezc[dx - 1], eyc[dx + 1],
                         eyc[dx], exn[dx], exc[dx], a.c0, a.c1, vbx, vby, vbz);
       grid::store_with_guards(a.g, a.out[0], ix, iy, vbx);
       grid::store_with_guards(a.g, a.out[1], ix, iy, vby);
       grid::store_with_guards(a.g, a.out[2], ix, iy, vbz);
     } else if constexpr (S == kEFull) {
-      // staged: 0 bx, 1 by, 2 bz, 3 ex, 4 ey, 5 ez, 6 jxm, 7 jxp, 8 jym, 9 jyp,
-      // 10 jzm, 11 jzp
+      // staged: 0 bx, 1 by, 2 bz; at the cell: ex ey ez jxm jxp jym jyp jzm jzp
       const T *bxc = staged_row<T>(buf, 0, dy, rb[0], nxg);
       const T *bxn = staged_row<T>(buf, 0, dy + 1, rb[0], nxg);
       const T *byc = staged_row<T>(buf, 1, dy, rb[1], nxg);
       const T *bzc = staged_row<T>(buf, 2, dy, rb[2], nxg);
       const T *bzs = staged_row<T>(buf, 2, dy - 1, rb[2], nxg);
-      T v[9];
-#pragma unroll
-      for (int k = 0; k < 9; ++k) v[k] = staged_row<T>(buf, 3 + k, dy, rb[3 + k], nxg)[dx];
       T vex, vey, vez;
-      grid::e_full_vals(v[0], v[1], v[2], bzc[dx], bzs[dx], bzc[dx - 1], byc[dx + 1], byc[dx],
-                        bxn[dx], bxc[dx], v[3], v[4], v[5], v[6], v[7], v[8], a.c0, a.c1, a.c2,
-                        vex, vey, vez);
+      grid::e_full_vals(cv[0][q], cv[1][q], cv[2][q], bzc[dx], bzs[dx], bzc[dx - 1], byc[dx + 1],
+                        byc[dx], bxn[dx], bxc[dx], cv[3][q], cv[4][q], cv[5][q], cv[6][q],
+                        cv[7][q], cv[8][q], a.c0, a.c1, a.c2, vex, vey, vez);
       grid::store_with_guards(a.g, a.out[0], ix, iy, vex);
       grid::store_with_guards(a.g, a.out[1], ix, iy, vey);
       grid::store_with_guards(a.g, a.out[2], ix, iy, vez);
@@ -226,51 +244,40 @@ __device__ __forceinline__ void compute_tile(const Args<T> &a, int t, const unsi
   }
 }
 
-// smem per CTA: two stage buffers and two mbarriers
+// shared memory per CTA: the staged boxes and the mbarrier
 template <typename T, int S>
 constexpr int smem_bytes() {
-  return 2 * Staged<S>::N * Geo<T>::ARRAY_BYTES + 128;
+  return Staged<S>::N * Geo<T>::ARRAY_BYTES + 128;
 }
 
-// The persistent stage kernel: CTA c takes tiles c, c+grid, ..; tile i+1's
-// boxes are in flight while tile i is computed.  One barrier per tile: after
-// the wait for tile i (a vote, so that a timeout ends every thread's loop at
-// the same point) every thread is done reading tile i-1's buffer, which then
-// takes tile i+1's boxes.  A wait that times out sets bit 1 of *status; the
-// CTA then waits (bounded) for the copies it issued and stops.
+// One tile per CTA, as many CTAs resident per SM as the shared memory
+// allows, so that the tiles' copies overlap one another.  Warp 0 issues the
+// tile's boxes; every thread loads the values it reads at its cells while
+// they are in flight, waits for the boxes (bounded: a timeout sets bit 1 of
+// *status and, after a second bounded wait for the copies, ends the thread)
+// and computes its cells.
 template <typename T, int S>
 __global__ void __launch_bounds__(256) k_tma_stage(const __grid_constant__ CUtensorMap map,
                                                    const Args<T> a) {
   using Gm = Geo<T>;
   constexpr int STAGE_BYTES = Staged<S>::N * Gm::ARRAY_BYTES;
   extern __shared__ __align__(128) unsigned char smem[];
-  uint64_t *bar = reinterpret_cast<uint64_t *>(smem + 2 * STAGE_BYTES);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem + STAGE_BYTES);
+  const int t = blockIdx.x;
   if (threadIdx.x == 0) {
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
+    mbar_init(bar, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
-  int t = blockIdx.x;
-  if (t >= a.ntiles) return;
-  if (threadIdx.x < 32) issue_tile<T, S>(a, &map, t, smem, &bar[0]);
-  for (int i = 0; t < a.ntiles; t += gridDim.x, ++i) {
-    const int s = i & 1;
-    const unsigned parity = (unsigned)((i >> 1) & 1);
-    const bool ok = mbar_wait_bounded(&bar[s], parity);
-    if (__syncthreads_or(!ok)) {
-      if (threadIdx.x == 0) atomicOr(a.status, 2);
-      mbar_wait_bounded(&bar[s], parity);  // the only copies in flight: tile i's
-      return;
-    }
-    const int tn = t + gridDim.x;
-    if (threadIdx.x < 32 && tn < a.ntiles) {
-      // order every thread's reads of this buffer (tile i-1) before the copies
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      issue_tile<T, S>(a, &map, tn, smem + (s ^ 1) * STAGE_BYTES, &bar[s ^ 1]);
-    }
-    compute_tile<T, S>(a, t, smem + s * STAGE_BYTES);
+  if (threadIdx.x < 32) issue_tile<T, S>(a, &map, t, smem, bar);
+  T cv[Staged<S>::NIN][Gm::ROWS];
+  load_cells<T, S>(a, t, cv);
+  if (!mbar_wait_bounded(bar, 0)) {
+    atomicOr(a.status, 2);
+    mbar_wait_bounded(bar, 0);
+    return;
   }
+  compute_tile<T, S>(a, t, smem, cv);
 }
 
 }  // namespace

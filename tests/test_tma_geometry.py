@@ -81,7 +81,7 @@ def check_grid(nx, ny, elem, nfield=13):
 
 @pytest.mark.parametrize("elem", [4, 8])
 @pytest.mark.parametrize("nx,ny", [(4, 4), (5, 7), (6, 9), (7, 16), (64, 32), (65, 33),
-                                   (126, 17), (128, 64), (200, 47)])
+                                   (126, 17), (128, 64), (200, 47), (257, 95), (300, 61)])
 def test_tiles_read_what_the_stencils_need(nx, ny, elem):
     check_grid(nx, ny, elem)
 
