@@ -267,18 +267,28 @@ __device__ __forceinline__ int floor_small(float f) { return f < 0.0f ? -1 : (f 
 
 __device__ __forceinline__ int wrap(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
 
+// 1/gamma of u = gamma v, its sum of squares rounded in one fixed order:
+// the push and the deposit stack's drain both take v from u
+__device__ __forceinline__ float inv_gamma(float ux, float uy, float uz) {
+  return rsqrtf(__fmaf_rn(uz, uz, __fmaf_rn(uy, uy, __fmaf_rn(ux, ux, 1.0f))));
+}
+
 // Deposits of particles outside their lane's cell go to global memory with
 // atomics.  Done where they arise, they would run with the one or two lanes
 // that need them while the rest of the warp waits; instead each warp stacks
 // them in shared memory and does 32 at a time, one per lane.  An entry is a
-// cell, the offsets in it and the charge-weighted velocity; kind 0 deposits
-// J (jm at the old position), kind 1 rho, J (jp) and the cell count at the
-// new position.
+// cell, the offsets in it and the particle's new u; kind 0 deposits J (jm
+// at the old position) and, in a regrouping push, writes the particle to
+// the back of its start cell's range (it came from another cell's range, so
+// its slot comes from an atomic -- one round trip per 32 such particles
+// instead of one per warp iteration that has any); kind 1 deposits rho, J
+// (jp) and the cell count at the new position.
 constexpr int kQCap = 96;  // < 32 left after a drain + at most 2 per lane
 struct DepQ {
   int cx[kQCap], cy[kQCap];
   float2 f[kQCap];
-  float4 q[kQCap];  // q*vx, q*vy, q*vz, kind
+  float4 q[kQCap];        // ux, uy, uz, kind
+  int32_t slot[kQCap];    // kind 0 of a regrouping push: the particle's slot
 };
 // A warp's shared scratch: its deposit stack while it pushes, then up to 24
 // block values of each of its lanes (value e of lane l at red[e*32 + l])
@@ -288,17 +298,37 @@ union WarpScratch {
   DepQ q;
   float red[kRedVals * 32];
 };
-static_assert(sizeof(DepQ) == sizeof(float) * kRedVals * 32, "the stack holds 24 rows");
+static_assert(sizeof(DepQ) >= sizeof(float) * kRedVals * 32, "the stack holds 24 rows");
 
+template <bool INPLACE>
 __device__ __forceinline__ void drain_entry(const Args32 &a, const DepQ &Q, int e) {
   const int cx = wrap(Q.cx[e], a.nx), cy = wrap(Q.cy[e], a.ny);  // entries are unwrapped
-  const float4 qq = Q.q[e];
+  const float4 uu = Q.q[e];
+  // v and q v as the push computed them
+  const float ginv = inv_gamma(uu.x, uu.y, uu.z);
+  const float vx = uu.x * ginv, vy = uu.y * ginv, vz = uu.z * ginv;
+  const float qx = a.qd * vx, qy = a.qd * vy, qz = a.qd * vz;
+  const float2 f = Q.f[e];
   Wts hx, hy, nxw, nyw;
-  weights2(cx, cy, Q.f[e], hx, hy, nxw, nyw);
-  deposit_j_atomic(a, hx, hy, nxw, nyw, qq.x, qq.y, qq.z);
-  if (qq.w != 0.0f) {
+  weights2(cx, cy, f, hx, hy, nxw, nyw);
+  deposit_j_atomic(a, hx, hy, nxw, nyw, qx, qy, qz);
+  if (uu.w != 0.0f) {
     scatter9(a.rho, a.nxg, nxw, nyw, a.qd);
     atomicAdd(a.cnt_next + cy * a.nx + cx, 1);
+  } else if constexpr (!INPLACE) {
+    // the new position relative to the start cell, as the push moved it
+    const float2 mv = fma2(make_float2(vx, vy), make_float2(a.dtdx, a.dtdy), f);
+    const int key = cy * a.nx + cx;  // the start cell's key
+    const int64_t pos = (int64_t)a.offB[key + 1] - 1 - atomicAdd(a.cursor + key, 1);
+    // a guard: the counts of the last push place every particle inside the
+    // buffer; a position outside it is counted and not written
+    if (pos < 0 || pos >= a.cap) {
+      atomicAdd(a.lost, 1.0);
+    } else {
+      reinterpret_cast<float4 *>(a.B)[pos] = make_float4(mv.x, mv.y, uu.x, uu.y);
+      a.B[4 * a.cap + pos] = uu.z;
+      a.slotB[pos] = Q.slot[e];
+    }
   }
 }
 
@@ -311,7 +341,7 @@ struct PartOut {
   bool in_cell_old;          // the start cell is the group cell
   bool need_old, need_new;   // deposits for the warp's stack
   int cx, cy, ncx, ncy;      // start and end cells, unwrapped
-  float fx, fy, nfx, nfy, qx, qy, qz;
+  float fx, fy, nfx, nfy;
 };
 
 // Gather, Boris, move and the in-cell deposits of one particle at (xr, yr)
@@ -369,12 +399,9 @@ __device__ __forceinline__ void push_one(const Args32 &a, float4 (*win)[WY][WXW]
   ux = gx + vvy * tz - vvz * ty + ebx.x;
   uy = gy + vvz * tx - vvx * tz + eby.x;
   uz = gz + vvx * ty - vvy * tx + ebz.x;
-  const float ginv = rsqrtf(1.0f + ux * ux + uy * uy + uz * uz);
+  const float ginv = inv_gamma(ux, uy, uz);
   const float vx = ux * ginv, vy = uy * ginv, vz = uz * ginv;
   const float qx = a.qd * vx, qy = a.qd * vy, qz = a.qd * vz;
-  o.qx = qx;
-  o.qy = qy;
-  o.qz = qz;
   o.ux = ux;
   o.uy = uy;
   o.uz = uz;
@@ -560,27 +587,20 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
         // write back grouped by the cell of the start of this step: particles
         // that started it in cell k take the next slots from the front of k's
         // segment in processing order (a running count per group, no atomics);
-        // the few that came from another cell's range fill it from the back
+        // the few that came from another cell's range fill it from the back,
+        // written by the deposit stack's drain with their kind-0 entry
         const unsigned inm = __ballot_sync(0xffffffffu, act && o.in_cell_old) & gmask;
-        int64_t pos = -1;
-        if (act) {
-          if (o.in_cell_old)
-            pos = (int64_t)front + home_count + __popc(inm & lt);
-          else {
-            const int key = wrap(o.cy, ny) * nx + wrap(o.cx, nx);  // the start cell's key
-            pos = (int64_t)a.offB[key + 1] - 1 - atomicAdd(a.cursor + key, 1);
-          }
+        if (act && o.in_cell_old) {
+          const int64_t pos = (int64_t)front + home_count + __popc(inm & lt);
           // a guard: the counts of the last push place every particle inside
           // the buffer; a position outside it is counted and not written
           if (pos < 0 || pos >= cap) {
             atomicAdd(a.lost, 1.0);
-            pos = -1;
+          } else {
+            B4[pos] = make_float4(o.mx, o.my, o.ux, o.uy);
+            Buz[pos] = o.uz;
+            a.slotB[pos] = cslot;
           }
-        }
-        if (pos >= 0) {
-          B4[pos] = make_float4(o.mx, o.my, o.ux, o.uy);
-          Buz[pos] = o.uz;
-          a.slotB[pos] = cslot;
         }
         home_count += __popc(inm);
       }
@@ -594,7 +614,8 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
           Q.cx[q] = o.cx;
           Q.cy[q] = o.cy;
           Q.f[q] = make_float2(o.fx, o.fy);
-          Q.q[q] = make_float4(o.qx, o.qy, o.qz, 0.0f);
+          Q.q[q] = make_float4(o.ux, o.uy, o.uz, 0.0f);
+          if constexpr (!INPLACE) Q.slot[q] = cslot;
         }
         const int qn1 = qn + __popc(m_old);
         if (o.need_new) {
@@ -602,19 +623,19 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
           Q.cx[q] = o.ncx;
           Q.cy[q] = o.ncy;
           Q.f[q] = make_float2(o.nfx, o.nfy);
-          Q.q[q] = make_float4(o.qx, o.qy, o.qz, 1.0f);
+          Q.q[q] = make_float4(o.ux, o.uy, o.uz, 1.0f);
         }
         qn = qn1 + __popc(m_new);
         __syncwarp();
         while (qn >= 32) {
           qn -= 32;
-          drain_entry(a, Q, qn + lane);
+          drain_entry<INPLACE>(a, Q, qn + lane);
           __syncwarp();
         }
       }
     }
 
-    if (lane < qn) drain_entry(a, Q, lane);
+    if (lane < qn) drain_entry<INPLACE>(a, Q, lane);
     qn = 0;
     // the group's new-position counts for cell k, and its register blocks
     const int stay = group_sum<G>((float)stay_new) + 0.5f;
