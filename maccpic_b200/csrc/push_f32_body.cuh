@@ -58,6 +58,7 @@ static_assert(sizeof(EnsPush32) <= 32764, "kernel parameters are limited to 3276
 struct Wts {
   int i;          // array index of the middle node
   float m, s, p;  // weights of nodes i-1, i, i+1
+  int u;          // integer nodes: the middle node is the cell's upper one (f >= 1/2)
 };
 
 // Packed FP32 pairs (sm_100a's f32x2 arithmetic) through the compiler's
@@ -79,15 +80,15 @@ __device__ __forceinline__ void weights2(int cx, int cy, float2 f, Wts &hx, Wts 
   const float2 d = add2(f, bc2(-0.5f)), e = add2(bc2(1.0f), make_float2(-f.x, -f.y));
   const float2 hm = mul2(mul2(half, e), e), hp = mul2(mul2(half, f), f);
   const float2 hs = fma2(make_float2(-d.x, -d.y), d, bc2(0.75f));
-  hx = Wts{cx + 1, hm.x, hs.x, hp.x};
-  hy = Wts{cy + 1, hm.y, hs.y, hp.y};
+  hx = Wts{cx + 1, hm.x, hs.x, hp.x, 0};
+  hy = Wts{cy + 1, hm.y, hs.y, hp.y, 0};
   const int ux = f.x >= 0.5f ? 1 : 0, uy = f.y >= 0.5f ? 1 : 0;
   const float2 h = add2(f, make_float2(-(float)ux, -(float)uy));
   const float2 am = add2(half, make_float2(-h.x, -h.y)), bp = add2(half, h);
   const float2 nm = mul2(mul2(half, am), am), np = mul2(mul2(half, bp), bp);
   const float2 ns = fma2(make_float2(-h.x, -h.y), h, bc2(0.75f));
-  nx = Wts{cx + 1 + ux, nm.x, ns.x, np.x};
-  ny = Wts{cy + 1 + uy, nm.y, ns.y, np.y};
+  nx = Wts{cx + 1 + ux, nm.x, ns.x, np.x, ux};
+  ny = Wts{cy + 1 + uy, nm.y, ns.y, np.y, uy};
 }
 
 // 9-point gather of an (E, B) pair; base points at node (i-1, j-1) of the
@@ -155,8 +156,12 @@ __device__ __forceinline__ float pick3(const float2 &lo, float last, int i) {
   return i == 0 ? lo.x : i == 1 ? lo.y : last;
 }
 
-__device__ __forceinline__ void spread4(const Wts &w, int c, float o[4]) {
-  const bool lo = (w.i == c + 1);
+// The integer-node weights of a particle of cell c as the 4 nodes c .. c+3
+// (array indices) the cell's particles can reach.  Only particles in the
+// lane's cell deposit into its block (the others with zero charge), so the
+// middle node's place is the particle's own u.
+__device__ __forceinline__ void spread4(const Wts &w, float o[4]) {
+  const bool lo = w.u == 0;
   o[0] = lo ? w.m : 0.0f;
   o[1] = lo ? w.s : w.m;
   o[2] = lo ? w.p : w.s;
@@ -168,8 +173,8 @@ __device__ __forceinline__ void block_add_j(Block32 &b, int cx, int cy, const Wt
                                             const Wts &hy, const Wts &nxw, const Wts &nyw,
                                             float qx, float qy, float qz) {
   float wxn[4], wyn[4];
-  spread4(nxw, cx, wxn);
-  spread4(nyw, cy, wyn);
+  spread4(nxw, wxn);
+  spread4(nyw, wyn);
   const float wxh[3] = {hx.m, hx.s, hx.p}, wyh[3] = {hy.m, hy.s, hy.p};
   const float2 n01 = make_float2(wxn[0], wxn[1]), n23 = make_float2(wxn[2], wxn[3]);
   // Jx(r, k) += (wyn[r] qx) wxh[k], Jz(r, k) += (wyh[r] qz) wxh[k]
@@ -197,8 +202,8 @@ __device__ __forceinline__ void block_add_j(Block32 &b, int cx, int cy, const Wt
 __device__ __forceinline__ void block_add_rho(Block32 &b, int cx, int cy, const Wts &nxw,
                                               const Wts &nyw, float q) {
   float wxn[4], wyn[4];
-  spread4(nxw, cx, wxn);
-  spread4(nyw, cy, wyn);
+  spread4(nxw, wxn);
+  spread4(nyw, wyn);
   const float2 n01 = make_float2(wxn[0], wxn[1]), n23 = make_float2(wxn[2], wxn[3]);
 #pragma unroll
   for (int r = 0; r < 4; ++r) {
