@@ -269,6 +269,15 @@ int em2g_set_sort_interval(em2g_ctx *ctx, int sort_interval);
  * em2 does (FP64: bitwise the same); only their speed differs. */
 int em2g_set_stencils(em2g_ctx *ctx, int mode);
 int em2g_get_stencils(em2g_ctx *ctx, int *mode);
+/* Self-test of the device waits' bounds (no reference counterpart: em2 has
+ * no device waits).  Every wait of a device thread on other threads is
+ * bounded: a wait that runs out records a status that the next call returns
+ * as EM2G_ERR_TIMEOUT, and the context stays usable.  This runs one wait of
+ * each kind that nothing ever releases: the CG's grid barrier (about 2 s)
+ * and a TMA-staged tile's mbarrier (about 1 s).  It returns the status each
+ * recorded: *cg_status = 1 and *tma_status = 2 when both bounds work.  No
+ * fault or trap is involved, and the context's state is left as it was. */
+int em2g_selftest_waits(em2g_ctx *ctx, int *cg_status, int *tma_status);
 
 /* ---- instrumentation ------------------------------------------------- */
 /* kernel launches since the last reset; with timing on, the number of

@@ -33,6 +33,7 @@ EXPORTS = [
     "em2g_move_curnt", "em2g_set_timing", "em2g_get_counters", "em2g_reset_counters",
     "em2g_smooth2_static", "em2g_setv_device", "em2g_diagnostics", "em2g_num_variants", "em2g_set_variant",
     "em2g_get_variant", "em2g_set_sort_interval", "em2g_set_stencils", "em2g_get_stencils",
+    "em2g_selftest_waits",
     "em2g_adj_create", "em2g_adj_destroy", "em2g_adj_forward", "em2g_adj_keep_all_fields",
     "em2g_adj_field_slots", "em2g_adj_get_field_slots",
     "em2g_adj_seed_fields_device",
@@ -131,6 +132,7 @@ def lib() -> C.CDLL:
         "em2g_set_sort_interval": (C.c_int, [ctx, C.c_int]),
         "em2g_set_stencils": (C.c_int, [ctx, C.c_int]),
         "em2g_get_stencils": (C.c_int, [ctx, C.POINTER(C.c_int)]),
+        "em2g_selftest_waits": (C.c_int, [ctx, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
         "em2g_adj_create": (C.c_int, [ctx, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
         "em2g_adj_destroy": (C.c_int, [ctx]),
         "em2g_adj_forward": (C.c_int, [ctx, C.c_int]),

@@ -983,6 +983,13 @@ int em2g_set_stencils(em2g_ctx *c, int mode) {
   return EM2G_OK;
 }
 
+int em2g_selftest_waits(em2g_ctx *c, int *cg_status, int *tma_status) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!cg_status || !tma_status) return fail(EM2G_ERR_INVALID, "null output");
+  return selftest_waits(c, cg_status, tma_status);
+}
+
 int em2g_get_stencils(em2g_ctx *c, int *mode) {
   int rc = check_ctx(c);
   if (rc) return rc;

@@ -191,6 +191,8 @@ int smooth2_f32(em2g_ctx *c, float *a);
 // fields_f64.cu); the field block and the smooth2 scratch must carry
 // tma_tail_elems() elements of tail
 int tma_init_f32(em2g_ctx *c);
+// em2g_selftest_waits (fields_f64.cu)
+int selftest_waits(em2g_ctx *c, int *cg_status, int *tma_status);
 int tma_init_f64(em2g_ctx *c);
 inline int64_t tma_tail_elems(const em2g_ctx *c, bool fp32) {
   return (int64_t)(fp32 ? 4 : 2) * c->g.nxg;  // 16 bytes' worth of rows

@@ -24,6 +24,30 @@ void cg_free(em2g_ctx *c) {
   c->cg = CgWork();
 }
 
+// Both bounded device waits made to run out on purpose (the probes of
+// grid_kernels.cuh and tma_stencil.cuh), on the context's stream and with
+// its CG workspace, which is left as the solver expects it.
+int selftest_waits(em2g_ctx *c, int *cg_status, int *tma_status) {
+  int st = 0;
+  EM2G_CUDA(cudaMemsetAsync(c->cg.bar, 0, sizeof(unsigned) * 2, c->stream));
+  EM2G_CUDA(cudaMemsetAsync(c->cg.status, 0, sizeof(int) * 2, c->stream));
+  grid::k_barrier_wait_probe<<<1, 32, 0, c->stream>>>(c->cg.bar, c->cg.status);
+  EM2G_CUDA(cudaGetLastError());
+  EM2G_CUDA(cudaMemcpyAsync(&st, c->cg.status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  EM2G_CUDA(cudaStreamSynchronize(c->stream));
+  *cg_status = st;
+  EM2G_CUDA(cudaMemsetAsync(c->cg.status, 0, sizeof(int) * 2, c->stream));
+  tma::k_tma_wait_probe<<<1, 32, 0, c->stream>>>(c->cg.status);
+  EM2G_CUDA(cudaGetLastError());
+  EM2G_CUDA(cudaMemcpyAsync(&st, c->cg.status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  EM2G_CUDA(cudaStreamSynchronize(c->stream));
+  *tma_status = st;
+  EM2G_CUDA(cudaMemsetAsync(c->cg.bar, 0, sizeof(unsigned) * 2, c->stream));
+  EM2G_CUDA(cudaMemsetAsync(c->cg.status, 0, sizeof(int) * 2, c->stream));
+  EM2G_CUDA(cudaStreamSynchronize(c->stream));
+  return EM2G_OK;
+}
+
 int fields_f64(em2g_ctx *c, int it, bool want_energies, int *cg_iters) {
   (void)cg_iters;  // read from cg.status by the caller after its last launch
   return grid::fields_t<double>(c, c->fld, c->smooth_tmp, it, want_energies);

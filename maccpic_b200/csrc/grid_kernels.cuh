@@ -338,6 +338,12 @@ __device__ bool grid_barrier(unsigned *bar, unsigned nblocks, int *status) {
   return *(volatile int *)status == 0;
 }
 
+// A probe of that bounded wait: one block arrives at a barrier counted for
+// two, so nothing releases it; its wait runs out after kSpinLimit polls and
+// records the timeout in status[0].  No fault and no trap: the context stays
+// usable (em2g_selftest_waits).
+__global__ void k_barrier_wait_probe(unsigned *bar, int *status) { grid_barrier(bar, 2u, status); }
+
 // sum of nb partials in a fixed order; result valid in every thread
 __device__ double sum_partials(const double *partial, int nb, double *sh) {
   if (threadIdx.x < 32) {

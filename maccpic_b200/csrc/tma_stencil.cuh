@@ -121,6 +121,19 @@ __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, i
       : "memory");
 }
 
+// A probe of the bounded tile wait: an mbarrier that no copy and no thread
+// completes, so the wait runs out after its bound and bit 1 of *status is
+// set, as a stage kernel does on a timeout (em2g_selftest_waits).
+__global__ void k_tma_wait_probe(int *status) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (!mbar_wait_bounded(&bar, 0) && threadIdx.x == 0) atomicOr(status, 2);
+}
+
 // tile t's origin: output cells ix0 .. ix0+TXO-1, iy0 .. iy0+TYO-1
 template <typename T>
 __device__ __forceinline__ void tile_origin(const Args<T> &a, int t, int &ix0, int &iy0) {
