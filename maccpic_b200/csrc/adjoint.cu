@@ -937,6 +937,7 @@ static int record_segment(em2g_adj *a, int k0, int k1, cudaStream_t st) {
 }
 
 int em2g_adj_forward(em2g_adj *a, int nsteps) {
+  em2g::NvtxRange nvtx_range("em2g adjoint forward");
   int rc = check_adj(a);
   if (rc) return rc;
   if (nsteps < 1 || nsteps > a->max_steps) return fail(EM2G_ERR_RANGE, "nsteps outside 1..max_steps");
@@ -979,6 +980,7 @@ int em2g_adj_seed_fields_device(em2g_adj *a, const double *dev6) {
 }
 
 int em2g_adj_backward(em2g_adj *a) {
+  em2g::NvtxRange nvtx_range("em2g adjoint backward");
   int rc = check_adj(a);
   if (rc) return rc;
   if (a->steps < 1) return fail(EM2G_ERR_INVALID, "run em2g_adj_forward first");

@@ -474,6 +474,7 @@ int em2g_get_field(em2g_ctx *c, int id, double *host) {
 }
 
 int em2g_set_fields(em2g_ctx *c, const double *host13) {
+  em2g::NvtxRange nvtx_range("em2g set_fields");
   int rc = check_ctx(c);
   if (rc) return rc;
   if (!host13) return fail(EM2G_ERR_INVALID, "null pointer");
@@ -482,6 +483,7 @@ int em2g_set_fields(em2g_ctx *c, const double *host13) {
 }
 
 int em2g_get_fields(em2g_ctx *c, double *host13) {
+  em2g::NvtxRange nvtx_range("em2g get_fields");
   int rc = check_ctx(c);
   if (rc) return rc;
   if (!host13) return fail(EM2G_ERR_INVALID, "null pointer");
@@ -739,6 +741,7 @@ static int particles_get(em2g_ctx *c, int isp, int64_t first, int64_t count,
 int em2g_set_particles(em2g_ctx *c, int isp, int64_t n, const double *x, const double *y,
                        const double *vx, const double *vy, const double *vz,
                        const double *gamma) {
+  em2g::NvtxRange nvtx_range("em2g set_particles");
   int rc = check_ctx(c);
   if (rc) return rc;
   if (isp < 0 || isp >= c->P.nsp) return fail(EM2G_ERR_INVALID, "bad species index");
@@ -758,6 +761,7 @@ int em2g_set_particles_device(em2g_ctx *c, int isp, int64_t n, const double *x,
 
 int em2g_get_particles(em2g_ctx *c, int isp, int64_t *n, double *x, double *y, double *vx,
                        double *vy, double *vz, double *gamma) {
+  em2g::NvtxRange nvtx_range("em2g get_particles");
   int rc = check_ctx(c);
   if (rc) return rc;
   if (isp < 0 || isp >= c->P.nsp) return fail(EM2G_ERR_INVALID, "bad species index");
@@ -819,6 +823,7 @@ int em2g_get_step(em2g_ctx *c, int *it) {
 }
 
 int em2g_move(em2g_ctx *c, double *ake_out) {
+  em2g::NvtxRange nvtx_range("em2g move");
   int rc = check_ctx(c);
   if (rc) return rc;
   if (is_fp32(c))
@@ -847,6 +852,7 @@ static int fast_push_all(em2g_ctx *c) {
 }
 
 int em2g_move_curnt(em2g_ctx *c, double *ake_out) {
+  em2g::NvtxRange nvtx_range("em2g move+curnt");
   int rc = check_ctx(c);
   if (rc) return rc;
   if ((rc = fast_push_all(c))) return rc;
@@ -919,6 +925,7 @@ int em2g_reset_counters(em2g_ctx *c) {
 }
 
 int em2g_curnt(em2g_ctx *c) {
+  em2g::NvtxRange nvtx_range("em2g curnt");
   int rc = check_ctx(c);
   if (rc) return rc;
   if (is_fp32(c))
@@ -935,6 +942,7 @@ int em2g_curnt(em2g_ctx *c) {
 }
 
 int em2g_fields(em2g_ctx *c, int it, double *energies_out, int *cg_iters_out) {
+  em2g::NvtxRange nvtx_range("em2g fields");
   int rc = check_ctx(c);
   if (rc) return rc;
   EM2G_CUDA(cudaMemsetAsync(c->cg.status, 0, sizeof(int) * 2, c->stream));
@@ -956,6 +964,7 @@ int em2g_diagnostics(em2g_ctx *c, double *out, int nout) {
 }
 
 int em2g_smooth2(em2g_ctx *c, int id) {
+  em2g::NvtxRange nvtx_range("em2g smooth2");
   int rc = check_ctx(c);
   if (rc) return rc;
   if (id < 0 || id >= EM2G_NFIELD) return fail(EM2G_ERR_INVALID, "bad field id");
@@ -1000,13 +1009,18 @@ int em2g_get_stencils(em2g_ctx *c, int *mode) {
 
 int em2g_step(em2g_ctx *c, int nsteps, double *ake_out, double *energies_out,
               int *cg_iters_out) {
+  em2g::NvtxRange nvtx_range("em2g step");
   int rc = check_ctx(c);
   if (rc) return rc;
   if (nsteps < 0) return fail(EM2G_ERR_INVALID, "nsteps < 0");
   EM2G_CUDA(cudaMemsetAsync(c->cg.status, 0, sizeof(int) * 2, c->stream));
   for (int k = 0; k < nsteps; ++k) {
-    if ((rc = fast_push_all(c))) return rc;
+    {
+      em2g::NvtxRange r("push (move+curnt)");
+      if ((rc = fast_push_all(c))) return rc;
+    }
     c->it += 1;
+    em2g::NvtxRange r("fields");
     rc = is_fp32(c) ? fields_f32(c, c->it, true) : fields_f64(c, c->it, true, nullptr);
     if (rc) return rc;
   }

@@ -3,6 +3,7 @@
 #pragma once
 #include <cuda.h>  // CUtensorMap (the map is encoded through the runtime's driver entry point)
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>  // header-only; inert unless a profiler is attached
 #include <stdint.h>
 #include <string>
 #include <vector>
@@ -28,6 +29,16 @@ constexpr int kDevLost = kDevOut - 1;
 // Sets the per-thread error message and returns the status (api.cu).
 int fail(int status, const std::string &msg);
 int cuda_fail(cudaError_t e, const char *what);
+
+// An NVTX range around one ABI call or step phase, so that a timeline
+// profiler groups the kernels each one launches under the em2 routine they
+// stand for (move, curnt, fields, ...).
+struct NvtxRange {
+  explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange &) = delete;
+  NvtxRange &operator=(const NvtxRange &) = delete;
+};
 
 #define EM2G_CUDA(call)                                  \
   do {                                                   \

@@ -421,6 +421,7 @@ int em2g_ens_get_particles(em2g_ens *e, int run, int isp, int64_t *n, double *x,
 
 int em2g_ens_step(em2g_ens *e, int nsteps, double *ake_out, double *energies_out,
                   int *cg_iters_out) {
+  em2g::NvtxRange nvtx_range("em2g ensemble step");
   int rc = check_ens(e);
   if (rc) return rc;
   if (nsteps < 0) return fail(EM2G_ERR_INVALID, "nsteps < 0");
