@@ -268,7 +268,15 @@ __device__ __forceinline__ void flush_rows(float *A, int nxg, int kx, int ky, co
   }
 }
 
-__device__ __forceinline__ int floor_small(float f) { return f < 0.0f ? -1 : (f >= 1.0f ? 1 : 0); }
+// The whole-cell part of a pair of offsets in (-1, 2) (-1, 0 or 1 each) and
+// what is left within that cell: floor as a float is exact, so the rest is
+// one packed subtraction.
+__device__ __forceinline__ void split_cell(float2 f, int &ox, int &oy, float2 &rest) {
+  const float2 fl = make_float2(floorf(f.x), floorf(f.y));
+  ox = (int)fl.x;
+  oy = (int)fl.y;
+  rest = add2(f, make_float2(-fl.x, -fl.y));
+}
 
 __device__ __forceinline__ int wrap(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
 
@@ -360,9 +368,11 @@ __device__ __forceinline__ void push_one(const Args32 &a, float4 (*win)[WY][WXW]
   constexpr int WX = WXW;
   const int nx = a.nx, ny = a.ny, nxg = a.nxg;
   // the cell the particle is in now (it may have left cell k last step)
-  const int ox = floor_small(xr), oy = floor_small(yr);
+  int ox, oy;
+  float2 fxy;
+  split_cell(make_float2(xr, yr), ox, oy, fxy);
   const int cx = kx + ox, cy = ky + oy;  // unwrapped
-  const float fx = xr - (float)ox, fy = yr - (float)oy;
+  const float fx = fxy.x, fy = fxy.y;
   o.ox = ox;
   o.oy = oy;
   o.in_cell_old = (ox == 0) && (oy == 0);
@@ -425,8 +435,10 @@ __device__ __forceinline__ void push_one(const Args32 &a, float4 (*win)[WY][WXW]
   const float2 mv = fma2(make_float2(vx, vy), make_float2(a.dtdx, a.dtdy), make_float2(fx, fy));
   o.mx = mv.x;
   o.my = mv.y;
-  const int nox = floor_small(mv.x), noy = floor_small(mv.y);
-  const float nfx = mv.x - (float)nox, nfy = mv.y - (float)noy;
+  int nox, noy;
+  float2 nf;
+  split_cell(mv, nox, noy, nf);
+  const float nfx = nf.x, nfy = nf.y;
   // rho and jp at the new position (pic/curnt.f90:197-303); with at least 4
   // cells a side, the new cell is the group cell exactly when the offsets
   // cancel
