@@ -11,6 +11,8 @@ import os
 
 PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG, "libem2g.so")
+# the bounds-checked build of the same library (maccpic_b200/build.py)
+LIB_CHECKED_PATH = os.path.join(PKG, "libem2g_checked.so")
 
 MAX_SPECIES = 4
 NFIELD = 13
@@ -74,16 +76,30 @@ class Em2gError(RuntimeError):
 
 
 _lib = None
+_lib_checked = None
 
 
 def lib() -> C.CDLL:
     """Load libem2g.so and declare argument types; raises if it is absent."""
     global _lib
-    if _lib is not None:
-        return _lib
-    if not os.path.exists(LIB_PATH):
-        raise RuntimeError(f"{LIB_PATH} not built: run `python -m maccpic_b200.build`")
-    L = C.CDLL(LIB_PATH)
+    if _lib is None:
+        _lib = _load(LIB_PATH)
+    return _lib
+
+
+def checked_lib() -> C.CDLL:
+    """Load libem2g_checked.so, the bounds-checked build (its FP32 push counts
+    and skips any out-of-range index instead of using it); raises if absent."""
+    global _lib_checked
+    if _lib_checked is None:
+        _lib_checked = _load(LIB_CHECKED_PATH)
+    return _lib_checked
+
+
+def _load(path: str) -> C.CDLL:
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} not built: run `python -m maccpic_b200.build`")
+    L = C.CDLL(path)
     dp, vp, ip, i64p = (C.POINTER(C.c_double), C.c_void_p, C.POINTER(C.c_int),
                         C.POINTER(C.c_int64))
     pp = C.POINTER(Em2gParams)
@@ -168,10 +184,11 @@ def lib() -> C.CDLL:
         fn = getattr(L, name)
         fn.restype = res
         fn.argtypes = args
-    _lib = L
     return L
 
 
-def check(status: int) -> None:
+def check(status: int, library: C.CDLL | None = None) -> None:
+    """Raise Em2gError for a nonzero status, with the message of the library
+    that returned it (libem2g.so unless another is given)."""
     if status != OK:
-        raise Em2gError(status, lib().em2g_last_error().decode())
+        raise Em2gError(status, (library or lib()).em2g_last_error().decode())

@@ -17,6 +17,17 @@
   X(32, 4, 1, 4) X(32, 4, 1, 5) X(32, 4, 1, 6) X(64, 4, 1, 2) X(64, 4, 1, 3)  \
   X(32, 8, 1, 2) X(32, 2, 1, 8) X(64, 2, 1, 4) X(32, 4, 2, 4) X(32, 4, 3, 4)
 
+// Bounds-checked build (-DEM2G_BOUNDS_CHECK: libem2g_checked.so, from
+// maccpic_b200/build.py): every index the push computes for shared or global
+// memory is checked before the access; one out of range is counted in
+// Args32::lost (the step then fails with EM2G_ERR_RANGE) and the access is
+// skipped -- no trap, no fault.  The ordinary build compiles the checks away.
+#ifdef EM2G_BOUNDS_CHECK
+#define EM2G_IN(cond, lost) ((cond) ? true : (atomicAdd((lost), 1.0), false))
+#else
+#define EM2G_IN(cond, lost) true
+#endif
+
 namespace em2g {
 namespace {
 
@@ -324,6 +335,11 @@ __device__ __forceinline__ void drain_entry(const Args32 &a, const DepQ &Q, int 
   const float2 f = Q.f[e];
   Wts hx, hy, nxw, nyw;
   weights2(cx, cy, f, hx, hy, nxw, nyw);
+  // every 3 x 3 stencil inside the guarded (nx+3) x (ny+3) arrays
+  if (!EM2G_IN(hx.i >= 1 && hx.i + 1 <= a.nx + 2 && nxw.i >= 1 && nxw.i + 1 <= a.nx + 2 &&
+                   hy.i >= 1 && hy.i + 1 <= a.ny + 2 && nyw.i >= 1 && nyw.i + 1 <= a.ny + 2,
+               a.lost))
+    return;
   deposit_j_atomic(a, hx, hy, nxw, nyw, qx, qy, qz);
   if (uu.w != 0.0f) {
     scatter9(a.rho, a.nxg, nxw, nyw, a.qd);
@@ -385,14 +401,38 @@ __device__ __forceinline__ void push_one(const Args32 &a, float4 (*win)[WY][WXW]
   // else from global memory at the wrapped cell
   float2 ebx, ebz, eby;
   if ((unsigned)cx < (unsigned)nx && (unsigned)cy < (unsigned)ny) {
-    ebx = gather_pair_win(&win[0][nyw.i - y0][hx.i - x0], WX, hx, nyw);
-    ebz = gather_pair_win(&win[1][hy.i - y0][hx.i - x0], WX, hx, hy);
-    eby = gather_pair_win(&win[2][hy.i - y0][nxw.i - x0], WX, nxw, hy);
+#ifdef EM2G_BOUNDS_CHECK
+    // three rows and (entries of) three columns from each stencil's corner
+    const int r0 = nyw.i - y0, r1 = hy.i - y0, c0 = hx.i - x0, c1 = nxw.i - x0;
+    if (!EM2G_IN(r0 >= 0 && r0 + 2 < WY && r1 >= 0 && r1 + 2 < WY && c0 >= 0 &&
+                     c0 + 2 < WX && c1 >= 0 && c1 + 2 < WX,
+                 a.lost)) {
+      ebx = ebz = eby = make_float2(0.0f, 0.0f);
+    } else
+#endif
+    {
+      ebx = gather_pair_win(&win[0][nyw.i - y0][hx.i - x0], WX, hx, nyw);
+      ebz = gather_pair_win(&win[1][hy.i - y0][hx.i - x0], WX, hx, hy);
+      eby = gather_pair_win(&win[2][hy.i - y0][nxw.i - x0], WX, nxw, hy);
+    }
   } else {
     const int sx = wrap(cx, nx) - cx, sy = wrap(cy, ny) - cy;
-    ebx = gather_pair(a.ebx + (int64_t)(nyw.i + sy - 1) * nxg + hx.i + sx - 1, nxg, hx, nyw);
-    ebz = gather_pair(a.ebz + (int64_t)(hy.i + sy - 1) * nxg + hx.i + sx - 1, nxg, hx, hy);
-    eby = gather_pair(a.eby + (int64_t)(hy.i + sy - 1) * nxg + nxw.i + sx - 1, nxg, nxw, hy);
+    const int64_t bx0 = (int64_t)(nyw.i + sy - 1) * nxg + hx.i + sx - 1;
+    const int64_t bz0 = (int64_t)(hy.i + sy - 1) * nxg + hx.i + sx - 1;
+    const int64_t by0 = (int64_t)(hy.i + sy - 1) * nxg + nxw.i + sx - 1;
+#ifdef EM2G_BOUNDS_CHECK
+    const int64_t w = (int64_t)nxg * (ny + 3), span = 2 * (int64_t)nxg + 2;
+    if (!EM2G_IN(bx0 >= 0 && bx0 + span < w && bz0 >= 0 && bz0 + span < w && by0 >= 0 &&
+                     by0 + span < w,
+                 a.lost)) {
+      ebx = ebz = eby = make_float2(0.0f, 0.0f);
+    } else
+#endif
+    {
+      ebx = gather_pair(a.ebx + bx0, nxg, hx, nyw);
+      ebz = gather_pair(a.ebz + bz0, nxg, hx, hy);
+      eby = gather_pair(a.eby + by0, nxg, nxw, hy);
+    }
   }
   // relativistic Boris on u (pic/move.f90:176-203).  The reciprocal square
   // roots and divisions are the hardware approximations (rsqrtf, a few ulp),
@@ -513,7 +553,7 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
   const float *__restrict__ Auz = a.A + 4 * cap;
   float4 *B4 = reinterpret_cast<float4 *>(a.B);
   float *Buz = a.B + 4 * cap;
-  if (beg + gl < end) {
+  if (beg + gl < end && EM2G_IN(beg + gl < cap, a.lost)) {
     const int32_t j = beg + gl;
     const float4 q = A4[j];
     pxr = q.x;
@@ -544,7 +584,7 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
       beg = valid ? a.offA[cell] : 0;
       front = (!INPLACE && valid) ? a.offB[cell] : 0;
       end = valid ? a.offA[cell + 1] : 0;
-      if (beg + gl < end) {
+      if (beg + gl < end && EM2G_IN(beg + gl < cap, a.lost)) {
         const int32_t j = beg + gl;
         const float4 q = A4[j];
         pxr = q.x;
@@ -574,7 +614,7 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
       const float cxr = pxr, cyr = pyr, cux = pux, cuy = puy, cuz = puz;
       const int32_t cslot = pslot;
       const int32_t j = i + G;
-      if (j < end) {
+      if (j < end && EM2G_IN(j < cap, a.lost)) {
         const float4 q = A4[j];
         pxr = q.x;
         pyr = q.y;
@@ -597,8 +637,10 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
           float xn = o.mx + (float)o.ox, yn = o.my + (float)o.oy;
           if (o.ox + (o.ncx - o.cx) == 0) xn = fminf(xn, kBelowOne);
           if (o.oy + (o.ncy - o.cy) == 0) yn = fminf(yn, kBelowOne);
-          B4[i] = make_float4(xn, yn, o.ux, o.uy);
-          Buz[i] = o.uz;
+          if (EM2G_IN(i < cap, a.lost)) {
+            B4[i] = make_float4(xn, yn, o.ux, o.uy);
+            Buz[i] = o.uz;
+          }
         }
       } else {
         // write back grouped by the cell of the start of this step: particles
@@ -626,7 +668,7 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
       const unsigned m_old = __ballot_sync(0xffffffffu, o.need_old);
       const unsigned m_new = __ballot_sync(0xffffffffu, o.need_new);
       if (m_old | m_new) {
-        if (o.need_old) {
+        if (o.need_old && EM2G_IN(qn + __popc(m_old & lt) < kQCap, a.lost)) {
           const int q = qn + __popc(m_old & lt);
           Q.cx[q] = o.cx;
           Q.cy[q] = o.cy;
@@ -635,7 +677,7 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
           if constexpr (!INPLACE) Q.slot[q] = cslot;
         }
         const int qn1 = qn + __popc(m_old);
-        if (o.need_new) {
+        if (o.need_new && EM2G_IN(qn1 + __popc(m_new & lt) < kQCap, a.lost)) {
           const int q = qn1 + __popc(m_new & lt);
           Q.cx[q] = o.ncx;
           Q.cy[q] = o.ncy;
@@ -657,6 +699,8 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
     // the group's new-position counts for cell k, and its register blocks
     const int stay = group_sum<G>((float)stay_new) + 0.5f;
     if (valid && gl == 0 && stay > 0) atomicAdd(a.cnt_next + cell, stay);
+    // the block's rows ky .. ky+3 and columns kx .. kx+3 lie in the arrays
+    valid = valid && EM2G_IN(kx + 3 <= nx + 2 && ky + 3 <= ny + 2, a.lost);
     if (__any_sync(0xffffffffu, valid && end > beg)) {
       // the G blocks of each cell summed through the warp's scratch (the
       // stack is empty now), in three passes: rho, Jx and Jy, Jz

@@ -112,17 +112,22 @@ def stream_handle(stream) -> C.c_void_p:
 class Em2Gpu:
     """One em2 run resident on one GPU."""
 
-    def __init__(self, params: RunParams):
+    def __init__(self, params: RunParams, library: C.CDLL | None = None):
+        """`library`: the loaded C library to run on (default libem2g.so;
+        _lib.checked_lib() is its bounds-checked build)."""
         self.p = params
-        self._L = _lib.lib()
+        self._L = library or _lib.lib()
         self._P = params.ctype()
         h = C.c_void_p()
-        check(self._L.em2g_create(C.byref(self._P), C.byref(h)))
+        self._check(self._L.em2g_create(C.byref(self._P), C.byref(h)))
         self._h = h
+
+    def _check(self, status: int) -> None:
+        check(status, self._L)
 
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:
-            check(self._L.em2g_destroy(self._h))
+            self._check(self._L.em2g_destroy(self._h))
             self._h = None
 
     def __del__(self):
@@ -143,7 +148,7 @@ class Em2Gpu:
         a = np.ascontiguousarray(fld, dtype=np.float64)
         if a.shape != (NFIELD,) + self.p.shape:
             raise ValueError(f"fields must have shape {(NFIELD,) + self.p.shape}")
-        check(self._L.em2g_set_fields(self._h, _dp(a)))
+        self._check(self._L.em2g_set_fields(self._h, _dp(a)))
 
     def get_fields(self, out: np.ndarray | None = None) -> np.ndarray:
         """All 13 arrays, shape (13, ny+3, nx+3); into `out` (C-contiguous
@@ -153,18 +158,18 @@ class Em2Gpu:
             out = np.empty(shape)
         else:
             _check_out(out, shape)
-        check(self._L.em2g_get_fields(self._h, _dp(out)))
+        self._check(self._L.em2g_get_fields(self._h, _dp(out)))
         return out
 
     def set_field(self, name: str, a: np.ndarray) -> None:
         a = np.ascontiguousarray(a, dtype=np.float64)
         if a.shape != self.p.shape:
             raise ValueError(f"field must have shape {self.p.shape}")
-        check(self._L.em2g_set_field(self._h, FIELD_ID[name], _dp(a)))
+        self._check(self._L.em2g_set_field(self._h, FIELD_ID[name], _dp(a)))
 
     def get_field(self, name: str) -> np.ndarray:
         out = np.empty(self.p.shape)
-        check(self._L.em2g_get_field(self._h, FIELD_ID[name], _dp(out)))
+        self._check(self._L.em2g_get_field(self._h, FIELD_ID[name], _dp(out)))
         return out
 
     def set_particles(self, isp: int, part: np.ndarray) -> None:
@@ -173,7 +178,7 @@ class Em2Gpu:
         if a.ndim != 2 or a.shape[0] != 6:
             raise ValueError("particles must have shape (6, n)")
         n = a.shape[1]
-        check(self._L.em2g_set_particles(self._h, isp, n, *[_dp(a[k]) for k in range(6)]))
+        self._check(self._L.em2g_set_particles(self._h, isp, n, *[_dp(a[k]) for k in range(6)]))
 
     def set_particles_device(self, isp: int, part) -> None:
         """part: a CUDA tensor (6, n) float64 on this context's device; the
@@ -185,7 +190,7 @@ class Em2Gpu:
         part = part.contiguous()
         n = part.shape[1]
         ptrs = [C.c_void_p(part[k].data_ptr()) for k in range(6)]
-        check(self._L.em2g_set_particles_device(self._h, isp, n, *ptrs))
+        self._check(self._L.em2g_set_particles_device(self._h, isp, n, *ptrs))
 
     def set_particles_slices(self, isp: int, n: int, slices) -> None:
         """n particles of species isp handed over one slice at a time, for
@@ -195,7 +200,7 @@ class Em2Gpu:
         The species keeps its old particles unless all n arrive and pass
         the library's checks."""
         L = self._L
-        check(L.em2g_particles_begin(self._h, isp, int(n)))
+        self._check(L.em2g_particles_begin(self._h, isp, int(n)))
         first = 0
         try:
             for a in slices:
@@ -213,14 +218,14 @@ class Em2Gpu:
                 if a.ndim != 2 or a.shape[0] != 6:
                     raise ValueError("slices must have shape (6, m)")
                 m = int(a.shape[1])
-                check(L.em2g_particles_add(self._h, isp, first, m, *ptrs, dev))
+                self._check(L.em2g_particles_add(self._h, isp, first, m, *ptrs, dev))
                 # the slice is read on the library's stream: wait for it before
                 # the caller may free or reuse its memory
-                check(L.em2g_synchronize(self._h))
+                self._check(L.em2g_synchronize(self._h))
                 first += m
         finally:
             rc = L.em2g_particles_end(self._h, isp)
-        check(rc)
+        self._check(rc)
 
     def get_particles_range(self, isp: int, first: int, count: int, out=None):
         """Slots first..first+count-1 of species isp as (6, count) x, y, vx,
@@ -237,36 +242,36 @@ class Em2Gpu:
                 raise ValueError("out must be a contiguous (6, count) float64 CUDA tensor")
             ptrs = [C.c_void_p(out[k].data_ptr()) for k in range(6)]
             dev = 1
-        check(self._L.em2g_get_particles_range(self._h, isp, int(first), int(count), *ptrs, dev))
+        self._check(self._L.em2g_get_particles_range(self._h, isp, int(first), int(count), *ptrs, dev))
         return out
 
     def set_stream(self, stream) -> None:
         """Enqueue further work on this cudaStream_t (int handle, or a torch
         stream); None returns to the context's own stream."""
-        check(self._L.em2g_set_stream(self._h, stream_handle(stream)))
+        self._check(self._L.em2g_set_stream(self._h, stream_handle(stream)))
 
     def num_variants(self) -> int:
         n = C.c_int()
-        check(self._L.em2g_num_variants(self._h, C.byref(n)))
+        self._check(self._L.em2g_num_variants(self._h, C.byref(n)))
         return n.value
 
     def set_variant(self, v: int) -> None:
-        check(self._L.em2g_set_variant(self._h, int(v)))
+        self._check(self._L.em2g_set_variant(self._h, int(v)))
 
     def set_sort_interval(self, k: int) -> None:
         """Regroup particles by cell every k-th step (FP32; k*c*dt < dx, dy)."""
-        check(self._L.em2g_set_sort_interval(self._h, int(k)))
+        self._check(self._L.em2g_set_sort_interval(self._h, int(k)))
         self.p.sort_interval = int(k)
 
     def set_stencils(self, mode: int) -> None:
         """How the Yee updates and smooth2 passes read their arrays: 0 direct
         loads per cell, 1 tiles staged in shared memory by tensor copies.
         The results are the same; only the speed differs."""
-        check(self._L.em2g_set_stencils(self._h, int(mode)))
+        self._check(self._L.em2g_set_stencils(self._h, int(mode)))
 
     def stencils(self) -> int:
         m = C.c_int(0)
-        check(self._L.em2g_get_stencils(self._h, C.byref(m)))
+        self._check(self._L.em2g_get_stencils(self._h, C.byref(m)))
         return m.value
 
     def max_sort_interval(self) -> int:
@@ -281,87 +286,87 @@ class Em2Gpu:
         """(index, name) of the fast-push kernel variant in use."""
         v = C.c_int()
         buf = C.create_string_buffer(64)
-        check(self._L.em2g_get_variant(self._h, C.byref(v), buf, 64))
+        self._check(self._L.em2g_get_variant(self._h, C.byref(v), buf, 64))
         return v.value, buf.value.decode()
 
     def set_timing(self, on: bool) -> None:
-        check(self._L.em2g_set_timing(self._h, int(bool(on))))
+        self._check(self._L.em2g_set_timing(self._h, int(bool(on))))
 
     def counters(self) -> dict:
         a, b, ms = C.c_int64(), C.c_int64(), C.c_double()
-        check(self._L.em2g_get_counters(self._h, C.byref(a), C.byref(b), C.byref(ms)))
+        self._check(self._L.em2g_get_counters(self._h, C.byref(a), C.byref(b), C.byref(ms)))
         return {"kernel_launches": a.value, "push_launches_timed": b.value,
                 "push_ms": ms.value}
 
     def reset_counters(self) -> None:
-        check(self._L.em2g_reset_counters(self._h))
+        self._check(self._L.em2g_reset_counters(self._h))
 
     def get_particles(self, isp: int, out: np.ndarray | None = None) -> np.ndarray:
         """(6, n) = x, y, vx, vy, vz, gamma in slot order; into `out`
         (C-contiguous float64 of that shape) if given."""
         n = C.c_int64()
-        check(self._L.em2g_get_particles(self._h, isp, C.byref(n), *([None] * 6)))
+        self._check(self._L.em2g_get_particles(self._h, isp, C.byref(n), *([None] * 6)))
         if out is None:
             out = np.empty((6, n.value))
         else:
             _check_out(out, (6, n.value))
         if n.value:
-            check(self._L.em2g_get_particles(self._h, isp, C.byref(n),
+            self._check(self._L.em2g_get_particles(self._h, isp, C.byref(n),
                                              *[_dp(out[k]) for k in range(6)]))
         return out
 
     @property
     def it(self) -> int:
         v = C.c_int()
-        check(self._L.em2g_get_step(self._h, C.byref(v)))
+        self._check(self._L.em2g_get_step(self._h, C.byref(v)))
         return v.value
 
     @it.setter
     def it(self, value: int) -> None:
-        check(self._L.em2g_set_step(self._h, int(value)))
+        self._check(self._L.em2g_set_step(self._h, int(value)))
 
     # ---- the subroutines --------------------------------------------------
     def move(self) -> np.ndarray:
         """pic/move.f90: gather + Boris; returns ake(1:nsp)."""
         ake = np.zeros(4)
-        check(self._L.em2g_move(self._h, _dp(ake)))
+        self._check(self._L.em2g_move(self._h, _dp(ake)))
         return ake[: self.p.nsp]
 
     def move_curnt(self) -> np.ndarray:
         """move then curnt in one fused particle kernel; returns ake."""
         ake = np.zeros(4)
-        check(self._L.em2g_move_curnt(self._h, _dp(ake)))
+        self._check(self._L.em2g_move_curnt(self._h, _dp(ake)))
         return ake[: self.p.nsp]
 
     def curnt(self) -> None:
         """pic/curnt.f90: deposit jm, move + wrap, deposit rho and jp."""
-        check(self._L.em2g_curnt(self._h))
+        self._check(self._L.em2g_curnt(self._h))
 
     def fields(self, it: int):
         """pic/fields.f90 for step ``it``; returns (cg iterations, energies or None)."""
         e6 = np.full(6, np.nan)
         n = C.c_int()
-        check(self._L.em2g_fields(self._h, int(it), _dp(e6), C.byref(n)))
+        self._check(self._L.em2g_fields(self._h, int(it), _dp(e6), C.byref(n)))
         return n.value, (e6 if it % self.p.isav == 0 else None)
 
     def diagnostics(self) -> dict:
         """Field energies of the current fields, reconnected flux of both
         sheets and the last Poisson residuals (FP64, computed on the GPU)."""
         out = np.zeros(10)
-        check(self._L.em2g_diagnostics(self._h, _dp(out), 10))
+        self._check(self._L.em2g_diagnostics(self._h, _dp(out), 10))
         return {"energies": out[:6].copy(), "flux": out[6:8].copy(),
                 "poisson_r2_before": out[8], "poisson_r2_after": out[9]}
 
     def smooth2(self, name: str) -> None:
         """pic/smooth.f90:95 on one resident field array."""
-        check(self._L.em2g_smooth2(self._h, FIELD_ID[name]))
+        self._check(self._L.em2g_smooth2(self._h, FIELD_ID[name]))
 
     def step(self, nsteps: int = 1) -> dict:
         """nsteps of {move; curnt; it+=1; fields(it)} on the fused fast path."""
         ake = np.zeros(4)
         e6 = np.full(6, np.nan)
         n = C.c_int()
-        check(self._L.em2g_step(self._h, int(nsteps), _dp(ake), _dp(e6), C.byref(n)))
+        self._check(self._L.em2g_step(self._h, int(nsteps), _dp(ake), _dp(e6), C.byref(n)))
         return {"ake": ake[: self.p.nsp].copy(), "cg_iters": n.value,
                 "energies": e6 if self.it % self.p.isav == 0 else None}
 

@@ -28,9 +28,11 @@ from .em2 import RunParams, _check_out, _dp, stream_handle
 class Em2Ensemble:
     """Independent FP32 runs resident on one GPU, stepped together."""
 
-    def __init__(self, runs: list[RunParams]):
+    def __init__(self, runs: list[RunParams], library=None):
+        """`library`: the loaded C library to run on (default libem2g.so;
+        _lib.checked_lib() is its bounds-checked build)."""
         self.runs = list(runs)
-        self._L = _lib.lib()
+        self._L = library or _lib.lib()
         arr = (_lib.Em2gParams * len(self.runs))()
         for k, rp in enumerate(self.runs):
             if rp.precision != _lib.FP32:
@@ -38,12 +40,15 @@ class Em2Ensemble:
             arr[k] = rp.ctype()
         self._arr = arr
         h = C.c_void_p()
-        check(self._L.em2g_ens_create(arr, len(self.runs), C.byref(h)))
+        self._check(self._L.em2g_ens_create(arr, len(self.runs), C.byref(h)))
         self._h = h
+
+    def _check(self, status: int) -> None:
+        check(status, self._L)
 
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:
-            check(self._L.em2g_ens_destroy(self._h))
+            self._check(self._L.em2g_ens_destroy(self._h))
             self._h = None
 
     def __del__(self):
@@ -66,7 +71,7 @@ class Em2Ensemble:
         a = np.ascontiguousarray(fld, dtype=np.float64)
         if a.shape != (NFIELD,) + self.runs[run].shape:
             raise ValueError(f"fields must have shape {(NFIELD,) + self.runs[run].shape}")
-        check(self._L.em2g_ens_set_fields(self._h, run, _dp(a)))
+        self._check(self._L.em2g_ens_set_fields(self._h, run, _dp(a)))
 
     def get_fields(self, run: int, out: np.ndarray | None = None) -> np.ndarray:
         """Run `run`'s 13 arrays; into `out` (C-contiguous float64 of shape
@@ -76,7 +81,7 @@ class Em2Ensemble:
             out = np.empty(shape)
         else:
             _check_out(out, shape)
-        check(self._L.em2g_ens_get_fields(self._h, run, _dp(out)))
+        self._check(self._L.em2g_ens_get_fields(self._h, run, _dp(out)))
         return out
 
     def set_particles(self, run: int, isp: int, part: np.ndarray) -> None:
@@ -84,7 +89,7 @@ class Em2Ensemble:
         a = np.ascontiguousarray(part, dtype=np.float64)
         if a.ndim != 2 or a.shape[0] != 6:
             raise ValueError("particles must have shape (6, n)")
-        check(self._L.em2g_ens_set_particles(self._h, run, isp, a.shape[1],
+        self._check(self._L.em2g_ens_set_particles(self._h, run, isp, a.shape[1],
                                              *[_dp(a[k]) for k in range(6)]))
 
     def set_particles_device(self, run: int, isp: int, part) -> None:
@@ -95,19 +100,19 @@ class Em2Ensemble:
         part = part.contiguous()
         torch.cuda.current_stream(part.device).synchronize()
         ptrs = [C.c_void_p(part[k].data_ptr()) for k in range(6)]
-        check(self._L.em2g_ens_set_particles_device(self._h, run, isp, part.shape[1], *ptrs))
+        self._check(self._L.em2g_ens_set_particles_device(self._h, run, isp, part.shape[1], *ptrs))
 
     def get_particles(self, run: int, isp: int, out: np.ndarray | None = None) -> np.ndarray:
         """(6, n) = x, y, vx, vy, vz, gamma of run `run`, species `isp`, in
         slot order; into `out` (C-contiguous float64 of that shape) if given."""
         n = C.c_int64()
-        check(self._L.em2g_ens_get_particles(self._h, run, isp, C.byref(n),
+        self._check(self._L.em2g_ens_get_particles(self._h, run, isp, C.byref(n),
                                              *([None] * 6)))
         if out is None:
             out = np.empty((6, n.value))
         else:
             _check_out(out, (6, n.value))
-        check(self._L.em2g_ens_get_particles(self._h, run, isp, C.byref(n),
+        self._check(self._L.em2g_ens_get_particles(self._h, run, isp, C.byref(n),
                                              *[_dp(out[k]) for k in range(6)]))
         return out
 
@@ -120,42 +125,42 @@ class Em2Ensemble:
         ake = np.zeros((nr, 4))
         e6 = np.full((nr, 6), np.nan)
         it = (C.c_int * nr)()
-        check(self._L.em2g_ens_step(self._h, int(nsteps), _dp(ake), _dp(e6), it))
+        self._check(self._L.em2g_ens_step(self._h, int(nsteps), _dp(ake), _dp(e6), it))
         return {"ake": ake, "energies": e6, "cg_iters": np.array(it[:], dtype=np.int64)}
 
     @property
     def it(self) -> int:
         v = C.c_int()
-        check(self._L.em2g_ens_get_step(self._h, C.byref(v)))
+        self._check(self._L.em2g_ens_get_step(self._h, C.byref(v)))
         return v.value
 
     def set_graph(self, on: bool) -> None:
-        check(self._L.em2g_ens_set_graph(self._h, 1 if on else 0))
+        self._check(self._L.em2g_ens_set_graph(self._h, 1 if on else 0))
 
     def phase_ms(self, n: int = 24):
         """Durations (ms) of the last fused step's phases: from the launch's
         start to its first grid barrier, then between barriers."""
         out = (C.c_int64 * n)()
-        check(self._L.em2g_ens_get_phase_ns(self._h, out, n))
+        self._check(self._L.em2g_ens_get_phase_ns(self._h, out, n))
         return [v / 1e6 for v in out]
 
     def set_fused(self, on: bool) -> None:
         """True: each step is one persistent, cooperative kernel launch
         (em2g_ens_set_fused); False: one launch per stage."""
-        check(self._L.em2g_ens_set_fused(self._h, 1 if on else 0))
+        self._check(self._L.em2g_ens_set_fused(self._h, 1 if on else 0))
 
     def num_variants(self) -> int:
         n = C.c_int()
-        check(self._L.em2g_ens_num_variants(self._h, C.byref(n)))
+        self._check(self._L.em2g_ens_num_variants(self._h, C.byref(n)))
         return n.value
 
     def set_variant(self, v: int) -> None:
-        check(self._L.em2g_ens_set_variant(self._h, int(v)))
+        self._check(self._L.em2g_ens_set_variant(self._h, int(v)))
 
     def set_sort_interval(self, k: int) -> None:
         """Regroup every run's particles by cell on every k-th step and update
         them in place in between (k * c * dt < dx, dy in every run)."""
-        check(self._L.em2g_ens_set_sort_interval(self._h, int(k)))
+        self._check(self._L.em2g_ens_set_sort_interval(self._h, int(k)))
         for r in self.runs:
             r.sort_interval = int(k)
 
@@ -167,17 +172,17 @@ class Em2Ensemble:
 
     def set_stream(self, stream) -> None:
         """As Em2Gpu.set_stream."""
-        check(self._L.em2g_ens_set_stream(self._h, stream_handle(stream)))
+        self._check(self._L.em2g_ens_set_stream(self._h, stream_handle(stream)))
 
     def counters(self) -> dict:
         k, g, per = C.c_int64(), C.c_int64(), C.c_int64()
-        check(self._L.em2g_ens_get_counters(self._h, C.byref(k), C.byref(g), C.byref(per)))
+        self._check(self._L.em2g_ens_get_counters(self._h, C.byref(k), C.byref(g), C.byref(per)))
         return {"kernel_launches": k.value, "graph_launches": g.value,
                 "kernels_per_step": per.value}
 
     def diagnostics(self, run: int) -> dict:
         out = np.full(10, np.nan)
-        check(self._L.em2g_ens_diagnostics(self._h, run, _dp(out), 10))
+        self._check(self._L.em2g_ens_diagnostics(self._h, run, _dp(out), 10))
         return {"energies": out[:6].copy(), "flux": out[6:8].copy(),
                 "poisson_r2": out[8:10].copy()}
 
