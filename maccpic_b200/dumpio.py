@@ -15,6 +15,11 @@ The restart point is after ``curnt`` of the last step and before its
 main loop carries on.  :func:`save` / :func:`load` do the same for an
 :class:`~maccpic_b200.em2.Em2Gpu` (or any object with get/set_fields and
 get/set_particles), so runs can move between em2 and this library.
+
+:func:`save_compact` / :func:`load_compact` keep the same state in one
+``.npz`` of FP64 arrays (fields, each species in slot order, the step
+counter and the grid size): half the bytes of em2's files, whose particle
+files frame every 8-byte value with 8 bytes of record markers.
 """
 from __future__ import annotations
 
@@ -129,3 +134,43 @@ def load(run, directory: str, counts, rank: int = 0) -> None:
     run.set_fields(fld)
     for s, p in enumerate(parts):
         run.set_particles(s, p)
+
+
+def save_compact(run, path: str) -> None:
+    """The run's whole state in one .npz: the 13 field arrays, every
+    species' (x, y, vx, vy, vz, gamma) in slot order, the step counter and
+    the grid.  `run` is an Em2Gpu or any object with get_fields,
+    get_particles, p (nx, ny, nsp) and it."""
+    nsp = run.p.nsp
+    arrays = {"fields": run.get_fields(), "it": np.int64(run.it),
+              "grid": np.array([run.p.nx, run.p.ny], dtype=np.int64)}
+    for s in range(nsp):
+        arrays[f"species{s}"] = run.get_particles(s)
+    tmp = path + ".part.npz"
+    np.savez(tmp, **arrays)
+    os.replace(tmp, path)  # a reader never sees a half-written file
+
+
+def load_compact(run, path: str) -> None:
+    """Restore a state written by save_compact into `run`, which must have
+    the same grid and species count; the step counter comes back too."""
+    with np.load(path) as z:
+        nx, ny = (int(v) for v in z["grid"])
+        if (nx, ny) != (run.p.nx, run.p.ny):
+            raise ValueError(f"checkpoint grid {nx}x{ny} differs from the run's "
+                             f"{run.p.nx}x{run.p.ny}")
+        nsp = sum(1 for k in z.files if k.startswith("species"))
+        if nsp != run.p.nsp:
+            raise ValueError(f"checkpoint holds {nsp} species, the run {run.p.nsp}")
+        fld = z["fields"]
+        if fld.shape != (13, ny + 3, nx + 3) or not np.all(np.isfinite(fld)):
+            raise ValueError("checkpoint fields have the wrong shape or non-finite values")
+        parts = [z[f"species{s}"] for s in range(nsp)]
+        for p in parts:
+            if p.ndim != 2 or p.shape[0] != 6 or not np.all(np.isfinite(p)):
+                raise ValueError("checkpoint particles have the wrong shape or non-finite values")
+        it = int(z["it"])
+    run.set_fields(fld)
+    for s, p in enumerate(parts):
+        run.set_particles(s, p)
+    run.it = it

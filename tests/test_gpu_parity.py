@@ -307,6 +307,36 @@ def test_gpu_restart_through_em2_files(gpu, tmp_path, oracle_lib):
             assert rel(h.get_particles(s), st.parts[s]) < 1e-12
 
 
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_gpu_compact_checkpoint(gpu, tmp_path, precision):
+    """dumpio.save_compact between full steps, load_compact into a new
+    context: it carries on with the same step counter and, stepping on, ends
+    where the context that was never stopped ends (FP64 bitwise in the
+    particles; the deposit's atomics order aside, to round-off)."""
+    from maccpic_b200 import _lib, dumpio
+    from maccpic_b200.em2 import Em2Gpu
+    op, rp, fld, parts = harris_case(nx=64, ny=32, ppc=8)
+    if precision == "fp32":
+        rp.precision = _lib.FP32
+    path = str(tmp_path / "state.npz")
+    with make_gpu(rp, fld, parts) as g:
+        g.step(6)
+        dumpio.save_compact(g, path)
+        g.step(4)
+        want_f, want_p = g.get_fields(), [g.get_particles(s) for s in range(2)]
+    with Em2Gpu(rp) as h:
+        dumpio.load_compact(h, path)
+        assert h.it == 6
+        h.step(4)
+        assert h.it == 10
+        got_f = h.get_fields()
+        for k in range(6):
+            assert rel(got_f[k], want_f[k]) < (1e-10 if precision == "fp64" else 1e-4), k
+        for s in range(2):
+            tol = 1e-12 if precision == "fp64" else 1e-4
+            assert np.abs(h.get_particles(s) - want_p[s]).max() < tol
+
+
 def test_every_push_variant_matches_the_oracle(gpu, oracle_lib):
     """The autotuner's kernel variants compute the same step."""
     from maccpic_b200.em2 import Em2Gpu

@@ -79,3 +79,65 @@ def test_split_run_through_restart_files_is_bitwise(tmp_path, oracle_lib):
     np.testing.assert_array_equal(b.fld, straight.fld)
     for s in range(2):
         np.testing.assert_array_equal(b.parts[s], straight.parts[s])
+
+
+class _HostRun:
+    """A stand-in with the interface save_compact / load_compact use."""
+
+    def __init__(self, nx, ny, nsp, fld=None, parts=None, it=0):
+        class P:
+            pass
+        self.p = P()
+        self.p.nx, self.p.ny, self.p.nsp = nx, ny, nsp
+        self.fld = fld if fld is not None else np.zeros((13, ny + 3, nx + 3))
+        self.parts = parts if parts is not None else [np.zeros((6, 0))] * nsp
+        self.it = it
+
+    def get_fields(self):
+        return self.fld.copy()
+
+    def set_fields(self, f):
+        self.fld = np.array(f, copy=True)
+
+    def get_particles(self, s):
+        return self.parts[s].copy()
+
+    def set_particles(self, s, p):
+        self.parts = list(self.parts)
+        self.parts[s] = np.array(p, copy=True)
+
+
+def test_compact_checkpoint_round_trip(tmp_path):
+    from maccpic_b200 import dumpio
+    rng = np.random.default_rng(4)
+    fld = rng.normal(size=(13, 11, 19))
+    parts = [rng.normal(size=(6, 3000)), rng.normal(size=(6, 5))]
+    a = _HostRun(16, 8, 2, fld, parts, it=123)
+    path = str(tmp_path / "state.npz")
+    dumpio.save_compact(a, path)
+    b = _HostRun(16, 8, 2)
+    dumpio.load_compact(b, path)
+    np.testing.assert_array_equal(b.fld, fld)
+    for x, y in zip(b.parts, parts):
+        np.testing.assert_array_equal(x, y)
+    assert b.it == 123
+    # about half of em2's restart bytes once particles dominate (em2's
+    # particle files frame every 8-byte value with 8 bytes of markers)
+    dumpio.write_restart(str(tmp_path / "em2"), fld, parts)
+    em2_bytes = sum(f.stat().st_size for f in (tmp_path / "em2").iterdir())
+    assert (tmp_path / "state.npz").stat().st_size < 0.75 * em2_bytes
+
+
+def test_compact_checkpoint_rejects_mismatches(tmp_path):
+    from maccpic_b200 import dumpio
+    a = _HostRun(16, 8, 2, parts=[np.ones((6, 3)), np.ones((6, 2))])
+    path = str(tmp_path / "s.npz")
+    dumpio.save_compact(a, path)
+    with pytest.raises(ValueError):
+        dumpio.load_compact(_HostRun(16, 9, 2), path)   # other grid
+    with pytest.raises(ValueError):
+        dumpio.load_compact(_HostRun(16, 8, 1), path)   # other species count
+    bad = _HostRun(16, 8, 2, parts=[np.full((6, 3), np.nan), np.ones((6, 2))])
+    dumpio.save_compact(bad, path)
+    with pytest.raises(ValueError):
+        dumpio.load_compact(_HostRun(16, 8, 2), path)   # non-finite particles
