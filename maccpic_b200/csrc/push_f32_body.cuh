@@ -83,21 +83,23 @@ __device__ __forceinline__ float2 bc2(float v) { return make_float2(v, v); }
 
 // The quadratic weights of both axes at once for offsets f = (fx, fy) in
 // cell (cx, cy) (the forms of the file header): cell-centred nodes, middle
-// index c+1: (1-f)^2/2, 3/4 - (f-1/2)^2, f^2/2; integer nodes, middle index
-// c+1+u with u = [f >= 1/2], h = f - u: (1/2-h)^2/2, 3/4 - h^2, (1/2+h)^2/2.
+// index c+1, with d = f - 1/2: (1/2-d)^2/2, 3/4 - d^2, (1/2+d)^2/2; integer
+// nodes, middle index c+1+u with u = [f >= 1/2], h = f - u: the same in h.
+// The three sum to 1 and differ by d (or h) at the ends, so with s = 3/4 -
+// d^2 and t = (1 - s)/2 the ends are t -+ d/2: one packed operation each.
 __device__ __forceinline__ void weights2(int cx, int cy, float2 f, Wts &hx, Wts &hy, Wts &nx,
                                          Wts &ny) {
-  const float2 half = bc2(0.5f);
-  const float2 d = add2(f, bc2(-0.5f)), e = add2(bc2(1.0f), make_float2(-f.x, -f.y));
-  const float2 hm = mul2(mul2(half, e), e), hp = mul2(mul2(half, f), f);
+  const float2 d = add2(f, bc2(-0.5f));
   const float2 hs = fma2(make_float2(-d.x, -d.y), d, bc2(0.75f));
+  const float2 ht = fma2(bc2(-0.5f), hs, bc2(0.5f));
+  const float2 hm = fma2(bc2(-0.5f), d, ht), hp = fma2(bc2(0.5f), d, ht);
   hx = Wts{cx + 1, hm.x, hs.x, hp.x, 0};
   hy = Wts{cy + 1, hm.y, hs.y, hp.y, 0};
   const int ux = f.x >= 0.5f ? 1 : 0, uy = f.y >= 0.5f ? 1 : 0;
   const float2 h = add2(f, make_float2(-(float)ux, -(float)uy));
-  const float2 am = add2(half, make_float2(-h.x, -h.y)), bp = add2(half, h);
-  const float2 nm = mul2(mul2(half, am), am), np = mul2(mul2(half, bp), bp);
   const float2 ns = fma2(make_float2(-h.x, -h.y), h, bc2(0.75f));
+  const float2 nt = fma2(bc2(-0.5f), ns, bc2(0.5f));
+  const float2 nm = fma2(bc2(-0.5f), h, nt), np = fma2(bc2(0.5f), h, nt);
   nx = Wts{cx + 1 + ux, nm.x, ns.x, np.x, ux};
   ny = Wts{cy + 1 + uy, nm.y, ns.y, np.y, uy};
 }
