@@ -96,7 +96,7 @@ __device__ __forceinline__ void weights2(int cx, int cy, float2 f, Wts &hx, Wts 
   hx = Wts{cx + 1, hm.x, hs.x, hp.x, 0};
   hy = Wts{cy + 1, hm.y, hs.y, hp.y, 0};
   const int ux = f.x >= 0.5f ? 1 : 0, uy = f.y >= 0.5f ? 1 : 0;
-  const float2 h = add2(f, make_float2(-(float)ux, -(float)uy));
+  const float2 h = add2(f, make_float2(f.x >= 0.5f ? -1.0f : 0.0f, f.y >= 0.5f ? -1.0f : 0.0f));
   const float2 ns = fma2(make_float2(-h.x, -h.y), h, bc2(0.75f));
   const float2 nt = fma2(bc2(-0.5f), ns, bc2(0.5f));
   const float2 nm = fma2(bc2(-0.5f), h, nt), np = fma2(bc2(0.5f), h, nt);
@@ -284,8 +284,9 @@ __device__ __forceinline__ void flush_rows(float *A, int nxg, int kx, int ky, co
 // The whole-cell part of a pair of offsets in (-1, 2) (-1, 0 or 1 each) and
 // what is left within that cell: floor as a float is exact, so the rest is
 // one packed subtraction.
-__device__ __forceinline__ void split_cell(float2 f, int &ox, int &oy, float2 &rest) {
-  const float2 fl = make_float2(floorf(f.x), floorf(f.y));
+__device__ __forceinline__ void split_cell(float2 f, int &ox, int &oy, float2 &rest,
+                                           float2 &fl) {
+  fl = make_float2(floorf(f.x), floorf(f.y));
   ox = (int)fl.x;
   oy = (int)fl.y;
   rest = add2(f, make_float2(-fl.x, -fl.y));
@@ -368,7 +369,8 @@ __device__ __forceinline__ void drain_entry(const Args32 &a, const DepQ &Q, int 
 // the periodic boundary); whoever indexes the arrays with them wraps them.
 struct PartOut {
   float mx, my, ux, uy, uz;  // new position relative to the start cell, new u
-  int ox, oy;                // start cell - group cell (-1, 0 or 1 each)
+  float oxf, oyf;            // start cell - group cell (-1, 0 or 1 each), as floats
+  bool home_x, home_y;       // the new position's cell is the group cell's column / row
   bool in_cell_old;          // the start cell is the group cell
   bool need_old, need_new;   // deposits for the warp's stack
   int cx, cy, ncx, ncy;      // start and end cells, unwrapped
@@ -388,11 +390,12 @@ __device__ __forceinline__ void push_one(const Args32 &a, float4 (*win)[WY][WXW]
   // the cell the particle is in now (it may have left cell k last step)
   int ox, oy;
   float2 fxy;
-  split_cell(make_float2(xr, yr), ox, oy, fxy);
+  float2 oxy;
+  split_cell(make_float2(xr, yr), ox, oy, fxy, oxy);
+  o.oxf = oxy.x;
+  o.oyf = oxy.y;
   const int cx = kx + ox, cy = ky + oy;  // unwrapped
   const float fx = fxy.x, fy = fxy.y;
-  o.ox = ox;
-  o.oy = oy;
   o.in_cell_old = (ox == 0) && (oy == 0);
   Wts hx, hy, nxw, nyw;  // array indices of the unwrapped cell
   weights2(cx, cy, make_float2(fx, fy), hx, hy, nxw, nyw);
@@ -478,13 +481,15 @@ __device__ __forceinline__ void push_one(const Args32 &a, float4 (*win)[WY][WXW]
   o.mx = mv.x;
   o.my = mv.y;
   int nox, noy;
-  float2 nf;
-  split_cell(mv, nox, noy, nf);
+  float2 nf, nfl;
+  split_cell(mv, nox, noy, nf, nfl);
   const float nfx = nf.x, nfy = nf.y;
   // rho and jp at the new position (pic/curnt.f90:197-303); with at least 4
   // cells a side, the new cell is the group cell exactly when the offsets
   // cancel
-  const bool stays = ox + nox == 0 && oy + noy == 0;
+  o.home_x = ox + nox == 0;
+  o.home_y = oy + noy == 0;
+  const bool stays = o.home_x && o.home_y;
   o.need_new = act && !stays;
   o.ncx = cx + nox;
   o.ncy = cy + noy;
@@ -636,9 +641,9 @@ __device__ __forceinline__ void push_segment(const Args32 &a, int x0, int y0, in
           // the group cell itself, 1 plus a tiny negative move can round to
           // exactly 1, which would read as the next cell (every other case is
           // exact or rounds within its cell)
-          float xn = o.mx + (float)o.ox, yn = o.my + (float)o.oy;
-          if (o.ox + (o.ncx - o.cx) == 0) xn = fminf(xn, kBelowOne);
-          if (o.oy + (o.ncy - o.cy) == 0) yn = fminf(yn, kBelowOne);
+          float xn = o.mx + o.oxf, yn = o.my + o.oyf;
+          if (o.home_x) xn = fminf(xn, kBelowOne);
+          if (o.home_y) yn = fminf(yn, kBelowOne);
           if (EM2G_IN(i < cap, a.lost)) {
             B4[i] = make_float4(xn, yn, o.ux, o.uy);
             Buz[i] = o.uz;
