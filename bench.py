@@ -416,9 +416,36 @@ def precision_compare(args, cfg, local, src, fields, stream, tuned):
             "final_fp64": dict(zip(names, q64[-1].tolist()))}
 
 
-def measure(args, cfg, precision, local, src, fields, stream, ws):
+def stencil_compare(g, stream, calls=20, rounds=3):
+    """The field solve alone (em2g_fields: fold, Yee, smooth2 of rho,
+    Poisson/CG) on the run's final state, with each stencil implementation
+    (direct loads, TMA-staged tiles), CUDA events on the run's stream; best
+    of `rounds` rounds of `calls` calls, each call with its own host
+    synchronisation."""
+    import torch
+    it = g.it + 1
+    best = {}
+    for _ in range(rounds):
+        for mode in (0, 1):
+            g.set_stencils(mode)
+            g.fields(it)
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            for _ in range(calls):
+                g.fields(it)
+            b.record(stream)
+            torch.cuda.synchronize()
+            best[mode] = min(best.get(mode, float("inf")), a.elapsed_time(b) / calls)
+    g.set_stencils(0)
+    return {"direct_ms_per_fields_call": best[0], "tma_ms_per_fields_call": best[1],
+            "calls": calls, "rounds": rounds}
+
+
+def measure(args, cfg, precision, local, src, fields, stream, ws, stencils=False):
     """Device-resident run: warm-up, then K timed steps.  Returns timings,
-    counters and the final fields and kinetic energies."""
+    counters and the final fields and kinetic energies; with `stencils`,
+    also the field solve timed with each stencil implementation."""
     import torch
     from maccpic_b200 import _lib
     from maccpic_b200.em2 import Em2Gpu
@@ -483,6 +510,8 @@ def measure(args, cfg, precision, local, src, fields, stream, ws):
     g.set_timing(False)
     out = {"ms": ms, "counters": cnt, "cg": cg, "clocks": clk.summary(), "ake": r["ake"],
            "tuned": tuned}
+    if stencils:
+        out["stencils"] = stencil_compare(g, stream)
     g.close()
     return out
 
@@ -505,7 +534,8 @@ def run_ours(args):
     rank_cfg = dataclasses.replace(cfg, seed=cfg.seed * 1000 + rank)
     src = ParticleSource(rank_cfg, local)
 
-    main = measure(args, cfg, _lib.FP32 if fp32 else _lib.FP64, local, src, fields, stream, ws)
+    main = measure(args, cfg, _lib.FP32 if fp32 else _lib.FP64, local, src, fields, stream, ws,
+                   stencils=ws == 1)
     ms = main["ms"]
     value = n_total * ws * args.steps / (ms / 1e3)
     # the FP64 path on the same initial state: its speed, timed as the main
@@ -588,6 +618,7 @@ def run_ours(args):
                          "avg_launch_ms": avg_ms},
             "gpu_launches": cnt["kernel_launches"],
             "clocks": main["clocks"],
+            "stencils": main.get("stencils"),
             "mixed_vs_fp64": compare,
             "adjoint_over_forward": adj["gradient_over_forward"] if adj else None,
             "adjoint": adj,
