@@ -4,13 +4,14 @@ against em2's forms in FP64.
 The push (maccpic_b200/csrc/push_f32_body.cuh, weights2 and split_cell)
 takes em2's quadratic-spline weights (pic/move.f90:76-84: 3/4-d^2 at the
 nearest node, (1/2-+d)^2/2 at its neighbours, d the offset from that node)
-in another order of operations: the middle weight s = 3/4 - d^2, t = (1 - s)/2, and the ends
-t -+ d/2, since the three sum to 1 and the ends differ by d.  Each packed
+in another order of operations: the middle weight s = 3/4 - d^2,
+t = (1 - s)/2, and the ends t -+ d/2, since the three sum to 1 and the ends differ by d.  Each packed
 FP32 operation rounds as its scalar counterpart, so float32 numpy with the
 same order is the kernel's arithmetic.  Checked here: the restated weights
-equal em2's to FP32 rounding over the cell, sum to exactly 1, and the cell
-split by floor gives offsets in [0, 1) for the whole (-1, 2) range the
-grouping allows.
+equal em2's to FP32 rounding over the cell and sum to 1 to FP32 rounding,
+and the cell split by floor gives a step of -1, 0 or 1 and an offset in
+[0, 1] (1 only by rounding, which the grouping rules absorb) over the whole
+(-1, 2) range the grouping allows.
 """
 import numpy as np
 
