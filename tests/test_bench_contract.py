@@ -58,3 +58,20 @@ def test_reference_arm_under_two_ranks_prints_from_rank_zero_only():
     lines = _json_lines(r.stdout)
     assert len(lines) == 1
     _check_line(lines[0], 2)
+
+
+def test_roofline_inputs_are_consistent():
+    """The push's committed DRAM traffic (profiles/, from an ncu capture) lies
+    within 15 % of the algorithmic bytes the bench divides by the launch
+    time (n x 48 B + W x 4 B x 20 at 2048x1024, 64 per cell): traffic far
+    above them would mean re-reads, far below a capture of another kernel.
+    The HBM peak is read from the measured figure when there is one."""
+    import bench
+    t = bench.profile_traffic("k_push_cells_f32_harris_2048x1024_ppc64")
+    n = 2048 * 1024 * 64
+    w = 2051 * 1027
+    alg = n * 48 + w * 4 * 20
+    assert t is not None and 0.85 < t / alg < 1.15
+    peak, kind = bench.peaks()
+    assert peak > 1000 and kind in ("measured", "fallback")
+    assert bench.profile_traffic("no_such_kernel") is None
